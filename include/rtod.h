@@ -1,0 +1,163 @@
+/*
+ * rtod.h - C ABI of the B200 sliding-window distance outlier detector.
+ *
+ * A point of the current window is an outlier when at most K window points
+ * (itself included) lie within distance R of it, i.e. when fewer than K
+ * other points do. The window holds the last W points of a stream and
+ * advances by S points per slide (W % S == 0).
+ *
+ * This ABI replaces RTOD's per-slide detector, stages 2-8 of its slide loop
+ * (src/ods/optixScan.cpp:1045-1121): the slide H2D copy, the host grid
+ * filter, the AABB kernel and BVH rebuild, the ray launch and the outlier
+ * read-back. RTOD has no plugin/FFI interface of its own; its boundary is
+ * the optixScan command line and compile-time macros, which rtod_config
+ * mirrors field by field (each field names the flag or macro it replaces).
+ * Its only C-ABI seam, `extern "C" void kGenAABB(double3*, double, unsigned,
+ * OptixAabb*)` (src/ods/optixScan.cpp:49, src/ods/aabb.cu:35-45), has no
+ * counterpart here: the grid build supersedes AABB generation.
+ *
+ * Conventions: every call returns RTOD_OK (0) or a negative RTOD_ERR_*;
+ * no C++ exception crosses the ABI (RTOD's CUDA_CHECK/OPTIX_CHECK throw
+ * sutil::Exception, src/sutil/Exception.h:80-113); rtod_last_error() gives
+ * the message of the calling thread's last failure. A handle owns its CUDA
+ * stream and graphs and must be used by one host thread at a time. Points
+ * are float32, point-major (n rows of `dim` values: the layout of RTOD's
+ * double3 vertices[], src/ods/optixScan.cpp:96), in host or device memory;
+ * the caller keeps ownership. Outlier IDs are global stream indices
+ * (0-based position of the point in the stream), sorted ascending; RTOD's
+ * ring-slot IDs are index % W (src/ods/optixScan.cpp:1097).
+ */
+#ifndef RTOD_H
+#define RTOD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RTOD_OK 0
+#define RTOD_ERR_CONFIG (-1)   /* invalid rtod_config */
+#define RTOD_ERR_ARG (-2)      /* invalid argument (null pointer, bad size) */
+#define RTOD_ERR_CUDA (-3)     /* a CUDA runtime call failed */
+#define RTOD_ERR_CAPACITY (-4) /* output buffer too small */
+#define RTOD_ERR_INPUT (-5)    /* non-finite coordinate, or |x|/R too large for the grid */
+#define RTOD_ERR_STATE (-6)    /* call out of order (e.g. detect before the window is full) */
+#define RTOD_ERR_TIMEOUT (-7)  /* a bounded device-side wait ran out */
+#define RTOD_ERR_NODEV (-8)    /* no CUDA device, or not sm_100 */
+
+/* Neighbour predicates. */
+#define RTOD_PRED_FP32_LE 0 /* fl32 d^2, summed left to right without FMA, d^2 <= fl32(fl32(R)^2) */
+#define RTOD_PRED_F64_LT 1  /* RTOD's double test: |dx| < R in 1-d, d^2 < R*R otherwise
+                               (src/ods/optixScan.cu:170-190) */
+
+typedef struct rtod_config {
+  int64_t window;      /* W  (--window, src/ods/optixScan.cpp:166-171) */
+  int64_t slide;       /* S  (--slide, :172-177); W % S == 0 (:1037) */
+  double R;            /* R  (--R, :179-185); > 0 */
+  int32_t K;           /* K  (--K, :186-192); >= 0 */
+  int32_t dim;         /* DIMENSION macro (src/ods/optixScan.h:10-12); 1..8 */
+  int32_t opt;         /* OPTIMIZATION macro (optixScan.h:22-24): 0 = no grid filter,
+                          1 and 2 = grid filter (identical results) */
+  int32_t pred;        /* RTOD_PRED_*; default RTOD_PRED_FP32_LE */
+  int32_t router;      /* 1 = learned router on (routes counted points into an early-exit
+                          and a full-sweep queue); results are identical either way */
+  int32_t tuner;       /* 1 = autotune cell width and block shape on the first slides */
+  int32_t cells_per_r; /* grid cells per R along each hashed dimension (1..3; 0 = auto) */
+  int32_t block_warps; /* warps per block of the range-count kernel (1..32; 0 = auto) */
+  int32_t use_graph;   /* 1 = replay each slide as a captured CUDA graph */
+  int32_t device;      /* CUDA device ordinal */
+  int32_t reserved[4];
+} rtod_config;
+
+/* Per-slide stage times in ms, averaged over the slides of the last call,
+   under the names of RTOD's Timer (src/ods/timer.h:16-24, :102-117). */
+typedef struct rtod_times {
+  double copy_new_points_h2d;      /* slide points host -> device */
+  double copy_filtered_points_h2d; /* always 0: nothing is gathered on the host */
+  double copy_outlier_d2h;         /* outlier IDs device -> host */
+  double prepare_cell;             /* ring update + cell hashing + cell occupancy */
+  double build_bvh;                /* scan + scatter into the cell-ordered SoA */
+  double detect_outlier;           /* range count + outlier compaction */
+  double total;                    /* whole slide */
+  double undetermined_per_slide;   /* points that needed an exact count ("BVH Node / slide",
+                                      src/ods/optixScan.cpp:1179) */
+  int64_t slides;
+} rtod_times;
+
+typedef struct rtod_handle rtod_handle;
+
+/* Fills *cfg with defaults: W=100000 S=5000 R=0.45 K=50 dim=1 opt=2,
+   FP32 predicate, router off, tuner off, auto grid, graphs on, device 0. */
+int rtod_config_init(rtod_config* cfg);
+
+/* Validates cfg and allocates all device state (replaces data_h2d, make_gas,
+   initialize_params and initialize_cell, src/ods/optixScan.cpp:232-426,
+   :674-724, :960-965). */
+int rtod_create(const rtod_config* cfg, rtod_handle** out);
+
+/* Appends n points to the stream. The first push must be exactly W points
+   (the initial window, src/ods/optixScan.cpp:1020-1034); every later push
+   must be exactly S points (one slide, :1051-1064) and must be followed by
+   rtod_detect before the next push. */
+int rtod_push_slide(rtod_handle* h, const float* pts, int64_t n);
+
+/* Detects the outliers of the window produced by the last push and copies
+   their sorted global indices to out_ids (host or device memory, room for
+   cap entries); *n_out receives the count even when it exceeds cap (then
+   RTOD_ERR_CAPACITY is returned). times may be NULL. */
+int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t* n_out, rtod_times* times);
+
+/* Runs a whole stream the way RTOD's detect_outlier does
+   (src/ods/optixScan.cpp:1019-1126): the first W points fill the window,
+   then up to max_slides slides (max_slides < 0: all) of S points each are
+   detected, slide j covering points [(j+1)S, W+(j+1)S). The handle must be
+   fresh (nothing pushed). out_offsets receives slides+1 CSR offsets into
+   out_ids; *slides_out the number of slides. pts may be host or device
+   memory (n * dim floats). times may be NULL. */
+int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides,
+             int64_t* out_offsets, int64_t* out_ids, int64_t ids_cap, int64_t* slides_out,
+             rtod_times* times);
+
+/* Clears the stream so that the handle can take a new first window. */
+int rtod_reset(rtod_handle* h);
+
+/* Number of slides detected since create/reset. */
+int64_t rtod_slides_done(const rtod_handle* h);
+
+/* The resolved grid and launch parameters (after autotuning, if on):
+   out[0] cells per R, out[1] warps per block of the range count,
+   out[2] hashed dimensions. */
+int rtod_get_tuning(const rtod_handle* h, int32_t out[3]);
+
+/* Counters since create: out[0] kernel launches issued by the library (a
+   graph replay counts each of its kernels), out[1] graph replays, out[2]
+   slides detected, out[3] points that needed an exact count. No counterpart
+   in RTOD (diagnostic). */
+int rtod_get_stats(const rtod_handle* h, int64_t out[4]);
+
+/* Diagnostic run: like rtod_run on a fresh handle but launches every kernel
+   individually with a CUDA event after each, and writes the average device
+   time per slide of each pipeline kernel, in order (ingest, hist, scan,
+   scatter, count, compact), to kernel_ms[0..n_kernels). Results are
+   discarded. The kernel names are given by rtod_kernel_name(i). No
+   counterpart in RTOD (it times stages with gettimeofday, src/ods/timer.h). */
+int rtod_profile_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides,
+                     double* kernel_ms, int32_t n_kernels);
+
+/* Name of pipeline kernel i (0-based) as used by rtod_profile_run, or NULL. */
+const char* rtod_kernel_name(int32_t i);
+
+void rtod_destroy(rtod_handle* h);
+
+/* Message of the calling thread's last failed call ("" if none). */
+const char* rtod_last_error(void);
+
+/* Library version string. */
+const char* rtod_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RTOD_H */

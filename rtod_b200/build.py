@@ -1,0 +1,57 @@
+"""Builds the native library rtod_b200/librtod.so with nvcc for sm_100a.
+
+The library is plain CUDA C++ with a C ABI (include/rtod.h); nothing in it
+depends on PyTorch. Usage: ``python -m rtod_b200.build [--verbose]``.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB = os.path.join(PKG, "librtod.so")
+SOURCES = ["rtod.cu"]
+HEADERS = ["kernels.cuh", "router.cuh", "batch.cuh"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def command(out: str = LIB, ptxas_verbose: bool = False) -> list[str]:
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+           "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared", "-I", os.path.join(ROOT, "include"),
+           "-o", out]
+    if ptxas_verbose:
+        cmd += ["-Xptxas", "-v"]
+    return cmd + [os.path.join(CSRC, s) for s in SOURCES]
+
+
+def stale(out: str = LIB) -> bool:
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    deps.append(os.path.join(ROOT, "include", "rtod.h"))
+    return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    if force or stale():
+        r = subprocess.run(command(ptxas_verbose=verbose), capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        if verbose:
+            sys.stdout.write(r.stdout + r.stderr)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force=True, verbose="--verbose" in sys.argv))

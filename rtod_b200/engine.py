@@ -1,0 +1,157 @@
+"""Python front end of the detector: the run surface of RTOD's optixScan.
+
+``Detector`` mirrors the parameters of ``optixScan`` (``--window --slide
+--R --K``, src/ods/optixScan.cpp:149-212) and its compile-time switches
+(``DIMENSION``, ``OPTIMIZATION``, src/ods/optixScan.h:10-24) and reproduces
+its slide loop (``detect_outlier``, src/ods/optixScan.cpp:1019-1126): the
+first W points fill the window, every later slide of S points yields the
+outliers of the new window. Results are sorted global stream indices
+(``Detector.ring_slots`` converts them to RTOD's ring-slot IDs). All work
+runs in librtod.so on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native
+from ._native import Config, Times, check, lib
+
+
+def _as_points(points, dim: int):
+    """(pointer, n, keepalive) for a point-major float32 array: a numpy array
+    (host) or a CUDA tensor exposing data_ptr() (device)."""
+    if hasattr(points, "data_ptr") and hasattr(points, "is_cuda"):
+        t = points
+        if t.dtype.__repr__() != "torch.float32" or not t.is_contiguous():
+            raise TypeError("device points must be a contiguous float32 tensor")
+        n = t.numel() // dim
+        if n * dim != t.numel():
+            raise ValueError(f"tensor size {t.numel()} is not a multiple of dim={dim}")
+        return ctypes.c_void_p(t.data_ptr()), n, t
+    a = np.ascontiguousarray(points, dtype=np.float32)
+    if a.ndim == 1 and dim == 1:
+        a = a[:, None]
+    if a.ndim != 2 or a.shape[1] != dim:
+        raise ValueError(f"expected points of shape (n, {dim}), got {a.shape}")
+    return a.ctypes.data_as(ctypes.c_void_p), a.shape[0], a
+
+
+@dataclass
+class RunResult:
+    """Outliers of every slide of a stream, in CSR form."""
+    offsets: np.ndarray  # int64 [slides + 1]
+    ids: np.ndarray      # int64 [offsets[-1]]
+    times: dict = field(default_factory=dict)
+
+    @property
+    def slides(self) -> int:
+        return len(self.offsets) - 1
+
+    def slide(self, j: int) -> np.ndarray:
+        return self.ids[self.offsets[j]:self.offsets[j + 1]]
+
+
+class Detector:
+    """Sliding-window distance outlier detector on one CUDA device.
+
+    A point of the window is an outlier when at most K window points (itself
+    included) lie within distance R of it.
+    """
+
+    def __init__(self, window: int, slide: int, R: float, K: int, dim: int = 1, opt: int = 2,
+                 pred: str = "fp32_le", router: bool = False, tuner: bool = False,
+                 cells_per_r: int = 0, block_warps: int = 0, use_graph: bool = True,
+                 device: int = 0):
+        cfg = Config()
+        check(lib().rtod_config_init(ctypes.byref(cfg)))
+        cfg.window, cfg.slide, cfg.R, cfg.K, cfg.dim, cfg.opt = window, slide, R, K, dim, opt
+        cfg.pred = _native.PRED[pred]
+        cfg.router, cfg.tuner = int(router), int(tuner)
+        cfg.cells_per_r, cfg.block_warps = cells_per_r, block_warps
+        cfg.use_graph, cfg.device = int(use_graph), device
+        self.cfg = cfg
+        self.window, self.slide, self.R, self.K, self.dim = window, slide, R, K, dim
+        self._h = ctypes.c_void_p()
+        check(lib().rtod_create(ctypes.byref(cfg), ctypes.byref(self._h)))
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self) -> None:
+        if self._h:
+            lib().rtod_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- streaming --------------------------------------------------------
+    def push(self, points) -> None:
+        """Appends W points (first call) or S points (each later call)."""
+        ptr, n, keep = _as_points(points, self.dim)
+        check(lib().rtod_push_slide(self._h, ptr, n))
+        del keep
+
+    def detect(self, times: bool = False):
+        """Outliers (sorted global indices) of the window after the last push."""
+        out = np.empty(self.window, np.int64)
+        n_out = ctypes.c_int64()
+        t = Times()
+        check(lib().rtod_detect(self._h, out.ctypes.data_as(ctypes.c_void_p), out.size,
+                                ctypes.byref(n_out), ctypes.byref(t) if times else None))
+        ids = out[:n_out.value].copy()
+        return (ids, t.as_dict()) if times else ids
+
+    def run(self, points, max_slides: int = 10000, times: bool = False, ids_cap: int | None = None,
+            out_ids=None) -> RunResult:
+        """Processes a whole stream (host array or CUDA tensor) like RTOD's
+        detect_outlier: fill with the first W points, then detect up to
+        max_slides slides (RTOD caps the loop at 10000, optixScan.cpp:1045)."""
+        ptr, n, keep = _as_points(points, self.dim)
+        slides = max(0, (n - self.window) // self.slide) if n >= self.window else 0
+        if max_slides is not None and max_slides >= 0:
+            slides = min(slides, max_slides)
+        off = np.zeros(slides + 1, np.int64)
+        if ids_cap is None:
+            ids_cap = max(1, slides * self.window)
+        if out_ids is None:
+            out = np.empty(ids_cap, np.int64)
+            out_ptr = out.ctypes.data_as(ctypes.c_void_p)
+        else:
+            out = out_ids
+            out_ptr = ctypes.c_void_p(out_ids.data_ptr())
+        ns = ctypes.c_int64()
+        t = Times()
+        check(lib().rtod_run(self._h, ptr, n, -1 if max_slides is None else max_slides,
+                             off.ctypes.data_as(ctypes.c_void_p), out_ptr, ids_cap,
+                             ctypes.byref(ns), ctypes.byref(t) if times else None))
+        del keep
+        ids = out[:off[-1]] if out_ids is not None else out[:off[-1]].copy()
+        return RunResult(off, ids, t.as_dict() if times else {})
+
+    def reset(self) -> None:
+        check(lib().rtod_reset(self._h))
+
+    @property
+    def slides_done(self) -> int:
+        return int(lib().rtod_slides_done(self._h))
+
+    @property
+    def tuning(self) -> dict:
+        a = (ctypes.c_int32 * 3)()
+        check(lib().rtod_get_tuning(self._h, a))
+        return {"cells_per_r": a[0], "block_warps": a[1], "hashed_dims": a[2]}
+
+    def ring_slots(self, ids: np.ndarray) -> np.ndarray:
+        """RTOD's outlier IDs (ring slots, optixScan.cpp:1097) for global indices."""
+        return np.asarray(ids, np.int64) % self.window

@@ -1,0 +1,147 @@
+"""GPU parity: the CUDA path, called through the C ABI, against the golden
+fixtures and the CPU oracle. Bit-exact: the per-slide outlier ID sets must be
+identical."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import golden_cases, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def rtod():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from rtod_b200 import build
+    build.build()
+    import rtod_b200
+    return rtod_b200
+
+
+def assert_same(res, off, ids):
+    np.testing.assert_array_equal(res.offsets, off)
+    np.testing.assert_array_equal(res.ids, ids)
+
+
+@pytest.mark.parametrize("path", golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
+@pytest.mark.parametrize("opt,graph,n", [(2, True, 0), (0, False, 0), (2, False, 1), (1, True, 3)])
+def test_run_matches_golden(rtod, path, opt, graph, n):
+    meta, pts, off, ids = load_golden(path)
+    with rtod.Detector(meta["W"], meta["S"], meta["R"], meta["K"], dim=pts.shape[1], opt=opt,
+                       pred=meta["pred"], use_graph=graph, cells_per_r=n) as det:
+        assert_same(det.run(pts), off, ids)
+
+
+@pytest.mark.parametrize("path", golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
+def test_push_detect_matches_golden(rtod, path):
+    meta, pts, off, ids = load_golden(path)
+    W, S = meta["W"], meta["S"]
+    with rtod.Detector(W, S, meta["R"], meta["K"], dim=pts.shape[1], pred=meta["pred"]) as det:
+        det.push(pts[:W])
+        for j in range(len(off) - 1):
+            det.push(pts[W + j * S:W + (j + 1) * S])
+            got = det.detect()
+            np.testing.assert_array_equal(got, ids[off[j]:off[j + 1]])
+        assert det.slides_done == len(off) - 1
+
+
+def oracle_check(rtod, oracle_mod, pts, W, S, R, K, slides, pred="fp32_le", **kw):
+    pts = pts[:W + slides * S]
+    off, ids, _ = oracle_mod.detect(pts, W, S, R, K, pred, engine="grid", threads=8)
+    with rtod.Detector(W, S, R, K, dim=pts.shape[1] if pts.ndim == 2 else 1, pred=pred, **kw) as det:
+        assert_same(det.run(pts), off, ids)
+
+
+def test_small_walk_full_stream(rtod, oracle_mod):
+    from rtod_b200 import datagen
+    w = datagen.small_walk()
+    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, w.slides)
+
+
+def test_stock_like_prefix(rtod, oracle_mod):
+    from rtod_b200 import datagen
+    w = datagen.stock_like()
+    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, 12)
+
+
+def test_sensor_like_prefix(rtod, oracle_mod):
+    from rtod_b200 import datagen
+    w = datagen.sensor_like()
+    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, 60)
+    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, 20, pred="f64_lt")
+
+
+@pytest.mark.parametrize("K", [30, 50, 70])
+def test_gaussian_like_K_sweep(rtod, oracle_mod, K):
+    from rtod_b200 import datagen
+    w = datagen.gaussian_like(K)
+    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, 6)
+
+
+@pytest.mark.parametrize("d", [2, 5, 8])
+def test_higher_dims(rtod, oracle_mod, d):
+    from rtod_b200 import datagen
+    pts = datagen.random_walk(30_000, 0.1, seed=40 + d, dim=d)
+    oracle_check(rtod, oracle_mod, pts, 6000, 600, 0.25 * d ** 0.5, 20, 15)
+
+
+def test_full_size_properties(rtod):
+    """Full stock-like stream (189 slides): every configuration of the grid
+    and launch gives the same outlier sets, IDs are sorted and in-window."""
+    from rtod_b200 import datagen
+    w = datagen.stock_like()
+    runs = []
+    for kw in (dict(), dict(opt=0), dict(cells_per_r=1), dict(cells_per_r=3, use_graph=False),
+               dict(block_warps=2)):
+        with rtod.Detector(w.window, w.slide, w.R, w.K, **kw) as det:
+            runs.append(det.run(w.points))
+    base = runs[0]
+    assert base.slides == w.slides
+    for r in runs[1:]:
+        assert_same(r, base.offsets, base.ids)
+    for j in range(base.slides):
+        s = base.slide(j)
+        lo = (j + 1) * w.slide
+        assert np.all(np.diff(s) > 0)
+        assert s.size == 0 or (s[0] >= lo and s[-1] < lo + w.window)
+
+
+def test_device_pointers(rtod):
+    import torch
+    meta, pts, off, ids = load_golden(golden_cases()[-1])
+    dev = torch.from_numpy(pts).cuda()
+    out = torch.empty(max(1, len(ids)) + 16, dtype=torch.int64, device="cuda")
+    with rtod.Detector(meta["W"], meta["S"], meta["R"], meta["K"], dim=pts.shape[1],
+                       pred=meta["pred"]) as det:
+        r = det.run(dev, out_ids=out, ids_cap=out.numel())
+        np.testing.assert_array_equal(r.offsets, off)
+        np.testing.assert_array_equal(r.ids.cpu().numpy(), ids)
+
+
+def test_input_errors(rtod):
+    pts = np.zeros(40, np.float32)
+    pts[25] = np.nan
+    with rtod.Detector(10, 5, 1.0, 2) as det:
+        with pytest.raises(rtod.RtodError, match="INPUT"):
+            det.run(pts)
+        det.reset()
+        det.run(np.zeros(40, np.float32))
+    big = np.zeros(40, np.float32)
+    big[30] = 3e30
+    with rtod.Detector(10, 5, 1e-6, 2) as det:
+        with pytest.raises(rtod.RtodError, match="INPUT"):
+            det.run(big)
+    with rtod.Detector(10, 5, 1.0, 2) as det:
+        with pytest.raises(rtod.RtodError, match="STATE"):
+            det.push(np.zeros(5, np.float32))  # first push must be W points
+        det.push(np.zeros(10, np.float32))
+        with pytest.raises(rtod.RtodError, match="STATE"):
+            det.detect()
+        det.push(np.zeros(5, np.float32))
+        with pytest.raises(rtod.RtodError, match="STATE"):
+            det.push(np.zeros(5, np.float32))  # detect must come first
+        assert det.detect().size == 0
