@@ -1,0 +1,359 @@
+#!/usr/bin/env python
+"""Benchmark of the sliding-window outlier detector on one or more B200s.
+
+Workload (N=1): the stock-like 1-d stream standing in for RTOD's STK run
+(script/run.py:25): 1,048,572 float32 values (random walk, N(0, 0.1) steps,
+0.5% U(-5, 5) jumps, seed 1), W=100,000, S=5,000, R=0.45, K=50,
+FP32 predicate, 189 slides. One step = one pass over the whole stream, as in
+RTOD's timed pass (src/ods/optixScan.cpp:1159-1168): fill with the first W
+points, then detect every slide.
+
+  value   stream points ingested per second (S * slides / step time), the
+          stream resident in HBM, outputs left in HBM; device time from CUDA
+          events on the library's stream, summed over the timed steps, max
+          over ranks; L2 flushed (256 MiB write) before every step.
+  e2e     the same through the public API with host buffers: pinned host
+          input copied in and the outlier IDs copied out inside every step;
+          host wall clock around each call (the call synchronises).
+
+Multi-GPU: replicas only (independent streams, no collective); every rank
+runs the same workload and value counts the points of all ranks.
+
+`--impl reference` times the CPU restatement of RTOD's detection path
+(oracle/, grid filter + exact count, all host threads) on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "µs/slide & points/s: learned-routed vs plain kernel, 1 B200, bit-exact outliers"
+UNIT = "points/s"
+FLUSH_BYTES = 256 << 20
+KERNEL_ORDER = ["k_ingest", "k_hist", "k_scan", "k_scatter", "k_count", "k_compact"]
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def workload():
+    from rtod_b200 import datagen
+    return datagen.stock_like()
+
+
+def workload_config(w, extra=None):
+    cfg = {"workload": w.name, "stream_points": w.n, "dim": w.dim, "window": w.window,
+           "slide": w.slide, "R": w.R, "K": w.K, "slides_per_step": w.slides,
+           "predicate": "fp32 d2 <= R2", "l2": "flushed before every step (256 MiB write)",
+           "parallelism": "replicas"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        rows = [r for r in csv.reader(io.StringIO(self.out or "")) if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def physical_gpu_index(local_rank: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        parts = [p.strip() for p in vis.split(",") if p.strip()]
+        if local_rank < len(parts) and parts[local_rank].isdigit():
+            return int(parts[local_rank])
+    return local_rank
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch of a kernel from the committed ncu summary
+    (profiles/ncu_traffic.txt lines: `<kernel> <workload> <bytes per launch>`)."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    try:
+        for line in open(path):
+            parts = line.split()
+            if len(parts) >= 3 and parts[0] == kernel and not line.startswith("#"):
+                return float(parts[2])
+    except OSError:
+        pass
+    return None
+
+
+def algorithmic_bytes(kernel: str, w, n_out_per_slide: float, undet_per_slide: float) -> float:
+    """Minimum DRAM bytes one launch (one slide) of each kernel must move."""
+    W, S, d = w.window, w.slide, w.dim
+    return {
+        "k_ingest": 4 * d * S + 4 * d * S + 8 * S,           # read slide, write ring + keys
+        "k_hist": 8 * W,                                      # read every key
+        "k_scan": 4 * 65536 * 3,                              # read counts, write starts+cursors
+        "k_scatter": 8 * W + 4 * d * W + (4 + 8 + 4 * d) * W,  # read keys+ring, write SoA
+        "k_count": (8 + 4 + 4 * d) * W,                       # read the cell-ordered SoA once
+        "k_compact": W + 8 * n_out_per_slide,                 # read flags, write IDs
+    }[kernel]
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, world, rank, local):
+    import torch
+    import torch.distributed as dist
+    from rtod_b200 import Detector
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    w = workload()
+    slides = w.slides
+    cap = slides * w.window // 4
+    pts_dev = torch.from_numpy(w.points).to(f"cuda:{local}")
+    out_dev = torch.empty(cap, dtype=torch.int64, device=f"cuda:{local}")
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    engines = {"plain": dict(router=False)}
+    results = {}
+    for name, kw in engines.items():
+        det = Detector(w.window, w.slide, w.R, w.K, dim=w.dim, device=local, **kw)
+        ref = None
+        for _ in range(max(3, args.warmup)):
+            det.reset()
+            r = det.run(pts_dev, out_ids=out_dev, ids_cap=cap, times=True)
+            ref = r.offsets.copy()
+        stats0 = det.stats
+        barrier()
+        dev_ms = 0.0
+        with ClockSampler(physical_gpu_index(local)) as clk:
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                det.reset()
+                r = det.run(pts_dev, out_ids=out_dev, ids_cap=cap, times=True)
+                dev_ms += r.times["total"] * r.slides
+        barrier()
+        stats1 = det.stats
+        assert np.array_equal(r.offsets, ref)
+        t_max = max_over_ranks(dev_ms)
+        n_outliers = int(r.offsets[-1])
+        # end to end through the public API with pinned host buffers
+        pts_pin = torch.from_numpy(w.points).pin_memory()
+        ids_pin = torch.empty(cap, dtype=torch.int64).pin_memory()
+        pts_np, ids_np = pts_pin.numpy(), ids_pin.numpy()
+        for _ in range(2):
+            det.reset()
+            det.run(pts_np, out_ids=ids_np, ids_cap=cap)
+        barrier()
+        e2e_s = 0.0
+        e2e_steps = max(3, min(args.steps, 50))
+        for _ in range(e2e_steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            det.reset()
+            t0 = time.perf_counter()
+            r2 = det.run(pts_np, out_ids=ids_np, ids_cap=cap)
+            e2e_s += time.perf_counter() - t0
+        barrier()
+        assert np.array_equal(r2.offsets, ref)
+        e2e_max = max_over_ranks(e2e_s)
+        # per-kernel device time of one pass (diagnostic, individual launches)
+        det.reset()
+        prof = det.profile(pts_dev)
+        det.close()
+        results[name] = dict(dev_ms=t_max, clocks=clk.summary(), launches=stats1["launches"] - stats0["launches"],
+                             n_outliers=n_outliers, undet=r.times["undetermined_per_slide"],
+                             e2e_s=e2e_max, e2e_steps=e2e_steps, prof=prof, h2d=w.n * w.dim * 4,
+                             d2h=(slides + 1) * 8 + n_outliers * 8 + slides * 8)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+    return w, results
+
+
+def cpu_baseline(w):
+    from oracle import oracle
+    oracle.build()
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    off, ids, st = oracle.detect(w.points, w.window, w.slide, w.R, w.K, engine="grid", threads=threads)
+    dt = time.perf_counter() - t0
+    slides = len(off) - 1
+    return {"value": slides * w.slide / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"whole stream once ({slides} slides), oracle grid engine, slides split over "
+                      f"{threads} threads", "us_per_slide": dt / slides * 1e6}, (off, ids)
+
+
+def emit_ours(args, world, w, res):
+    r = res["plain"]
+    K = args.steps
+    slides = w.slides
+    t_s = r["dev_ms"] / 1e3
+    value = world * K * slides * w.slide / t_s
+    us_slide = r["dev_ms"] * 1e3 / (K * slides)
+    # roofline of the dominant kernel
+    prof = r["prof"]
+    dom = max(prof, key=prof.get)
+    n_out = r["n_outliers"] / slides
+    alg = algorithmic_bytes(dom, w, n_out, r["undet"])
+    peak, peak_kind = hbm_peak()
+    achieved = alg / (prof[dom] / 1e3) / 1e9
+    traffic = ncu_traffic(dom)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": r["dev_ms"] / K, "us_per_slide": us_slide,
+        "window_points_per_s": world * K * slides * w.window / t_s,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded stand-in for RTOD's STK stream)",
+        "config": workload_config(w, {"engine": "plain grid kernel (router off), graph replay per slide"}),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": alg, "launch_ms": prof[dom],
+                     "kernel_ms_per_slide": prof},
+        "clocks": r["clocks"],
+        "gpu_launches": r["launches"],
+        "e2e": {"value": world * r["e2e_steps"] * slides * w.slide / r["e2e_s"], "unit": UNIT,
+                "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
+                "us_per_slide": r["e2e_s"] / (r["e2e_steps"] * slides) * 1e6},
+        "outliers_per_slide": n_out, "undetermined_per_slide": r["undet"],
+    }
+    if not args.no_cpu_baseline and world == 1:
+        cb, _ = cpu_baseline(w)
+        line["cpu_baseline"] = cb
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU restatement of RTOD's path, all host threads
+# ---------------------------------------------------------------------------
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    from oracle import oracle
+    oracle.build()
+    w = workload()
+    threads = os.cpu_count() or 1
+    for _ in range(max(1, min(args.warmup, 2))):
+        oracle.detect(w.points, w.window, w.slide, w.R, w.K, engine="grid", threads=threads)
+    steps = max(1, min(args.steps, 5))
+    t = 0.0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        off, _, _ = oracle.detect(w.points, w.window, w.slide, w.R, w.K, engine="grid", threads=threads)
+        t += time.perf_counter() - t0
+    slides = len(off) - 1
+    value = steps * slides * w.slide / t
+    sample = (f"{steps} pass(es) over the whole stream ({slides} slides each), CPU restatement of "
+              f"RTOD's grid filter + exact count, slides split over {threads} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": t / steps * 1e3,
+        "us_per_slide": t / (steps * slides) * 1e6, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded stand-in for RTOD's STK stream)",
+        "config": workload_config(w, {"engine": "reference CPU path (oracle port; RTOD itself needs "
+                                                 "OptiX + RT cores and cannot run here)"}),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    out = run_ours(args, world, rank, local)
+    if out is not None:
+        w, res = out
+        emit_ours(args, world, w, res)
+
+
+if __name__ == "__main__":
+    main()

@@ -127,8 +127,15 @@ class Detector:
         if out_ids is None:
             out = np.empty(ids_cap, np.int64)
             out_ptr = out.ctypes.data_as(ctypes.c_void_p)
+        elif isinstance(out_ids, np.ndarray):
+            if out_ids.dtype != np.int64 or not out_ids.flags.c_contiguous:
+                raise TypeError("out_ids must be a contiguous int64 array")
+            out = out_ids
+            ids_cap = min(ids_cap, out.size)
+            out_ptr = out.ctypes.data_as(ctypes.c_void_p)
         else:
             out = out_ids
+            ids_cap = min(ids_cap, out.numel())
             out_ptr = ctypes.c_void_p(out_ids.data_ptr())
         ns = ctypes.c_int64()
         t = Times()
@@ -137,7 +144,29 @@ class Detector:
                              ctypes.byref(ns), ctypes.byref(t) if times else None))
         del keep
         ids = out[:off[-1]] if out_ids is not None else out[:off[-1]].copy()
+        self.last_stats = self.stats
         return RunResult(off, ids, t.as_dict() if times else {})
+
+    @property
+    def stats(self) -> dict:
+        a = (ctypes.c_int64 * 4)()
+        check(lib().rtod_get_stats(self._h, a))
+        return {"launches": a[0], "graph_replays": a[1], "slides": a[2], "undetermined": a[3]}
+
+    def profile(self, points, max_slides: int = -1) -> dict:
+        """Average device ms per slide of each pipeline kernel (diagnostic run
+        on a fresh handle; every kernel launched on its own with CUDA events)."""
+        ptr, n, keep = _as_points(points, self.dim)
+        ms = (ctypes.c_double * 8)()
+        check(lib().rtod_profile_run(self._h, ptr, n, max_slides, ms, 8))
+        del keep
+        out = {}
+        for i in range(8):
+            name = lib().rtod_kernel_name(i)
+            if name is None:
+                break
+            out[name.decode()] = ms[i]
+        return out
 
     def reset(self) -> None:
         check(lib().rtod_reset(self._h))
