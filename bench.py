@@ -52,6 +52,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", choices=["bench", "ncu"], default="bench",
+                    help="ncu: a short pass (20 slides, no L2 flush buffer) for profiler captures")
     return ap.parse_args()
 
 
@@ -343,9 +345,26 @@ def run_reference(args, world, rank):
     }))
 
 
+def run_ncu_case(args, local):
+    """A short pass of the same workload for ncu captures: 3 passes of 20 slides."""
+    import torch
+    from rtod_b200 import Detector
+    w = workload()
+    torch.cuda.set_device(local)
+    pts = torch.from_numpy(w.points).to(f"cuda:{local}")
+    with Detector(w.window, w.slide, w.R, w.K, dim=w.dim, device=local) as det:
+        for _ in range(3):
+            det.reset()
+            r = det.run(pts, max_slides=20)
+    print(json.dumps({"mode": "ncu", "slides": r.slides, "outliers": int(r.offsets[-1])}))
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_env()
+    if args.mode == "ncu":
+        run_ncu_case(args, local)
+        return
     if args.impl == "reference":
         run_reference(args, world, rank)
         return

@@ -64,10 +64,12 @@ typedef struct rtod_config {
                           and a full-sweep queue); results are identical either way */
   int32_t tuner;       /* 1 = autotune cell width and block shape on the first slides */
   int32_t cells_per_r; /* grid cells per R along each hashed dimension (1..3; 0 = auto) */
-  int32_t block_warps; /* warps per block of the range-count kernel (1..32; 0 = auto) */
-  int32_t use_graph;   /* 1 = replay each slide as a captured CUDA graph */
+  int32_t block_warps; /* warps per block of the range-count kernel (1, 2, 4, 8; 0 = auto) */
+  int32_t use_graph;   /* 1 = replay each launch sequence as a captured CUDA graph */
   int32_t device;      /* CUDA device ordinal */
-  int32_t reserved[4];
+  int32_t batch;       /* rtod_run: windows detected per launch (0 = auto); each window is
+                          processed on its own, so results do not depend on it */
+  int32_t reserved[3];
 } rtod_config;
 
 /* Per-slide stage times in ms, averaged over the slides of the last call,
@@ -132,21 +134,44 @@ int rtod_get_tuning(const rtod_handle* h, int32_t out[3]);
 
 /* Counters since create: out[0] kernel launches issued by the library (a
    graph replay counts each of its kernels), out[1] graph replays, out[2]
-   slides detected, out[3] points that needed an exact count. No counterpart
-   in RTOD (diagnostic). */
-int rtod_get_stats(const rtod_handle* h, int64_t out[4]);
+   slides detected, out[3] points that needed an exact count, out[4] device
+   bytes currently allocated by the handle (RTOD's "[Mem] Device memory used
+   for data", src/ods/optixScan.cpp:1172-1174). */
+int rtod_get_stats(const rtod_handle* h, int64_t out[5]);
 
 /* Diagnostic run: like rtod_run on a fresh handle but launches every kernel
    individually with a CUDA event after each, and writes the average device
-   time per slide of each pipeline kernel, in order (ingest, hist, scan,
-   scatter, count, compact), to kernel_ms[0..n_kernels). Results are
-   discarded. The kernel names are given by rtod_kernel_name(i). No
+   time per slide of each pipeline kernel, in order (keys, hist, scan,
+   scatter, count, compact, and the router's training step), to
+   kernel_ms[0..n_kernels). A batch of B
+   windows shares one launch of each kernel; its time is divided by B. The
+   kernel names are given by rtod_kernel_name(i). Results are discarded. No
    counterpart in RTOD (it times stages with gettimeofday, src/ods/timer.h). */
 int rtod_profile_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides,
                      double* kernel_ms, int32_t n_kernels);
 
 /* Name of pipeline kernel i (0-based) as used by rtod_profile_run, or NULL. */
 const char* rtod_kernel_name(int32_t i);
+
+/* Learned router state (rtod_config.router = 1). params (may be NULL)
+   receives the network's rtod_mlp_param_count() parameters; info receives
+   [0] training steps, [1] last training loss, [2] points routed to the
+   early-exit queue, [3] to the full-sweep queue, [4] misroutes (predicted
+   inlier but outlier, or the reverse), [5] routing threshold. No counterpart
+   in RTOD (it has no learned component). */
+int rtod_router_info(rtod_handle* h, float* params, double info[6]);
+
+/* Router network test entry points (no counterpart in RTOD), run on the
+   given device with host buffers: parameter count; forward logits
+   (n x 4) of n feature rows (n x 3); mean cross-entropy loss and its
+   gradient for labels y in 0..3; one Adam step (step number t >= 1,
+   beta1 0.9, beta2 0.999, eps 1e-8) updating params, m and v in place. */
+int rtod_mlp_param_count(void);
+int rtod_mlp_forward(int32_t device, const float* params, const float* x, int64_t n, float* logits);
+int rtod_mlp_grad(int32_t device, const float* params, const float* x, const int32_t* y, int64_t n,
+                  float* grad, float* loss);
+int rtod_mlp_adam(int32_t device, float* params, float* m, float* v, int32_t t, const float* x,
+                  const int32_t* y, int64_t n, float lr, float* loss);
 
 void rtod_destroy(rtod_handle* h);
 

@@ -32,8 +32,8 @@ class Config(ctypes.Structure):
         ("K", ctypes.c_int32), ("dim", ctypes.c_int32), ("opt", ctypes.c_int32),
         ("pred", ctypes.c_int32), ("router", ctypes.c_int32), ("tuner", ctypes.c_int32),
         ("cells_per_r", ctypes.c_int32), ("block_warps", ctypes.c_int32),
-        ("use_graph", ctypes.c_int32), ("device", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("use_graph", ctypes.c_int32), ("device", ctypes.c_int32), ("batch", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
 
@@ -67,6 +67,11 @@ SIGNATURES = [
     ("rtod_get_stats", _i32, [_vp, _vp]),
     ("rtod_profile_run", _i32, [_vp, _vp, _i64, _i64, _vp, _i32]),
     ("rtod_kernel_name", ctypes.c_char_p, [_i32]),
+    ("rtod_router_info", _i32, [_vp, _vp, _vp]),
+    ("rtod_mlp_param_count", _i32, []),
+    ("rtod_mlp_forward", _i32, [_i32, _vp, _vp, _i64, _vp]),
+    ("rtod_mlp_grad", _i32, [_i32, _vp, _vp, _vp, _i64, _vp, _vp]),
+    ("rtod_mlp_adam", _i32, [_i32, _vp, _vp, _vp, _i32, _vp, _vp, _i64, ctypes.c_float, _vp]),
     ("rtod_destroy", None, [_vp]),
     ("rtod_last_error", ctypes.c_char_p, []),
     ("rtod_version", ctypes.c_char_p, []),

@@ -1,24 +1,47 @@
-// Device code of the per-slide detector pipeline (sm_100a).
+// Device code of the detector pipeline (sm_100a), batched over jobs.
 //
-// One slide runs six kernels, in stream order:
-//   k_ingest   ring-buffer window update: the S new points go to their ring
-//              slots (slot = global index % W) as SoA, each gets its packed
-//              grid-cell key; per-slide bins and flags are cleared.
-//              Replaces the H2D at src/ods/optixScan.cpp:1051-1058, the host
-//              mirror at :1062-1064 and the resets at :1047-1050.
-//   k_hist     cell occupancy: per-bin point counts and a "bin holds more
-//              than one cell" flag. Replaces the expire/insert bookkeeping of
-//              prepare_c_non_points_queue (:967-981) and FixQueue (state.h).
-//   k_scan     exclusive scan of the bin counts -> bin starts.
-//   k_scatter  counting sort of the window into cell order (slot, key and
-//              coordinates as SoA). Together with k_scan this replaces
-//              kGenAABB (aabb.cu:5-45) and the BVH rebuild (:378-426).
-//   k_count    range count with K early exit and safe-inlier skip. Replaces
-//              the ray launch and intersection program (optixScan.cu:21-75,
-//              :158-199) and the all-inlier cell filter (:983-993).
-//   k_compact  outlier flags -> sorted global indices, per-slide counters;
-//              replaces the D2H + host pick at :1083-1101 and advances the
-//              window (:1103-1108).
+// A job is the detection of one window of one stream. Every kernel takes a
+// Batch (a table of jobs) and uses blockIdx.y as the job index, so one launch
+// serves B windows: consecutive windows of one resident stream (rtod_run),
+// the current window of many streams (batched streaming), or the single
+// window of a push/detect step. A batch runs five kernels in stream order:
+//
+//   k_hist     cell occupancy of each window: per-bin point counts and the
+//              per-bin key range (a bin holds one cell iff min == max). Replaces the expire /
+//              insert bookkeeping of prepare_c_non_points_queue
+//              (src/ods/optixScan.cpp:967-981) and FixQueue (state.h:15-57).
+//   k_scan     exclusive scan of the bin counts -> bin starts (16 tiles per
+//              window chained by a warp-parallel decoupled look-back).
+//   k_scatter  counting sort of the window into cell order (window offset,
+//              cell key and coordinates as SoA) and classification: points
+//              of a bin that holds one cell with more than K points are
+//              inliers (safe-inlier skip, the all-inlier cell filter of
+//              :983-993); every other point goes to the query queue.
+//              k_scan + k_scatter replace kGenAABB (aabb.cu:5-45), the BVH
+//              rebuild (:378-426) and the undetermined-point gather
+//              (:995-1016).
+//   k_count    range count of the queued points, one warp per point, K early
+//              exit. Replaces the ray launch and intersection program
+//              (optixScan.cu:21-75, :158-199). With the learned router on
+//              (router.cuh), k_scatter splits the queue into an early-exit and
+//              a full-sweep queue and k_count treats them differently; the
+//              router network is trained after the batch by k_train.
+//   k_compact  outlier bitset -> sorted global indices appended to the batch
+//              output in job order; per-slide records; window advance.
+//              Replaces the D2H + host pick of :1083-1101 and :1103-1108.
+//
+// Points come either from a ring (push/detect streaming: SoA [D][W], ring
+// slot = global index % W, filled by k_ingest, which replaces the slide H2D
+// and host mirror of :1051-1064) or straight from a stream resident in HBM
+// (point-major, keys precomputed by k_keys).
+//
+// Scratch arrays clean up after themselves for the next batch: k_scatter
+// hands bin counts back to zero (it claims positions with atomicSub),
+// k_count resets the per-bin key ranges and the compaction look-back words, k_compact
+// clears the outlier bits it read, and the last k_compact block resets the
+// per-job counters. Consecutive kernels use programmatic dependent launch:
+// each kernel lets the next one launch early and waits (griddepcontrol.wait)
+// for its predecessor to complete before touching shared data.
 #pragma once
 
 #include <cstdint>
@@ -27,61 +50,88 @@
 namespace rtod {
 
 constexpr int NB_LOG2 = 16;
-constexpr uint32_t NB = 1u << NB_LOG2;  // bins of the cell hash table
+constexpr uint32_t NB = 1u << NB_LOG2;  // bins of the cell hash table, per job
 constexpr uint32_t NB_MASK = NB - 1;
-constexpr uint64_t EMPTY_KEY = ~0ull;
+constexpr unsigned long long EMPTY_KEY = ~0ull;
+constexpr int SCAN_TILE = 4096;             // bins per k_scan tile (16 per thread)
+constexpr int SCAN_TILES = NB / SCAN_TILE;  // 16
+constexpr int CMP_TILE = 8192;              // window offsets per k_compact tile (32 per thread)
+constexpr int SPIN_LIMIT = 1 << 22;         // bounded waits (then DERR_TIMEOUT)
 
 // Device error codes (first one wins).
-enum : int32_t { DERR_NONE = 0, DERR_NONFINITE = 1, DERR_RANGE = 2, DERR_CAPACITY = 3 };
+enum : int32_t {
+  DERR_NONE = 0, DERR_NONFINITE = 1, DERR_RANGE = 2, DERR_CAPACITY = 3, DERR_TIMEOUT = 4
+};
 
-// Stream state that lives on the device, so that a captured slide graph can
-// be replayed without host-side parameter changes.
-struct DevState {
-  int64_t n_ingested;   // points written to the ring so far (= next global index)
-  int64_t out_total;    // outlier IDs appended to out_ids so far
-  int64_t slide;        // slides detected so far
-  int64_t undet_total;  // counted (undetermined) points summed over slides
-  int32_t err;          // DERR_*
-  int32_t n_out;        // outliers of the last slide
-  int32_t n_undet;      // counted points of the last slide
+// Per-job counters (device). lo is the first global index of the job's
+// window; after each detection it advances by lo_step.
+struct JobCtr {
+  int64_t lo;
+  int64_t lo_step;
+  int32_t n_undet;       // queued points: early-exit queue (router on) or the only queue
+  int32_t n_out;         // outliers found
+  uint32_t scan_ticket;  // k_scan tile tickets
+  uint32_t cmp_ticket;   // k_compact tile tickets
+  int32_t n_sweep;       // queued points of the full-sweep queue (router on)
   int32_t pad;
 };
 
-struct KParams {
-  int64_t W, S;
-  int32_t D;       // dimensions
-  int32_t h;       // hashed dimensions (min(D, 3))
-  int32_t n;       // cells per R: cell side = R*(1+2^-12)/n, stencil reach n cells
-  int32_t K;
-  int32_t filter;  // safe-inlier skip (grid filter) enabled
-  int32_t src_staging;  // 1: src holds exactly the points being ingested
-  double cell;
-  double R, R2;
-  float R2f;
-  const float* src;     // points to ingest, point-major
-  float* ring;          // [D][W]
-  uint64_t* ckey;       // [W] packed cell key per ring slot
-  uint32_t* bin_count;  // [NB]
-  uint32_t* bin_start;  // [NB + 1]
-  uint32_t* cursor;     // [NB]
-  uint64_t* owner;      // [NB] first cell key seen in a bin
-  uint8_t* mixed;       // [NB] bin holds points of more than one cell
-  uint32_t* s_slot;     // [W] cell-ordered: ring slot
-  uint64_t* s_ckey;     // [W] cell-ordered: cell key
-  float* s_x;           // [D][W] cell-ordered coordinates
-  uint8_t* flags;       // [W] per ring slot: outlier this slide
-  uint8_t* prev;        // [W] per ring slot: capped count of the last slide
-  DevState* state;
-  int64_t* out_ids;     // appended sorted outlier IDs
-  int64_t out_cap;
-  int32_t* slide_nout;  // per-slide outlier counts (run mode), may be null
-  int32_t* slide_undet; // per-slide counted points (run mode), may be null
-  int64_t slide_rec_cap;
+// Per-handle state (device).
+struct BatchState {
+  int64_t out_total;    // outlier IDs appended to out_ids so far
+  int64_t slides;       // windows detected so far
+  int64_t undet_total;  // queued points summed over windows
+  int32_t err;          // DERR_*
+  uint32_t done;        // finished k_compact tiles of the running batch
 };
 
-__device__ __forceinline__ void set_err(DevState* st, int32_t code) {
-  atomicCAS(&st->err, 0, code);
-}
+struct Job {
+  int64_t W, S, Wp;  // window, slide, padded SoA row stride (multiple of 4, >= W + 4)
+  double cell;       // cell side: R * (1 + 2^-12) / n
+  double R, R2;
+  float R2f;         // fl32(fl32(R)^2)
+  int32_t K;
+  int32_t n;         // cells per R = stencil reach in cells
+  int32_t filter;    // safe-inlier skip enabled
+  int32_t ring;      // 1: ring source, 0: resident stream
+  const float* pts;       // ring: SoA [D][W] by slot; stream: point-major [N][D]
+  const uint64_t* keys;   // ring: [W] by slot; stream: [N] by global index
+  const float* stage;     // ring: the points k_ingest writes (point-major)
+  uint8_t* prev;          // last capped count per source position (255 = safe, 254 = none)
+  uint32_t* bin_count;    // [NB]
+  uint32_t* bin_start;    // [NB + 1]
+  unsigned long long* kmin;   // [NB] smallest cell key in a bin (EMPTY_KEY when none)
+  unsigned long long* kmax;   // [NB] largest cell key in a bin (0 when none)
+  uint32_t* s_off;        // [W] cell-ordered: window offset (global index - lo)
+  uint64_t* s_ckey;       // [W] cell-ordered: cell key
+  float* s_x;             // [D][Wp] cell-ordered coordinates
+  uint32_t* queue;        // [W] cell-ordered positions that need an exact count; with the
+                          // router on, the early-exit queue grows from the front and the
+                          // full-sweep queue from the back
+  float* feat;            // [W][3] router features, at the same index as the queue entry
+  uint32_t* flags;        // [ceil(W / 32)] outlier bit per window offset
+  unsigned long long* scan_status;  // [SCAN_TILES]
+  unsigned long long* cmp_status;   // [ceil(W / CMP_TILE)]
+  JobCtr* ctr;
+  int32_t* rec_nout;      // per-slide outlier counts, indexed (lo - S) / S; may be null
+  int32_t* rec_undet;
+  int64_t rec_cap;
+};
+
+struct RouterState;
+
+// Kernel argument: the jobs of one launch and the shared output.
+struct Batch {
+  const Job* jobs;
+  int32_t njobs;
+  BatchState* bs;
+  RouterState* router;  // learned router (used when the kernels are built with ROUTE)
+  int64_t* out_ids;  // outlier IDs of all jobs, concatenated in job order
+  int64_t out_cap;
+  int64_t cmp_tiles; // k_compact tiles over all jobs
+};
+
+__device__ __forceinline__ void set_err(BatchState* bs, int32_t code) { atomicCAS(&bs->err, 0, code); }
 
 // ---------------------------------------------------------------------------
 // Grid cells. Cell coordinate k_i = floor(x_i / cell) in double precision,
@@ -89,9 +139,9 @@ __device__ __forceinline__ void set_err(DevState* st, int32_t code) {
 // |x/cell| below the limits below, any pair accepted by either predicate has
 // |k_i(p) - k_i(q)| <= n (the stencil), and for D <= 3, n >= 2 two points of
 // one cell are always neighbours (so a cell with more than K points is
-// all-inlier). Limits keep the double rounding of x/cell below 2^-16 cells.
+// all-inlier). The limits keep the double rounding of x/cell below 2^-16 cells.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double coord_limit(int h) {
+__host__ __device__ __forceinline__ double coord_limit(int h) {
   return h == 1 ? 68719476736.0 /* 2^36 */ : (h == 2 ? 1073741824.0 /* 2^30 */ : 1048576.0 /* 2^20 */);
 }
 
@@ -130,10 +180,38 @@ __device__ __forceinline__ uint32_t bin_of_key(uint64_t key, int h) {
   return bin_of(k, h);
 }
 
+template <int D>
+struct Hashed {
+  static constexpr int value = D < 3 ? D : 3;
+};
+
+// Cell key of one point; *code = DERR_NONFINITE for a non-finite coordinate,
+// DERR_RANGE for one too large for the grid (then the key is zero).
+template <int D>
+__device__ __forceinline__ uint64_t cell_key(const float* x, double cell, int32_t* code) {
+  constexpr int H = Hashed<D>::value;
+  const double lim = coord_limit(H);
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < D; ++d) ok &= isfinite(x[d]);
+  int64_t k[3] = {0, 0, 0};
+  bool inr = true;
+#pragma unroll
+  for (int d = 0; d < H; ++d) {
+    const double q = floor(__ddiv_rn((double)x[d], cell));
+    inr &= (q > -lim) && (q < lim);
+    k[d] = inr ? (int64_t)q : 0;
+  }
+  *code = !ok ? DERR_NONFINITE : (!inr ? DERR_RANGE : DERR_NONE);
+  if (*code) k[0] = k[1] = k[2] = 0;
+  return pack_key(k, H);
+}
+
 // ---------------------------------------------------------------------------
-// Neighbour predicates (see rtod.h). PRED 0: FP32, each subtract, multiply and
-// add rounded on its own (no FMA contraction), summed left to right,
-// d2 <= R2f. PRED 1: RTOD's double test (src/ods/optixScan.cu:170-190).
+// Neighbour predicates. PRED 0: FP32, each subtract, multiply and add
+// rounded on its own (no FMA contraction), summed left to right,
+// d2 <= fl32(fl32(R)^2). PRED 1: RTOD's double test
+// (src/ods/optixScan.cu:170-190): |dx| < R in 1-d, d^2 < R*R otherwise.
 // ---------------------------------------------------------------------------
 template <int D, int PRED>
 __device__ __forceinline__ bool is_nbr(const float* q, const float* c, float R2f, double R, double R2) {
@@ -141,8 +219,8 @@ __device__ __forceinline__ bool is_nbr(const float* q, const float* c, float R2f
     float s = 0.0f;
 #pragma unroll
     for (int i = 0; i < D; ++i) {
-      float dx = __fsub_rn(q[i], c[i]);
-      float t = __fmul_rn(dx, dx);
+      const float dx = __fsub_rn(q[i], c[i]);
+      const float t = __fmul_rn(dx, dx);
       s = (i == 0) ? t : __fadd_rn(s, t);
     }
     return s <= R2f;
@@ -153,19 +231,14 @@ __device__ __forceinline__ bool is_nbr(const float* q, const float* c, float R2f
       double s = 0.0;
 #pragma unroll
       for (int i = 0; i < D; ++i) {
-        double dx = __dsub_rn((double)q[i], (double)c[i]);
-        double t = __dmul_rn(dx, dx);
+        const double dx = __dsub_rn((double)q[i], (double)c[i]);
+        const double t = __dmul_rn(dx, dx);
         s = (i == 0) ? t : __dadd_rn(s, t);
       }
       return s < R2;
     }
   }
 }
-
-template <int D>
-struct Hashed {
-  static constexpr int value = D < 3 ? D : 3;
-};
 
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
@@ -174,156 +247,245 @@ __device__ __forceinline__ unsigned lanemask_lt() {
 }
 
 // ---------------------------------------------------------------------------
-// k_ingest: ring update (+ per-slide resets).
+// Programmatic dependent launch, release/acquire and single-pass scans.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;"); }
+
+__device__ __forceinline__ void st_release(unsigned long long* a, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(a), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long* a) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(a) : "memory");
+  return v;
+}
+
+constexpr unsigned long long LB_AGG = 1ull << 62;     // tile total published
+constexpr unsigned long long LB_PREFIX = 2ull << 62;  // inclusive prefix published
+
+// Exclusive prefix of `tile` over all earlier tiles of one scan, computed by
+// one full warp: publishes the tile total, then inspects the 32 nearest
+// predecessors at once and sums back to the nearest published prefix, then
+// publishes its own inclusive prefix. Tiles are claimed in ticket order, so
+// every predecessor is running or done and the chain always resolves; each
+// wait is still bounded (DERR_TIMEOUT, partial sum used).
+__device__ uint32_t warp_lookback(unsigned long long* status, uint32_t tile, uint32_t total,
+                                  BatchState* bs) {
+  const int lane = threadIdx.x & 31;
+  if (tile == 0) {
+    if (lane == 0) st_release(&status[0], LB_PREFIX | total);
+    return 0;
+  }
+  if (lane == 0) st_release(&status[tile], LB_AGG | total);
+  uint32_t acc = 0;
+  int64_t base = (int64_t)tile - 1;
+  while (true) {
+    const int64_t idx = base - lane;
+    unsigned long long v = LB_PREFIX;  // before tile 0: an empty prefix
+    if (idx >= 0) {
+      int it = 0;
+      while (((v = ld_acquire(&status[idx])) >> 62) == 0) {
+        if (++it > SPIN_LIMIT) {
+          set_err(bs, DERR_TIMEOUT);
+          v = LB_PREFIX;
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    const unsigned pref = __ballot_sync(0xffffffffu, (v >> 62) == 2);
+    const int stop = pref ? __ffs(pref) - 1 : 31;
+    uint32_t val = lane <= stop ? (uint32_t)(v & 0xffffffffull) : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+    acc += val;
+    if (pref) break;
+    base -= 32;
+  }
+  if (lane == 0) st_release(&status[tile], LB_PREFIX | (acc + total));
+  return acc;
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim.x <= 1024).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* total, uint32_t* smem33) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  uint32_t inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) smem33[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    const uint32_t w = lane < nw ? smem33[lane] : 0;
+    uint32_t wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    smem33[lane] = wi - w;
+    if (lane == 31) smem33[32] = wi;
+  }
+  __syncthreads();
+  const uint32_t r = smem33[wid] + inc - v;
+  *total = smem33[32];
+  __syncthreads();
+  return r;
+}
+
+// Window offset i of a job -> source position (ring slot or global index).
+__device__ __forceinline__ int64_t source_pos(const Job& jb, int64_t lo, int64_t i) {
+  const int64_t g = lo + i;
+  return jb.ring ? g % jb.W : g;
+}
+
+template <int D>
+__device__ __forceinline__ void load_point(const Job& jb, int64_t src, float* x) {
+  if (jb.ring) {
+#pragma unroll
+    for (int d = 0; d < D; ++d) x[d] = jb.pts[(int64_t)d * jb.W + src];
+  } else {
+#pragma unroll
+    for (int d = 0; d < D; ++d) x[d] = jb.pts[src * D + d];
+  }
+}
+
+}  // namespace rtod
+
+#include "router.cuh"
+
+namespace rtod {
+
+// ---------------------------------------------------------------------------
+// k_keys: cell keys of a resident stream, global indices [g0, g1).
 // ---------------------------------------------------------------------------
 template <int D>
-__global__ void __launch_bounds__(256) k_ingest(KParams p, int64_t n_new) {
-  DevState* st = p.state;
-  const int64_t base = st->n_ingested;
-  const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_keys(const float* pts, int64_t g0, int64_t g1, double cell,
+                                              uint64_t* keys, uint8_t* prev, BatchState* bs) {
+  pdl_trigger();
+  pdl_wait();
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  if (tid == 0) st->n_undet = 0;
-  for (int64_t i = tid; i < NB; i += stride) {
-    p.bin_count[i] = 0;
-    p.owner[i] = EMPTY_KEY;
-    p.mixed[i] = 0;
-  }
-  for (int64_t i = tid; i < p.W; i += stride) p.flags[i] = 0;
-  constexpr int H = Hashed<D>::value;
-  const double lim = coord_limit(H);
-  for (int64_t i = tid; i < n_new; i += stride) {
-    const int64_t g = base + i;
-    const int64_t slot = g % p.W;
-    const float* s = p.src + (p.src_staging ? i : g) * D;
+  for (int64_t g = g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < g1; g += stride) {
     float x[D];
-    bool ok = true;
 #pragma unroll
-    for (int d = 0; d < D; ++d) {
-      x[d] = s[d];
-      ok &= isfinite(x[d]);
-    }
-    int64_t k[3] = {0, 0, 0};
-    bool inr = true;
-#pragma unroll
-    for (int d = 0; d < H; ++d) {
-      double qd = floor(__ddiv_rn((double)x[d], p.cell));
-      inr &= (qd > -lim) && (qd < lim);
-      k[d] = inr ? (int64_t)qd : 0;
-    }
-    if (!ok) set_err(st, DERR_NONFINITE);
-    else if (!inr) set_err(st, DERR_RANGE);
-#pragma unroll
-    for (int d = 0; d < D; ++d) p.ring[(int64_t)d * p.W + slot] = x[d];
-    p.ckey[slot] = pack_key(k, H);
-    p.prev[slot] = 254;  // no count yet
+    for (int d = 0; d < D; ++d) x[d] = pts[g * D + d];
+    int32_t code;
+    keys[g] = cell_key<D>(x, cell, &code);
+    prev[g] = 254;
+    if (code) set_err(bs, code);
   }
 }
 
-// Window commit for the initial fill (no detection).
-__global__ void k_advance(DevState* st, int64_t n) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) st->n_ingested += n;
+// ---------------------------------------------------------------------------
+// k_ingest: ring update of every job. fill = 1 writes the first W points
+// (global indices [0, W)); otherwise the S newest points of the job's window
+// [lo, lo + W), i.e. [lo + W - S, lo + W). Slot = global index % W.
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(256) k_ingest(Batch b, int32_t fill) {
+  pdl_trigger();
+  pdl_wait();
+  const Job& jb = b.jobs[blockIdx.y];
+  float* ring = const_cast<float*>(jb.pts);
+  uint64_t* keys = const_cast<uint64_t*>(jb.keys);
+  const int64_t n_new = fill ? jb.W : jb.S;
+  const int64_t base = fill ? 0 : jb.ctr->lo + jb.W - jb.S;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += stride) {
+    const int64_t slot = (base + i) % jb.W;
+    float x[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) x[d] = jb.stage[i * D + d];
+    int32_t code;
+    const uint64_t key = cell_key<D>(x, jb.cell, &code);
+    if (code) set_err(b.bs, code);
+#pragma unroll
+    for (int d = 0; d < D; ++d) ring[(int64_t)d * jb.W + slot] = x[d];
+    keys[slot] = key;
+    jb.prev[slot] = 254;
+  }
 }
 
 // ---------------------------------------------------------------------------
-// k_hist: per-bin counts, warp-aggregated; "mixed" marks bins shared by cells.
+// k_hist: per-bin counts and the smallest / largest cell key per bin (a bin
+// holds a single cell iff they are equal), warp-aggregated, with atomics
+// whose results are not needed (no round trip on the critical path).
 // ---------------------------------------------------------------------------
-template <int H>
-__global__ void __launch_bounds__(256) k_hist(KParams p) {
+template <int D>
+__global__ void __launch_bounds__(256) k_hist(Batch b) {
+  pdl_trigger();
+  pdl_wait();
+  constexpr int H = Hashed<D>::value;
+  const Job& jb = b.jobs[blockIdx.y];
+  const int64_t lo = jb.ctr->lo;
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t w0 = warp * 32; w0 < p.W; w0 += nwarps * 32) {
-    const int64_t slot = w0 + lane;
-    const bool valid = slot < p.W;
-    const uint64_t key = valid ? p.ckey[slot] : EMPTY_KEY;
+  for (int64_t w0 = warp * 32; w0 < jb.W; w0 += nwarps * 32) {
+    const int64_t i = w0 + lane;
+    const bool valid = i < jb.W;
+    const uint64_t key = valid ? jb.keys[source_pos(jb, lo, i)] : EMPTY_KEY;
     const uint32_t bin = valid ? bin_of_key(key, H) : 0xffffffffu;
     const unsigned peers = __match_any_sync(0xffffffffu, bin);
     const int leader = __ffs(peers) - 1;
     const uint64_t lkey = __shfl_sync(0xffffffffu, key, leader);
-    const unsigned diff = __ballot_sync(0xffffffffu, key != lkey) & peers;
     if (valid && lane == leader) {
-      atomicAdd(&p.bin_count[bin], (uint32_t)__popc(peers));
-      const unsigned long long old =
-          atomicCAS((unsigned long long*)&p.owner[bin], (unsigned long long)EMPTY_KEY,
-                    (unsigned long long)key);
-      if (diff || (old != EMPTY_KEY && old != key)) p.mixed[bin] = 1;
+      atomicAdd(&jb.bin_count[bin], (uint32_t)__popc(peers));
+      atomicMin(&jb.kmin[bin], (unsigned long long)key);
+      atomicMax(&jb.kmax[bin], (unsigned long long)key);
+    } else if (valid && key != lkey) {
+      atomicMin(&jb.kmin[bin], (unsigned long long)key);
+      atomicMax(&jb.kmax[bin], (unsigned long long)key);
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// k_scan: exclusive scan of NB bin counts, one block of 1024 threads.
+// k_scan: exclusive scan of each job's NB bin counts. Grid (SCAN_TILES, jobs),
+// 256 threads; each thread owns 16 consecutive bins (four coalesced uint4).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_scan(KParams p) {
-  constexpr int PER = NB / 1024;  // 64 bins per thread
-  __shared__ uint32_t wsum[32];
-  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-  const uint4* src = reinterpret_cast<const uint4*>(p.bin_count + t * PER);
+__global__ void __launch_bounds__(256) k_scan(Batch b) {
+  __shared__ uint32_t sm[33];
+  __shared__ uint32_t s_tile, s_prefix;
+  pdl_trigger();
+  pdl_wait();
+  const Job& jb = b.jobs[blockIdx.y];
+  if (threadIdx.x == 0) s_tile = atomicAdd(&jb.ctr->scan_ticket, 1u);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  const uint32_t b0 = tile * SCAN_TILE + threadIdx.x * 16;
+  uint4 v[4];
   uint32_t sum = 0;
 #pragma unroll
-  for (int j = 0; j < PER / 4; ++j) {
-    uint4 v = src[j];
-    sum += v.x + v.y + v.z + v.w;
+  for (int q = 0; q < 4; ++q) {
+    v[q] = *reinterpret_cast<const uint4*>(jb.bin_count + b0 + 4 * q);
+    sum += v[q].x + v[q].y + v[q].z + v[q].w;
   }
-  uint32_t inc = sum;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += y;
-  }
-  if (lane == 31) wsum[wid] = inc;
-  __syncthreads();
-  if (wid == 0) {
-    uint32_t v = wsum[lane], vi = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xffffffffu, vi, o);
-      if (lane >= o) vi += y;
+  uint32_t total;
+  const uint32_t ex = block_exclusive_scan(sum, &total, sm);
+  if (threadIdx.x < 32) {
+    const uint32_t pre = warp_lookback(jb.scan_status, tile, total, b.bs);
+    if (threadIdx.x == 0) {
+      s_prefix = pre;
+      if (tile == SCAN_TILES - 1) {
+        jb.bin_start[NB] = pre + total;
+        jb.ctr->scan_ticket = 0;
+      }
     }
-    wsum[lane] = vi - v;
   }
   __syncthreads();
-  uint32_t run = wsum[wid] + inc - sum;
-  uint4* dst = reinterpret_cast<uint4*>(p.bin_start + t * PER);
-  uint4* cur = reinterpret_cast<uint4*>(p.cursor + t * PER);
+  uint32_t run = s_prefix + ex;
 #pragma unroll
-  for (int j = 0; j < PER / 4; ++j) {
-    uint4 v = src[j], o;
-    o.x = run; run += v.x;
-    o.y = run; run += v.y;
-    o.z = run; run += v.z;
-    o.w = run; run += v.w;
-    dst[j] = o;
-    cur[j] = o;
-  }
-  if (t == 1023) p.bin_start[NB] = run;
-}
-
-// ---------------------------------------------------------------------------
-// k_scatter: window -> cell-ordered SoA (counting sort, warp-aggregated).
-// ---------------------------------------------------------------------------
-template <int D>
-__global__ void __launch_bounds__(256) k_scatter(KParams p) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t w0 = warp * 32; w0 < p.W; w0 += nwarps * 32) {
-    const int64_t slot = w0 + lane;
-    const bool valid = slot < p.W;
-    const uint64_t key = valid ? p.ckey[slot] : EMPTY_KEY;
-    const uint32_t bin = valid ? bin_of_key(key, Hashed<D>::value) : 0xffffffffu;
-    const unsigned peers = __match_any_sync(0xffffffffu, bin);
-    const int leader = __ffs(peers) - 1;
-    uint32_t base = 0;
-    if (valid && lane == leader) base = atomicAdd(&p.cursor[bin], (uint32_t)__popc(peers));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (valid) {
-      const uint32_t pos = base + __popc(peers & lanemask_lt());
-      p.s_slot[pos] = (uint32_t)slot;
-      p.s_ckey[pos] = key;
-#pragma unroll
-      for (int d = 0; d < D; ++d) p.s_x[(int64_t)d * p.W + pos] = p.ring[(int64_t)d * p.W + slot];
-    }
+  for (int q = 0; q < 4; ++q) {
+    uint4 o;
+    o.x = run; run += v[q].x;
+    o.y = run; run += v[q].y;
+    o.z = run; run += v[q].z;
+    o.w = run; run += v[q].w;
+    *reinterpret_cast<uint4*>(jb.bin_start + b0 + 4 * q) = o;
   }
 }
 
@@ -360,133 +522,415 @@ __device__ __forceinline__ bool for_each_run(const uint32_t* bin_start, const in
 }
 
 // ---------------------------------------------------------------------------
-// k_count (plain): one warp per 32 cell-ordered points. Points of a bin that
-// holds a single cell with more than K points are inliers without any test
-// (safe-inlier skip). Every other point is counted by the whole warp:
-// 32 candidates per step, tested with the predicate, tallied with
-// ballot/popc, stopping as soon as the count exceeds K.
+// k_scatter: window -> cell-ordered SoA (counting sort, warp-aggregated;
+// positions are claimed with atomicSub so the bin counts end at zero),
+// safe-inlier classification and the query queue.
 // ---------------------------------------------------------------------------
-template <int D, int PRED>
-__global__ void __launch_bounds__(256) k_count(KParams p) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t pos = warp * 32 + lane;
-  const bool valid = pos < p.W;
-  if (warp * 32 >= p.W) return;
+template <int D, bool ROUTE>
+__global__ void __launch_bounds__(256) k_scatter(Batch b) {
+  pdl_trigger();
+  pdl_wait();
   constexpr int H = Hashed<D>::value;
-  const uint64_t key = valid ? p.s_ckey[pos] : 0;
-  const uint32_t slot = valid ? p.s_slot[pos] : 0;
-  bool need = valid;
-  if (valid && p.filter) {
-    const uint32_t b = bin_of_key(key, H);
-    const uint32_t cnt = p.bin_start[b + 1] - p.bin_start[b];
-    if (cnt > (uint32_t)p.K && !p.mixed[b]) need = false;
-  }
-  if (valid && !need) p.prev[slot] = 255;
-  float x[D];
+  const Job& jb = b.jobs[blockIdx.y];
+  const int64_t lo = jb.ctr->lo;
+  if (blockIdx.x == 0 && threadIdx.x < SCAN_TILES) jb.scan_status[threadIdx.x] = 0;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = lanemask_lt();
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t w0 = warp * 32; w0 < jb.W; w0 += nwarps * 32) {
+    const int64_t i = w0 + lane;
+    const bool valid = i < jb.W;
+    const int64_t src = valid ? source_pos(jb, lo, i) : 0;
+    const uint64_t key = valid ? jb.keys[src] : EMPTY_KEY;
+    const uint32_t bin = valid ? bin_of_key(key, H) : 0xffffffffu;
+    const unsigned peers = __match_any_sync(0xffffffffu, bin);
+    const int leader = __ffs(peers) - 1;
+    const uint32_t c = (uint32_t)__popc(peers);
+    uint32_t top = 0;
+    if (valid && lane == leader) top = atomicSub(&jb.bin_count[bin], c);
+    top = __shfl_sync(0xffffffffu, top, leader);
+    bool safe = false;
+    uint32_t pos = 0, cnt = 0;
+    if (valid) {
+      const uint32_t bs0 = jb.bin_start[bin];
+      pos = bs0 + top - c + __popc(peers & lt);
+      float x[D];
+      load_point<D>(jb, src, x);
+      jb.s_off[pos] = (uint32_t)i;
+      jb.s_ckey[pos] = key;
 #pragma unroll
-  for (int d = 0; d < D; ++d) x[d] = valid ? p.s_x[(int64_t)d * p.W + pos] : 0.0f;
-  unsigned todo = __ballot_sync(0xffffffffu, need);
-  if (lane == 0 && todo) atomicAdd(&p.state->n_undet, __popc(todo));
-  while (todo) {
-    const int q = __ffs(todo) - 1;
-    todo &= todo - 1;
-    float qx[D];
-#pragma unroll
-    for (int d = 0; d < D; ++d) qx[d] = __shfl_sync(0xffffffffu, x[d], q);
-    const uint64_t qkey = __shfl_sync(0xffffffffu, key, q);
-    const uint32_t qslot = __shfl_sync(0xffffffffu, slot, q);
-    int64_t k[3];
-    unpack_key(qkey, H, k);
-    int total = 0;
-    const bool done = for_each_run<H>(p.bin_start, k, p.n, [&](uint32_t rs, uint32_t re) {
-      for (uint32_t b = rs; b < re; b += 32) {
-        const uint32_t c = b + lane;
-        bool in = false;
-        if (c < re) {
-          float cx[D];
-#pragma unroll
-          for (int d = 0; d < D; ++d) cx[d] = p.s_x[(int64_t)d * p.W + c];
-          in = is_nbr<D, PRED>(qx, cx, p.R2f, p.R, p.R2);
-        }
-        total += __popc(__ballot_sync(0xffffffffu, in));
-        if (total > p.K) return true;
+      for (int d = 0; d < D; ++d) jb.s_x[(int64_t)d * jb.Wp + pos] = x[d];
+      cnt = jb.bin_start[bin + 1] - bs0;
+      if (jb.filter) safe = cnt > (uint32_t)jb.K && jb.kmin[bin] == jb.kmax[bin];
+      if (safe) jb.prev[src] = 255;
+    }
+    const bool need = valid && !safe;
+    bool sweep = false;
+    float f[MLP_IN] = {0.0f, 0.0f, 0.0f};
+    if constexpr (ROUTE) {
+      if (__any_sync(0xffffffffu, need) && need) {
+        // Router features and prediction (one lane per point).
+        int64_t k[3];
+        unpack_key(key, H, k);
+        uint32_t stencil = 0;
+        for_each_run<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
+          stencil += re - rs;
+          return false;
+        });
+        f[0] = log2f(1.0f + (float)cnt) * 0.125f;
+        f[1] = log2f(1.0f + (float)stencil) * 0.125f;
+        f[2] = prev_feature(jb.prev[src], jb.K);
+        float z[MLP_B];
+        mlp_forward(b.router->params, f, z);
+        sweep = stencil <= b.router->max_sweep && p_inlier(z) < b.router->threshold;
       }
-      return false;
-    });
+    }
+    const unsigned need_e = __ballot_sync(0xffffffffu, need && !sweep);
+    if (need_e) {
+      uint32_t qb = 0;
+      const int ql = __ffs(need_e) - 1;
+      if (lane == ql) qb = (uint32_t)atomicAdd(&jb.ctr->n_undet, __popc(need_e));
+      qb = __shfl_sync(0xffffffffu, qb, ql);
+      if (need && !sweep) {
+        const uint32_t q = qb + __popc(need_e & lt);
+        jb.queue[q] = pos;
+        if constexpr (ROUTE) {
+#pragma unroll
+          for (int j = 0; j < MLP_IN; ++j) jb.feat[(int64_t)q * MLP_IN + j] = f[j];
+        }
+      }
+    }
+    if constexpr (ROUTE) {
+      const unsigned need_s = __ballot_sync(0xffffffffu, sweep);
+      if (need_s) {
+        uint32_t qb = 0;
+        const int ql = __ffs(need_s) - 1;
+        if (lane == ql) qb = (uint32_t)atomicAdd(&jb.ctr->n_sweep, __popc(need_s));
+        qb = __shfl_sync(0xffffffffu, qb, ql);
+        if (sweep) {
+          const uint32_t q = (uint32_t)jb.W - 1 - (qb + __popc(need_s & lt));
+          jb.queue[q] = pos;
+#pragma unroll
+          for (int j = 0; j < MLP_IN; ++j) jb.feat[(int64_t)q * MLP_IN + j] = f[j];
+        }
+      }
+      if (lane == 0 && (need_e || need_s)) {
+        atomicAdd(&b.router->routed_early, (unsigned long long)__popc(need_e));
+        atomicAdd(&b.router->routed_sweep, (unsigned long long)__popc(need_s));
+      }
+    }
+  }
+}
+
+// Counts the neighbours of query qx among the candidates of one run
+// [rs, re), 128 per step: each lane loads 4 consecutive candidates per
+// dimension with one float4, the warp tallies them with ballot/popc.
+// Returns true once the running total exceeds K.
+template <int D, int PRED>
+__device__ __forceinline__ bool count_run(const Job& jb, const float* qx, uint32_t rs, uint32_t re,
+                                          int& total) {
+  const int lane = threadIdx.x & 31;
+  for (uint32_t b = rs & ~3u; b < re; b += 128) {
+    const uint32_t c0 = b + 4 * lane;
+    bool in[4] = {false, false, false, false};
+    if (c0 < re) {
+      float4 v[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) v[d] = *reinterpret_cast<const float4*>(jb.s_x + (int64_t)d * jb.Wp + c0);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        float cx[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) cx[d] = (&v[d].x)[e];
+        const uint32_t c = c0 + e;
+        in[e] = c >= rs && c < re && is_nbr<D, PRED>(qx, cx, jb.R2f, jb.R, jb.R2);
+      }
+    }
+    total += __popc(__ballot_sync(0xffffffffu, in[0])) + __popc(__ballot_sync(0xffffffffu, in[1])) +
+             __popc(__ballot_sync(0xffffffffu, in[2])) + __popc(__ballot_sync(0xffffffffu, in[3]));
+    if (total > jb.K) return true;
+  }
+  return false;
+}
+
+// Exact count of one queued point by the whole warp: `total` receives the
+// count (capped just above K); returns true if it exceeded K.
+template <int D, int PRED>
+__device__ __forceinline__ bool count_query(const Job& jb, uint32_t pos, int& total) {
+  constexpr int H = Hashed<D>::value;
+  float qx[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) qx[d] = jb.s_x[(int64_t)d * jb.Wp + pos];
+  int64_t k[3];
+  unpack_key(jb.s_ckey[pos], H, k);
+  total = 0;
+  return for_each_run<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
+    return count_run<D, PRED>(jb, qx, rs, re, total);
+  });
+}
+
+// Stencil runs, nearest first: the point's own cell, then its neighbours
+// along the last hashed dimension outward (one bin each), then the other
+// rows of the stencil. Covers exactly the same candidates as for_each_run.
+template <int h, typename F>
+__device__ __forceinline__ bool for_each_run_near(const uint32_t* bin_start, const int64_t* k, int n, F&& f) {
+  const int span = 2 * n + 1;
+  // centre row, one cell at a time: offsets 0, -1, +1, -2, +2, ...
+  for (int t = 0; t < span; ++t) {
+    const int o = (t == 0) ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
+    int64_t c[3] = {k[0], h > 1 ? k[1] : 0, h > 2 ? k[2] : 0};
+    c[h - 1] += o;
+    const uint32_t b0 = bin_of(c, h);
+    if (f(bin_start[b0], bin_start[b0 + 1])) return true;
+  }
+  if (h == 1) return false;
+  const int rows = (h == 2) ? span : span * span;
+  const int centre = (h == 2) ? n : n * span + n;
+  for (int r = 0; r < rows; ++r) {
+    if (r == centre) continue;
+    int64_t c[3];
+    if (h == 2) {
+      c[0] = k[0] + r - n;
+      c[1] = k[1] - n;
+    } else {
+      c[0] = k[0] + r / span - n;
+      c[1] = k[1] + r % span - n;
+      c[2] = k[2] - n;
+    }
+    const uint32_t b0 = bin_of(c, h);
+    const uint32_t b1 = (b0 + 2 * n) & NB_MASK;
+    if (b0 <= b1) {
+      if (f(bin_start[b0], bin_start[b1 + 1])) return true;
+    } else {
+      if (f(bin_start[b0], bin_start[NB])) return true;
+      if (f(bin_start[0], bin_start[b1 + 1])) return true;
+    }
+  }
+  return false;
+}
+
+// Exact count of one queued point by the whole warp, nearest cells first.
+template <int D, int PRED>
+__device__ __forceinline__ bool count_query_near(const Job& jb, uint32_t pos, int& total) {
+  constexpr int H = Hashed<D>::value;
+  float qx[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) qx[d] = jb.s_x[(int64_t)d * jb.Wp + pos];
+  int64_t k[3];
+  unpack_key(jb.s_ckey[pos], H, k);
+  total = 0;
+  return for_each_run_near<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
+    return count_run<D, PRED>(jb, qx, rs, re, total);
+  });
+}
+
+// Exact count of one queued point by one lane (full-sweep queue).
+template <int D, int PRED>
+__device__ __forceinline__ bool count_query_lane(const Job& jb, uint32_t pos, int& total) {
+  constexpr int H = Hashed<D>::value;
+  float qx[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) qx[d] = jb.s_x[(int64_t)d * jb.Wp + pos];
+  int64_t k[3];
+  unpack_key(jb.s_ckey[pos], H, k);
+  total = 0;
+  return for_each_run<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
+    for (uint32_t c = rs; c < re; ++c) {
+      float cx[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) cx[d] = jb.s_x[(int64_t)d * jb.Wp + c];
+      total += is_nbr<D, PRED>(qx, cx, jb.R2f, jb.R, jb.R2);
+      if (total > jb.K) return true;
+    }
+    return false;
+  });
+}
+
+// Records the result of one counted point (one thread).
+__device__ __forceinline__ void record_count(const Job& jb, int64_t lo, uint32_t pos, bool inlier, int total) {
+  const uint32_t i = jb.s_off[pos];
+  if (!inlier) {
+    atomicOr(&jb.flags[i >> 5], 1u << (i & 31));
+    atomicAdd(&jb.ctr->n_out, 1);
+  }
+  jb.prev[source_pos(jb, lo, i)] = (uint8_t)(total < 253 ? total : 253);
+}
+
+// Training sample of one routed point (one thread): its features and the
+// bucket of its exact capped count. Also counts misroutes.
+__device__ __forceinline__ void record_sample(const Job& jb, RouterState* rs, int64_t q, int total,
+                                              bool routed_early) {
+  const int lab = count_bucket(total, jb.K);
+  if ((lab == 3) != routed_early) atomicAdd(&rs->misrouted, 1ull);
+  if (*(volatile uint32_t*)&rs->n_samples >= TRAIN_CAP) return;
+  const uint32_t s = atomicAdd(&rs->n_samples, 1u);
+  if (s >= TRAIN_CAP) return;
+#pragma unroll
+  for (int j = 0; j < MLP_IN; ++j) rs->samples[s][j] = jb.feat[q * MLP_IN + j];
+  rs->samples[s][3] = (float)lab;
+}
+
+// Per-job cleanup done by k_count: per-bin key ranges and compaction
+// look-back words.
+__device__ __forceinline__ void reset_bins(const Job& jb) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < NB; t += stride) {
+    jb.kmin[t] = EMPTY_KEY;
+    jb.kmax[t] = 0;
+  }
+  const int64_t tiles = (jb.W + CMP_TILE - 1) / CMP_TILE;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += stride)
+    jb.cmp_status[t] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// k_count: the exact count always decides: outlier iff count <= K.
+//   plain (ROUTE = false): one warp per queued point, warps striding over
+//     the queue, stencil rows in order.
+//   routed: early-exit queue as above but nearest cells first; full-sweep
+//     queue one lane per point, 32 points per warp; every counted point
+//     becomes a training sample of the router.
+// ---------------------------------------------------------------------------
+template <int D, int PRED, bool ROUTE>
+__global__ void __launch_bounds__(256) k_count(Batch b) {
+  pdl_trigger();
+  pdl_wait();
+  const Job& jb = b.jobs[blockIdx.y];
+  reset_bins(jb);
+  const int lane = threadIdx.x & 31;
+  const int64_t lo = jb.ctr->lo;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t nq = jb.ctr->n_undet;
+  for (int64_t q = warp; q < nq; q += nwarps) {
+    const uint32_t pos = jb.queue[q];
+    int total;
+    const bool inlier = ROUTE ? count_query_near<D, PRED>(jb, pos, total) : count_query<D, PRED>(jb, pos, total);
     if (lane == 0) {
-      if (!done) p.flags[qslot] = 1;
-      p.prev[qslot] = (uint8_t)(total < 253 ? total : 253);
+      record_count(jb, lo, pos, inlier, total);
+      if constexpr (ROUTE) record_sample(jb, b.router, q, total, true);
+    }
+  }
+  if constexpr (ROUTE) {
+    const int64_t ns = jb.ctr->n_sweep;
+    for (int64_t c0 = warp * 32; c0 < ns; c0 += nwarps * 32) {
+      const int64_t idx = c0 + lane;
+      if (idx < ns) {
+        const int64_t q = jb.W - 1 - idx;
+        const uint32_t pos = jb.queue[q];
+        int total;
+        const bool inlier = count_query_lane<D, PRED>(jb, pos, total);
+        record_count(jb, lo, pos, inlier, total);
+        record_sample(jb, b.router, q, total, false);
+      }
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// k_compact: outlier flags in ring order -> sorted global indices, appended to
-// out_ids; per-slide counters; window advance. One block of 1024 threads.
+// k_compact: outlier bits in window order -> sorted global indices, appended
+// to the batch output after the outliers of the earlier jobs. Grid
+// (max tiles per job, jobs); a tile covers CMP_TILE window offsets, one
+// 32-bit word per thread, tiles chained by decoupled look-back. The last
+// tile of the batch records per-slide counts, advances every job's window
+// and resets the per-job counters.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_compact(KParams p) {
-  __shared__ uint32_t wsum[32];
-  __shared__ int64_t s_base;
-  __shared__ int s_fail;
-  DevState* st = p.state;
-  const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
-  const int64_t lo = st->n_ingested + p.S - p.W;  // first index of the detected window
-  const int64_t slot0 = lo % p.W;
-  const int64_t per = (p.W + 1023) / 1024;
-  const int64_t i0 = min((int64_t)t * per, p.W), i1 = min(i0 + per, p.W);
-  uint32_t cnt = 0;
-  for (int64_t i = i0; i < i1; ++i) {
-    int64_t s = slot0 + i;
-    if (s >= p.W) s -= p.W;
-    cnt += p.flags[s];
-  }
-  uint32_t inc = cnt;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += y;
-  }
-  if (lane == 31) wsum[wid] = inc;
-  __syncthreads();
+__global__ void __launch_bounds__(256) k_compact(Batch b) {
+  __shared__ uint32_t sm[33];
+  __shared__ uint32_t s_tile, s_prefix, s_last;
+  __shared__ int64_t s_jobbase;
+  __shared__ int64_t s_red[2][8];
+  pdl_trigger();
+  pdl_wait();
+  const Job& jb = b.jobs[blockIdx.y];
+  const int64_t ntiles = (jb.W + CMP_TILE - 1) / CMP_TILE;
+  if (blockIdx.x >= ntiles) return;  // smaller job in a mixed batch
+  BatchState* bs = b.bs;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   if (wid == 0) {
-    uint32_t v = wsum[lane], vi = v;
+    // Output base of this job: IDs of all earlier jobs of the batch come first.
+    int64_t part = 0;
+    for (int j = lane; j < (int)blockIdx.y; j += 32) part += b.jobs[j].ctr->n_out;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(0xffffffffu, vi, o);
-      if (lane >= o) vi += y;
-    }
-    wsum[lane] = vi - v;
-    if (lane == 31) {
-      const int64_t total = vi;
-      const int64_t base = st->out_total;
-      s_base = base;
-      s_fail = (base + total > p.out_cap);
-      if (s_fail) set_err(st, DERR_CAPACITY);
-      st->n_out = (int32_t)total;
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if (lane == 0) {
+      s_jobbase = bs->out_total + part;
+      s_tile = atomicAdd(&jb.ctr->cmp_ticket, 1u);
     }
   }
   __syncthreads();
-  if (!s_fail) {
-    int64_t o = s_base + wsum[wid] + inc - cnt;
-    for (int64_t i = i0; i < i1; ++i) {
-      int64_t s = slot0 + i;
-      if (s >= p.W) s -= p.W;
-      if (p.flags[s]) p.out_ids[o++] = lo + i;
-    }
+  const uint32_t tile = s_tile;
+  const int64_t lo = jb.ctr->lo;
+  const int64_t wi = ((int64_t)tile * CMP_TILE >> 5) + threadIdx.x;  // bitset word
+  const int64_t nwords = (jb.W + 31) >> 5;
+  uint32_t bits = 0;
+  if (wi < nwords) {
+    bits = jb.flags[wi];
+    if (bits) jb.flags[wi] = 0;
+  }
+  uint32_t total;
+  const uint32_t ex = block_exclusive_scan(__popc(bits), &total, sm);
+  if (wid == 0) {
+    const uint32_t pre = warp_lookback(jb.cmp_status, tile, total, bs);
+    if (lane == 0) s_prefix = pre;
   }
   __syncthreads();
-  if (t == 0) {
-    const int64_t j = st->slide;
-    const int32_t nout = st->n_out;
-    if (p.slide_nout && j < p.slide_rec_cap) {
-      p.slide_nout[j] = nout;
-      p.slide_undet[j] = st->n_undet;
+  int64_t o = s_jobbase + s_prefix + ex;
+  while (bits) {
+    const int e = __ffs(bits) - 1;
+    bits &= bits - 1;
+    if (o < b.out_cap) b.out_ids[o] = lo + wi * 32 + e;
+    else set_err(bs, DERR_CAPACITY);
+    ++o;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&bs->done, 1u) == (uint32_t)(b.cmp_tiles - 1));
+  __syncthreads();
+  if (!s_last) return;
+  // Last tile of the batch: per-slide records, window advance, counter reset
+  // (one job per thread) and the batch totals.
+  __threadfence();
+  int64_t add = 0, und = 0;
+  for (int j = threadIdx.x; j < b.njobs; j += blockDim.x) {
+    const Job& J = b.jobs[j];
+    JobCtr* c = J.ctr;
+    const int32_t nout = *(volatile int32_t*)&c->n_out;
+    const int32_t nund = *(volatile int32_t*)&c->n_undet + *(volatile int32_t*)&c->n_sweep;
+    const int64_t slide = (c->lo - J.S) / J.S;
+    if (J.rec_nout && slide >= 0 && slide < J.rec_cap) {
+      J.rec_nout[slide] = nout;
+      J.rec_undet[slide] = nund;
     }
-    if (!s_fail) st->out_total += nout;
-    st->undet_total += st->n_undet;
-    st->slide = j + 1;
-    st->n_ingested += p.S;
+    add += nout;
+    und += nund;
+    c->lo += c->lo_step;
+    c->n_out = 0;
+    c->n_undet = 0;
+    c->n_sweep = 0;
+    c->cmp_ticket = 0;
+  }
+#pragma unroll
+  for (int o2 = 16; o2 > 0; o2 >>= 1) {
+    add += __shfl_xor_sync(0xffffffffu, add, o2);
+    und += __shfl_xor_sync(0xffffffffu, und, o2);
+  }
+  if (lane == 0) {
+    s_red[0][wid] = add;
+    s_red[1][wid] = und;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t ta = 0, tu = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      ta += s_red[0][w];
+      tu += s_red[1][w];
+    }
+    bs->out_total += ta;
+    bs->undet_total += tu;
+    bs->slides += b.njobs;
+    bs->done = 0;
   }
 }
 

@@ -1,9 +1,10 @@
 // Host engine and C ABI of the detector (include/rtod.h).
 //
-// One rtod_handle = one stream. It owns a CUDA stream, the device ring and
-// the cell-ordered SoA, and (optionally) a captured CUDA graph of one slide.
-// The slide pipeline reads all per-slide positions from a DevState block in
-// device memory, so the same graph is replayed for every slide.
+// One rtod_handle = one stream. It owns a CUDA stream, a pool of per-window
+// scratch buffers (one per job of a batch), the ring used by push/detect,
+// the resident copy of a stream used by rtod_run, and captured CUDA graphs
+// of a batch. All per-window positions live on the device (JobCtr), so a
+// captured batch is replayed unchanged.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -13,6 +14,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/rtod.h"
@@ -36,16 +38,16 @@ int fail(int code, const char* fmt, ...) {
   return code;
 }
 
-#define CU(call)                                                                       \
-  do {                                                                                 \
-    cudaError_t e_ = (call);                                                           \
-    if (e_ != cudaSuccess)                                                             \
+#define CU(call)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (call);                                                             \
+    if (e_ != cudaSuccess)                                                               \
       return fail(RTOD_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
-                  __FILE__, __LINE__);                                                 \
+                  __FILE__, __LINE__);                                                   \
   } while (0)
 
-#define DISPATCH_D(D_, ...)                      \
-  switch (D_) {                                  \
+#define DISPATCH_D(D_, ...)                              \
+  switch (D_) {                                          \
     case 1: { constexpr int D = 1; __VA_ARGS__; } break; \
     case 2: { constexpr int D = 2; __VA_ARGS__; } break; \
     case 3: { constexpr int D = 3; __VA_ARGS__; } break; \
@@ -54,14 +56,14 @@ int fail(int code, const char* fmt, ...) {
     case 6: { constexpr int D = 6; __VA_ARGS__; } break; \
     case 7: { constexpr int D = 7; __VA_ARGS__; } break; \
     case 8: { constexpr int D = 8; __VA_ARGS__; } break; \
-    default: break;                              \
+    default: break;                                      \
   }
 
-#define DISPATCH_DP(D_, P_, ...)                                        \
-  if ((P_) == 0) {                                                      \
-    DISPATCH_D(D_, { constexpr int PRED = 0; __VA_ARGS__; });           \
-  } else {                                                              \
-    DISPATCH_D(D_, { constexpr int PRED = 1; __VA_ARGS__; });           \
+#define DISPATCH_DP(D_, P_, ...)                              \
+  if ((P_) == 0) {                                            \
+    DISPATCH_D(D_, { constexpr int PRED = 0; __VA_ARGS__; }); \
+  } else {                                                    \
+    DISPATCH_D(D_, { constexpr int PRED = 1; __VA_ARGS__; }); \
   }
 
 bool is_device_ptr(const void* p) {
@@ -74,61 +76,162 @@ bool is_device_ptr(const void* p) {
 }
 
 template <typename T>
-int dalloc(T** p, size_t count) {
+int dalloc(T** p, size_t count, int64_t* counter) {
   *p = nullptr;
   if (count == 0) count = 1;
   CU(cudaMalloc((void**)p, count * sizeof(T)));
+  *counter += (int64_t)(count * sizeof(T));
   return RTOD_OK;
 }
+
+template <typename T>
+void dfree(T*& p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// Launches a kernel with programmatic dependent launch allowed, so that its
+// blocks can be scheduled while the previous kernel in the stream finishes;
+// every kernel waits (griddepcontrol.wait) before reading its inputs.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, int block, cudaStream_t st, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+// Scratch of one job (one window in flight).
+struct Scratch {
+  uint32_t* bin_count = nullptr;
+  uint32_t* bin_start = nullptr;
+  unsigned long long* kmin = nullptr;
+  unsigned long long* kmax = nullptr;
+  uint32_t* s_off = nullptr;
+  uint64_t* s_ckey = nullptr;
+  float* s_x = nullptr;
+  uint32_t* queue = nullptr;
+  float* feat = nullptr;
+  uint32_t* flags = nullptr;
+  unsigned long long* scan_status = nullptr;
+  unsigned long long* cmp_status = nullptr;
+};
+
+constexpr int kPipeKernels = 7;
+const char* kKernelNames[kPipeKernels] = {"k_keys",  "k_hist",    "k_scan", "k_scatter",
+                                          "k_count", "k_compact", "k_train"};
+
+// Initial router parameters: uniform(-a, a) with a = sqrt(6 / (fan_in + fan_out))
+// (Glorot & Bengio 2010) from a fixed-seed xorshift generator, zero biases
+// except a prior towards bucket 3 (most counted points are inliers).
+void init_router(RouterState* r) {
+  std::memset(r, 0, sizeof(RouterState));
+  uint64_t st = 0x9e3779b97f4a7c15ull;
+  auto uni = [&](float a) {
+    st ^= st << 13;
+    st ^= st >> 7;
+    st ^= st << 17;
+    return (float)((double)(st >> 11) / 9007199254740992.0 * 2.0 - 1.0) * a;
+  };
+  const float a1 = std::sqrt(6.0f / (MLP_IN + MLP_H)), a2 = std::sqrt(6.0f / (MLP_H + MLP_H)),
+              a3 = std::sqrt(6.0f / (MLP_H + MLP_B));
+  for (int i = 0; i < MLP_H * MLP_IN; ++i) r->params[OFF_W1 + i] = uni(a1);
+  for (int i = 0; i < MLP_H * MLP_H; ++i) r->params[OFF_W2 + i] = uni(a2);
+  for (int i = 0; i < MLP_B * MLP_H; ++i) r->params[OFF_W3 + i] = uni(a3);
+  r->params[OFF_B3 + 3] = 2.0f;
+  r->b1t = r->b2t = 1.0f;
+  r->lr = 1e-3f;
+  r->beta1 = 0.9f;
+  r->beta2 = 0.999f;
+  r->eps = 1e-8f;
+  r->threshold = 0.5f;
+  r->max_sweep = 64;
+  r->min_samples = 256;
+}
+
+enum Mode { MODE_NONE = 0, MODE_RING = 1, MODE_RUN = 2 };
+
+struct EventSet {
+  std::vector<cudaEvent_t> ev;
+  cudaEvent_t make() {
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    ev.push_back(e);
+    return e;
+  }
+  ~EventSet() {
+    for (auto e : ev) cudaEventDestroy(e);
+  }
+};
 
 }  // namespace
 
 struct rtod_handle {
-  rtod_config cfg;
+  rtod_config cfg{};
   int device = 0;
   int sm_count = 148;
   cudaStream_t stream = nullptr;
-  KParams kp{};
-  int32_t block_warps = 8;
+  int64_t W = 0, S = 0, Wp = 0;
+  int D = 1;
+  int n = 2;
+  int filter = 1;
+  double cell = 0;
+  float R2f = 0;
+  int block_warps = 8;
+  int batch_max = 32;
+  int64_t device_bytes = 0;
 
-  // device buffers owned by the handle
-  float* ring = nullptr;
-  uint64_t* ckey = nullptr;
-  uint32_t* bin_count = nullptr;
-  uint32_t* bin_start = nullptr;
-  uint32_t* cursor = nullptr;
-  uint64_t* owner = nullptr;
-  uint8_t* mixed = nullptr;
-  uint32_t* s_slot = nullptr;
-  uint64_t* s_ckey = nullptr;
-  float* s_x = nullptr;
-  uint8_t* flags = nullptr;
-  uint8_t* prev = nullptr;
-  DevState* state = nullptr;
-  float* staging = nullptr;   // W * D floats
-  int64_t* ids = nullptr;     // result buffer
+  std::vector<Scratch> pool;  // allocated lazily up to batch_max
+  JobCtr* ctr = nullptr;      // [batch_max]
+  JobCtr* ctr_init = nullptr; // pinned host [batch_max]
+  Job* jobs_dev = nullptr;    // [batch_max]
+  std::vector<Job> tab_host;  // last uploaded job table
+  BatchState* bs = nullptr;
+  RouterState* router = nullptr;
+
+  float* ring = nullptr;  // SoA [D][W]
+  uint64_t* ring_keys = nullptr;
+  uint8_t* ring_prev = nullptr;
+  float* staging = nullptr;  // W * D floats
+
+  float* run_buf = nullptr;
+  int64_t run_buf_cap = 0;  // floats
+  uint64_t* run_keys = nullptr;
+  uint8_t* run_prev = nullptr;
+  int64_t run_key_cap = 0;
+  int32_t* rec_nout = nullptr;
+  int32_t* rec_undet = nullptr;
+  int64_t rec_cap = 0;
+  int64_t* ids = nullptr;
   int64_t ids_cap = 0;
-  int32_t* slide_nout = nullptr;
-  int32_t* slide_undet = nullptr;
-  int64_t slide_rec_cap = 0;
-  float* run_buf = nullptr;   // resident copy of a host stream (rtod_run)
-  int64_t run_buf_cap = 0;    // floats
 
-  // host mirror of the stream position
+  int mode = MODE_NONE;
   int64_t n_pushed = 0;
   int64_t slides_done = 0;
   bool pending = false;
   bool poisoned = false;
 
-  // slide graph (captured for a given src pointer and output buffers)
   cudaGraphExec_t graph = nullptr;
-  KParams graph_kp{};  // kernel parameters baked into the graph
+  Batch graph_batch{};
+  int graph_ring = -1;
 
   cudaEvent_t ev[8] = {};
-  int64_t launches = 0;       // kernels issued (graph replays count their kernels)
+  int64_t launches = 0;
   int64_t graph_replays = 0;
   int64_t undet_total = 0;
-  cudaEvent_t* kev = nullptr; // per-kernel events of a profiled run (7 per slide)
 };
 
 namespace {
@@ -136,13 +239,12 @@ namespace {
 int check_config(const rtod_config* c) {
   if (!c) return fail(RTOD_ERR_ARG, "config is null");
   if (c->window < 1 || c->slide < 1 || c->slide > c->window)
-    return fail(RTOD_ERR_CONFIG, "need 1 <= slide <= window (got W=%lld S=%lld)",
-                (long long)c->window, (long long)c->slide);
+    return fail(RTOD_ERR_CONFIG, "need 1 <= slide <= window (got W=%lld S=%lld)", (long long)c->window,
+                (long long)c->slide);
   if (c->window % c->slide != 0)
     return fail(RTOD_ERR_CONFIG, "window %% slide must be 0 (W=%lld S=%lld)", (long long)c->window,
                 (long long)c->slide);
-  if (c->window > (1ll << 31) - 64)
-    return fail(RTOD_ERR_CONFIG, "window too large (max 2^31-64 points)");
+  if (c->window > (1ll << 31) - 64) return fail(RTOD_ERR_CONFIG, "window too large (max 2^31-64 points)");
   if (!(c->R >= 1e-18) || !(c->R <= 1e18) || !std::isfinite(c->R))
     return fail(RTOD_ERR_CONFIG, "R must be finite and in [1e-18, 1e18] (got %g)", c->R);
   if (c->K < 0) return fail(RTOD_ERR_CONFIG, "K must be >= 0");
@@ -154,162 +256,385 @@ int check_config(const rtod_config* c) {
   if (c->block_warps != 0 && c->block_warps != 1 && c->block_warps != 2 && c->block_warps != 4 &&
       c->block_warps != 8)
     return fail(RTOD_ERR_CONFIG, "block_warps must be 0 (auto), 1, 2, 4 or 8");
+  if (c->batch < 0 || c->batch > 256) return fail(RTOD_ERR_CONFIG, "batch must be 0..256");
   return RTOD_OK;
 }
 
-// Derives the grid parameters from the configuration and the cells per R.
 void set_grid(rtod_handle* h, int n) {
-  KParams& k = h->kp;
-  k.n = n;
-  k.cell = h->cfg.R * (1.0 + std::ldexp(1.0, -12)) / (double)n;
+  h->n = n;
+  h->cell = h->cfg.R * (1.0 + std::ldexp(1.0, -12)) / (double)n;
   // A cell is provably all-inlier when it holds more than K points only if
   // its diagonal is below R: needs every dimension hashed and n >= 2.
-  k.filter = (h->cfg.opt >= 1 && h->cfg.dim <= 3 && n >= 2) ? 1 : 0;
-}
-
-int launch_ingest(rtod_handle* h, int64_t n_new) {
-  int64_t work = std::max<int64_t>(std::max<int64_t>(NB, h->kp.W), n_new);
-  int blocks = (int)std::min<int64_t>((work + 255) / 256, (int64_t)h->sm_count * 8);
-  DISPATCH_D(h->kp.D, (k_ingest<D><<<blocks, 256, 0, h->stream>>>(h->kp, n_new)));
-  CU(cudaGetLastError());
-  h->launches++;
-  return RTOD_OK;
-}
-
-constexpr int kSlideKernels = 6;
-const char* kKernelNames[kSlideKernels] = {"k_ingest", "k_hist", "k_scan", "k_scatter", "k_count",
-                                           "k_compact"};
-
-// Stages of one slide. ev (may be null) receives 3 timestamps: ev[1] after
-// ingest+hist, ev[2] after scan+scatter, ev[3] after count+compact. kev (may
-// be null) receives one timestamp after each of the six kernels.
-int launch_slide(rtod_handle* h, cudaEvent_t* ev, cudaEvent_t* kev = nullptr) {
-  const KParams& kp = h->kp;
-  cudaStream_t st = h->stream;
-  int r = launch_ingest(h, kp.S);
-  if (r) return r;
-  if (kev) CU(cudaEventRecord(kev[0], st));
-  int wblocks = (int)std::min<int64_t>((kp.W + 255) / 256, (int64_t)h->sm_count * 16);
-  DISPATCH_D(kp.D, (k_hist<Hashed<D>::value><<<wblocks, 256, 0, st>>>(kp)));
-  if (kev) CU(cudaEventRecord(kev[1], st));
-  if (ev) CU(cudaEventRecord(ev[1], st));
-  k_scan<<<1, 1024, 0, st>>>(kp);
-  if (kev) CU(cudaEventRecord(kev[2], st));
-  DISPATCH_D(kp.D, (k_scatter<D><<<wblocks, 256, 0, st>>>(kp)));
-  if (kev) CU(cudaEventRecord(kev[3], st));
-  if (ev) CU(cudaEventRecord(ev[2], st));
-  int64_t warps = (kp.W + 31) / 32;
-  int wpb = h->block_warps;
-  int cblocks = (int)((warps + wpb - 1) / wpb);
-  DISPATCH_DP(kp.D, h->cfg.pred, (k_count<D, PRED><<<cblocks, wpb * 32, 0, st>>>(kp)));
-  if (kev) CU(cudaEventRecord(kev[4], st));
-  k_compact<<<1, 1024, 0, st>>>(kp);
-  CU(cudaGetLastError());
-  if (kev) CU(cudaEventRecord(kev[5], st));
-  if (ev) CU(cudaEventRecord(ev[3], st));
-  h->launches += kSlideKernels - 1;
-  return RTOD_OK;
+  h->filter = (h->cfg.opt >= 1 && h->cfg.dim <= 3 && n >= 2) ? 1 : 0;
 }
 
 void drop_graph(rtod_handle* h) {
   if (h->graph) cudaGraphExecDestroy(h->graph);
   h->graph = nullptr;
+  h->graph_ring = -1;
 }
 
-int ensure_graph(rtod_handle* h) {
-  if (h->graph && std::memcmp(&h->graph_kp, &h->kp, sizeof(KParams)) == 0) return RTOD_OK;
-  drop_graph(h);
-  cudaGraph_t g;
-  CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  const int64_t before = h->launches;
-  int r = launch_slide(h, nullptr);
-  h->launches = before;
-  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
-  if (r) return r;
-  if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-  e = cudaGraphInstantiate(&h->graph, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
-  h->graph_kp = h->kp;
+int ensure_pool(rtod_handle* h, int jobs) {
+  const int64_t W = h->W, Wp = h->Wp, D = h->D;
+  const int64_t cmp_tiles = (W + CMP_TILE - 1) / CMP_TILE;
+  while ((int)h->pool.size() < jobs) {
+    Scratch s;
+    int64_t* c = &h->device_bytes;
+    bool ok = !dalloc(&s.bin_count, NB, c) && !dalloc(&s.bin_start, NB + 1, c) && !dalloc(&s.kmin, NB, c) &&
+              !dalloc(&s.kmax, NB, c) && !dalloc(&s.s_off, (size_t)W, c) && !dalloc(&s.s_ckey, (size_t)W, c) &&
+              !dalloc(&s.s_x, (size_t)(Wp * D), c) && !dalloc(&s.queue, (size_t)W, c) &&
+              !dalloc(&s.feat, (size_t)(h->cfg.router ? W * MLP_IN : 1), c) &&
+              !dalloc(&s.flags, (size_t)((W + 31) / 32), c) && !dalloc(&s.scan_status, SCAN_TILES, c) &&
+              !dalloc(&s.cmp_status, (size_t)cmp_tiles, c);
+    h->pool.push_back(s);
+    if (!ok) return RTOD_ERR_CUDA;
+    CU(cudaMemset(s.bin_count, 0, NB * sizeof(uint32_t)));
+    CU(cudaMemset(s.kmin, 0xff, NB * sizeof(unsigned long long)));
+    CU(cudaMemset(s.kmax, 0, NB * sizeof(unsigned long long)));
+    CU(cudaMemset(s.s_x, 0, (size_t)(Wp * D) * sizeof(float)));
+    CU(cudaMemset(s.flags, 0, (size_t)((W + 31) / 32) * sizeof(uint32_t)));
+    CU(cudaMemset(s.scan_status, 0, SCAN_TILES * sizeof(unsigned long long)));
+    CU(cudaMemset(s.cmp_status, 0, (size_t)cmp_tiles * sizeof(unsigned long long)));
+  }
   return RTOD_OK;
 }
 
-int run_slide(rtod_handle* h, cudaEvent_t* ev) {
-  if (h->cfg.use_graph && !ev) {
-    int r = ensure_graph(h);
-    if (r) return r;
-    CU(cudaGraphLaunch(h->graph, h->stream));
-    h->launches += kSlideKernels;
-    h->graph_replays++;
-    return RTOD_OK;
+// Clears all scratch and counters (after an error may have left a batch
+// unfinished, and on reset).
+int scrub(rtod_handle* h) {
+  const int64_t W = h->W;
+  const int64_t cmp_tiles = (W + CMP_TILE - 1) / CMP_TILE;
+  for (Scratch& s : h->pool) {
+    CU(cudaMemsetAsync(s.bin_count, 0, NB * sizeof(uint32_t), h->stream));
+    CU(cudaMemsetAsync(s.kmin, 0xff, NB * sizeof(unsigned long long), h->stream));
+    CU(cudaMemsetAsync(s.kmax, 0, NB * sizeof(unsigned long long), h->stream));
+    CU(cudaMemsetAsync(s.flags, 0, (size_t)((W + 31) / 32) * sizeof(uint32_t), h->stream));
+    CU(cudaMemsetAsync(s.scan_status, 0, SCAN_TILES * sizeof(unsigned long long), h->stream));
+    CU(cudaMemsetAsync(s.cmp_status, 0, (size_t)cmp_tiles * sizeof(unsigned long long), h->stream));
   }
-  return launch_slide(h, ev);
+  CU(cudaMemsetAsync(h->ctr, 0, sizeof(JobCtr) * h->batch_max, h->stream));
+  CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
+  return RTOD_OK;
 }
 
-int check_device_error(rtod_handle* h, const DevState& s) {
+Job make_job(rtod_handle* h, int j, bool ring, const float* stream_pts) {
+  Job jb{};
+  jb.W = h->W;
+  jb.S = h->S;
+  jb.Wp = h->Wp;
+  jb.cell = h->cell;
+  jb.R = h->cfg.R;
+  jb.R2 = h->cfg.R * h->cfg.R;
+  jb.R2f = h->R2f;
+  jb.K = h->cfg.K;
+  jb.n = h->n;
+  jb.filter = h->filter;
+  jb.ring = ring ? 1 : 0;
+  jb.pts = ring ? h->ring : stream_pts;
+  jb.keys = ring ? h->ring_keys : h->run_keys;
+  jb.stage = h->staging;
+  jb.prev = ring ? h->ring_prev : h->run_prev;
+  const Scratch& s = h->pool[j];
+  jb.bin_count = s.bin_count;
+  jb.bin_start = s.bin_start;
+  jb.kmin = s.kmin;
+  jb.kmax = s.kmax;
+  jb.s_off = s.s_off;
+  jb.s_ckey = s.s_ckey;
+  jb.s_x = s.s_x;
+  jb.queue = s.queue;
+  jb.feat = s.feat;
+  jb.flags = s.flags;
+  jb.scan_status = s.scan_status;
+  jb.cmp_status = s.cmp_status;
+  jb.ctr = h->ctr + j;
+  jb.rec_nout = ring ? nullptr : h->rec_nout;
+  jb.rec_undet = ring ? nullptr : h->rec_undet;
+  jb.rec_cap = ring ? 0 : h->rec_cap;
+  return jb;
+}
+
+// Uploads the job table for a mode (only when it changed, so that captured
+// graphs stay valid) and initialises the job counters: job j starts at
+// window lo = first_lo + j*S and advances by jobs*S per batch.
+int configure(rtod_handle* h, int mode, int jobs, int64_t first_lo, const float* stream_pts) {
+  int r = ensure_pool(h, jobs);
+  if (r) return r;
+  std::vector<Job> tab((size_t)jobs);
+  for (int j = 0; j < jobs; ++j) tab[j] = make_job(h, j, mode == MODE_RING, stream_pts);
+  if (tab.size() != h->tab_host.size() ||
+      std::memcmp(tab.data(), h->tab_host.data(), sizeof(Job) * tab.size()) != 0) {
+    CU(cudaMemcpy(h->jobs_dev, tab.data(), sizeof(Job) * jobs, cudaMemcpyHostToDevice));
+    h->tab_host = tab;
+    drop_graph(h);
+  }
+  for (int j = 0; j < jobs; ++j) {
+    h->ctr_init[j] = JobCtr{};
+    h->ctr_init[j].lo = first_lo + (int64_t)j * h->S;
+    h->ctr_init[j].lo_step = (int64_t)jobs * h->S;
+  }
+  // Pinned source; every public call ends with a stream sync, so the buffer
+  // is never rewritten while a copy from it is pending.
+  CU(cudaMemcpyAsync(h->ctr, h->ctr_init, sizeof(JobCtr) * jobs, cudaMemcpyHostToDevice, h->stream));
+  h->mode = mode;
+  return RTOD_OK;
+}
+
+Batch make_batch(rtod_handle* h, int njobs, int64_t out_cap) {
+  Batch b{};
+  b.jobs = h->jobs_dev;
+  b.njobs = njobs;
+  b.bs = h->bs;
+  b.router = h->router;
+  b.out_ids = h->ids;
+  b.out_cap = out_cap;
+  b.cmp_tiles = (int64_t)njobs * ((h->W + CMP_TILE - 1) / CMP_TILE);
+  return b;
+}
+
+// Launches one batch: [ingest] hist scan scatter count compact. kev (may be
+// null) receives an event after each kernel (kev[0] after ingest, or at the
+// start when there is none).
+int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev) {
+  cudaStream_t st = h->stream;
+  const int64_t W = h->W, nj = b.njobs;
+  const unsigned gy = (unsigned)nj;
+  if (ingest) {
+    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>((h->S + 255) / 256, h->sm_count * 4));
+    DISPATCH_D(h->D, CU(launch_k(k_ingest<D>, dim3((unsigned)gx, gy), 256, st, b, 0)));
+    h->launches++;
+  }
+  if (kev) CU(cudaEventRecord(kev[0], st));
+  const int64_t wx = std::max<int64_t>(
+      1, std::min<int64_t>((W + 255) / 256, std::max<int64_t>(2, (h->sm_count * 16 + nj - 1) / nj)));
+  DISPATCH_D(h->D, CU(launch_k(k_hist<D>, dim3((unsigned)wx, gy), 256, st, b)));
+  if (kev) CU(cudaEventRecord(kev[1], st));
+  CU(launch_k(k_scan, dim3(SCAN_TILES, gy), 256, st, b));
+  if (kev) CU(cudaEventRecord(kev[2], st));
+  if (h->cfg.router) {
+    DISPATCH_D(h->D, CU(launch_k(k_scatter<D, true>, dim3((unsigned)wx, gy), 256, st, b)));
+  } else {
+    DISPATCH_D(h->D, CU(launch_k(k_scatter<D, false>, dim3((unsigned)wx, gy), 256, st, b)));
+  }
+  if (kev) CU(cudaEventRecord(kev[3], st));
+  const int wpb = h->block_warps;
+  const int64_t cx = std::max<int64_t>(1, (int64_t)h->sm_count * (64 / wpb) / nj);
+  if (h->cfg.router) {
+    DISPATCH_DP(h->D, h->cfg.pred, CU(launch_k(k_count<D, PRED, true>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
+  } else {
+    DISPATCH_DP(h->D, h->cfg.pred, CU(launch_k(k_count<D, PRED, false>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
+  }
+  if (kev) CU(cudaEventRecord(kev[4], st));
+  CU(launch_k(k_compact, dim3((unsigned)((W + CMP_TILE - 1) / CMP_TILE), gy), 256, st, b));
+  if (kev) CU(cudaEventRecord(kev[5], st));
+  h->launches += 5;
+  if (h->cfg.router) {
+    // Online training on the counts of this batch (one block; it returns at
+    // once until enough samples are buffered).
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = TRAIN_SMEM;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CU(cudaLaunchKernelEx(&cfg, k_train, h->router));
+    h->launches += 1;
+  }
+  if (kev) CU(cudaEventRecord(kev[6], st));
+  return RTOD_OK;
+}
+
+// Runs one batch, replaying a captured graph when graphs are on.
+int run_batch(rtod_handle* h, const Batch& b, bool ingest) {
+  if (!h->cfg.use_graph) return launch_batch(h, b, ingest, nullptr);
+  if (!h->graph || h->graph_ring != (int)ingest || std::memcmp(&h->graph_batch, &b, sizeof(Batch)) != 0) {
+    drop_graph(h);
+    cudaGraph_t g;
+    CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = h->launches;
+    int r = launch_batch(h, b, ingest, nullptr);
+    h->launches = before;
+    cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (r) return r;
+    if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    h->graph_batch = b;
+    h->graph_ring = (int)ingest;
+  }
+  CU(cudaGraphLaunch(h->graph, h->stream));
+  h->launches += (ingest ? 6 : 5) + (h->cfg.router ? 1 : 0);
+  h->graph_replays++;
+  return RTOD_OK;
+}
+
+int check_device_error(rtod_handle* h, const BatchState& s) {
   if (s.err == DERR_NONE) return RTOD_OK;
   h->poisoned = true;
   switch (s.err) {
     case DERR_NONFINITE: return fail(RTOD_ERR_INPUT, "non-finite coordinate in the stream");
-    case DERR_RANGE:
-      return fail(RTOD_ERR_INPUT, "coordinate too large for the grid (|x| / cell beyond the limit)");
+    case DERR_RANGE: return fail(RTOD_ERR_INPUT, "coordinate too large for the grid (|x| / cell beyond the limit)");
     case DERR_CAPACITY: return fail(RTOD_ERR_CAPACITY, "outlier ID buffer too small");
+    case DERR_TIMEOUT: return fail(RTOD_ERR_TIMEOUT, "a bounded device-side wait ran out");
     default: return fail(RTOD_ERR_CUDA, "device error %d", s.err);
   }
 }
 
+// Scratch cleans up after every completed batch, so a reset only clears the
+// counters, unless an error may have left a batch half done.
 int reset_state(rtod_handle* h) {
-  CU(cudaMemsetAsync(h->state, 0, sizeof(DevState), h->stream));
+  int r;
+  if (h->poisoned) {
+    r = scrub(h);
+  } else {
+    CU(cudaMemsetAsync(h->ctr, 0, sizeof(JobCtr) * h->batch_max, h->stream));
+    CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
+    r = RTOD_OK;
+  }
+  if (r) return r;
   h->n_pushed = 0;
   h->slides_done = 0;
   h->pending = false;
   h->poisoned = false;
+  h->mode = MODE_NONE;
   return RTOD_OK;
 }
 
 int ensure_ids(rtod_handle* h, int64_t cap) {
   if (cap <= h->ids_cap) return RTOD_OK;
-  if (h->ids) cudaFree(h->ids);
-  h->ids = nullptr;
+  if (h->ids) h->device_bytes -= h->ids_cap * 8;
+  dfree(h->ids);
   h->ids_cap = 0;
-  if (dalloc(&h->ids, (size_t)cap)) return RTOD_ERR_CUDA;
+  if (dalloc(&h->ids, (size_t)cap, &h->device_bytes)) return RTOD_ERR_CUDA;
   h->ids_cap = cap;
-  h->kp.out_ids = h->ids;
   drop_graph(h);
   return RTOD_OK;
 }
 
-int ensure_slide_records(rtod_handle* h, int64_t n) {
-  if (n <= h->slide_rec_cap) return RTOD_OK;
-  if (h->slide_nout) cudaFree(h->slide_nout);
-  if (h->slide_undet) cudaFree(h->slide_undet);
-  h->slide_nout = h->slide_undet = nullptr;
-  h->slide_rec_cap = 0;
-  if (dalloc(&h->slide_nout, (size_t)n) || dalloc(&h->slide_undet, (size_t)n)) return RTOD_ERR_CUDA;
-  h->slide_rec_cap = n;
-  h->kp.slide_nout = h->slide_nout;
-  h->kp.slide_undet = h->slide_undet;
-  h->kp.slide_rec_cap = n;
-  drop_graph(h);
+int ensure_records(rtod_handle* h, int64_t n) {
+  if (n <= h->rec_cap) return RTOD_OK;
+  if (h->rec_nout) h->device_bytes -= h->rec_cap * 8;
+  dfree(h->rec_nout);
+  dfree(h->rec_undet);
+  h->rec_cap = 0;
+  if (dalloc(&h->rec_nout, (size_t)n, &h->device_bytes) || dalloc(&h->rec_undet, (size_t)n, &h->device_bytes))
+    return RTOD_ERR_CUDA;
+  h->rec_cap = n;
+  return RTOD_OK;
+}
+
+// Device copy of a stream of `used` points (a host pointer is copied into the
+// handle's run buffer) plus room for its keys and router features.
+int stage_stream(rtod_handle* h, const float* pts, int64_t used, const float** src) {
+  const int64_t D = h->D;
+  *src = pts;
+  if (!is_device_ptr(pts)) {
+    if (h->run_buf_cap < used * D) {
+      if (h->run_buf) h->device_bytes -= h->run_buf_cap * 4;
+      dfree(h->run_buf);
+      h->run_buf_cap = 0;
+      if (dalloc(&h->run_buf, (size_t)(used * D), &h->device_bytes)) return RTOD_ERR_CUDA;
+      h->run_buf_cap = used * D;
+    }
+    CU(cudaMemcpyAsync(h->run_buf, pts, (size_t)(used * D) * sizeof(float), cudaMemcpyHostToDevice, h->stream));
+    *src = h->run_buf;
+  }
+  if (h->run_key_cap < used) {
+    if (h->run_keys) h->device_bytes -= h->run_key_cap * 9;
+    dfree(h->run_keys);
+    dfree(h->run_prev);
+    h->run_key_cap = 0;
+    if (dalloc(&h->run_keys, (size_t)used, &h->device_bytes) || dalloc(&h->run_prev, (size_t)used, &h->device_bytes))
+      return RTOD_ERR_CUDA;
+    h->run_key_cap = used;
+  }
+  return RTOD_OK;
+}
+
+int pick_batch(const rtod_handle* h, int64_t slides) {
+  const int64_t b = h->cfg.batch ? h->cfg.batch : h->batch_max;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(b, slides));
+}
+
+int64_t count_slides(const rtod_handle* h, int64_t n, int64_t max_slides) {
+  int64_t sl = n >= h->W ? (n - h->W) / h->S : 0;
+  if (max_slides >= 0) sl = std::min(sl, max_slides);
+  return sl;
+}
+
+// Shared body of rtod_run and rtod_profile_run: the stream is copied in (if
+// on the host), its cell keys computed, then the slides are detected in
+// batches of B consecutive windows. kev (may be null) gets 8 events per
+// batch: one before and one after each kernel (the last one after the
+// router's training step, or right after k_compact without router).
+int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap, cudaEvent_t e_begin,
+               cudaEvent_t e_keys, std::vector<cudaEvent_t>* kev, BatchState* out_state,
+               std::vector<int32_t>* nout, std::vector<int32_t>* nund) {
+  const int64_t W = h->W, S = h->S;
+  const int64_t used = W + slides * S;
+  int r;
+  const float* src;
+  if ((r = ensure_records(h, slides))) return r;
+  if ((r = ensure_ids(h, std::max<int64_t>(1, std::min(ids_cap, slides * W))))) return r;
+  const int B = pick_batch(h, slides);
+  if ((r = ensure_pool(h, B))) return r;
+  if (e_begin) CU(cudaEventRecord(e_begin, h->stream));
+  if ((r = stage_stream(h, pts, used, &src))) return r;
+  if ((r = configure(h, MODE_RUN, B, S, src))) return r;  // first detected window: [S, W + S)
+  CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
+  const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((used + 255) / 256, h->sm_count * 8));
+  DISPATCH_D(h->D, CU(launch_k(k_keys<D>, dim3(kx), 256, h->stream, src, (int64_t)0, used, h->cell, h->run_keys,
+                               h->run_prev, h->bs)));
+  h->launches++;
+  if (e_keys) CU(cudaEventRecord(e_keys, h->stream));
+  const int64_t out_cap = std::min(ids_cap, h->ids_cap);
+  const int64_t full = slides / B, rem = slides % B;
+  const Batch bfull = make_batch(h, B, out_cap);
+  for (int64_t i = 0; i < full + (rem ? 1 : 0); ++i) {
+    const Batch b = i < full ? bfull : make_batch(h, (int)rem, out_cap);
+    if (kev) {
+      cudaEvent_t* e = &(*kev)[(size_t)i * 8];
+      CU(cudaEventRecord(e[0], h->stream));
+      r = launch_batch(h, b, false, e + 1);
+    } else {
+      r = i < full ? run_batch(h, b, false) : launch_batch(h, b, false, nullptr);
+    }
+    if (r) return r;
+  }
+  nout->resize((size_t)slides);
+  nund->resize((size_t)slides);
+  CU(cudaMemcpyAsync(out_state, h->bs, sizeof(BatchState), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaMemcpyAsync(nout->data(), h->rec_nout, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaMemcpyAsync(nund->data(), h->rec_undet, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  h->n_pushed = used;
+  h->slides_done = slides;
+  if ((r = check_device_error(h, *out_state))) return r;
+  h->undet_total += out_state->undet_total;
   return RTOD_OK;
 }
 
 void free_all(rtod_handle* h) {
   drop_graph(h);
-  void* bufs[] = {h->ring, h->ckey, h->bin_count, h->bin_start, h->cursor, h->owner, h->mixed,
-                  h->s_slot, h->s_ckey, h->s_x, h->flags, h->prev, h->state, h->staging, h->ids,
-                  h->slide_nout, h->slide_undet, h->run_buf};
-  for (void* b : bufs)
-    if (b) cudaFree(b);
+  for (Scratch& s : h->pool) {
+    dfree(s.bin_count); dfree(s.bin_start); dfree(s.kmin); dfree(s.kmax); dfree(s.s_off);
+    dfree(s.s_ckey); dfree(s.s_x); dfree(s.queue); dfree(s.feat); dfree(s.flags); dfree(s.scan_status);
+    dfree(s.cmp_status);
+  }
+  h->pool.clear();
+  dfree(h->ctr); dfree(h->jobs_dev); dfree(h->bs); dfree(h->router); dfree(h->ring); dfree(h->ring_keys);
+  dfree(h->ring_prev); dfree(h->staging); dfree(h->run_buf); dfree(h->run_keys); dfree(h->run_prev);
+  dfree(h->rec_nout); dfree(h->rec_undet); dfree(h->ids);
+  if (h->ctr_init) cudaFreeHost(h->ctr_init);
+  h->ctr_init = nullptr;
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   if (h->stream) cudaStreamDestroy(h->stream);
-}
-
-float elapsed(cudaEvent_t a, cudaEvent_t b) {
-  float ms = 0;
-  cudaEventElapsedTime(&ms, a, b);
-  return ms;
 }
 
 }  // namespace
@@ -318,7 +643,7 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 // C ABI
 // ---------------------------------------------------------------------------
 
-RTOD_API const char* rtod_version(void) { return "rtod-b200 0.1 (sm_100a)"; }
+RTOD_API const char* rtod_version(void) { return "rtod-b200 0.2 (sm_100a)"; }
 
 RTOD_API const char* rtod_last_error(void) { return g_last_error.c_str(); }
 
@@ -350,8 +675,8 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
   cudaDeviceProp prop;
   CU(cudaGetDeviceProperties(&prop, cfg->device));
   if (prop.major != 10)
-    return fail(RTOD_ERR_NODEV, "device %d is sm_%d%d; this library is built for sm_100a only",
-                cfg->device, prop.major, prop.minor);
+    return fail(RTOD_ERR_NODEV, "device %d is sm_%d%d; this library is built for sm_100a only", cfg->device,
+                prop.major, prop.minor);
   CU(cudaSetDevice(cfg->device));
 
   rtod_handle* h = new (std::nothrow) rtod_handle();
@@ -360,60 +685,48 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
   h->device = cfg->device;
   h->sm_count = prop.multiProcessorCount;
   h->block_warps = cfg->block_warps ? cfg->block_warps : 8;
-
-  const int64_t W = cfg->window, S = cfg->slide;
-  const int D = cfg->dim;
-  KParams& k = h->kp;
-  k.W = W;
-  k.S = S;
-  k.D = D;
-  k.h = D < 3 ? D : 3;
-  k.K = cfg->K;
-  k.R = cfg->R;
-  k.R2 = cfg->R * cfg->R;
+  h->W = cfg->window;
+  h->S = cfg->slide;
+  h->D = cfg->dim;
+  h->Wp = ((h->W + 3) / 4) * 4 + 4;  // padded SoA row: float4 loads stay in bounds
   {
     volatile float rf = (float)cfg->R;
     volatile float r2f = rf * rf;
-    k.R2f = r2f;
+    h->R2f = r2f;
   }
   set_grid(h, cfg->cells_per_r ? cfg->cells_per_r : 2);
+  // Windows per rtod_run launch: up to 32, within ~1 GiB of scratch.
+  const int64_t per_job = (int64_t)NB * 24 + h->W * (4 + 8 + 4 + 4) + h->Wp * h->D * 4 + h->W / 8;
+  h->batch_max = (int)std::max<int64_t>(1, std::min<int64_t>(32, (1ll << 30) / per_job));
+  if (cfg->batch) h->batch_max = cfg->batch;
 
+  int64_t* c = &h->device_bytes;
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
-  ok = ok && !dalloc(&h->ring, (size_t)(W * D)) && !dalloc(&h->ckey, (size_t)W) &&
-       !dalloc(&h->bin_count, NB) && !dalloc(&h->bin_start, NB + 1) && !dalloc(&h->cursor, NB) &&
-       !dalloc(&h->owner, NB) && !dalloc(&h->mixed, NB) && !dalloc(&h->s_slot, (size_t)W) &&
-       !dalloc(&h->s_ckey, (size_t)W) && !dalloc(&h->s_x, (size_t)(W * D)) &&
-       !dalloc(&h->flags, (size_t)W) && !dalloc(&h->prev, (size_t)W) && !dalloc(&h->state, 1) &&
-       !dalloc(&h->staging, (size_t)(W * D));
+  ok = ok && !dalloc(&h->ctr, (size_t)h->batch_max, c) && !dalloc(&h->jobs_dev, (size_t)h->batch_max, c) &&
+       !dalloc(&h->bs, 1, c) && !dalloc(&h->ring, (size_t)(h->W * h->D), c) &&
+       !dalloc(&h->ring_keys, (size_t)h->W, c) && !dalloc(&h->ring_prev, (size_t)h->W, c) &&
+       !dalloc(&h->staging, (size_t)(h->W * h->D), c);
+  ok = ok && cudaMallocHost((void**)&h->ctr_init, sizeof(JobCtr) * h->batch_max) == cudaSuccess;
+  ok = ok && !dalloc(&h->router, 1, c);
+  if (ok) {
+    RouterState* init = new (std::nothrow) RouterState;
+    ok = init != nullptr;
+    if (ok) {
+      init_router(init);
+      ok = cudaMemcpy(h->router, init, sizeof(RouterState), cudaMemcpyHostToDevice) == cudaSuccess;
+      delete init;
+    }
+  }
+  ok = ok && cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM) ==
+                 cudaSuccess;
   for (auto& e : h->ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
+  if (ok) ok = !ensure_pool(h, 1) && !ensure_ids(h, h->W);
+  if (ok) ok = !reset_state(h) && cudaStreamSynchronize(h->stream) == cudaSuccess;
   if (!ok) {
     std::string msg = g_last_error.empty() ? "device allocation failed" : g_last_error;
     free_all(h);
     delete h;
     return fail(RTOD_ERR_CUDA, "%s", msg.c_str());
-  }
-  k.ring = h->ring;
-  k.ckey = h->ckey;
-  k.bin_count = h->bin_count;
-  k.bin_start = h->bin_start;
-  k.cursor = h->cursor;
-  k.owner = h->owner;
-  k.mixed = h->mixed;
-  k.s_slot = h->s_slot;
-  k.s_ckey = h->s_ckey;
-  k.s_x = h->s_x;
-  k.flags = h->flags;
-  k.prev = h->prev;
-  k.state = h->state;
-  k.src = h->staging;
-  k.src_staging = 1;
-  r = ensure_ids(h, W);
-  if (!r) r = reset_state(h);
-  if (!r && cudaStreamSynchronize(h->stream) != cudaSuccess) r = fail(RTOD_ERR_CUDA, "init sync failed");
-  if (r) {
-    free_all(h);
-    delete h;
-    return r;
   }
   *out = h;
   return RTOD_OK;
@@ -440,36 +753,48 @@ RTOD_API int64_t rtod_slides_done(const rtod_handle* h) { return h ? h->slides_d
 
 RTOD_API int rtod_get_tuning(const rtod_handle* h, int32_t out[3]) {
   if (!h || !out) return fail(RTOD_ERR_ARG, "null argument");
-  out[0] = h->kp.n;
+  out[0] = h->n;
   out[1] = h->block_warps;
-  out[2] = h->kp.h;
+  out[2] = h->D < 3 ? h->D : 3;
   return RTOD_OK;
 }
+
+RTOD_API int rtod_get_stats(const rtod_handle* h, int64_t out[5]) {
+  if (!h || !out) return fail(RTOD_ERR_ARG, "null argument");
+  out[0] = h->launches;
+  out[1] = h->graph_replays;
+  out[2] = h->slides_done;
+  out[3] = h->undet_total;
+  out[4] = h->device_bytes;
+  return RTOD_OK;
+}
+
+RTOD_API const char* rtod_kernel_name(int32_t i) { return (i >= 0 && i < kPipeKernels) ? kKernelNames[i] : nullptr; }
 
 RTOD_API int rtod_push_slide(rtod_handle* h, const float* pts, int64_t n) {
   if (!h || !pts) return fail(RTOD_ERR_ARG, "null argument");
   if (h->poisoned) return fail(RTOD_ERR_STATE, "handle is in an error state; call rtod_reset");
   CU(cudaSetDevice(h->device));
-  const int64_t W = h->kp.W, S = h->kp.S, D = h->kp.D;
+  const int64_t W = h->W, S = h->S, D = h->D;
   if (h->n_pushed == 0) {
     if (n != W) return fail(RTOD_ERR_STATE, "the first push must hold exactly W=%lld points", (long long)W);
   } else {
+    if (h->mode != MODE_RING) return fail(RTOD_ERR_STATE, "the handle is not streaming; call rtod_reset");
     if (h->pending) return fail(RTOD_ERR_STATE, "rtod_detect must follow each slide push");
     if (n != S) return fail(RTOD_ERR_STATE, "a slide push must hold exactly S=%lld points", (long long)S);
   }
   CU(cudaEventRecord(h->ev[4], h->stream));
   CU(cudaMemcpyAsync(h->staging, pts, (size_t)(n * D) * sizeof(float), cudaMemcpyDefault, h->stream));
   CU(cudaEventRecord(h->ev[5], h->stream));
-  h->kp.src = h->staging;
-  h->kp.src_staging = 1;
   if (h->n_pushed == 0) {
-    int r = launch_ingest(h, W);
+    int r = configure(h, MODE_RING, 1, S, nullptr);  // first detected window: [S, W + S)
     if (r) return r;
-    k_advance<<<1, 32, 0, h->stream>>>(h->state, W);
-    CU(cudaGetLastError());
+    const Batch b = make_batch(h, 1, h->ids_cap);
+    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>((W + 255) / 256, h->sm_count * 8));
+    DISPATCH_D(h->D, CU(launch_k(k_ingest<D>, dim3((unsigned)gx, 1), 256, h->stream, b, 1)));
     h->launches++;
-    DevState s;
-    CU(cudaMemcpyAsync(&s, h->state, sizeof s, cudaMemcpyDeviceToHost, h->stream));
+    BatchState s;
+    CU(cudaMemcpyAsync(&s, h->bs, sizeof s, cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     r = check_device_error(h, s);
     if (r) return r;
@@ -485,37 +810,42 @@ RTOD_API int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t*
   if (h->poisoned) return fail(RTOD_ERR_STATE, "handle is in an error state; call rtod_reset");
   if (!h->pending) return fail(RTOD_ERR_STATE, "no pushed slide to detect");
   CU(cudaSetDevice(h->device));
-  // Per-call output: results start at the beginning of the ID buffer.
-  CU(cudaMemsetAsync(&h->state->out_total, 0, sizeof(int64_t), h->stream));
-  h->kp.out_cap = h->ids_cap;
-  cudaEvent_t* ev = times ? h->ev : nullptr;
-  if (ev) CU(cudaEventRecord(ev[0], h->stream));
-  int r = run_slide(h, ev);
+  // Per-call output: this slide's IDs start at the beginning of the buffer.
+  CU(cudaMemsetAsync(&h->bs->out_total, 0, sizeof(int64_t), h->stream));
+  const Batch b = make_batch(h, 1, h->ids_cap);
+  cudaEvent_t kev[7];
+  EventSet es;
+  if (times) {
+    for (auto& e : kev) e = es.make();
+    CU(cudaEventRecord(h->ev[0], h->stream));
+  }
+  int r = times ? launch_batch(h, b, true, kev) : run_batch(h, b, true);
   if (r) return r;
-  DevState s;
-  CU(cudaMemcpyAsync(&s, h->state, sizeof s, cudaMemcpyDeviceToHost, h->stream));
+  BatchState s;
+  CU(cudaMemcpyAsync(&s, h->bs, sizeof s, cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
   h->pending = false;
   r = check_device_error(h, s);
   if (r) return r;
   h->slides_done++;
-  h->undet_total += s.n_undet;
-  *n_out = s.n_out;
-  if (s.n_out > cap) return fail(RTOD_ERR_CAPACITY, "%d outliers but room for %lld", s.n_out, (long long)cap);
-  if (ev) CU(cudaEventRecord(ev[6], h->stream));
-  if (s.n_out > 0)
-    CU(cudaMemcpyAsync(out_ids, h->ids, (size_t)s.n_out * sizeof(int64_t), cudaMemcpyDefault, h->stream));
-  if (ev) CU(cudaEventRecord(ev[7], h->stream));
+  h->undet_total = s.undet_total;
+  *n_out = s.out_total;
+  if (s.out_total > cap)
+    return fail(RTOD_ERR_CAPACITY, "%lld outliers but room for %lld", (long long)s.out_total, (long long)cap);
+  if (times) CU(cudaEventRecord(h->ev[6], h->stream));
+  if (s.out_total > 0)
+    CU(cudaMemcpyAsync(out_ids, h->ids, (size_t)s.out_total * sizeof(int64_t), cudaMemcpyDefault, h->stream));
+  if (times) CU(cudaEventRecord(h->ev[7], h->stream));
   CU(cudaStreamSynchronize(h->stream));
   if (times) {
     std::memset(times, 0, sizeof *times);
     times->copy_new_points_h2d = elapsed(h->ev[4], h->ev[5]);
-    times->prepare_cell = elapsed(h->ev[0], h->ev[1]);
-    times->build_bvh = elapsed(h->ev[1], h->ev[2]);
-    times->detect_outlier = elapsed(h->ev[2], h->ev[3]);
+    times->prepare_cell = elapsed(h->ev[0], kev[1]);   // ring update + occupancy
+    times->build_bvh = elapsed(kev[1], kev[3]);       // scan + scatter
+    times->detect_outlier = elapsed(kev[3], kev[5]);  // count + compact
     times->copy_outlier_d2h = elapsed(h->ev[6], h->ev[7]);
-    times->total = times->copy_new_points_h2d + elapsed(h->ev[0], h->ev[3]) + times->copy_outlier_d2h;
-    times->undetermined_per_slide = s.n_undet;
+    times->total = times->copy_new_points_h2d + elapsed(h->ev[0], kev[5]) + times->copy_outlier_d2h;
+    times->undetermined_per_slide = (double)s.undet_total;
     times->slides = 1;
   }
   return RTOD_OK;
@@ -529,81 +859,27 @@ RTOD_API int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_s
   if (h->n_pushed != 0) return fail(RTOD_ERR_STATE, "rtod_run needs a fresh handle (call rtod_reset)");
   if (n < 0 || ids_cap < 0) return fail(RTOD_ERR_ARG, "negative size");
   CU(cudaSetDevice(h->device));
-  const int64_t W = h->kp.W, S = h->kp.S, D = h->kp.D;
-  int64_t slides = n >= W ? (n - W) / S : 0;
-  if (max_slides >= 0) slides = std::min(slides, max_slides);
-  *slides_out = slides;
   out_offsets[0] = 0;
+  const int64_t slides = count_slides(h, n, max_slides);
+  *slides_out = slides;
   if (slides == 0) return RTOD_OK;
-  const int64_t used = W + slides * S;
-  int r;
-  // Device input.
-  cudaEvent_t t0, t1, t2, t3;
-  bool timing = times != nullptr;
-  std::vector<cudaEvent_t> evs;
-  auto mk = [&](cudaEvent_t* e) { cudaEventCreate(e); evs.push_back(*e); };
-  mk(&t0); mk(&t1); mk(&t2); mk(&t3);
-  struct Cleanup {
-    std::vector<cudaEvent_t>& e;
-    ~Cleanup() { for (auto x : e) cudaEventDestroy(x); }
-  } cleanup{evs};
-  CU(cudaEventRecord(t0, h->stream));
-  const float* src = pts;
-  if (!is_device_ptr(pts)) {
-    if (h->run_buf_cap < used * D) {
-      if (h->run_buf) cudaFree(h->run_buf);
-      h->run_buf = nullptr;
-      h->run_buf_cap = 0;
-      if (dalloc(&h->run_buf, (size_t)(used * D))) return RTOD_ERR_CUDA;
-      h->run_buf_cap = used * D;
-    }
-    CU(cudaMemcpyAsync(h->run_buf, pts, (size_t)(used * D) * sizeof(float), cudaMemcpyHostToDevice, h->stream));
-    src = h->run_buf;
-  }
-  CU(cudaEventRecord(t1, h->stream));
-  if ((r = ensure_ids(h, std::max<int64_t>(1, std::min(ids_cap, slides * W))))) return r;
-  if ((r = ensure_slide_records(h, slides))) return r;
-  h->kp.out_cap = std::min(ids_cap, h->ids_cap);
-  h->kp.src = src;
-  h->kp.src_staging = 0;
-  if ((r = reset_state(h))) return r;
-  if ((r = launch_ingest(h, W))) return r;
-  k_advance<<<1, 32, 0, h->stream>>>(h->state, W);
-  CU(cudaGetLastError());
-  h->launches++;
-  h->n_pushed = W;
-  // Per-stage events only when a breakdown is requested without graphs.
-  const bool stage = timing && !h->cfg.use_graph;
-  std::vector<cudaEvent_t> sev;
+  EventSet es;
+  cudaEvent_t t0 = es.make(), t1 = es.make(), t2 = es.make(), d0 = es.make(), d1 = es.make();
+  // Stage split (only without graphs): events around every kernel of every batch.
+  std::vector<cudaEvent_t> kev;
+  const bool stage = times && !h->cfg.use_graph;
   if (stage) {
-    sev.resize((size_t)slides * 4);
-    for (auto& e : sev) mk(&e);
+    const int B = pick_batch(h, slides);
+    kev.resize((size_t)((slides + B - 1) / B) * 8);
+    for (auto& e : kev) e = es.make();
   }
+  BatchState s{};
+  std::vector<int32_t> nout, nund;
+  int r = run_stream(h, pts, slides, ids_cap, t0, t1, stage ? &kev : nullptr, &s, &nout, &nund);
+  if (r) return r;
   CU(cudaEventRecord(t2, h->stream));
-  for (int64_t j = 0; j < slides; ++j) {
-    if (stage) {
-      CU(cudaEventRecord(sev[j * 4], h->stream));
-      r = launch_slide(h, &sev[j * 4]);
-    } else {
-      r = run_slide(h, nullptr);
-    }
-    if (r) return r;
-  }
-  CU(cudaEventRecord(t3, h->stream));
-  DevState s;
-  std::vector<int32_t> nout((size_t)slides), nund((size_t)slides);
-  CU(cudaMemcpyAsync(&s, h->state, sizeof s, cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaMemcpyAsync(nout.data(), h->slide_nout, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaMemcpyAsync(nund.data(), h->slide_undet, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
-  h->n_pushed = used;
-  h->slides_done = slides;
-  if ((r = check_device_error(h, s))) return r;
-  h->undet_total += s.undet_total;
   for (int64_t j = 0; j < slides; ++j) out_offsets[j + 1] = out_offsets[j] + nout[j];
   if (out_offsets[slides] != s.out_total) return fail(RTOD_ERR_CUDA, "inconsistent outlier totals");
-  cudaEvent_t d0, d1;
-  mk(&d0); mk(&d1);
   CU(cudaEventRecord(d0, h->stream));
   if (s.out_total > 0)
     CU(cudaMemcpyAsync(out_ids, h->ids, (size_t)s.out_total * sizeof(int64_t), cudaMemcpyDefault, h->stream));
@@ -613,97 +889,165 @@ RTOD_API int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_s
     std::memset(times, 0, sizeof *times);
     const double inv = 1.0 / (double)slides;
     times->slides = slides;
-    times->copy_new_points_h2d = elapsed(t0, t1) * inv;
     times->copy_outlier_d2h = elapsed(d0, d1) * inv;
     if (stage) {
-      double pc = 0, bb = 0, de = 0;
-      for (int64_t j = 0; j < slides; ++j) {
-        pc += elapsed(sev[j * 4], sev[j * 4 + 1]);
-        bb += elapsed(sev[j * 4 + 1], sev[j * 4 + 2]);
-        de += elapsed(sev[j * 4 + 2], sev[j * 4 + 3]);
+      const int64_t nb = (int64_t)kev.size() / 8;
+      double pc = elapsed(t0, t1), bb = 0, de = 0;  // input copy + cell keys count as preparing cells
+      for (int64_t i = 0; i < nb; ++i) {
+        const cudaEvent_t* e = &kev[(size_t)i * 8];
+        pc += elapsed(e[0], e[2]);  // hist
+        bb += elapsed(e[2], e[4]);  // scan + scatter
+        de += elapsed(e[4], e[7]);  // count + compact (+ router training)
       }
       times->prepare_cell = pc * inv;
       times->build_bvh = bb * inv;
       times->detect_outlier = de * inv;
     }
-    // Everything on the library stream: input copy, state reset, initial
-    // fill, all slides and the outlier copy-out (the counts read-back and
-    // its host wait are the only parts outside).
-    times->total = (elapsed(t0, t3) + elapsed(d0, d1)) * inv;
+    // Everything on the library stream: input copy, keys, all batches and the
+    // outlier copy-out (the per-slide counts read-back and its host wait are
+    // the only parts outside).
+    times->total = (elapsed(t0, t2) + elapsed(d0, d1)) * inv;
     times->undetermined_per_slide = (double)s.undet_total * inv;
   }
   return RTOD_OK;
 }
 
-RTOD_API int rtod_get_stats(const rtod_handle* h, int64_t out[4]) {
-  if (!h || !out) return fail(RTOD_ERR_ARG, "null argument");
-  out[0] = h->launches;
-  out[1] = h->graph_replays;
-  out[2] = h->slides_done;
-  out[3] = h->undet_total;
+RTOD_API int rtod_profile_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides, double* kernel_ms,
+                              int32_t n_kernels) {
+  if (!h || !pts || !kernel_ms || n_kernels < 1) return fail(RTOD_ERR_ARG, "null argument");
+  if (h->poisoned) return fail(RTOD_ERR_STATE, "handle is in an error state; call rtod_reset");
+  if (h->n_pushed != 0) return fail(RTOD_ERR_STATE, "rtod_profile_run needs a fresh handle");
+  CU(cudaSetDevice(h->device));
+  const int64_t slides = count_slides(h, n, max_slides);
+  if (slides == 0) return fail(RTOD_ERR_ARG, "stream shorter than one slide");
+  const int B = pick_batch(h, slides);
+  const int64_t nb = (slides + B - 1) / B;
+  EventSet es;
+  cudaEvent_t t0 = es.make(), t1 = es.make();
+  std::vector<cudaEvent_t> kev((size_t)nb * 8);
+  for (auto& e : kev) e = es.make();
+  BatchState s{};
+  std::vector<int32_t> nout, nund;
+  int r = run_stream(h, pts, slides, slides * h->W, t0, t1, &kev, &s, &nout, &nund);
+  if (r) return r;
+  for (int i = 0; i < n_kernels; ++i) kernel_ms[i] = 0;
+  kernel_ms[0] = elapsed(t0, t1);  // input copy (host streams only) + cell keys of the stream
+  for (int64_t i = 0; i < nb; ++i) {
+    const cudaEvent_t* e = &kev[(size_t)i * 8];
+    for (int k = 1; k < kPipeKernels && k < n_kernels; ++k) kernel_ms[k] += elapsed(e[k], e[k + 1]);
+  }
+  for (int i = 0; i < n_kernels; ++i) kernel_ms[i] /= (double)slides;
   return RTOD_OK;
 }
 
-RTOD_API const char* rtod_kernel_name(int32_t i) {
-  return (i >= 0 && i < kSlideKernels) ? kKernelNames[i] : nullptr;
+// ---------------------------------------------------------------------------
+// Router diagnostics and test entry points
+// ---------------------------------------------------------------------------
+
+RTOD_API int rtod_router_info(rtod_handle* h, float* params, double info[6]) {
+  if (!h || !info) return fail(RTOD_ERR_ARG, "null argument");
+  CU(cudaSetDevice(h->device));
+  CU(cudaStreamSynchronize(h->stream));
+  RouterState* r = new (std::nothrow) RouterState;
+  if (!r) return fail(RTOD_ERR_ARG, "out of host memory");
+  cudaError_t e = cudaMemcpy(r, h->router, sizeof(RouterState), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    delete r;
+    return fail(RTOD_ERR_CUDA, "router read failed: %s", cudaGetErrorString(e));
+  }
+  if (params) std::memcpy(params, r->params, sizeof(float) * MLP_P);
+  info[0] = (double)r->steps;
+  info[1] = (double)r->last_loss;
+  info[2] = (double)r->routed_early;
+  info[3] = (double)r->routed_sweep;
+  info[4] = (double)r->misrouted;
+  info[5] = (double)r->threshold;
+  delete r;
+  return RTOD_OK;
 }
 
-RTOD_API int rtod_profile_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides,
-                              double* kernel_ms, int32_t n_kernels) {
-  if (!h || !pts || !kernel_ms || n_kernels < 1) return fail(RTOD_ERR_ARG, "null argument");
-  if (h->n_pushed != 0) return fail(RTOD_ERR_STATE, "rtod_profile_run needs a fresh handle");
-  CU(cudaSetDevice(h->device));
-  const int64_t W = h->kp.W, S = h->kp.S, D = h->kp.D;
-  int64_t slides = n >= W ? (n - W) / S : 0;
-  if (max_slides >= 0) slides = std::min(slides, max_slides);
-  if (slides == 0) return fail(RTOD_ERR_ARG, "stream shorter than one slide");
-  const int64_t used = W + slides * S;
-  const float* src = pts;
-  int r;
-  if (!is_device_ptr(pts)) {
-    if (h->run_buf_cap < used * D) {
-      if (h->run_buf) cudaFree(h->run_buf);
-      h->run_buf = nullptr;
-      h->run_buf_cap = 0;
-      if (dalloc(&h->run_buf, (size_t)(used * D))) return RTOD_ERR_CUDA;
-      h->run_buf_cap = used * D;
-    }
-    CU(cudaMemcpyAsync(h->run_buf, pts, (size_t)(used * D) * sizeof(float), cudaMemcpyHostToDevice, h->stream));
-    src = h->run_buf;
+namespace {
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
   }
-  if ((r = ensure_ids(h, std::max<int64_t>(1, slides * W)))) return r;
-  if ((r = ensure_slide_records(h, slides))) return r;
-  h->kp.out_cap = h->ids_cap;
-  h->kp.src = src;
-  h->kp.src_staging = 0;
-  if ((r = reset_state(h))) return r;
-  if ((r = launch_ingest(h, W))) return r;
-  k_advance<<<1, 32, 0, h->stream>>>(h->state, W);
+};
+}  // namespace
+
+RTOD_API int rtod_mlp_param_count(void) { return MLP_P; }
+
+RTOD_API int rtod_mlp_forward(int32_t device, const float* params, const float* x, int64_t n, float* logits) {
+  if (!params || !x || !logits || n < 1 || n > (1 << 24)) return fail(RTOD_ERR_ARG, "bad argument");
+  CU(cudaSetDevice(device));
+  DevBuf dp, dx, dz;
+  CU(cudaMalloc(&dp.p, sizeof(float) * MLP_P));
+  CU(cudaMalloc(&dx.p, sizeof(float) * MLP_IN * n));
+  CU(cudaMalloc(&dz.p, sizeof(float) * MLP_B * n));
+  CU(cudaMemcpy(dp.p, params, sizeof(float) * MLP_P, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dx.p, x, sizeof(float) * MLP_IN * n, cudaMemcpyHostToDevice));
+  k_mlp_forward<<<(unsigned)((n + 255) / 256), 256>>>((float*)dp.p, (float*)dx.p, (int)n, (float*)dz.p);
   CU(cudaGetLastError());
-  h->launches++;
-  std::vector<cudaEvent_t> ev((size_t)slides * (kSlideKernels + 1));
-  for (auto& e : ev) CU(cudaEventCreate(&e));
-  struct Cleanup {
-    std::vector<cudaEvent_t>& e;
-    ~Cleanup() { for (auto x : e) cudaEventDestroy(x); }
-  } cleanup{ev};
-  for (int64_t j = 0; j < slides; ++j) {
-    cudaEvent_t* e = &ev[(size_t)j * (kSlideKernels + 1)];
-    CU(cudaEventRecord(e[0], h->stream));
-    if ((r = launch_slide(h, nullptr, e + 1))) return r;
-  }
-  DevState s;
-  CU(cudaMemcpyAsync(&s, h->state, sizeof s, cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
-  h->n_pushed = used;
-  h->slides_done = slides;
-  if ((r = check_device_error(h, s))) return r;
-  h->undet_total += s.undet_total;
-  for (int i = 0; i < n_kernels; ++i) kernel_ms[i] = 0;
-  for (int64_t j = 0; j < slides; ++j) {
-    cudaEvent_t* e = &ev[(size_t)j * (kSlideKernels + 1)];
-    for (int i = 0; i < kSlideKernels && i < n_kernels; ++i) kernel_ms[i] += elapsed(e[i], e[i + 1]);
-  }
-  for (int i = 0; i < n_kernels; ++i) kernel_ms[i] /= (double)slides;
+  CU(cudaMemcpy(logits, dz.p, sizeof(float) * MLP_B * n, cudaMemcpyDeviceToHost));
+  return RTOD_OK;
+}
+
+RTOD_API int rtod_mlp_grad(int32_t device, const float* params, const float* x, const int32_t* y, int64_t n,
+                           float* grad, float* loss) {
+  if (!params || !x || !y || !grad || !loss || n < 1 || n > (1 << 20)) return fail(RTOD_ERR_ARG, "bad argument");
+  for (int64_t i = 0; i < n; ++i)
+    if (y[i] < 0 || y[i] >= MLP_B) return fail(RTOD_ERR_ARG, "label out of range");
+  CU(cudaSetDevice(device));
+  CU(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM));
+  DevBuf dp, dx, dy, dg, dl, dyf;
+  CU(cudaMalloc(&dp.p, sizeof(float) * MLP_P));
+  CU(cudaMalloc(&dx.p, sizeof(float) * MLP_IN * n));
+  CU(cudaMalloc(&dy.p, sizeof(int32_t) * n));
+  CU(cudaMalloc(&dyf.p, sizeof(float) * n));
+  CU(cudaMalloc(&dg.p, sizeof(float) * MLP_P));
+  CU(cudaMalloc(&dl.p, sizeof(float)));
+  CU(cudaMemcpy(dp.p, params, sizeof(float) * MLP_P, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dx.p, x, sizeof(float) * MLP_IN * n, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dy.p, y, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+  k_mlp_grad<<<1, 256, TRAIN_SMEM>>>((float*)dp.p, (float*)dx.p, (int32_t*)dy.p, (int)n, (float*)dg.p,
+                                     (float*)dl.p, (float*)dyf.p);
+  CU(cudaGetLastError());
+  CU(cudaMemcpy(grad, dg.p, sizeof(float) * MLP_P, cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(loss, dl.p, sizeof(float), cudaMemcpyDeviceToHost));
+  return RTOD_OK;
+}
+
+RTOD_API int rtod_mlp_adam(int32_t device, float* params, float* m, float* v, int32_t t, const float* x,
+                           const int32_t* y, int64_t n, float lr, float* loss) {
+  if (!params || !m || !v || !x || !y || !loss || n < 1 || n > (1 << 20) || t < 1)
+    return fail(RTOD_ERR_ARG, "bad argument");
+  for (int64_t i = 0; i < n; ++i)
+    if (y[i] < 0 || y[i] >= MLP_B) return fail(RTOD_ERR_ARG, "label out of range");
+  CU(cudaSetDevice(device));
+  CU(cudaFuncSetAttribute(k_mlp_adam, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM));
+  const float beta1 = 0.9f, beta2 = 0.999f;
+  float bt[2] = {std::pow(beta1, (float)(t - 1)), std::pow(beta2, (float)(t - 1))};
+  DevBuf dp, dm, dv, dbt, dx, dy, dl, dyf;
+  CU(cudaMalloc(&dp.p, sizeof(float) * MLP_P));
+  CU(cudaMalloc(&dm.p, sizeof(float) * MLP_P));
+  CU(cudaMalloc(&dv.p, sizeof(float) * MLP_P));
+  CU(cudaMalloc(&dbt.p, sizeof(float) * 2));
+  CU(cudaMalloc(&dx.p, sizeof(float) * MLP_IN * n));
+  CU(cudaMalloc(&dy.p, sizeof(int32_t) * n));
+  CU(cudaMalloc(&dyf.p, sizeof(float) * n));
+  CU(cudaMalloc(&dl.p, sizeof(float)));
+  CU(cudaMemcpy(dp.p, params, sizeof(float) * MLP_P, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dm.p, m, sizeof(float) * MLP_P, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dv.p, v, sizeof(float) * MLP_P, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dbt.p, bt, sizeof(float) * 2, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dx.p, x, sizeof(float) * MLP_IN * n, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(dy.p, y, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+  k_mlp_adam<<<1, 256, TRAIN_SMEM>>>((float*)dp.p, (float*)dm.p, (float*)dv.p, (float*)dbt.p, (float*)dx.p,
+                                     (int32_t*)dy.p, (int)n, lr, beta1, beta2, 1e-8f, (float*)dl.p, (float*)dyf.p);
+  CU(cudaGetLastError());
+  CU(cudaMemcpy(params, dp.p, sizeof(float) * MLP_P, cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(m, dm.p, sizeof(float) * MLP_P, cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(v, dv.p, sizeof(float) * MLP_P, cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(loss, dl.p, sizeof(float), cudaMemcpyDeviceToHost));
   return RTOD_OK;
 }

@@ -64,14 +64,14 @@ class Detector:
     def __init__(self, window: int, slide: int, R: float, K: int, dim: int = 1, opt: int = 2,
                  pred: str = "fp32_le", router: bool = False, tuner: bool = False,
                  cells_per_r: int = 0, block_warps: int = 0, use_graph: bool = True,
-                 device: int = 0):
+                 batch: int = 0, device: int = 0):
         cfg = Config()
         check(lib().rtod_config_init(ctypes.byref(cfg)))
         cfg.window, cfg.slide, cfg.R, cfg.K, cfg.dim, cfg.opt = window, slide, R, K, dim, opt
         cfg.pred = _native.PRED[pred]
         cfg.router, cfg.tuner = int(router), int(tuner)
         cfg.cells_per_r, cfg.block_warps = cells_per_r, block_warps
-        cfg.use_graph, cfg.device = int(use_graph), device
+        cfg.use_graph, cfg.device, cfg.batch = int(use_graph), device, batch
         self.cfg = cfg
         self.window, self.slide, self.R, self.K, self.dim = window, slide, R, K, dim
         self._h = ctypes.c_void_p()
@@ -144,14 +144,14 @@ class Detector:
                              ctypes.byref(ns), ctypes.byref(t) if times else None))
         del keep
         ids = out[:off[-1]] if out_ids is not None else out[:off[-1]].copy()
-        self.last_stats = self.stats
         return RunResult(off, ids, t.as_dict() if times else {})
 
     @property
     def stats(self) -> dict:
-        a = (ctypes.c_int64 * 4)()
+        a = (ctypes.c_int64 * 5)()
         check(lib().rtod_get_stats(self._h, a))
-        return {"launches": a[0], "graph_replays": a[1], "slides": a[2], "undetermined": a[3]}
+        return {"launches": a[0], "graph_replays": a[1], "slides": a[2], "undetermined": a[3],
+                "device_bytes": a[4]}
 
     def profile(self, points, max_slides: int = -1) -> dict:
         """Average device ms per slide of each pipeline kernel (diagnostic run
@@ -170,6 +170,16 @@ class Detector:
 
     def reset(self) -> None:
         check(lib().rtod_reset(self._h))
+
+    def router_info(self) -> dict:
+        """Learned-router state: parameters, training steps and routing counters."""
+        params = np.zeros(int(lib().rtod_mlp_param_count()), np.float32)
+        info = np.zeros(6, np.float64)
+        check(lib().rtod_router_info(self._h, params.ctypes.data_as(ctypes.c_void_p),
+                                     info.ctypes.data_as(ctypes.c_void_p)))
+        return {"params": params, "steps": int(info[0]), "last_loss": float(info[1]),
+                "routed_early": int(info[2]), "routed_sweep": int(info[3]),
+                "misrouted": int(info[4]), "threshold": float(info[5])}
 
     @property
     def slides_done(self) -> int:
