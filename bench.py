@@ -165,7 +165,9 @@ def algorithmic_bytes(kernel: str, w, n_out_per_slide: float, undet_per_slide: f
         "k_scan": 4 * 65536 * 3,                              # read counts, write starts+cursors
         "k_scatter": 8 * W + 4 * d * W + (4 + 8 + 4 * d) * W,  # read keys+ring, write SoA
         "k_count": (8 + 4 + 4 * d) * W,                       # read the cell-ordered SoA once
-        "k_compact": W + 8 * n_out_per_slide,                 # read flags, write IDs
+        "k_compact": W / 8 + 8 * n_out_per_slide,             # read the outlier bits, write IDs
+        "k_keys": 4 * d * S + 8 * S,                          # per slide: read points, write keys
+        "k_train": 2048 * 16 + 3 * 1316 * 4 * 2,              # samples + params/moments (per batch)
     }[kernel]
 
 
@@ -199,20 +201,21 @@ def run_ours(args, world, rank, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    engines = {"plain": dict(router=False)}
-    results = {}
-    for name, kw in engines.items():
+    def measure(kw, steps, full):
+        """Device-timed passes of one engine configuration; with full=True also
+        the clocks, the end-to-end passes and the per-kernel profile."""
         det = Detector(w.window, w.slide, w.R, w.K, dim=w.dim, device=local, **kw)
         ref = None
         for _ in range(max(3, args.warmup)):
             det.reset()
             r = det.run(pts_dev, out_ids=out_dev, ids_cap=cap, times=True)
             ref = r.offsets.copy()
+        ids_ref = out_dev[:int(ref[-1])].cpu().numpy()
         stats0 = det.stats
         barrier()
         dev_ms = 0.0
         with ClockSampler(physical_gpu_index(local)) as clk:
-            for _ in range(args.steps):
+            for _ in range(steps):
                 flush.zero_()
                 torch.cuda.synchronize()
                 det.reset()
@@ -221,36 +224,54 @@ def run_ours(args, world, rank, local):
         barrier()
         stats1 = det.stats
         assert np.array_equal(r.offsets, ref)
-        t_max = max_over_ranks(dev_ms)
-        n_outliers = int(r.offsets[-1])
-        # end to end through the public API with pinned host buffers
-        pts_pin = torch.from_numpy(w.points).pin_memory()
-        ids_pin = torch.empty(cap, dtype=torch.int64).pin_memory()
-        pts_np, ids_np = pts_pin.numpy(), ids_pin.numpy()
-        for _ in range(2):
+        out = dict(dev_ms=max_over_ranks(dev_ms), steps=steps, offsets=ref, ids=ids_ref,
+                   launches=stats1["launches"] - stats0["launches"],
+                   undet=r.times["undetermined_per_slide"], n_outliers=int(ref[-1]))
+        if full:
+            out["clocks"] = clk.summary()
+            # end to end through the public API with pinned host buffers
+            pts_pin = torch.from_numpy(w.points).pin_memory()
+            ids_pin = torch.empty(cap, dtype=torch.int64).pin_memory()
+            pts_np, ids_np = pts_pin.numpy(), ids_pin.numpy()
+            for _ in range(2):
+                det.reset()
+                det.run(pts_np, out_ids=ids_np, ids_cap=cap)
+            barrier()
+            e2e_s = 0.0
+            e2e_steps = max(3, min(steps, 50))
+            for _ in range(e2e_steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                det.reset()
+                t0 = time.perf_counter()
+                r2 = det.run(pts_np, out_ids=ids_np, ids_cap=cap)
+                e2e_s += time.perf_counter() - t0
+            barrier()
+            assert np.array_equal(r2.offsets, ref) and np.array_equal(r2.ids, ids_ref)
+            out.update(e2e_s=max_over_ranks(e2e_s), e2e_steps=e2e_steps, h2d=w.n * w.dim * 4,
+                       d2h=(slides + 1) * 8 + out["n_outliers"] * 8 + slides * 8)
+            # per-kernel device time of one pass (diagnostic, individual launches)
             det.reset()
-            det.run(pts_np, out_ids=ids_np, ids_cap=cap)
-        barrier()
-        e2e_s = 0.0
-        e2e_steps = max(3, min(args.steps, 50))
-        for _ in range(e2e_steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            det.reset()
-            t0 = time.perf_counter()
-            r2 = det.run(pts_np, out_ids=ids_np, ids_cap=cap)
-            e2e_s += time.perf_counter() - t0
-        barrier()
-        assert np.array_equal(r2.offsets, ref)
-        e2e_max = max_over_ranks(e2e_s)
-        # per-kernel device time of one pass (diagnostic, individual launches)
-        det.reset()
-        prof = det.profile(pts_dev)
+            out["prof"] = det.profile(pts_dev)
+            if kw.get("router"):
+                info = det.router_info()
+                out["router"] = {k: info[k] for k in ("steps", "last_loss", "routed_early",
+                                                      "routed_sweep", "misrouted")}
         det.close()
-        results[name] = dict(dev_ms=t_max, clocks=clk.summary(), launches=stats1["launches"] - stats0["launches"],
-                             n_outliers=n_outliers, undet=r.times["undetermined_per_slide"],
-                             e2e_s=e2e_max, e2e_steps=e2e_steps, prof=prof, h2d=w.n * w.dim * 4,
-                             d2h=(slides + 1) * 8 + n_outliers * 8 + slides * 8)
+        return out
+
+    results = {
+        # headline: learned router on, B consecutive windows per launch, graph replay
+        "routed_batched": measure(dict(router=True), args.steps, True),
+        # the plain grid kernel: one window per launch (graph replay per slide), no router
+        "plain": measure(dict(router=False, batch=1), args.steps, False),
+        # batching without the router (isolates the router's share)
+        "plain_batched": measure(dict(router=False), args.steps, False),
+    }
+    base = results["routed_batched"]
+    for name, r in results.items():
+        assert np.array_equal(r["offsets"], base["offsets"]), name
+        assert np.array_equal(r["ids"], base["ids"]), name
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
@@ -272,7 +293,7 @@ def cpu_baseline(w):
 
 
 def emit_ours(args, world, w, res):
-    r = res["plain"]
+    r = res["routed_batched"]
     K = args.steps
     slides = w.slides
     t_s = r["dev_ms"] / 1e3
@@ -292,7 +313,8 @@ def emit_ours(args, world, w, res):
         "window_points_per_s": world * K * slides * w.window / t_s,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded stand-in for RTOD's STK stream)",
-        "config": workload_config(w, {"engine": "plain grid kernel (router off), graph replay per slide"}),
+        "config": workload_config(w, {"engine": "learned-routed batched engine (router on, "
+                                                 "consecutive windows per launch, graph replay)"}),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
@@ -304,6 +326,12 @@ def emit_ours(args, world, w, res):
                 "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
                 "us_per_slide": r["e2e_s"] / (r["e2e_steps"] * slides) * 1e6},
         "outliers_per_slide": n_out, "undetermined_per_slide": r["undet"],
+        "router": r.get("router"),
+        "engines": {name: {"us_per_slide": e["dev_ms"] * 1e3 / (e["steps"] * slides),
+                           "points_per_s": world * e["steps"] * slides * w.slide / (e["dev_ms"] / 1e3),
+                           "gpu_launches_per_step": e["launches"] / e["steps"]}
+                    for name, e in res.items()},
+        "bit_exact_across_engines": True,
     }
     if not args.no_cpu_baseline and world == 1:
         cb, _ = cpu_baseline(w)

@@ -153,6 +153,34 @@ int rtod_profile_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_sl
 /* Name of pipeline kernel i (0-based) as used by rtod_profile_run, or NULL. */
 const char* rtod_kernel_name(int32_t i);
 
+/* ------------------------------------------------------------------------
+   Batched streams: many independent streams, each with its own window,
+   slide, R, K and dimension, advanced together one slide per step. A step
+   detects the pushed slide of every stream in one replay of a captured CUDA
+   graph (streams grouped by dimension and predicate, one launch sequence per
+   group, all groups in the graph). No counterpart in RTOD (one stream per
+   process). The learned router, when on, is shared by all streams
+   (cfgs[0].router decides for all).
+   ------------------------------------------------------------------------ */
+typedef struct rtod_batch rtod_batch;
+
+int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_batch** out);
+
+/* Stream s: first push W points, then S points before each step (a stream
+   without a pushed slide sits the step out). */
+int rtod_batch_push(rtod_batch* b, int32_t s, const float* pts, int64_t n);
+
+/* Detects the pushed slide of every stream that has one. out_offsets
+   (n_streams + 1 entries) receives CSR offsets into out_ids by stream (a
+   stream that sat out gets an empty range); *n_total the number of IDs. */
+int rtod_batch_step(rtod_batch* b, int64_t* out_offsets, int64_t* out_ids, int64_t cap, int64_t* n_total);
+
+/* out[0] steps, out[1] kernel launches (graph replays count their kernels),
+   out[2] window detections summed over streams, out[3] groups. */
+int rtod_batch_stats(const rtod_batch* b, int64_t out[4]);
+
+void rtod_batch_destroy(rtod_batch* b);
+
 /* Learned router state (rtod_config.router = 1). params (may be NULL)
    receives the network's rtod_mlp_param_count() parameters; info receives
    [0] training steps, [1] last training loss, [2] points routed to the

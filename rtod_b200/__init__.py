@@ -6,6 +6,6 @@ outlier IDs, per-stage times), with the OptiX/RT-core path replaced by
 hand-written CUDA kernels behind the C ABI in include/rtod.h.
 """
 from ._native import RtodError  # noqa: F401
-from .engine import Detector, RunResult  # noqa: F401
+from .engine import BatchDetector, Detector, RunResult  # noqa: F401
 
-__all__ = ["Detector", "RunResult", "RtodError"]
+__all__ = ["Detector", "BatchDetector", "RunResult", "RtodError"]

@@ -73,7 +73,7 @@ struct JobCtr {
   uint32_t scan_ticket;  // k_scan tile tickets
   uint32_t cmp_ticket;   // k_compact tile tickets
   int32_t n_sweep;       // queued points of the full-sweep queue (router on)
-  int32_t pad;
+  int32_t last_nout;     // outliers of the job's last detected window
 };
 
 // Per-handle state (device).
@@ -126,12 +126,16 @@ struct Batch {
   int32_t njobs;
   BatchState* bs;
   RouterState* router;  // learned router (used when the kernels are built with ROUTE)
+  const int32_t* active; // per job: 0 = skip this job in this launch (null: all active)
+  int32_t* job_nout;     // per job: outliers of this launch's window (may be null)
   int64_t* out_ids;  // outlier IDs of all jobs, concatenated in job order
   int64_t out_cap;
   int64_t cmp_tiles; // k_compact tiles over all jobs
 };
 
 __device__ __forceinline__ void set_err(BatchState* bs, int32_t code) { atomicCAS(&bs->err, 0, code); }
+
+__device__ __forceinline__ bool job_active(const Batch& b) { return !b.active || b.active[blockIdx.y]; }
 
 // ---------------------------------------------------------------------------
 // Grid cells. Cell coordinate k_i = floor(x_i / cell) in double precision,
@@ -388,6 +392,7 @@ template <int D>
 __global__ void __launch_bounds__(256) k_ingest(Batch b, int32_t fill) {
   pdl_trigger();
   pdl_wait();
+  if (!job_active(b)) return;
   const Job& jb = b.jobs[blockIdx.y];
   float* ring = const_cast<float*>(jb.pts);
   uint64_t* keys = const_cast<uint64_t*>(jb.keys);
@@ -418,6 +423,7 @@ template <int D>
 __global__ void __launch_bounds__(256) k_hist(Batch b) {
   pdl_trigger();
   pdl_wait();
+  if (!job_active(b)) return;
   constexpr int H = Hashed<D>::value;
   const Job& jb = b.jobs[blockIdx.y];
   const int64_t lo = jb.ctr->lo;
@@ -452,6 +458,7 @@ __global__ void __launch_bounds__(256) k_scan(Batch b) {
   __shared__ uint32_t s_tile, s_prefix;
   pdl_trigger();
   pdl_wait();
+  if (!job_active(b)) return;
   const Job& jb = b.jobs[blockIdx.y];
   if (threadIdx.x == 0) s_tile = atomicAdd(&jb.ctr->scan_ticket, 1u);
   __syncthreads();
@@ -530,6 +537,7 @@ template <int D, bool ROUTE>
 __global__ void __launch_bounds__(256) k_scatter(Batch b) {
   pdl_trigger();
   pdl_wait();
+  if (!job_active(b)) return;
   constexpr int H = Hashed<D>::value;
   const Job& jb = b.jobs[blockIdx.y];
   const int64_t lo = jb.ctr->lo;
@@ -796,6 +804,7 @@ template <int D, int PRED, bool ROUTE>
 __global__ void __launch_bounds__(256) k_count(Batch b) {
   pdl_trigger();
   pdl_wait();
+  if (!job_active(b)) return;
   const Job& jb = b.jobs[blockIdx.y];
   reset_bins(jb);
   const int lane = threadIdx.x & 31;
@@ -840,7 +849,7 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t s_tile, s_prefix, s_last;
   __shared__ int64_t s_jobbase;
-  __shared__ int64_t s_red[2][8];
+  __shared__ int64_t s_red[3][8];
   pdl_trigger();
   pdl_wait();
   const Job& jb = b.jobs[blockIdx.y];
@@ -848,7 +857,8 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
   if (blockIdx.x >= ntiles) return;  // smaller job in a mixed batch
   BatchState* bs = b.bs;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (wid == 0) {
+  const bool act = job_active(b);
+  if (act && wid == 0) {
     // Output base of this job: IDs of all earlier jobs of the batch come first.
     int64_t part = 0;
     for (int j = lane; j < (int)blockIdx.y; j += 32) part += b.jobs[j].ctr->n_out;
@@ -860,29 +870,31 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
     }
   }
   __syncthreads();
-  const uint32_t tile = s_tile;
-  const int64_t lo = jb.ctr->lo;
-  const int64_t wi = ((int64_t)tile * CMP_TILE >> 5) + threadIdx.x;  // bitset word
-  const int64_t nwords = (jb.W + 31) >> 5;
-  uint32_t bits = 0;
-  if (wi < nwords) {
-    bits = jb.flags[wi];
-    if (bits) jb.flags[wi] = 0;
-  }
-  uint32_t total;
-  const uint32_t ex = block_exclusive_scan(__popc(bits), &total, sm);
-  if (wid == 0) {
-    const uint32_t pre = warp_lookback(jb.cmp_status, tile, total, bs);
-    if (lane == 0) s_prefix = pre;
-  }
-  __syncthreads();
-  int64_t o = s_jobbase + s_prefix + ex;
-  while (bits) {
-    const int e = __ffs(bits) - 1;
-    bits &= bits - 1;
-    if (o < b.out_cap) b.out_ids[o] = lo + wi * 32 + e;
-    else set_err(bs, DERR_CAPACITY);
-    ++o;
+  if (act) {
+    const uint32_t tile = s_tile;
+    const int64_t lo = jb.ctr->lo;
+    const int64_t wi = ((int64_t)tile * CMP_TILE >> 5) + threadIdx.x;  // bitset word
+    const int64_t nwords = (jb.W + 31) >> 5;
+    uint32_t bits = 0;
+    if (wi < nwords) {
+      bits = jb.flags[wi];
+      if (bits) jb.flags[wi] = 0;
+    }
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(__popc(bits), &total, sm);
+    if (wid == 0) {
+      const uint32_t pre = warp_lookback(jb.cmp_status, tile, total, bs);
+      if (lane == 0) s_prefix = pre;
+    }
+    __syncthreads();
+    int64_t o = s_jobbase + s_prefix + ex;
+    while (bits) {
+      const int e = __ffs(bits) - 1;
+      bits &= bits - 1;
+      if (o < b.out_cap) b.out_ids[o] = lo + wi * 32 + e;
+      else set_err(bs, DERR_CAPACITY);
+      ++o;
+    }
   }
   __threadfence();
   __syncthreads();
@@ -892,8 +904,12 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
   // Last tile of the batch: per-slide records, window advance, counter reset
   // (one job per thread) and the batch totals.
   __threadfence();
-  int64_t add = 0, und = 0;
+  int64_t add = 0, und = 0, nact = 0;
   for (int j = threadIdx.x; j < b.njobs; j += blockDim.x) {
+    if (b.active && !b.active[j]) {
+      if (b.job_nout) b.job_nout[j] = 0;
+      continue;
+    }
     const Job& J = b.jobs[j];
     JobCtr* c = J.ctr;
     const int32_t nout = *(volatile int32_t*)&c->n_out;
@@ -905,6 +921,9 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
     }
     add += nout;
     und += nund;
+    nact += 1;
+    c->last_nout = nout;
+    if (b.job_nout) b.job_nout[j] = nout;
     c->lo += c->lo_step;
     c->n_out = 0;
     c->n_undet = 0;
@@ -915,21 +934,24 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
   for (int o2 = 16; o2 > 0; o2 >>= 1) {
     add += __shfl_xor_sync(0xffffffffu, add, o2);
     und += __shfl_xor_sync(0xffffffffu, und, o2);
+    nact += __shfl_xor_sync(0xffffffffu, nact, o2);
   }
   if (lane == 0) {
     s_red[0][wid] = add;
     s_red[1][wid] = und;
+    s_red[2][wid] = nact;
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    int64_t ta = 0, tu = 0;
+    int64_t ta = 0, tu = 0, tn = 0;
     for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
       ta += s_red[0][w];
       tu += s_red[1][w];
+      tn += s_red[2][w];
     }
     bs->out_total += ta;
     bs->undet_total += tu;
-    bs->slides += b.njobs;
+    bs->slides += tn;
     bs->done = 0;
   }
 }

@@ -392,43 +392,51 @@ Batch make_batch(rtod_handle* h, int njobs, int64_t out_cap) {
   return b;
 }
 
-// Launches one batch: [ingest] hist scan scatter count compact. kev (may be
-// null) receives an event after each kernel (kev[0] after ingest, or at the
-// start when there is none).
-int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev) {
-  cudaStream_t st = h->stream;
-  const int64_t W = h->W, nj = b.njobs;
+// Launch geometry of a group of jobs that share a dimension and predicate.
+struct Geom {
+  int64_t Wmax, Smax;
+  int D, pred, route, sm_count, block_warps;
+  RouterState* router;
+};
+
+// Launches one batch: [ingest] hist scan scatter count compact [train].
+// kev (may be null) receives an event after each kernel (kev[0] after ingest,
+// or at the start when there is none; kev[6] after training or compact).
+// Returns the number of kernels launched in *nk.
+int launch_group(const Geom& g, const Batch& b, bool ingest, cudaStream_t st, cudaEvent_t* kev, int64_t* nk) {
+  const int64_t W = g.Wmax, nj = b.njobs;
   const unsigned gy = (unsigned)nj;
+  int64_t launched = 0;
   if (ingest) {
-    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>((h->S + 255) / 256, h->sm_count * 4));
-    DISPATCH_D(h->D, CU(launch_k(k_ingest<D>, dim3((unsigned)gx, gy), 256, st, b, 0)));
-    h->launches++;
+    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>((g.Smax + 255) / 256, g.sm_count * 4));
+    DISPATCH_D(g.D, CU(launch_k(k_ingest<D>, dim3((unsigned)gx, gy), 256, st, b, 0)));
+    launched++;
   }
   if (kev) CU(cudaEventRecord(kev[0], st));
   const int64_t wx = std::max<int64_t>(
-      1, std::min<int64_t>((W + 255) / 256, std::max<int64_t>(2, (h->sm_count * 16 + nj - 1) / nj)));
-  DISPATCH_D(h->D, CU(launch_k(k_hist<D>, dim3((unsigned)wx, gy), 256, st, b)));
+      1, std::min<int64_t>((W + 255) / 256, std::max<int64_t>(2, (g.sm_count * 16 + nj - 1) / nj)));
+  DISPATCH_D(g.D, CU(launch_k(k_hist<D>, dim3((unsigned)wx, gy), 256, st, b)));
   if (kev) CU(cudaEventRecord(kev[1], st));
   CU(launch_k(k_scan, dim3(SCAN_TILES, gy), 256, st, b));
   if (kev) CU(cudaEventRecord(kev[2], st));
-  if (h->cfg.router) {
-    DISPATCH_D(h->D, CU(launch_k(k_scatter<D, true>, dim3((unsigned)wx, gy), 256, st, b)));
+  if (g.route) {
+    DISPATCH_D(g.D, CU(launch_k(k_scatter<D, true>, dim3((unsigned)wx, gy), 256, st, b)));
   } else {
-    DISPATCH_D(h->D, CU(launch_k(k_scatter<D, false>, dim3((unsigned)wx, gy), 256, st, b)));
+    DISPATCH_D(g.D, CU(launch_k(k_scatter<D, false>, dim3((unsigned)wx, gy), 256, st, b)));
   }
   if (kev) CU(cudaEventRecord(kev[3], st));
-  const int wpb = h->block_warps;
-  const int64_t cx = std::max<int64_t>(1, (int64_t)h->sm_count * (64 / wpb) / nj);
-  if (h->cfg.router) {
-    DISPATCH_DP(h->D, h->cfg.pred, CU(launch_k(k_count<D, PRED, true>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
+  const int wpb = g.block_warps;
+  const int64_t cx = std::max<int64_t>(1, (int64_t)g.sm_count * (64 / wpb) / nj);
+  if (g.route) {
+    DISPATCH_DP(g.D, g.pred, CU(launch_k(k_count<D, PRED, true>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
   } else {
-    DISPATCH_DP(h->D, h->cfg.pred, CU(launch_k(k_count<D, PRED, false>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
+    DISPATCH_DP(g.D, g.pred, CU(launch_k(k_count<D, PRED, false>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
   }
   if (kev) CU(cudaEventRecord(kev[4], st));
   CU(launch_k(k_compact, dim3((unsigned)((W + CMP_TILE - 1) / CMP_TILE), gy), 256, st, b));
   if (kev) CU(cudaEventRecord(kev[5], st));
-  h->launches += 5;
-  if (h->cfg.router) {
+  launched += 5;
+  if (g.route) {
     // Online training on the counts of this batch (one block; it returns at
     // once until enough samples are buffered).
     cudaLaunchConfig_t cfg = {};
@@ -441,11 +449,23 @@ int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev) 
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    CU(cudaLaunchKernelEx(&cfg, k_train, h->router));
-    h->launches += 1;
+    CU(cudaLaunchKernelEx(&cfg, k_train, g.router));
+    launched++;
   }
   if (kev) CU(cudaEventRecord(kev[6], st));
+  if (nk) *nk = launched;
   return RTOD_OK;
+}
+
+Geom geom_of(const rtod_handle* h) {
+  return Geom{h->W, h->S, h->D, h->cfg.pred, h->cfg.router, h->sm_count, h->block_warps, h->router};
+}
+
+int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev) {
+  int64_t nk = 0;
+  int r = launch_group(geom_of(h), b, ingest, h->stream, kev, &nk);
+  h->launches += nk;
+  return r;
 }
 
 // Runs one batch, replaying a captured graph when graphs are on.
@@ -1049,5 +1069,273 @@ RTOD_API int rtod_mlp_adam(int32_t device, float* params, float* m, float* v, in
   CU(cudaMemcpy(m, dm.p, sizeof(float) * MLP_P, cudaMemcpyDeviceToHost));
   CU(cudaMemcpy(v, dv.p, sizeof(float) * MLP_P, cudaMemcpyDeviceToHost));
   CU(cudaMemcpy(loss, dl.p, sizeof(float), cudaMemcpyDeviceToHost));
+  return RTOD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batched streams
+// ---------------------------------------------------------------------------
+
+struct rtod_batch {
+  int device = 0;
+  int n = 0;
+  int route = 0;
+  cudaStream_t stream = nullptr;
+  std::vector<rtod_handle*> hs;
+  struct Group {
+    Geom geom{};
+    std::vector<int> streams;
+    Job* jobs = nullptr;
+    BatchState* bs = nullptr;
+    int64_t* out = nullptr;
+    int64_t out_cap = 0;
+    int32_t* active = nullptr;    // device [n in group]
+    int32_t* active_h = nullptr;  // pinned host
+    int32_t* nout = nullptr;      // device [n in group]
+    int32_t* nout_h = nullptr;    // pinned host
+    BatchState* bs_h = nullptr;   // pinned host
+    int64_t cmp_tiles = 0;
+  };
+  std::vector<Group> groups;
+  RouterState* router = nullptr;
+  std::vector<char> filled, pending;
+  cudaGraphExec_t graph = nullptr;
+  int64_t steps = 0, launches = 0, detections = 0;
+};
+
+namespace {
+
+void batch_free(rtod_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (auto& g : b->groups) {
+    dfree(g.jobs); dfree(g.bs); dfree(g.out); dfree(g.active); dfree(g.nout);
+    if (g.active_h) cudaFreeHost(g.active_h);
+    if (g.nout_h) cudaFreeHost(g.nout_h);
+    if (g.bs_h) cudaFreeHost(g.bs_h);
+  }
+  dfree(b->router);
+  for (auto* h : b->hs)
+    if (h) rtod_destroy(h);
+  if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+Batch group_batch(const rtod_batch::Group& g, RouterState* router) {
+  Batch bt{};
+  bt.jobs = g.jobs;
+  bt.njobs = (int32_t)g.streams.size();
+  bt.bs = g.bs;
+  bt.router = router;
+  bt.out_ids = g.out;
+  bt.out_cap = g.out_cap;
+  bt.cmp_tiles = g.cmp_tiles;
+  bt.active = g.active;
+  bt.job_nout = g.nout;
+  return bt;
+}
+
+// One step for all groups: active flags in, counters reset, pipeline, counts out.
+int batch_enqueue(rtod_batch* b, int64_t* nk_total) {
+  int64_t total = 0;
+  for (auto& g : b->groups) {
+    const int ng = (int)g.streams.size();
+    CU(cudaMemcpyAsync(g.active, g.active_h, sizeof(int32_t) * ng, cudaMemcpyHostToDevice, b->stream));
+    CU(cudaMemsetAsync(&g.bs->out_total, 0, sizeof(int64_t), b->stream));
+    int64_t nk = 0;
+    int r = launch_group(g.geom, group_batch(g, b->router), true, b->stream, nullptr, &nk);
+    if (r) return r;
+    total += nk;
+    CU(cudaMemcpyAsync(g.nout_h, g.nout, sizeof(int32_t) * ng, cudaMemcpyDeviceToHost, b->stream));
+    CU(cudaMemcpyAsync(g.bs_h, g.bs, sizeof(BatchState), cudaMemcpyDeviceToHost, b->stream));
+  }
+  *nk_total = total;
+  return RTOD_OK;
+}
+
+}  // namespace
+
+RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_batch** out) {
+  if (!cfgs || !out || n_streams < 1 || n_streams > 4096) return fail(RTOD_ERR_ARG, "bad argument");
+  *out = nullptr;
+  for (int i = 0; i < n_streams; ++i) {
+    int r = check_config(&cfgs[i]);
+    if (r) return r;
+    if (cfgs[i].device != cfgs[0].device) return fail(RTOD_ERR_CONFIG, "all streams must use one device");
+  }
+  rtod_batch* b = new (std::nothrow) rtod_batch();
+  if (!b) return fail(RTOD_ERR_ARG, "out of host memory");
+  b->device = cfgs[0].device;
+  b->n = n_streams;
+  b->route = cfgs[0].router ? 1 : 0;
+  b->filled.assign(n_streams, 0);
+  b->pending.assign(n_streams, 0);
+  auto bail = [&](int code) {
+    std::string msg = g_last_error;
+    batch_free(b);
+    delete b;
+    g_last_error = msg;
+    return code;
+  };
+  for (int i = 0; i < n_streams; ++i) {
+    rtod_config c = cfgs[i];
+    c.batch = 1;
+    c.router = b->route;
+    c.use_graph = 0;
+    rtod_handle* h = nullptr;
+    int r = rtod_create(&c, &h);
+    if (r) return bail(r);
+    b->hs.push_back(h);
+  }
+  if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking))
+    return bail(fail(RTOD_ERR_CUDA, "stream creation failed"));
+  int64_t dummy = 0;
+  if (dalloc(&b->router, 1, &dummy)) return bail(RTOD_ERR_CUDA);
+  {
+    RouterState* init = new (std::nothrow) RouterState;
+    if (!init) return bail(fail(RTOD_ERR_ARG, "out of host memory"));
+    init_router(init);
+    cudaError_t e = cudaMemcpy(b->router, init, sizeof(RouterState), cudaMemcpyHostToDevice);
+    delete init;
+    if (e != cudaSuccess) return bail(fail(RTOD_ERR_CUDA, "router init failed"));
+  }
+  // Group the streams by (dimension, predicate).
+  for (int i = 0; i < n_streams; ++i) {
+    const rtod_handle* h = b->hs[i];
+    rtod_batch::Group* g = nullptr;
+    for (auto& x : b->groups)
+      if (x.geom.D == h->D && x.geom.pred == h->cfg.pred) g = &x;
+    if (!g) {
+      b->groups.emplace_back();
+      g = &b->groups.back();
+      g->geom = Geom{0, 0, h->D, h->cfg.pred, b->route, h->sm_count, h->block_warps, b->router};
+    }
+    g->streams.push_back(i);
+    g->geom.Wmax = std::max(g->geom.Wmax, h->W);
+    g->geom.Smax = std::max(g->geom.Smax, h->S);
+  }
+  for (auto& g : b->groups) {
+    const int ng = (int)g.streams.size();
+    std::vector<Job> tab(ng);
+    for (int k = 0; k < ng; ++k) {
+      rtod_handle* h = b->hs[g.streams[k]];
+      tab[k] = make_job(h, 0, true, nullptr);
+      g.out_cap += h->W;
+      g.cmp_tiles += (h->W + CMP_TILE - 1) / CMP_TILE;
+    }
+    if (dalloc(&g.jobs, ng, &dummy) || dalloc(&g.bs, 1, &dummy) || dalloc(&g.out, (size_t)g.out_cap, &dummy) ||
+        dalloc(&g.active, ng, &dummy) || dalloc(&g.nout, ng, &dummy))
+      return bail(RTOD_ERR_CUDA);
+    if (cudaMallocHost((void**)&g.active_h, sizeof(int32_t) * ng) || cudaMallocHost((void**)&g.nout_h, sizeof(int32_t) * ng) ||
+        cudaMallocHost((void**)&g.bs_h, sizeof(BatchState)))
+      return bail(fail(RTOD_ERR_CUDA, "pinned allocation failed"));
+    if (cudaMemcpy(g.jobs, tab.data(), sizeof(Job) * ng, cudaMemcpyHostToDevice) ||
+        cudaMemset(g.bs, 0, sizeof(BatchState)))
+      return bail(fail(RTOD_ERR_CUDA, "group setup failed"));
+  }
+  *out = b;
+  return RTOD_OK;
+}
+
+RTOD_API void rtod_batch_destroy(rtod_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  batch_free(b);
+  delete b;
+}
+
+RTOD_API int rtod_batch_push(rtod_batch* b, int32_t s, const float* pts, int64_t n) {
+  if (!b || !pts || s < 0 || s >= b->n) return fail(RTOD_ERR_ARG, "bad argument");
+  rtod_handle* h = b->hs[s];
+  CU(cudaSetDevice(b->device));
+  if (!b->filled[s]) {
+    int r = rtod_push_slide(h, pts, n);  // first push: exactly W points, fills the ring
+    if (r) return r;
+    b->filled[s] = 1;
+    return RTOD_OK;
+  }
+  if (b->pending[s]) return fail(RTOD_ERR_STATE, "stream %d already has a pending slide", s);
+  if (n != h->S) return fail(RTOD_ERR_STATE, "stream %d: a slide push must hold exactly S=%lld points", s,
+                             (long long)h->S);
+  CU(cudaMemcpyAsync(h->staging, pts, (size_t)(n * h->D) * sizeof(float), cudaMemcpyDefault, b->stream));
+  b->pending[s] = 1;
+  return RTOD_OK;
+}
+
+RTOD_API int rtod_batch_step(rtod_batch* b, int64_t* out_offsets, int64_t* out_ids, int64_t cap, int64_t* n_total) {
+  if (!b || !out_offsets || !n_total || (cap > 0 && !out_ids)) return fail(RTOD_ERR_ARG, "null argument");
+  CU(cudaSetDevice(b->device));
+  int any = 0;
+  for (auto& g : b->groups)
+    for (size_t k = 0; k < g.streams.size(); ++k) {
+      g.active_h[k] = b->pending[g.streams[k]] ? 1 : 0;
+      any |= g.active_h[k];
+    }
+  if (!any) return fail(RTOD_ERR_STATE, "no stream has a pushed slide");
+  int64_t nk = 0;
+  if (!b->graph) {
+    cudaGraph_t gr;
+    CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int r = batch_enqueue(b, &nk);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
+    if (r) return r;
+    if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+    b->launches -= nk;  // counted again below
+  } else {
+    for (auto& g : b->groups) nk += 6 + (b->route ? 1 : 0);
+  }
+  CU(cudaGraphLaunch(b->graph, b->stream));
+  CU(cudaStreamSynchronize(b->stream));
+  b->launches += nk;
+  b->steps++;
+  // Per-stream counts and errors, then the IDs group by group.
+  std::vector<int64_t> cnt(b->n, 0);
+  std::vector<int64_t> start(b->n, 0);  // offset of the stream's IDs inside its group output
+  for (auto& g : b->groups) {
+    rtod_handle* h0 = b->hs[g.streams[0]];
+    int r = check_device_error(h0, *g.bs_h);
+    if (r) {
+      for (int s : g.streams) b->hs[s]->poisoned = true;
+      return r;
+    }
+    int64_t off = 0;
+    for (size_t k = 0; k < g.streams.size(); ++k) {
+      const int s = g.streams[k];
+      cnt[s] = g.active_h[k] ? g.nout_h[k] : 0;
+      start[s] = off;
+      off += cnt[s];
+    }
+  }
+  out_offsets[0] = 0;
+  for (int s = 0; s < b->n; ++s) out_offsets[s + 1] = out_offsets[s] + cnt[s];
+  *n_total = out_offsets[b->n];
+  if (*n_total > cap) return fail(RTOD_ERR_CAPACITY, "%lld outliers but room for %lld", (long long)*n_total,
+                                  (long long)cap);
+  for (auto& g : b->groups) {
+    for (size_t k = 0; k < g.streams.size(); ++k) {
+      const int s = g.streams[k];
+      if (cnt[s] > 0)
+        CU(cudaMemcpyAsync(out_ids + out_offsets[s], g.out + start[s], sizeof(int64_t) * cnt[s], cudaMemcpyDefault,
+                           b->stream));
+    }
+  }
+  CU(cudaStreamSynchronize(b->stream));
+  for (int s = 0; s < b->n; ++s)
+    if (b->pending[s]) {
+      b->pending[s] = 0;
+      b->hs[s]->slides_done++;
+      b->detections++;
+    }
+  return RTOD_OK;
+}
+
+RTOD_API int rtod_batch_stats(const rtod_batch* b, int64_t out[4]) {
+  if (!b || !out) return fail(RTOD_ERR_ARG, "null argument");
+  out[0] = b->steps;
+  out[1] = b->launches;
+  out[2] = b->detections;
+  out[3] = (int64_t)b->groups.size();
   return RTOD_OK;
 }

@@ -194,3 +194,67 @@ class Detector:
     def ring_slots(self, ids: np.ndarray) -> np.ndarray:
         """RTOD's outlier IDs (ring slots, optixScan.cpp:1097) for global indices."""
         return np.asarray(ids, np.int64) % self.window
+
+
+class BatchDetector:
+    """Many independent streams advanced together, one slide per step; each
+    step detects every stream that was pushed a slide, in one replay of a
+    captured CUDA graph (streams grouped by dimension and predicate).
+
+    ``streams`` is a list of dicts with the Detector parameters (window,
+    slide, R, K, dim, opt, pred); ``router`` switches the shared learned
+    router on for all of them."""
+
+    def __init__(self, streams, router: bool = False, device: int = 0):
+        n = len(streams)
+        cfgs = (Config * n)()
+        for i, st in enumerate(streams):
+            check(lib().rtod_config_init(ctypes.byref(cfgs[i])))
+            c = cfgs[i]
+            c.window, c.slide, c.R, c.K = st["window"], st["slide"], st["R"], st["K"]
+            c.dim, c.opt = st.get("dim", 1), st.get("opt", 2)
+            c.pred = _native.PRED[st.get("pred", "fp32_le")]
+            c.router, c.device = int(router), device
+        self.streams = [dict(s) for s in streams]
+        self._b = ctypes.c_void_p()
+        check(lib().rtod_batch_create(cfgs, n, ctypes.byref(self._b)))
+        self._cap = sum(int(s["window"]) for s in streams)
+        self._out = np.empty(self._cap, np.int64)
+
+    def close(self) -> None:
+        if self._b:
+            lib().rtod_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def push(self, s: int, points) -> None:
+        ptr, n, keep = _as_points(points, int(self.streams[s].get("dim", 1)))
+        check(lib().rtod_batch_push(self._b, s, ptr, n))
+        del keep
+
+    def step(self):
+        """Per-stream sorted outlier IDs of this step (empty for streams that
+        sat the step out)."""
+        off = np.zeros(len(self.streams) + 1, np.int64)
+        n = ctypes.c_int64()
+        check(lib().rtod_batch_step(self._b, off.ctypes.data_as(ctypes.c_void_p),
+                                    self._out.ctypes.data_as(ctypes.c_void_p), self._cap,
+                                    ctypes.byref(n)))
+        return [self._out[off[i]:off[i + 1]].copy() for i in range(len(self.streams))]
+
+    @property
+    def stats(self) -> dict:
+        a = (ctypes.c_int64 * 4)()
+        check(lib().rtod_batch_stats(self._b, a))
+        return {"steps": a[0], "launches": a[1], "detections": a[2], "groups": a[3]}

@@ -1,0 +1,74 @@
+"""Batched streams (many uneven streams advanced together, one graph replay
+per step) against the CPU oracle, stream by stream, slide by slide."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def rtod():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from rtod_b200 import build
+    build.build()
+    import rtod_b200
+    return rtod_b200
+
+
+def make_streams(n=9, seed=5):
+    from rtod_b200 import datagen
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        d = [1, 3, 8][i % 3]
+        W = int(rng.choice([2000, 3000, 5000, 8000]))
+        S = W // int(rng.choice([4, 10, 20]))
+        slides = 12
+        if rng.random() < 0.5:
+            pts = datagen.random_walk(W + slides * S, 0.1, seed=100 + i, dim=d)
+        else:
+            pts = datagen.gaussian_mixture(W + slides * S, seed=100 + i, dim=d)
+        R = {1: 0.05, 3: 0.3, 8: 0.6}[d] if i % 2 else {1: 0.02, 3: 0.2, 8: 0.5}[d]
+        out.append(dict(window=W, slide=S, R=R, K=10 + i, dim=d, points=pts, slides=slides,
+                        pred="f64_lt" if i == 4 else "fp32_le"))
+    return out
+
+
+@pytest.mark.parametrize("router", [False, True])
+def test_batch_matches_oracle(rtod, oracle_mod, router):
+    streams = make_streams()
+    expect = []
+    for st in streams:
+        off, ids, _ = oracle_mod.detect(st["points"], st["window"], st["slide"], st["R"], st["K"],
+                                        st["pred"], engine="grid", threads=4)
+        expect.append((off, ids))
+    cfg = [{k: st[k] for k in ("window", "slide", "R", "K", "dim", "pred")} for st in streams]
+    with rtod.BatchDetector(cfg, router=router) as bd:
+        for i, st in enumerate(streams):
+            bd.push(i, st["points"][:st["window"]])
+        done = [0] * len(streams)
+        for step in range(14):
+            for i, st in enumerate(streams):
+                # stream 2 sits out every third step; all stop after their slides
+                if done[i] < st["slides"] and not (i == 2 and step % 3 == 1):
+                    W, S = st["window"], st["slide"]
+                    bd.push(i, st["points"][W + done[i] * S:W + (done[i] + 1) * S])
+            pushed = [done[i] < st["slides"] and not (i == 2 and step % 3 == 1)
+                      for i, st in enumerate(streams)]
+            if not any(pushed):
+                break
+            res = bd.step()
+            for i, st in enumerate(streams):
+                if pushed[i]:
+                    off, ids = expect[i]
+                    j = done[i]
+                    np.testing.assert_array_equal(res[i], ids[off[j]:off[j + 1]])
+                    done[i] += 1
+                else:
+                    assert res[i].size == 0
+        assert all(done[i] == st["slides"] for i, st in enumerate(streams))
+        stats = bd.stats
+        assert stats["groups"] == 4  # d=1, d=3, d=8 with fp32, and the f64 stream
+        assert stats["detections"] == sum(st["slides"] for st in streams)
