@@ -253,6 +253,7 @@ def run_ours(args, world, rank, local):
             # per-kernel device time of one pass (diagnostic, individual launches)
             det.reset()
             out["prof"] = det.profile(pts_dev)
+            out["tuning"] = det.tuning
             if kw.get("router"):
                 info = det.router_info()
                 out["router"] = {k: info[k] for k in ("steps", "last_loss", "routed_early",
@@ -262,7 +263,7 @@ def run_ours(args, world, rank, local):
 
     results = {
         # headline: learned router on, B consecutive windows per launch, graph replay
-        "routed_batched": measure(dict(router=True), args.steps, True),
+        "routed_batched": measure(dict(router=True, tuner=True), args.steps, True),
         # the plain grid kernel: one window per launch (graph replay per slide), no router
         "plain": measure(dict(router=False, batch=1), args.steps, False),
         # batching without the router (isolates the router's share)
@@ -313,7 +314,7 @@ def emit_ours(args, world, w, res):
         "window_points_per_s": world * K * slides * w.window / t_s,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded stand-in for RTOD's STK stream)",
-        "config": workload_config(w, {"engine": "learned-routed batched engine (router on, "
+        "config": workload_config(w, {"engine": "learned-routed batched engine (router on, autotuned, "
                                                  "consecutive windows per launch, graph replay)"}),
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
@@ -327,6 +328,7 @@ def emit_ours(args, world, w, res):
                 "us_per_slide": r["e2e_s"] / (r["e2e_steps"] * slides) * 1e6},
         "outliers_per_slide": n_out, "undetermined_per_slide": r["undet"],
         "router": r.get("router"),
+        "tuning": r.get("tuning"),
         "engines": {name: {"us_per_slide": e["dev_ms"] * 1e3 / (e["steps"] * slides),
                            "points_per_s": world * e["steps"] * slides * w.slide / (e["dev_ms"] / 1e3),
                            "gpu_launches_per_step": e["launches"] / e["steps"]}

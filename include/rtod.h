@@ -63,7 +63,8 @@ typedef struct rtod_config {
   int32_t router;      /* 1 = learned router on (routes counted points into an early-exit
                           and a full-sweep queue); results are identical either way */
   int32_t tuner;       /* 1 = autotune cell width and block shape on the first slides */
-  int32_t cells_per_r; /* grid cells per R along each hashed dimension (1..3; 0 = auto) */
+  int32_t cells_per_r; /* grid cells per R along each hashed dimension (1..3, 1..8 in 1-d;
+                          0 = auto) */
   int32_t block_warps; /* warps per block of the range-count kernel (1, 2, 4, 8; 0 = auto) */
   int32_t use_graph;   /* 1 = replay each launch sequence as a captured CUDA graph */
   int32_t device;      /* CUDA device ordinal */
@@ -129,8 +130,13 @@ int64_t rtod_slides_done(const rtod_handle* h);
 
 /* The resolved grid and launch parameters (after autotuning, if on):
    out[0] cells per R, out[1] warps per block of the range count,
-   out[2] hashed dimensions. */
-int rtod_get_tuning(const rtod_handle* h, int32_t out[3]);
+   out[2] hashed dimensions, out[3] windows per rtod_run launch.
+   With rtod_config.tuner = 1 the first rtod_run times candidate settings
+   (cells per R 1..3 or up to 6 in 1-d, 2/4/8 warps per block, 8..64 windows per launch and,
+   with the router on, its routing threshold and full-sweep size limit) on a
+   prefix of the stream and keeps the fastest; the choice is cached per
+   configuration for the rest of the process. Results do not depend on it. */
+int rtod_get_tuning(const rtod_handle* h, int32_t out[4]);
 
 /* Counters since create: out[0] kernel launches issued by the library (a
    graph replay counts each of its kernels), out[1] graph replays, out[2]

@@ -171,7 +171,7 @@ __device__ __forceinline__ void unpack_key(uint64_t key, int h, int64_t* k) {
 
 // Bin of a cell. Consecutive cells along the last hashed dimension land in
 // consecutive bins (mod NB), so a stencil row of 2n+1 cells is one run of
-// bins; rows of one stencil never share a bin for n <= 3.
+// bins; rows of one stencil never share a bin for n <= 3 (1-d: any n).
 __device__ __forceinline__ uint32_t bin_of(const int64_t* k, int h) {
   if (h == 1) return (uint32_t)k[0] & NB_MASK;
   if (h == 2) return ((uint32_t)k[1] + ((uint32_t)k[0] << 8)) & NB_MASK;
@@ -419,32 +419,47 @@ __global__ void __launch_bounds__(256) k_ingest(Batch b, int32_t fill) {
 // holds a single cell iff they are equal), warp-aggregated, with atomics
 // whose results are not needed (no round trip on the critical path).
 // ---------------------------------------------------------------------------
+// Points handled per lane per loop iteration by k_hist and k_scatter: their
+// loads and atomics are all issued before any result is used.
+template <int D>
+struct Unroll {
+  static constexpr int value = D <= 3 ? 4 : 2;
+};
+
 template <int D>
 __global__ void __launch_bounds__(256) k_hist(Batch b) {
   pdl_trigger();
   pdl_wait();
   if (!job_active(b)) return;
   constexpr int H = Hashed<D>::value;
+  constexpr int U = Unroll<D>::value;
   const Job& jb = b.jobs[blockIdx.y];
   const int64_t lo = jb.ctr->lo;
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t w0 = warp * 32; w0 < jb.W; w0 += nwarps * 32) {
-    const int64_t i = w0 + lane;
-    const bool valid = i < jb.W;
-    const uint64_t key = valid ? jb.keys[source_pos(jb, lo, i)] : EMPTY_KEY;
-    const uint32_t bin = valid ? bin_of_key(key, H) : 0xffffffffu;
-    const unsigned peers = __match_any_sync(0xffffffffu, bin);
-    const int leader = __ffs(peers) - 1;
-    const uint64_t lkey = __shfl_sync(0xffffffffu, key, leader);
-    if (valid && lane == leader) {
-      atomicAdd(&jb.bin_count[bin], (uint32_t)__popc(peers));
-      atomicMin(&jb.kmin[bin], (unsigned long long)key);
-      atomicMax(&jb.kmax[bin], (unsigned long long)key);
-    } else if (valid && key != lkey) {
-      atomicMin(&jb.kmin[bin], (unsigned long long)key);
-      atomicMax(&jb.kmax[bin], (unsigned long long)key);
+  for (int64_t w0 = warp * 32 * U; w0 < jb.W; w0 += nwarps * 32 * U) {
+    uint64_t key[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = w0 + u * 32 + lane;
+      key[u] = i < jb.W ? jb.keys[source_pos(jb, lo, i)] : EMPTY_KEY;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const bool valid = key[u] != EMPTY_KEY;
+      const uint32_t bin = valid ? bin_of_key(key[u], H) : 0xffffffffu;
+      const unsigned peers = __match_any_sync(0xffffffffu, bin);
+      const int leader = __ffs(peers) - 1;
+      const uint64_t lkey = __shfl_sync(0xffffffffu, key[u], leader);
+      if (valid && lane == leader) {
+        atomicAdd(&jb.bin_count[bin], (uint32_t)__popc(peers));
+        atomicMin(&jb.kmin[bin], (unsigned long long)key[u]);
+        atomicMax(&jb.kmax[bin], (unsigned long long)key[u]);
+      } else if (valid && key[u] != lkey) {
+        atomicMin(&jb.kmin[bin], (unsigned long long)key[u]);
+        atomicMax(&jb.kmax[bin], (unsigned long long)key[u]);
+      }
     }
   }
 }
@@ -533,12 +548,48 @@ __device__ __forceinline__ bool for_each_run(const uint32_t* bin_start, const in
 // positions are claimed with atomicSub so the bin counts end at zero),
 // safe-inlier classification and the query queue.
 // ---------------------------------------------------------------------------
+// 1-d group filter. With cells of R(1+2^-12)/n, any n-1 consecutive cells
+// span less than R (with the same margin argument as one cell for n = 2),
+// so a point is an inlier if some run of n-1 consecutive cells containing its
+// cell holds more than K points, provided every bin of the run holds exactly
+// its expected cell (or nothing). Returns true when such a run exists.
+__device__ __forceinline__ bool group_safe_1d(const Job& jb, uint64_t key, uint32_t b) {
+  const int m = jb.n - 1;
+  if (m < 2 || b < (uint32_t)(m - 1) || b + m > NB - 1) return false;
+  constexpr int MMAX = 7;
+  uint32_t bs[2 * MMAX];
+  bool ok[2 * MMAX - 1];
+#pragma unroll
+  for (int t = 0; t < 2 * MMAX; ++t)
+    if (t < 2 * m) bs[t] = jb.bin_start[b - m + 1 + t];
+#pragma unroll
+  for (int t = 0; t < 2 * MMAX - 1; ++t) {
+    if (t < 2 * m - 1) {
+      const uint32_t j = b - m + 1 + t;
+      const unsigned long long want = key + (unsigned long long)(t - (m - 1));
+      ok[t] = bs[t + 1] == bs[t] || (jb.kmin[j] == want && jb.kmax[j] == want);
+    }
+  }
+#pragma unroll
+  for (int g = 0; g < MMAX; ++g) {
+    if (g < m) {
+      bool pure = true;
+#pragma unroll
+      for (int t = 0; t < MMAX; ++t)
+        if (t < m) pure &= ok[g + t];
+      if (pure && bs[g + m] - bs[g] > (uint32_t)jb.K) return true;
+    }
+  }
+  return false;
+}
+
 template <int D, bool ROUTE>
 __global__ void __launch_bounds__(256) k_scatter(Batch b) {
   pdl_trigger();
   pdl_wait();
   if (!job_active(b)) return;
   constexpr int H = Hashed<D>::value;
+  constexpr int U = Unroll<D>::value;
   const Job& jb = b.jobs[blockIdx.y];
   const int64_t lo = jb.ctr->lo;
   if (blockIdx.x == 0 && threadIdx.x < SCAN_TILES) jb.scan_status[threadIdx.x] = 0;
@@ -546,86 +597,107 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
   const unsigned lt = lanemask_lt();
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t w0 = warp * 32; w0 < jb.W; w0 += nwarps * 32) {
-    const int64_t i = w0 + lane;
-    const bool valid = i < jb.W;
-    const int64_t src = valid ? source_pos(jb, lo, i) : 0;
-    const uint64_t key = valid ? jb.keys[src] : EMPTY_KEY;
-    const uint32_t bin = valid ? bin_of_key(key, H) : 0xffffffffu;
-    const unsigned peers = __match_any_sync(0xffffffffu, bin);
-    const int leader = __ffs(peers) - 1;
-    const uint32_t c = (uint32_t)__popc(peers);
-    uint32_t top = 0;
-    if (valid && lane == leader) top = atomicSub(&jb.bin_count[bin], c);
-    top = __shfl_sync(0xffffffffu, top, leader);
-    bool safe = false;
-    uint32_t pos = 0, cnt = 0;
-    if (valid) {
-      const uint32_t bs0 = jb.bin_start[bin];
-      pos = bs0 + top - c + __popc(peers & lt);
-      float x[D];
-      load_point<D>(jb, src, x);
-      jb.s_off[pos] = (uint32_t)i;
-      jb.s_ckey[pos] = key;
+  for (int64_t w0 = warp * 32 * U; w0 < jb.W; w0 += nwarps * 32 * U) {
+    int64_t src[U];
+    uint64_t key[U];
+    uint32_t bin[U], top[U], peers[U];
+    int leader[U];
+    // 1. keys of U chunks
 #pragma unroll
-      for (int d = 0; d < D; ++d) jb.s_x[(int64_t)d * jb.Wp + pos] = x[d];
-      cnt = jb.bin_start[bin + 1] - bs0;
-      if (jb.filter) safe = cnt > (uint32_t)jb.K && jb.kmin[bin] == jb.kmax[bin];
-      if (safe) jb.prev[src] = 255;
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = w0 + u * 32 + lane;
+      src[u] = i < jb.W ? source_pos(jb, lo, i) : -1;
+      key[u] = src[u] >= 0 ? jb.keys[src[u]] : EMPTY_KEY;
     }
-    const bool need = valid && !safe;
-    bool sweep = false;
-    float f[MLP_IN] = {0.0f, 0.0f, 0.0f};
-    if constexpr (ROUTE) {
-      if (__any_sync(0xffffffffu, need) && need) {
-        // Router features and prediction (one lane per point).
-        int64_t k[3];
-        unpack_key(key, H, k);
-        uint32_t stencil = 0;
-        for_each_run<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
-          stencil += re - rs;
-          return false;
-        });
-        f[0] = log2f(1.0f + (float)cnt) * 0.125f;
-        f[1] = log2f(1.0f + (float)stencil) * 0.125f;
-        f[2] = prev_feature(jb.prev[src], jb.K);
-        float z[MLP_B];
-        mlp_forward(b.router->params, f, z);
-        sweep = stencil <= b.router->max_sweep && p_inlier(z) < b.router->threshold;
+    // 2. claim positions (U independent atomics in flight)
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      bin[u] = src[u] >= 0 ? bin_of_key(key[u], H) : 0xffffffffu;
+      peers[u] = __match_any_sync(0xffffffffu, bin[u]);
+      leader[u] = __ffs(peers[u]) - 1;
+      top[u] = 0;
+      if (src[u] >= 0 && lane == leader[u]) top[u] = atomicSub(&jb.bin_count[bin[u]], (uint32_t)__popc(peers[u]));
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      top[u] = __shfl_sync(0xffffffffu, top[u], leader[u]);
+      const bool valid = src[u] >= 0;
+      const int64_t i = w0 + u * 32 + lane;
+      bool safe = false;
+      uint32_t pos = 0, cnt = 0;
+      if (valid) {
+        const uint32_t bs0 = jb.bin_start[bin[u]];
+        const uint32_t bs1 = jb.bin_start[bin[u] + 1];
+        pos = bs0 + top[u] - (uint32_t)__popc(peers[u]) + __popc(peers[u] & lt);
+        float x[D];
+        load_point<D>(jb, src[u], x);
+        jb.s_off[pos] = (uint32_t)i;
+        jb.s_ckey[pos] = key[u];
+#pragma unroll
+        for (int d = 0; d < D; ++d) jb.s_x[(int64_t)d * jb.Wp + pos] = x[d];
+        cnt = bs1 - bs0;
+        if (jb.filter) {
+          safe = cnt > (uint32_t)jb.K && jb.kmin[bin[u]] == jb.kmax[bin[u]];
+          if constexpr (H == 1) {
+            if (!safe && jb.n >= 3) safe = group_safe_1d(jb, key[u], bin[u]);
+          }
+        }
+        if (safe) jb.prev[src[u]] = 255;
       }
-    }
-    const unsigned need_e = __ballot_sync(0xffffffffu, need && !sweep);
-    if (need_e) {
-      uint32_t qb = 0;
-      const int ql = __ffs(need_e) - 1;
-      if (lane == ql) qb = (uint32_t)atomicAdd(&jb.ctr->n_undet, __popc(need_e));
-      qb = __shfl_sync(0xffffffffu, qb, ql);
-      if (need && !sweep) {
-        const uint32_t q = qb + __popc(need_e & lt);
-        jb.queue[q] = pos;
-        if constexpr (ROUTE) {
-#pragma unroll
-          for (int j = 0; j < MLP_IN; ++j) jb.feat[(int64_t)q * MLP_IN + j] = f[j];
+      const bool need = valid && !safe;
+      bool sweep = false;
+      float f[MLP_IN] = {0.0f, 0.0f, 0.0f};
+      if constexpr (ROUTE) {
+        if (__any_sync(0xffffffffu, need) && need) {
+          // Router features and prediction (one lane per point).
+          int64_t k[3];
+          unpack_key(key[u], H, k);
+          uint32_t stencil = 0;
+          for_each_run<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
+            stencil += re - rs;
+            return false;
+          });
+          f[0] = log2f(1.0f + (float)cnt) * 0.125f;
+          f[1] = log2f(1.0f + (float)stencil) * 0.125f;
+          f[2] = prev_feature(jb.prev[src[u]], jb.K);
+          float z[MLP_B];
+          mlp_forward(b.router->params, f, z);
+          sweep = stencil <= b.router->max_sweep && p_inlier(z) < b.router->threshold;
         }
       }
-    }
-    if constexpr (ROUTE) {
-      const unsigned need_s = __ballot_sync(0xffffffffu, sweep);
-      if (need_s) {
+      const unsigned need_e = __ballot_sync(0xffffffffu, need && !sweep);
+      if (need_e) {
         uint32_t qb = 0;
-        const int ql = __ffs(need_s) - 1;
-        if (lane == ql) qb = (uint32_t)atomicAdd(&jb.ctr->n_sweep, __popc(need_s));
+        const int ql = __ffs(need_e) - 1;
+        if (lane == ql) qb = (uint32_t)atomicAdd(&jb.ctr->n_undet, __popc(need_e));
         qb = __shfl_sync(0xffffffffu, qb, ql);
-        if (sweep) {
-          const uint32_t q = (uint32_t)jb.W - 1 - (qb + __popc(need_s & lt));
+        if (need && !sweep) {
+          const uint32_t q = qb + __popc(need_e & lt);
           jb.queue[q] = pos;
+          if constexpr (ROUTE) {
 #pragma unroll
-          for (int j = 0; j < MLP_IN; ++j) jb.feat[(int64_t)q * MLP_IN + j] = f[j];
+            for (int j = 0; j < MLP_IN; ++j) jb.feat[(int64_t)q * MLP_IN + j] = f[j];
+          }
         }
       }
-      if (lane == 0 && (need_e || need_s)) {
-        atomicAdd(&b.router->routed_early, (unsigned long long)__popc(need_e));
-        atomicAdd(&b.router->routed_sweep, (unsigned long long)__popc(need_s));
+      if constexpr (ROUTE) {
+        const unsigned need_s = __ballot_sync(0xffffffffu, sweep);
+        if (need_s) {
+          uint32_t qb = 0;
+          const int ql = __ffs(need_s) - 1;
+          if (lane == ql) qb = (uint32_t)atomicAdd(&jb.ctr->n_sweep, __popc(need_s));
+          qb = __shfl_sync(0xffffffffu, qb, ql);
+          if (sweep) {
+            const uint32_t q = (uint32_t)jb.W - 1 - (qb + __popc(need_s & lt));
+            jb.queue[q] = pos;
+#pragma unroll
+            for (int j = 0; j < MLP_IN; ++j) jb.feat[(int64_t)q * MLP_IN + j] = f[j];
+          }
+        }
+        if (lane == 0 && (need_e || need_s)) {
+          atomicAdd(&b.router->routed_early, (unsigned long long)__popc(need_e));
+          atomicAdd(&b.router->routed_sweep, (unsigned long long)__popc(need_s));
+        }
       }
     }
   }

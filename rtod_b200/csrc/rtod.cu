@@ -12,6 +12,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cstddef>
+#include <mutex>
 #include <new>
 #include <string>
 #include <utility>
@@ -232,6 +234,9 @@ struct rtod_handle {
   int64_t launches = 0;
   int64_t graph_replays = 0;
   int64_t undet_total = 0;
+  bool tuned = false;
+  float threshold = 0.5f;
+  uint32_t max_sweep = 64;
 };
 
 namespace {
@@ -252,7 +257,8 @@ int check_config(const rtod_config* c) {
   if (c->opt < 0 || c->opt > 2) return fail(RTOD_ERR_CONFIG, "opt must be 0, 1 or 2");
   if (c->pred != RTOD_PRED_FP32_LE && c->pred != RTOD_PRED_F64_LT)
     return fail(RTOD_ERR_CONFIG, "unknown predicate %d", c->pred);
-  if (c->cells_per_r < 0 || c->cells_per_r > 3) return fail(RTOD_ERR_CONFIG, "cells_per_r must be 0..3");
+  if (c->cells_per_r < 0 || c->cells_per_r > (c->dim == 1 ? 8 : 3))
+    return fail(RTOD_ERR_CONFIG, "cells_per_r must be 0..3 (0..8 in 1-d)");
   if (c->block_warps != 0 && c->block_warps != 1 && c->block_warps != 2 && c->block_warps != 4 &&
       c->block_warps != 8)
     return fail(RTOD_ERR_CONFIG, "block_warps must be 0 (auto), 1, 2, 4 or 8");
@@ -413,8 +419,9 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, cudaStream_t st, cu
     launched++;
   }
   if (kev) CU(cudaEventRecord(kev[0], st));
+  const int64_t per_block = 256 * (g.D <= 3 ? 4 : 2);  // points per block per loop iteration
   const int64_t wx = std::max<int64_t>(
-      1, std::min<int64_t>((W + 255) / 256, std::max<int64_t>(2, (g.sm_count * 16 + nj - 1) / nj)));
+      1, std::min<int64_t>((W + per_block - 1) / per_block, std::max<int64_t>(2, (g.sm_count * 16 + nj - 1) / nj)));
   DISPATCH_D(g.D, CU(launch_k(k_hist<D>, dim3((unsigned)wx, gy), 256, st, b)));
   if (kev) CU(cudaEventRecord(kev[1], st));
   CU(launch_k(k_scan, dim3(SCAN_TILES, gy), 256, st, b));
@@ -659,6 +666,150 @@ void free_all(rtod_handle* h) {
 
 }  // namespace
 
+namespace {
+
+// ---------------------------------------------------------------------------
+// Autotuner: coordinate descent over the launch and grid parameters, each
+// candidate timed (CUDA events, second of two passes) on a prefix of the
+// stream. Results never depend on these parameters; only the time does.
+// The best setting is cached per configuration for the rest of the process.
+// ---------------------------------------------------------------------------
+struct Tuning {
+  int n = 2;
+  int block_warps = 8;
+  int batch = 32;
+  float threshold = 0.5f;
+  uint32_t max_sweep = 64;
+};
+
+struct TuneEntry {
+  rtod_config cfg;
+  Tuning t;
+};
+
+std::mutex g_tune_mu;
+std::vector<TuneEntry> g_tune_cache;
+
+bool same_problem(const rtod_config& a, const rtod_config& b) {
+  return a.window == b.window && a.slide == b.slide && a.R == b.R && a.K == b.K && a.dim == b.dim &&
+         a.opt == b.opt && a.pred == b.pred && a.router == b.router && a.device == b.device;
+}
+
+int apply_tuning(rtod_handle* h, const Tuning& t) {
+  set_grid(h, t.n);
+  h->block_warps = t.block_warps;
+  h->cfg.batch = std::min(t.batch, h->batch_max);
+  h->threshold = t.threshold;
+  h->max_sweep = t.max_sweep;
+  if (h->router) {
+    CU(cudaMemcpy((char*)h->router + offsetof(RouterState, threshold), &t.threshold, sizeof(float),
+                  cudaMemcpyHostToDevice));
+    CU(cudaMemcpy((char*)h->router + offsetof(RouterState, max_sweep), &t.max_sweep, sizeof(uint32_t),
+                  cudaMemcpyHostToDevice));
+  }
+  drop_graph(h);
+  return RTOD_OK;
+}
+
+// Device ms of one pass over `slides` slides of a device-resident stream.
+int time_pass(rtod_handle* h, const float* dev_pts, int64_t slides, float* ms) {
+  EventSet es;
+  cudaEvent_t a = es.make(), b = es.make();
+  float best = 1e30f;
+  for (int rep = 0; rep < 2; ++rep) {
+    int r = reset_state(h);
+    if (r) return r;
+    BatchState s{};
+    std::vector<int32_t> nout, nund;
+    CU(cudaEventRecord(a, h->stream));
+    r = run_stream(h, dev_pts, slides, slides * h->W, nullptr, nullptr, nullptr, &s, &nout, &nund);
+    if (r) return r;
+    CU(cudaEventRecord(b, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    best = std::min(best, elapsed(a, b));
+  }
+  *ms = best;
+  return RTOD_OK;
+}
+
+int autotune(rtod_handle* h, const float* pts, int64_t slides_total) {
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (const auto& e : g_tune_cache)
+      if (same_problem(e.cfg, h->cfg)) {
+        h->tuned = true;
+        return apply_tuning(h, e.t);
+      }
+  }
+  const int64_t W = h->W, S = h->S, D = h->D;
+  const int64_t slides = std::min<int64_t>(slides_total, 96);
+  const int64_t used = W + slides * S;
+  // A private device copy of the prefix, so that trials never touch the caller's stream buffers.
+  float* dev = nullptr;
+  CU(cudaMalloc((void**)&dev, (size_t)(used * D) * sizeof(float)));
+  struct Free {
+    float* p;
+    ~Free() { cudaFree(p); }
+  } fr{dev};
+  CU(cudaMemcpy(dev, pts, (size_t)(used * D) * sizeof(float), cudaMemcpyDefault));
+  Tuning best;
+  best.batch = std::min(32, h->batch_max);
+  int r = apply_tuning(h, best);
+  if (r) return r;
+  float best_ms;
+  if ((r = time_pass(h, dev, slides, &best_ms))) return r;
+  auto trial = [&](Tuning t) -> int {
+    int rr = apply_tuning(h, t);
+    if (rr) return rr;
+    float ms;
+    if ((rr = time_pass(h, dev, slides, &ms))) return rr;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = t;
+    }
+    return RTOD_OK;
+  };
+  for (int n : {1, 3, 4, 6}) {
+    if (n > 3 && h->D != 1) continue;
+    Tuning t = best;
+    t.n = n;
+    if ((r = trial(t))) return r;
+  }
+  for (int bw : {2, 4}) {
+    Tuning t = best;
+    t.block_warps = bw;
+    if ((r = trial(t))) return r;
+  }
+  for (int bt : {8, 16, 64}) {
+    if (bt > h->batch_max) continue;
+    Tuning t = best;
+    t.batch = bt;
+    if ((r = trial(t))) return r;
+  }
+  if (h->cfg.router) {
+    for (float th : {0.3f, 0.7f}) {
+      Tuning t = best;
+      t.threshold = th;
+      if ((r = trial(t))) return r;
+    }
+    for (uint32_t ms : {32u, 128u}) {
+      Tuning t = best;
+      t.max_sweep = ms;
+      if ((r = trial(t))) return r;
+    }
+  }
+  if ((r = apply_tuning(h, best))) return r;
+  if ((r = reset_state(h))) return r;
+  CU(cudaStreamSynchronize(h->stream));
+  h->tuned = true;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache.push_back(TuneEntry{h->cfg, best});
+  g_tune_cache.back().cfg.batch = 0;
+  return RTOD_OK;
+}
+
+}  // namespace
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -771,11 +922,12 @@ RTOD_API int rtod_reset(rtod_handle* h) {
 
 RTOD_API int64_t rtod_slides_done(const rtod_handle* h) { return h ? h->slides_done : -1; }
 
-RTOD_API int rtod_get_tuning(const rtod_handle* h, int32_t out[3]) {
+RTOD_API int rtod_get_tuning(const rtod_handle* h, int32_t out[4]) {
   if (!h || !out) return fail(RTOD_ERR_ARG, "null argument");
   out[0] = h->n;
   out[1] = h->block_warps;
   out[2] = h->D < 3 ? h->D : 3;
+  out[3] = (int32_t)(h->cfg.batch ? std::min(h->cfg.batch, h->batch_max) : h->batch_max);
   return RTOD_OK;
 }
 
@@ -883,6 +1035,10 @@ RTOD_API int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_s
   const int64_t slides = count_slides(h, n, max_slides);
   *slides_out = slides;
   if (slides == 0) return RTOD_OK;
+  if (h->cfg.tuner && !h->tuned) {
+    int rt = autotune(h, pts, slides);
+    if (rt) return rt;
+  }
   EventSet es;
   cudaEvent_t t0 = es.make(), t1 = es.make(), t2 = es.make(), d0 = es.make(), d1 = es.make();
   // Stage split (only without graphs): events around every kernel of every batch.

@@ -187,9 +187,9 @@ class Detector:
 
     @property
     def tuning(self) -> dict:
-        a = (ctypes.c_int32 * 3)()
+        a = (ctypes.c_int32 * 4)()
         check(lib().rtod_get_tuning(self._h, a))
-        return {"cells_per_r": a[0], "block_warps": a[1], "hashed_dims": a[2]}
+        return {"cells_per_r": a[0], "block_warps": a[1], "hashed_dims": a[2], "batch": a[3]}
 
     def ring_slots(self, ids: np.ndarray) -> np.ndarray:
         """RTOD's outlier IDs (ring slots, optixScan.cpp:1097) for global indices."""

@@ -1,0 +1,51 @@
+"""The optixScan-compatible command line: flags, text formats and report."""
+import numpy as np
+import pytest
+
+from rtod_b200 import cli
+
+
+def test_flags_match_reference_surface():
+    ap = cli.build_parser()
+    a = ap.parse_args(["--n", "1048572", "--R", "0.45", "--K", "50", "--window", "100000",
+                       "--slide", "5000", "-f", "x.txt", "--start_copy_pos", "2",
+                       "--launch_ray_num", "7"])
+    assert (a.n, a.R, a.K, a.window, a.slide, a.file, a.start_copy_pos) == (
+        1048572, 0.45, 50, 100000, 5000, "x.txt", 2)
+    assert a.opt == 2 and a.warmup == 10 and a.max_slides == 10000
+
+
+def test_read_text_1d_and_3d(tmp_path):
+    p1 = tmp_path / "s.txt"
+    p1.write_text("1.5\n-2.25\n3\n4e-3\n")
+    x = cli.read_text(str(p1), 3, 1)
+    np.testing.assert_array_equal(x[:, 0], np.array([1.5, -2.25, 3.0], np.float32))
+    p3 = tmp_path / "t.txt"
+    p3.write_text("1,2,3\n4,5,6\n")
+    y = cli.read_text(str(p3), 10, 3)
+    assert y.shape == (2, 3) and y[1, 2] == 6.0
+
+
+@pytest.mark.gpu
+def test_cli_report_and_outliers(tmp_path, capsys, oracle_mod):
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from rtod_b200 import datagen
+    pts = datagen.random_walk(6000, 0.1, seed=3)
+    f = tmp_path / "walk.txt"
+    f.write_text("\n".join(repr(float(v)) for v in pts[:, 0]) + "\n")
+    rc = cli.main(["--n", "6000", "--R", "0.2", "--K", "8", "--window", "2000", "--slide", "200",
+                   "-f", str(f), "--warmup", "1", "--print-outliers"])
+    assert rc == 0
+    out = capsys.readouterr().out
+    for key in ("[Time] copy new points h2d", "[Time] prepare cell", "[Time] build BVH",
+                "[Time] detect outlier", "[Time] total time for a slide", "BVH Node / slide",
+                "[Mem] Device memory used for data(MB)", "Window size: 2000"):
+        assert key in out
+    off, ids, _ = oracle_mod.detect(pts, 2000, 200, 0.2, 8)
+    lines = [l for l in out.splitlines() if l.startswith("slide ")]
+    assert len(lines) == len(off) - 1
+    for j, line in enumerate(lines):
+        got = [int(t) for t in line.split(":", 1)[1].split()]
+        assert got == ids[off[j]:off[j + 1]].tolist()

@@ -49,7 +49,7 @@ def test_batch_matches_oracle(rtod, oracle_mod, router):
         for i, st in enumerate(streams):
             bd.push(i, st["points"][:st["window"]])
         done = [0] * len(streams)
-        for step in range(14):
+        for step in range(40):
             for i, st in enumerate(streams):
                 # stream 2 sits out every third step; all stop after their slides
                 if done[i] < st["slides"] and not (i == 2 and step % 3 == 1):
@@ -58,7 +58,7 @@ def test_batch_matches_oracle(rtod, oracle_mod, router):
             pushed = [done[i] < st["slides"] and not (i == 2 and step % 3 == 1)
                       for i, st in enumerate(streams)]
             if not any(pushed):
-                break
+                continue
             res = bd.step()
             for i, st in enumerate(streams):
                 if pushed[i]:

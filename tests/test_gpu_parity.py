@@ -96,7 +96,7 @@ def test_full_size_properties(rtod):
     w = datagen.stock_like()
     runs = []
     for kw in (dict(), dict(opt=0), dict(cells_per_r=1), dict(cells_per_r=3, use_graph=False),
-               dict(block_warps=2)):
+               dict(block_warps=2), dict(cells_per_r=4), dict(cells_per_r=7, batch=5)):
         with rtod.Detector(w.window, w.slide, w.R, w.K, **kw) as det:
             runs.append(det.run(w.points))
     base = runs[0]
@@ -145,3 +145,34 @@ def test_input_errors(rtod):
         with pytest.raises(rtod.RtodError, match="STATE"):
             det.push(np.zeros(5, np.float32))  # detect must come first
         assert det.detect().size == 0
+
+
+@pytest.mark.parametrize("router", [False, True])
+def test_autotuner_keeps_results(rtod, router):
+    """The autotuner only changes speed: tuned and default runs agree, and the
+    chosen settings are among the candidates."""
+    from rtod_b200 import datagen
+    w = datagen.sensor_like()
+    pts = w.points[:w.window + 150 * w.slide]
+    with rtod.Detector(w.window, w.slide, w.R, w.K, dim=3) as base, \
+            rtod.Detector(w.window, w.slide, w.R, w.K, dim=3, tuner=True, router=router) as tuned:
+        a = base.run(pts)
+        b = tuned.run(pts)
+        assert_same(b, a.offsets, a.ids)
+        t = tuned.tuning
+        assert t["cells_per_r"] in (1, 2, 3) and t["block_warps"] in (2, 4, 8)
+        assert t["batch"] in (8, 16, 32, 64)
+        tuned.reset()
+        assert_same(tuned.run(pts), a.offsets, a.ids)
+
+
+@pytest.mark.parametrize("path", [p for p in golden_cases() if load_golden(p)[1].shape[1] == 1],
+                         ids=lambda p: os.path.basename(p)[:-4])
+@pytest.mark.parametrize("n", [4, 6, 8])
+def test_fine_cells_1d_match_golden(rtod, path, n):
+    """1-d grids of R/n cells: the group filter (runs of n-1 cells) and the
+    wider stencil give the same outliers."""
+    meta, pts, off, ids = load_golden(path)
+    with rtod.Detector(meta["W"], meta["S"], meta["R"], meta["K"], pred=meta["pred"],
+                       cells_per_r=n) as det:
+        assert_same(det.run(pts), off, ids)
