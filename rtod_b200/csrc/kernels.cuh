@@ -44,6 +44,7 @@
 // for its predecessor to complete before touching shared data.
 #pragma once
 
+#include <climits>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -74,6 +75,8 @@ struct JobCtr {
   uint32_t cmp_ticket;   // k_compact tile tickets
   int32_t n_sweep;       // queued points of the full-sweep queue (router on)
   int32_t last_nout;     // outliers of the job's last detected window
+  int32_t pure;          // current window: no two of its cells share a bin
+  int32_t pad;
 };
 
 // Per-handle state (device).
@@ -97,6 +100,8 @@ struct Job {
   const float* pts;       // ring: SoA [D][W] by slot; stream: point-major [N][D]
   const uint64_t* keys;   // ring: [W] by slot; stream: [N] by global index
   const float* stage;     // ring: the points k_ingest writes (point-major)
+  const long long* blk_lo;  // stream: per slide block (S points), min cell coordinate per
+  const long long* blk_hi;  //   hashed dimension ([blocks][3]); null for a ring
   uint8_t* prev;          // last capped count per source position (255 = safe, 254 = none)
   uint32_t* bin_count;    // [NB]
   uint32_t* bin_start;    // [NB + 1]
@@ -368,18 +373,53 @@ namespace rtod {
 // ---------------------------------------------------------------------------
 template <int D>
 __global__ void __launch_bounds__(256) k_keys(const float* pts, int64_t g0, int64_t g1, double cell,
-                                              uint64_t* keys, uint8_t* prev, BatchState* bs) {
+                                              uint64_t* keys, uint8_t* prev, BatchState* bs, int64_t S,
+                                              long long* blk_lo, long long* blk_hi) {
   pdl_trigger();
   pdl_wait();
+  constexpr int H = Hashed<D>::value;
+  const int lane = threadIdx.x & 31;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t g = g0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; g < g1; g += stride) {
-    float x[D];
+  for (int64_t base = g0 + (int64_t)blockIdx.x * blockDim.x; base < g1; base += stride) {
+    const int64_t g = base + threadIdx.x;
+    const bool valid = g < g1;
+    int64_t k[3] = {0, 0, 0};
+    int64_t blk = -1;
+    if (valid) {
+      float x[D];
 #pragma unroll
-    for (int d = 0; d < D; ++d) x[d] = pts[g * D + d];
-    int32_t code;
-    keys[g] = cell_key<D>(x, cell, &code);
-    prev[g] = 254;
-    if (code) set_err(bs, code);
+      for (int d = 0; d < D; ++d) x[d] = pts[g * D + d];
+      int32_t code;
+      const uint64_t key = cell_key<D>(x, cell, &code);
+      keys[g] = key;
+      prev[g] = 254;
+      if (code) set_err(bs, code);
+      unpack_key(key, H, k);
+      blk = g / S;
+    }
+    // Per slide block, the range of cell coordinates: reduced over the lanes
+    // of each block present in the warp, then one atomic per block and dim.
+    unsigned todo = __ballot_sync(0xffffffffu, valid);
+    while (todo) {
+      const int ld = __ffs(todo) - 1;
+      const int64_t bid = __shfl_sync(0xffffffffu, blk, ld);
+      const unsigned grp = __ballot_sync(0xffffffffu, valid && blk == bid);
+      todo &= ~grp;
+      const bool in = (grp >> lane) & 1;
+#pragma unroll
+      for (int d = 0; d < H; ++d) {
+        long long mn = in ? k[d] : LLONG_MAX, mx = in ? k[d] : LLONG_MIN;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          mn = min(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+          mx = max(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        }
+        if (lane == ld) {
+          atomicMin(&blk_lo[bid * 3 + d], mn);
+          atomicMax(&blk_hi[bid * 3 + d], mx);
+        }
+      }
+    }
   }
 }
 
@@ -426,8 +466,52 @@ struct Unroll {
   static constexpr int value = D <= 3 ? 4 : 2;
 };
 
+// Whether no two cells of the job's current window can share a bin: from the
+// per-slide-block coordinate ranges of a resident stream (a ring has none).
+// The bin map is injective on boxes of at most 65536 cells (1-d),
+// 256 x 256 (2-d) or 16 x 64 x 64 (3-d). One warp computes it.
+template <int H>
+__device__ __forceinline__ bool window_pure(const Job& jb, int64_t lo) {
+  if (!jb.blk_lo) return false;
+  const int lane = threadIdx.x & 31;
+  const int64_t b0 = lo / jb.S, nb = jb.W / jb.S;
+  if (nb > 4096) return false;
+  long long mn[3] = {LLONG_MAX, LLONG_MAX, LLONG_MAX}, mx[3] = {LLONG_MIN, LLONG_MIN, LLONG_MIN};
+  for (int64_t t = lane; t < nb; t += 32) {
+#pragma unroll
+    for (int d = 0; d < H; ++d) {
+      mn[d] = min(mn[d], jb.blk_lo[(b0 + t) * 3 + d]);
+      mx[d] = max(mx[d], jb.blk_hi[(b0 + t) * 3 + d]);
+    }
+  }
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < H; ++d) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      mn[d] = min(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
+      mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
+    }
+    const long long span = mx[d] - mn[d] + 1;
+    const long long cap = H == 1 ? 65536 : (H == 2 ? 256 : (d == 0 ? 16 : 64));
+    ok &= span <= cap;
+  }
+  return ok;
+}
+
+
+
+constexpr int HIST_SLOTS = 256;  // block-local aggregation table of k_hist and k_scatter
+
+// k_hist: per-bin counts (and, unless the window is pure, the per-bin key
+// range), aggregated first per warp, then per block in a shared-memory hash
+// table, then flushed to global memory with one atomic per bin per block.
 template <int D>
 __global__ void __launch_bounds__(256) k_hist(Batch b) {
+  __shared__ uint32_t hbin[HIST_SLOTS];
+  __shared__ uint32_t hcnt[HIST_SLOTS];
+  __shared__ unsigned long long hmin[HIST_SLOTS], hmax[HIST_SLOTS];
+  __shared__ int s_pure;
   pdl_trigger();
   pdl_wait();
   if (!job_active(b)) return;
@@ -436,9 +520,24 @@ __global__ void __launch_bounds__(256) k_hist(Batch b) {
   const Job& jb = b.jobs[blockIdx.y];
   const int64_t lo = jb.ctr->lo;
   const int lane = threadIdx.x & 31;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t w0 = warp * 32 * U; w0 < jb.W; w0 += nwarps * 32 * U) {
+  if (threadIdx.x < 32) {
+    const bool pure = window_pure<H>(jb, lo);
+    if (threadIdx.x == 0) {
+      s_pure = pure;
+      if (blockIdx.x == 0) jb.ctr->pure = pure;
+    }
+  }
+  for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
+    hbin[t] = 0xffffffffu;
+    hcnt[t] = 0;
+    hmin[t] = EMPTY_KEY;
+    hmax[t] = 0;
+  }
+  __syncthreads();
+  const bool pure = s_pure;
+  const int64_t chunk = (int64_t)blockDim.x * U;
+  for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < jb.W; c0 += (int64_t)gridDim.x * chunk) {
+    const int64_t w0 = c0 + (int64_t)(threadIdx.x >> 5) * 32 * U;
     uint64_t key[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -452,13 +551,46 @@ __global__ void __launch_bounds__(256) k_hist(Batch b) {
       const unsigned peers = __match_any_sync(0xffffffffu, bin);
       const int leader = __ffs(peers) - 1;
       const uint64_t lkey = __shfl_sync(0xffffffffu, key[u], leader);
+      const bool mixed_grp = (__ballot_sync(0xffffffffu, key[u] != lkey) & peers) != 0;
+      int slot = -1;
       if (valid && lane == leader) {
-        atomicAdd(&jb.bin_count[bin], (uint32_t)__popc(peers));
-        atomicMin(&jb.kmin[bin], (unsigned long long)key[u]);
-        atomicMax(&jb.kmax[bin], (unsigned long long)key[u]);
-      } else if (valid && key[u] != lkey) {
-        atomicMin(&jb.kmin[bin], (unsigned long long)key[u]);
-        atomicMax(&jb.kmax[bin], (unsigned long long)key[u]);
+        const uint32_t c = (uint32_t)__popc(peers);
+        uint32_t sl = (bin * 2654435761u) >> (32 - 8);
+#pragma unroll 1
+        for (int probe = 0; probe < 8; ++probe) {
+          const uint32_t old = atomicCAS(&hbin[sl], 0xffffffffu, bin);
+          if (old == 0xffffffffu || old == bin) {
+            atomicAdd(&hcnt[sl], c);
+            slot = (int)sl;
+            break;
+          }
+          sl = (sl + 1) & (HIST_SLOTS - 1);
+        }
+        if (slot < 0) atomicAdd(&jb.bin_count[bin], c);
+      }
+      if (!pure) {
+        // key range of the bin: the leader alone when the group's keys agree
+        slot = __shfl_sync(0xffffffffu, slot, leader);
+        if (valid && (mixed_grp || lane == leader)) {
+          if (slot >= 0) {
+            atomicMin(&hmin[slot], (unsigned long long)key[u]);
+            atomicMax(&hmax[slot], (unsigned long long)key[u]);
+          } else {
+            atomicMin(&jb.kmin[bin], (unsigned long long)key[u]);
+            atomicMax(&jb.kmax[bin], (unsigned long long)key[u]);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
+    const uint32_t bin = hbin[t];
+    if (bin != 0xffffffffu) {
+      atomicAdd(&jb.bin_count[bin], hcnt[t]);
+      if (!pure) {
+        atomicMin(&jb.kmin[bin], hmin[t]);
+        atomicMax(&jb.kmax[bin], hmax[t]);
       }
     }
   }
@@ -553,7 +685,7 @@ __device__ __forceinline__ bool for_each_run(const uint32_t* bin_start, const in
 // so a point is an inlier if some run of n-1 consecutive cells containing its
 // cell holds more than K points, provided every bin of the run holds exactly
 // its expected cell (or nothing). Returns true when such a run exists.
-__device__ __forceinline__ bool group_safe_1d(const Job& jb, uint64_t key, uint32_t b) {
+__device__ __forceinline__ bool group_safe_1d(const Job& jb, uint64_t key, uint32_t b, bool pure) {
   const int m = jb.n - 1;
   if (m < 2 || b < (uint32_t)(m - 1) || b + m > NB - 1) return false;
   constexpr int MMAX = 7;
@@ -567,7 +699,7 @@ __device__ __forceinline__ bool group_safe_1d(const Job& jb, uint64_t key, uint3
     if (t < 2 * m - 1) {
       const uint32_t j = b - m + 1 + t;
       const unsigned long long want = key + (unsigned long long)(t - (m - 1));
-      ok[t] = bs[t + 1] == bs[t] || (jb.kmin[j] == want && jb.kmax[j] == want);
+      ok[t] = pure || bs[t + 1] == bs[t] || (jb.kmin[j] == want && jb.kmax[j] == want);
     }
   }
 #pragma unroll
@@ -585,6 +717,10 @@ __device__ __forceinline__ bool group_safe_1d(const Job& jb, uint64_t key, uint3
 
 template <int D, bool ROUTE>
 __global__ void __launch_bounds__(256) k_scatter(Batch b) {
+  // Block-local table: bin, points of the chunk in the bin, claimed base.
+  __shared__ uint32_t tbin[HIST_SLOTS];
+  __shared__ uint32_t tcnt[HIST_SLOTS];
+  __shared__ uint32_t tbase[HIST_SLOTS];
   pdl_trigger();
   pdl_wait();
   if (!job_active(b)) return;
@@ -592,35 +728,72 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
   constexpr int U = Unroll<D>::value;
   const Job& jb = b.jobs[blockIdx.y];
   const int64_t lo = jb.ctr->lo;
+  const bool pure = jb.ctr->pure;
   if (blockIdx.x == 0 && threadIdx.x < SCAN_TILES) jb.scan_status[threadIdx.x] = 0;
+  for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
+    tbin[t] = 0xffffffffu;
+    tcnt[t] = 0;
+  }
+  __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned lt = lanemask_lt();
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t w0 = warp * 32 * U; w0 < jb.W; w0 += nwarps * 32 * U) {
+  const int64_t chunk = (int64_t)blockDim.x * U;
+  for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < jb.W; c0 += (int64_t)gridDim.x * chunk) {
+    const int64_t w0 = c0 + (int64_t)(threadIdx.x >> 5) * 32 * U;
     int64_t src[U];
     uint64_t key[U];
-    uint32_t bin[U], top[U], peers[U];
-    int leader[U];
-    // 1. keys of U chunks
+    uint32_t bin[U], peers[U], goff[U];
+    int leader[U], slot[U];
+    // 1. keys of U chunks of 32
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t i = w0 + u * 32 + lane;
       src[u] = i < jb.W ? source_pos(jb, lo, i) : -1;
       key[u] = src[u] >= 0 ? jb.keys[src[u]] : EMPTY_KEY;
     }
-    // 2. claim positions (U independent atomics in flight)
+    // 2. per warp group: slot in the block table and offset inside the block's share
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       bin[u] = src[u] >= 0 ? bin_of_key(key[u], H) : 0xffffffffu;
       peers[u] = __match_any_sync(0xffffffffu, bin[u]);
       leader[u] = __ffs(peers[u]) - 1;
-      top[u] = 0;
-      if (src[u] >= 0 && lane == leader[u]) top[u] = atomicSub(&jb.bin_count[bin[u]], (uint32_t)__popc(peers[u]));
+      int sl_found = -1;
+      uint32_t off = 0;
+      if (src[u] >= 0 && lane == leader[u]) {
+        const uint32_t c = (uint32_t)__popc(peers[u]);
+        uint32_t sl = (bin[u] * 2654435761u) >> (32 - 8);
+#pragma unroll 1
+        for (int probe = 0; probe < 8; ++probe) {
+          const uint32_t old = atomicCAS(&tbin[sl], 0xffffffffu, bin[u]);
+          if (old == 0xffffffffu || old == bin[u]) {
+            off = atomicAdd(&tcnt[sl], c);
+            sl_found = (int)sl;
+            break;
+          }
+          sl = (sl + 1) & (HIST_SLOTS - 1);
+        }
+        if (sl_found < 0) {  // table full: claim directly
+          const uint32_t top = atomicSub(&jb.bin_count[bin[u]], c);
+          off = top - c;
+        }
+      }
+      slot[u] = __shfl_sync(0xffffffffu, sl_found, leader[u]);
+      goff[u] = __shfl_sync(0xffffffffu, off, leader[u]) + __popc(peers[u] & lt);
     }
+    __syncthreads();
+    // 3. one claim per bin of the chunk (positions [top - cnt, top) of the bin)
+    for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
+      const uint32_t bb = tbin[t];
+      if (bb != 0xffffffffu) {
+        const uint32_t c = tcnt[t];
+        tbase[t] = atomicSub(&jb.bin_count[bb], c) - c;
+        tbin[t] = 0xffffffffu;
+        tcnt[t] = 0;
+      }
+    }
+    __syncthreads();
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      top[u] = __shfl_sync(0xffffffffu, top[u], leader[u]);
       const bool valid = src[u] >= 0;
       const int64_t i = w0 + u * 32 + lane;
       bool safe = false;
@@ -628,7 +801,7 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
       if (valid) {
         const uint32_t bs0 = jb.bin_start[bin[u]];
         const uint32_t bs1 = jb.bin_start[bin[u] + 1];
-        pos = bs0 + top[u] - (uint32_t)__popc(peers[u]) + __popc(peers[u] & lt);
+        pos = bs0 + goff[u] + (slot[u] >= 0 ? tbase[slot[u]] : 0u);
         float x[D];
         load_point<D>(jb, src[u], x);
         jb.s_off[pos] = (uint32_t)i;
@@ -637,9 +810,9 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
         for (int d = 0; d < D; ++d) jb.s_x[(int64_t)d * jb.Wp + pos] = x[d];
         cnt = bs1 - bs0;
         if (jb.filter) {
-          safe = cnt > (uint32_t)jb.K && jb.kmin[bin[u]] == jb.kmax[bin[u]];
+          safe = cnt > (uint32_t)jb.K && (pure || jb.kmin[bin[u]] == jb.kmax[bin[u]]);
           if constexpr (H == 1) {
-            if (!safe && jb.n >= 3) safe = group_safe_1d(jb, key[u], bin[u]);
+            if (!safe && jb.n >= 3) safe = group_safe_1d(jb, key[u], bin[u], pure);
           }
         }
         if (safe) jb.prev[src[u]] = 255;
@@ -648,21 +821,19 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
       bool sweep = false;
       float f[MLP_IN] = {0.0f, 0.0f, 0.0f};
       if constexpr (ROUTE) {
-        if (__any_sync(0xffffffffu, need) && need) {
-          // Router features and prediction (one lane per point).
+        if (need) {
+          // Router features (own bin, stencil row, last count) and one table lookup.
           int64_t k[3];
           unpack_key(key[u], H, k);
-          uint32_t stencil = 0;
-          for_each_run<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
-            stencil += re - rs;
-            return false;
-          });
+          int64_t c[3] = {k[0], k[1], k[2]};
+          c[H - 1] -= jb.n;
+          const uint32_t r0 = bin_of(c, H), r1 = r0 + 2 * jb.n + 1;
+          const uint32_t row = r1 <= NB ? jb.bin_start[r1] - jb.bin_start[r0] : 0xffffffu;
           f[0] = log2f(1.0f + (float)cnt) * 0.125f;
-          f[1] = log2f(1.0f + (float)stencil) * 0.125f;
+          f[1] = log2f(1.0f + (float)row) * 0.125f;
           f[2] = prev_feature(jb.prev[src[u]], jb.K);
-          float z[MLP_B];
-          mlp_forward(b.router->params, f, z);
-          sweep = stencil <= b.router->max_sweep && p_inlier(z) < b.router->threshold;
+          const uint32_t rows = H == 1 ? 1u : (H == 2 ? 2u * jb.n + 1u : (2u * jb.n + 1u) * (2u * jb.n + 1u));
+          sweep = row * rows <= b.router->max_sweep && !route_early(b.router, f);
         }
       }
       const unsigned need_e = __ballot_sync(0xffffffffu, need && !sweep);
@@ -734,11 +905,121 @@ __device__ __forceinline__ bool count_run(const Job& jb, const float* qx, uint32
   return false;
 }
 
+// ---------------------------------------------------------------------------
+// Row-parallel count for 2 and 3 hashed dimensions. The (2n+1)^(h-1) stencil
+// rows are taken nearest first (centre row, then by distance); lane r fetches
+// the bounds of rows r and r+32 in one round trip, a warp scan turns the row
+// lengths into offsets of one virtual concatenated candidate list, and the
+// warp consumes that list 128 candidates per step across row boundaries (each
+// lane finds the row of its candidates by binary search over the offsets).
+// Returns false in *ok when a row wraps around the end of the bin table; the
+// caller then uses the row-by-row count.
+// ---------------------------------------------------------------------------
+__constant__ uint8_t c_rows2[3][7] = {{1, 0, 2}, {2, 1, 3, 0, 4}, {3, 2, 4, 1, 5, 0, 6}};
+__constant__ uint8_t c_rows3[3][49] = {
+    {4, 3, 5, 1, 7, 0, 2, 6, 8},
+    {12, 11, 13, 7, 17, 6, 8, 16, 18, 10, 14, 2, 22, 5, 9, 15, 19, 1, 3, 21, 23, 0, 4, 20, 24},
+    {24, 23, 25, 17, 31, 16, 18, 30, 32, 22, 26, 10, 38, 15, 19, 29, 33, 9, 11, 37, 39, 8, 12, 36, 40,
+     21, 27, 3, 45, 14, 20, 28, 34, 2, 4, 44, 46, 7, 13, 35, 41, 1, 5, 43, 47, 0, 6, 42, 48}};
+
+template <int D, int PRED>
+__device__ __forceinline__ bool count_query_rows(const Job& jb, uint32_t pos, int& total, bool* ok) {
+  constexpr int H = Hashed<D>::value;
+  static_assert(H >= 2, "row-parallel count needs 2 or 3 hashed dimensions");
+  const int lane = threadIdx.x & 31;
+  const int n = jb.n, span = 2 * n + 1;
+  const int rows = (H == 2) ? span : span * span;
+  float qx[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) qx[d] = jb.s_x[(int64_t)d * jb.Wp + pos];
+  int64_t k[3];
+  unpack_key(jb.s_ckey[pos], H, k);
+  uint32_t rs[2] = {0, 0}, len[2] = {0, 0};
+  bool wrap = false;
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    const int slot = lane + 32 * t;
+    if (slot < rows) {
+      const int r = (H == 2) ? c_rows2[n - 1][slot] : c_rows3[n - 1][slot];
+      int64_t c[3];
+      if (H == 2) {
+        c[0] = k[0] + r - n;
+        c[1] = k[1] - n;
+      } else {
+        c[0] = k[0] + r / span - n;
+        c[1] = k[1] + r % span - n;
+        c[2] = k[2] - n;
+      }
+      const uint32_t b0 = bin_of(c, H);
+      if (b0 + 2 * n > NB_MASK) {
+        wrap = true;
+      } else {
+        rs[t] = jb.bin_start[b0];
+        len[t] = jb.bin_start[b0 + 2 * n + 1] - rs[t];
+      }
+    }
+  }
+  total = 0;
+  *ok = !__any_sync(0xffffffffu, wrap);
+  if (!*ok) return false;
+  // exclusive offsets of the 64 row slots (slot = lane + 32 t)
+  uint32_t off[2], T = 0;
+#pragma unroll
+  for (int t = 0; t < 2; ++t) {
+    uint32_t inc = len[t];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    off[t] = T + inc - len[t];
+    T += __shfl_sync(0xffffffffu, inc, 31);
+  }
+  for (uint32_t v0 = 0; v0 < T; v0 += 128) {
+    bool in[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const uint32_t v = v0 + 32 * e + lane;
+      in[e] = false;
+      // row slot holding v: the last slot whose offset is <= v (binary search over 64 slots)
+      int lo_s = 0;
+#pragma unroll
+      for (int step = 32; step > 0; step >>= 1) {
+        const int cand = lo_s + step;
+        const uint32_t o0 = __shfl_sync(0xffffffffu, off[0], cand & 31);
+        const uint32_t o1 = __shfl_sync(0xffffffffu, off[1], cand & 31);
+        const uint32_t oc = cand < 32 ? o0 : o1;
+        if (cand < 64 && oc <= v) lo_s = cand;
+      }
+      const uint32_t base0 = __shfl_sync(0xffffffffu, rs[0], lo_s & 31);
+      const uint32_t base1 = __shfl_sync(0xffffffffu, rs[1], lo_s & 31);
+      const uint32_t oo0 = __shfl_sync(0xffffffffu, off[0], lo_s & 31);
+      const uint32_t oo1 = __shfl_sync(0xffffffffu, off[1], lo_s & 31);
+      if (v < T) {
+        const uint32_t c = (lo_s < 32 ? base0 : base1) + (v - (lo_s < 32 ? oo0 : oo1));
+        float cx[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) cx[d] = jb.s_x[(int64_t)d * jb.Wp + c];
+        in[e] = is_nbr<D, PRED>(qx, cx, jb.R2f, jb.R, jb.R2);
+      }
+    }
+    total += __popc(__ballot_sync(0xffffffffu, in[0])) + __popc(__ballot_sync(0xffffffffu, in[1])) +
+             __popc(__ballot_sync(0xffffffffu, in[2])) + __popc(__ballot_sync(0xffffffffu, in[3]));
+    if (total > jb.K) return true;
+  }
+  return false;
+}
+
 // Exact count of one queued point by the whole warp: `total` receives the
 // count (capped just above K); returns true if it exceeded K.
 template <int D, int PRED>
 __device__ __forceinline__ bool count_query(const Job& jb, uint32_t pos, int& total) {
   constexpr int H = Hashed<D>::value;
+  if constexpr (H >= 2) {
+    bool ok;
+    const bool r = count_query_rows<D, PRED>(jb, pos, total, &ok);
+    if (ok) return r;
+  }
   float qx[D];
 #pragma unroll
   for (int d = 0; d < D; ++d) qx[d] = jb.s_x[(int64_t)d * jb.Wp + pos];
@@ -746,61 +1027,6 @@ __device__ __forceinline__ bool count_query(const Job& jb, uint32_t pos, int& to
   unpack_key(jb.s_ckey[pos], H, k);
   total = 0;
   return for_each_run<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
-    return count_run<D, PRED>(jb, qx, rs, re, total);
-  });
-}
-
-// Stencil runs, nearest first: the point's own cell, then its neighbours
-// along the last hashed dimension outward (one bin each), then the other
-// rows of the stencil. Covers exactly the same candidates as for_each_run.
-template <int h, typename F>
-__device__ __forceinline__ bool for_each_run_near(const uint32_t* bin_start, const int64_t* k, int n, F&& f) {
-  const int span = 2 * n + 1;
-  // centre row, one cell at a time: offsets 0, -1, +1, -2, +2, ...
-  for (int t = 0; t < span; ++t) {
-    const int o = (t == 0) ? 0 : ((t & 1) ? -((t + 1) >> 1) : (t >> 1));
-    int64_t c[3] = {k[0], h > 1 ? k[1] : 0, h > 2 ? k[2] : 0};
-    c[h - 1] += o;
-    const uint32_t b0 = bin_of(c, h);
-    if (f(bin_start[b0], bin_start[b0 + 1])) return true;
-  }
-  if (h == 1) return false;
-  const int rows = (h == 2) ? span : span * span;
-  const int centre = (h == 2) ? n : n * span + n;
-  for (int r = 0; r < rows; ++r) {
-    if (r == centre) continue;
-    int64_t c[3];
-    if (h == 2) {
-      c[0] = k[0] + r - n;
-      c[1] = k[1] - n;
-    } else {
-      c[0] = k[0] + r / span - n;
-      c[1] = k[1] + r % span - n;
-      c[2] = k[2] - n;
-    }
-    const uint32_t b0 = bin_of(c, h);
-    const uint32_t b1 = (b0 + 2 * n) & NB_MASK;
-    if (b0 <= b1) {
-      if (f(bin_start[b0], bin_start[b1 + 1])) return true;
-    } else {
-      if (f(bin_start[b0], bin_start[NB])) return true;
-      if (f(bin_start[0], bin_start[b1 + 1])) return true;
-    }
-  }
-  return false;
-}
-
-// Exact count of one queued point by the whole warp, nearest cells first.
-template <int D, int PRED>
-__device__ __forceinline__ bool count_query_near(const Job& jb, uint32_t pos, int& total) {
-  constexpr int H = Hashed<D>::value;
-  float qx[D];
-#pragma unroll
-  for (int d = 0; d < D; ++d) qx[d] = jb.s_x[(int64_t)d * jb.Wp + pos];
-  int64_t k[3];
-  unpack_key(jb.s_ckey[pos], H, k);
-  total = 0;
-  return for_each_run_near<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
     return count_run<D, PRED>(jb, qx, rs, re, total);
   });
 }
@@ -844,6 +1070,9 @@ __device__ __forceinline__ void record_sample(const Job& jb, RouterState* rs, in
   const int lab = count_bucket(total, jb.K);
   if ((lab == 3) != routed_early) atomicAdd(&rs->misrouted, 1ull);
   if (*(volatile uint32_t*)&rs->n_samples >= TRAIN_CAP) return;
+  // Most counted points are inliers: keep one inlier sample in INLIER_THIN so
+  // that the buckets are closer to balanced.
+  if (lab == 3 && (atomicAdd(&rs->inliers_seen, 1u) % INLIER_THIN) != 0) return;
   const uint32_t s = atomicAdd(&rs->n_samples, 1u);
   if (s >= TRAIN_CAP) return;
 #pragma unroll
@@ -868,9 +1097,9 @@ __device__ __forceinline__ void reset_bins(const Job& jb) {
 // k_count: the exact count always decides: outlier iff count <= K.
 //   plain (ROUTE = false): one warp per queued point, warps striding over
 //     the queue, stencil rows in order.
-//   routed: early-exit queue as above but nearest cells first; full-sweep
-//     queue one lane per point, 32 points per warp; every counted point
-//     becomes a training sample of the router.
+//   routed: early-exit queue as above; full-sweep queue one lane per point,
+//     32 points per warp, each lane sweeping its own (short) candidate list;
+//     every counted point becomes a training sample of the router.
 // ---------------------------------------------------------------------------
 template <int D, int PRED, bool ROUTE>
 __global__ void __launch_bounds__(256) k_count(Batch b) {
@@ -887,7 +1116,7 @@ __global__ void __launch_bounds__(256) k_count(Batch b) {
   for (int64_t q = warp; q < nq; q += nwarps) {
     const uint32_t pos = jb.queue[q];
     int total;
-    const bool inlier = ROUTE ? count_query_near<D, PRED>(jb, pos, total) : count_query<D, PRED>(jb, pos, total);
+    const bool inlier = count_query<D, PRED>(jb, pos, total);
     if (lane == 0) {
       record_count(jb, lo, pos, inlier, total);
       if constexpr (ROUTE) record_sample(jb, b.router, q, total, true);

@@ -1,24 +1,30 @@
 // Learned router: a small MLP that predicts the neighbour-count bucket of a
 // point that needs an exact count, and routes it into one of two queues.
 //
-//   early-exit queue  predicted inliers (or long candidate lists): one warp per
-//                     point, candidates scanned nearest cell first so that the
-//                     count passes K as soon as possible;
+//   early-exit queue  predicted inliers (and every point with a long candidate
+//                     list): one warp per point, 128 candidates per step,
+//                     stopping as soon as the count passes K;
 //   full-sweep queue  predicted outliers with a short candidate list: one lane
 //                     per point, 32 points per warp, each lane sweeps its own
 //                     candidates (no warp-wide step per candidate).
 //
 // The exact count always decides the result; a misroute only costs time, and
 // the result is identical with the router on or off. The network is trained
-// online, on the GPU, on the capped counts k_count has just produced.
+// online, on the GPU, on the capped counts k_count has just produced (one
+// Adam step every few batches).
 //
 // Network: x (3) -> relu(W1 x + b1) (32) -> relu(W2 h1 + b2) (32) -> W3 h2 + b3 (4)
 // Parameter packing (floats): W1[32][3], b1[32], W2[32][32], b2[32], W3[4][32], b3[4]
 // Loss: mean softmax cross-entropy; optimiser: Adam (Kingma & Ba 2015).
 // Features: f0 = log2(1 + points in the point's bin) / 8,
-//           f1 = log2(1 + candidates in its stencil) / 8,
+//           f1 = log2(1 + points in its stencil row) / 8 (the whole stencil
+//                in 1-d, the centre row of cells along the last hashed
+//                dimension otherwise),
 //           f2 = its capped count in the previous window / (K + 1)
 //                (-1 if none yet, 2 if it was a safe inlier).
+// Inference: after every training step k_table evaluates the network at the
+// centres of a 32 x 32 x 16 grid over (f0, f1, f2) and stores P(count > K)
+// as a byte; k_scatter routes a point by one lookup of its grid cell.
 // Buckets of the capped count c (self included): 0: c <= K/4, 1: c <= K/2,
 // 2: c <= K, 3: c > K.
 #pragma once
@@ -36,8 +42,12 @@ constexpr int OFF_B2 = OFF_W2 + MLP_H * MLP_H;    // 1152
 constexpr int OFF_W3 = OFF_B2 + MLP_H;            // 1184
 constexpr int OFF_B3 = OFF_W3 + MLP_B * MLP_H;    // 1312
 constexpr int MLP_P = OFF_B3 + MLP_B;             // 1316 parameters
-constexpr int TRAIN_CAP = 2048;                   // training samples kept per batch
+constexpr int TRAIN_CAP = 2048;                   // training samples buffered between steps
 constexpr int TRAIN_CHUNK = 128;                  // samples per chunk of k_train
+constexpr int TRAIN_MAX = 256;                    // samples used by one training step
+constexpr uint32_t INLIER_THIN = 16;              // inlier samples kept: one in 16
+constexpr int TQ0 = 32, TQ1 = 32, TQ2 = 16;       // routing table grid
+constexpr float F0_MAX = 1.5f, F1_MAX = 2.5f, F2_MIN = -1.0f, F2_MAX = 2.0f;
 
 // Router state (device), one per handle.
 struct RouterState {
@@ -52,10 +62,24 @@ struct RouterState {
   uint32_t min_samples;  // train once at least this many samples are buffered
   float last_loss;
   uint32_t n_samples;  // samples buffered (atomic counter)
+  uint32_t inliers_seen;  // inlier samples offered (for thinning)
   float samples[TRAIN_CAP][4];  // f0, f1, f2, label
   // routing counters (since create)
   unsigned long long routed_early, routed_sweep, misrouted;
+  uint8_t table[TQ0][TQ1][TQ2];  // P(count > K) * 255 at the grid-cell centres
 };
+
+__device__ __forceinline__ int quant(float v, float lo, float hi, int n) {
+  const int q = (int)((v - lo) * (float)n / (hi - lo));
+  return q < 0 ? 0 : (q >= n ? n - 1 : q);
+}
+
+// Routing decision of one point from its features: true = early-exit queue.
+__device__ __forceinline__ bool route_early(const RouterState* rs, const float* f) {
+  const int q0 = quant(f[0], 0.0f, F0_MAX, TQ0), q1 = quant(f[1], 0.0f, F1_MAX, TQ1),
+            q2 = quant(f[2], F2_MIN, F2_MAX, TQ2);
+  return (float)rs->table[q0][q1][q2] >= rs->threshold * 255.0f;
+}
 
 __device__ __forceinline__ int count_bucket(int c, int K) {
   return c > K ? 3 : (4 * c <= K ? 0 : (2 * c <= K ? 1 : 2));
@@ -241,13 +265,13 @@ __device__ void mlp_train_block(float* P, float* m, float* v, float* b1t, float*
   }
 }
 
-// Online training after a batch: one Adam step on the buffered samples once
+// Online training: one Adam step on up to TRAIN_MAX buffered samples once
 // enough have accumulated; the buffer is then emptied.
 __global__ void __launch_bounds__(256) k_train(RouterState* rs) {
   extern __shared__ float smem[];
   pdl_trigger();
   pdl_wait();
-  const uint32_t n = min(rs->n_samples, (uint32_t)TRAIN_CAP);
+  const uint32_t n = min(rs->n_samples, (uint32_t)TRAIN_MAX);
   if (n < rs->min_samples || n == 0) return;
   float loss = 0.0f;
   mlp_train_block(rs->params, rs->m, rs->v, &rs->b1t, &rs->b2t, rs->lr, rs->beta1, rs->beta2, rs->eps,
@@ -257,6 +281,20 @@ __global__ void __launch_bounds__(256) k_train(RouterState* rs) {
     rs->steps += 1;
     rs->n_samples = 0;
   }
+}
+
+// Routing table from the current parameters: one thread per grid cell.
+__global__ void __launch_bounds__(256) k_table(RouterState* rs) {
+  pdl_trigger();
+  pdl_wait();
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= TQ0 * TQ1 * TQ2) return;
+  const int q2 = t % TQ2, q1 = (t / TQ2) % TQ1, q0 = t / (TQ2 * TQ1);
+  const float x[MLP_IN] = {(q0 + 0.5f) * F0_MAX / TQ0, (q1 + 0.5f) * F1_MAX / TQ1,
+                           F2_MIN + (q2 + 0.5f) * (F2_MAX - F2_MIN) / TQ2};
+  float z[MLP_B];
+  mlp_forward(rs->params, x, z);
+  rs->table[q0][q1][q2] = (uint8_t)fminf(255.0f, p_inlier(z) * 255.0f + 0.5f);
 }
 
 // Test kernels behind the diagnostic C ABI: gradients of a given batch and

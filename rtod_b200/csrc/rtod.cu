@@ -214,6 +214,9 @@ struct rtod_handle {
   uint64_t* run_keys = nullptr;
   uint8_t* run_prev = nullptr;
   int64_t run_key_cap = 0;
+  long long* run_blk_lo = nullptr;  // per slide block: cell coordinate range [blocks][3]
+  long long* run_blk_hi = nullptr;
+  int64_t run_blk_cap = 0;
   int32_t* rec_nout = nullptr;
   int32_t* rec_undet = nullptr;
   int64_t rec_cap = 0;
@@ -226,9 +229,11 @@ struct rtod_handle {
   bool pending = false;
   bool poisoned = false;
 
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graphs[2] = {nullptr, nullptr};  // without / with the router's training step
+  int64_t graph_kernels[2] = {0, 0};
   Batch graph_batch{};
   int graph_ring = -1;
+  int64_t batches = 0;
 
   cudaEvent_t ev[8] = {};
   int64_t launches = 0;
@@ -275,8 +280,10 @@ void set_grid(rtod_handle* h, int n) {
 }
 
 void drop_graph(rtod_handle* h) {
-  if (h->graph) cudaGraphExecDestroy(h->graph);
-  h->graph = nullptr;
+  for (auto& g : h->graphs) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+  }
   h->graph_ring = -1;
 }
 
@@ -339,6 +346,8 @@ Job make_job(rtod_handle* h, int j, bool ring, const float* stream_pts) {
   jb.pts = ring ? h->ring : stream_pts;
   jb.keys = ring ? h->ring_keys : h->run_keys;
   jb.stage = h->staging;
+  jb.blk_lo = ring ? nullptr : h->run_blk_lo;
+  jb.blk_hi = ring ? nullptr : h->run_blk_hi;
   jb.prev = ring ? h->ring_prev : h->run_prev;
   const Scratch& s = h->pool[j];
   jb.bin_count = s.bin_count;
@@ -409,7 +418,8 @@ struct Geom {
 // kev (may be null) receives an event after each kernel (kev[0] after ingest,
 // or at the start when there is none; kev[6] after training or compact).
 // Returns the number of kernels launched in *nk.
-int launch_group(const Geom& g, const Batch& b, bool ingest, cudaStream_t st, cudaEvent_t* kev, int64_t* nk) {
+int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStream_t st, cudaEvent_t* kev,
+                 int64_t* nk) {
   const int64_t W = g.Wmax, nj = b.njobs;
   const unsigned gy = (unsigned)nj;
   int64_t launched = 0;
@@ -443,9 +453,9 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, cudaStream_t st, cu
   CU(launch_k(k_compact, dim3((unsigned)((W + CMP_TILE - 1) / CMP_TILE), gy), 256, st, b));
   if (kev) CU(cudaEventRecord(kev[5], st));
   launched += 5;
-  if (g.route) {
-    // Online training on the counts of this batch (one block; it returns at
-    // once until enough samples are buffered).
+  if (g.route && train) {
+    // Online training on the buffered counts (one block; it returns at once
+    // until enough samples are buffered), then the routing table.
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(1);
     cfg.blockDim = dim3(256);
@@ -457,7 +467,8 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, cudaStream_t st, cu
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     CU(cudaLaunchKernelEx(&cfg, k_train, g.router));
-    launched++;
+    CU(launch_k(k_table, dim3((TQ0 * TQ1 * TQ2 + 255) / 256), 256, st, g.router));
+    launched += 2;
   }
   if (kev) CU(cudaEventRecord(kev[6], st));
   if (nk) *nk = launched;
@@ -468,34 +479,41 @@ Geom geom_of(const rtod_handle* h) {
   return Geom{h->W, h->S, h->D, h->cfg.pred, h->cfg.router, h->sm_count, h->block_warps, h->router};
 }
 
+constexpr int kTrainEvery = 8;  // batches between two router training steps
+
+bool train_now(rtod_handle* h) { return h->cfg.router && (h->batches++ % kTrainEvery) == 0; }
+
 int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev) {
   int64_t nk = 0;
-  int r = launch_group(geom_of(h), b, ingest, h->stream, kev, &nk);
+  int r = launch_group(geom_of(h), b, ingest, train_now(h), h->stream, kev, &nk);
   h->launches += nk;
   return r;
 }
 
-// Runs one batch, replaying a captured graph when graphs are on.
+// Runs one batch, replaying a captured graph when graphs are on (two graphs
+// with the router: with and without the training step).
 int run_batch(rtod_handle* h, const Batch& b, bool ingest) {
   if (!h->cfg.use_graph) return launch_batch(h, b, ingest, nullptr);
-  if (!h->graph || h->graph_ring != (int)ingest || std::memcmp(&h->graph_batch, &b, sizeof(Batch)) != 0) {
-    drop_graph(h);
+  const bool train = train_now(h);
+  cudaGraphExec_t& gx = h->graphs[train ? 1 : 0];
+  if (!gx || h->graph_ring != (int)ingest || std::memcmp(&h->graph_batch, &b, sizeof(Batch)) != 0) {
+    if (h->graph_ring != (int)ingest || std::memcmp(&h->graph_batch, &b, sizeof(Batch)) != 0) drop_graph(h);
     cudaGraph_t g;
     CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    const int64_t before = h->launches;
-    int r = launch_batch(h, b, ingest, nullptr);
-    h->launches = before;
+    int64_t nk = 0;
+    int r = launch_group(geom_of(h), b, ingest, train, h->stream, nullptr, &nk);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (r) return r;
     if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&h->graph, g, 0);
+    e = cudaGraphInstantiate(&gx, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
     h->graph_batch = b;
     h->graph_ring = (int)ingest;
+    h->graph_kernels[train ? 1 : 0] = nk;
   }
-  CU(cudaGraphLaunch(h->graph, h->stream));
-  h->launches += (ingest ? 6 : 5) + (h->cfg.router ? 1 : 0);
+  CU(cudaGraphLaunch(gx, h->stream));
+  h->launches += h->graph_kernels[train ? 1 : 0];
   h->graph_replays++;
   return RTOD_OK;
 }
@@ -580,6 +598,20 @@ int stage_stream(rtod_handle* h, const float* pts, int64_t used, const float** s
       return RTOD_ERR_CUDA;
     h->run_key_cap = used;
   }
+  const int64_t blocks = used / h->S + 1;
+  if (h->run_blk_cap < blocks) {
+    if (h->run_blk_lo) h->device_bytes -= h->run_blk_cap * 48;
+    dfree(h->run_blk_lo);
+    dfree(h->run_blk_hi);
+    h->run_blk_cap = 0;
+    if (dalloc(&h->run_blk_lo, (size_t)(blocks * 3), &h->device_bytes) ||
+        dalloc(&h->run_blk_hi, (size_t)(blocks * 3), &h->device_bytes))
+      return RTOD_ERR_CUDA;
+    h->run_blk_cap = blocks;
+  }
+  // +inf / -inf patterns for the atomic min / max of k_keys
+  CU(cudaMemsetAsync(h->run_blk_lo, 0x7f, (size_t)(blocks * 3) * sizeof(long long), h->stream));
+  CU(cudaMemsetAsync(h->run_blk_hi, 0x80, (size_t)(blocks * 3) * sizeof(long long), h->stream));
   return RTOD_OK;
 }
 
@@ -616,7 +648,7 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
   CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
   const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((used + 255) / 256, h->sm_count * 8));
   DISPATCH_D(h->D, CU(launch_k(k_keys<D>, dim3(kx), 256, h->stream, src, (int64_t)0, used, h->cell, h->run_keys,
-                               h->run_prev, h->bs)));
+                               h->run_prev, h->bs, h->S, h->run_blk_lo, h->run_blk_hi)));
   h->launches++;
   if (e_keys) CU(cudaEventRecord(e_keys, h->stream));
   const int64_t out_cap = std::min(ids_cap, h->ids_cap);
@@ -656,6 +688,7 @@ void free_all(rtod_handle* h) {
   h->pool.clear();
   dfree(h->ctr); dfree(h->jobs_dev); dfree(h->bs); dfree(h->router); dfree(h->ring); dfree(h->ring_keys);
   dfree(h->ring_prev); dfree(h->staging); dfree(h->run_buf); dfree(h->run_keys); dfree(h->run_prev);
+  dfree(h->run_blk_lo); dfree(h->run_blk_hi);
   dfree(h->rec_nout); dfree(h->rec_undet); dfree(h->ids);
   if (h->ctr_init) cudaFreeHost(h->ctr_init);
   h->ctr_init = nullptr;
@@ -890,6 +923,10 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
   }
   ok = ok && cudaFuncSetAttribute(k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM) ==
                  cudaSuccess;
+  if (ok) {
+    k_table<<<(TQ0 * TQ1 * TQ2 + 255) / 256, 256, 0, h->stream>>>(h->router);
+    ok = cudaGetLastError() == cudaSuccess;
+  }
   for (auto& e : h->ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
   if (ok) ok = !ensure_pool(h, 1) && !ensure_ids(h, h->W);
   if (ok) ok = !reset_state(h) && cudaStreamSynchronize(h->stream) == cudaSuccess;
@@ -1255,14 +1292,16 @@ struct rtod_batch {
   std::vector<Group> groups;
   RouterState* router = nullptr;
   std::vector<char> filled, pending;
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graphs[2] = {nullptr, nullptr};  // without / with the router's training step
+  int64_t graph_kernels[2] = {0, 0};
   int64_t steps = 0, launches = 0, detections = 0;
 };
 
 namespace {
 
 void batch_free(rtod_batch* b) {
-  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (auto g : b->graphs)
+    if (g) cudaGraphExecDestroy(g);
   for (auto& g : b->groups) {
     dfree(g.jobs); dfree(g.bs); dfree(g.out); dfree(g.active); dfree(g.nout);
     if (g.active_h) cudaFreeHost(g.active_h);
@@ -1290,14 +1329,14 @@ Batch group_batch(const rtod_batch::Group& g, RouterState* router) {
 }
 
 // One step for all groups: active flags in, counters reset, pipeline, counts out.
-int batch_enqueue(rtod_batch* b, int64_t* nk_total) {
+int batch_enqueue(rtod_batch* b, bool train, int64_t* nk_total) {
   int64_t total = 0;
   for (auto& g : b->groups) {
     const int ng = (int)g.streams.size();
     CU(cudaMemcpyAsync(g.active, g.active_h, sizeof(int32_t) * ng, cudaMemcpyHostToDevice, b->stream));
     CU(cudaMemsetAsync(&g.bs->out_total, 0, sizeof(int64_t), b->stream));
     int64_t nk = 0;
-    int r = launch_group(g.geom, group_batch(g, b->router), true, b->stream, nullptr, &nk);
+    int r = launch_group(g.geom, group_batch(g, b->router), true, train, b->stream, nullptr, &nk);
     if (r) return r;
     total += nk;
     CU(cudaMemcpyAsync(g.nout_h, g.nout, sizeof(int32_t) * ng, cudaMemcpyDeviceToHost, b->stream));
@@ -1352,6 +1391,8 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
     cudaError_t e = cudaMemcpy(b->router, init, sizeof(RouterState), cudaMemcpyHostToDevice);
     delete init;
     if (e != cudaSuccess) return bail(fail(RTOD_ERR_CUDA, "router init failed"));
+    k_table<<<(TQ0 * TQ1 * TQ2 + 255) / 256, 256, 0, b->stream>>>(b->router);
+    if (cudaGetLastError() != cudaSuccess) return bail(fail(RTOD_ERR_CUDA, "router table failed"));
   }
   // Group the streams by (dimension, predicate).
   for (int i = 0; i < n_streams; ++i) {
@@ -1427,22 +1468,23 @@ RTOD_API int rtod_batch_step(rtod_batch* b, int64_t* out_offsets, int64_t* out_i
       any |= g.active_h[k];
     }
   if (!any) return fail(RTOD_ERR_STATE, "no stream has a pushed slide");
-  int64_t nk = 0;
-  if (!b->graph) {
+  const bool train = b->route && (b->steps % kTrainEvery) == 0;
+  cudaGraphExec_t& gx = b->graphs[train ? 1 : 0];
+  if (!gx) {
     cudaGraph_t gr;
     CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    int r = batch_enqueue(b, &nk);
+    int64_t nk0 = 0;
+    int r = batch_enqueue(b, train, &nk0);
     cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
     if (r) return r;
     if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&b->graph, gr, 0);
+    e = cudaGraphInstantiate(&gx, gr, 0);
     cudaGraphDestroy(gr);
     if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
-    b->launches -= nk;  // counted again below
-  } else {
-    for (auto& g : b->groups) nk += 6 + (b->route ? 1 : 0);
+    b->graph_kernels[train ? 1 : 0] = nk0;
   }
-  CU(cudaGraphLaunch(b->graph, b->stream));
+  const int64_t nk = b->graph_kernels[train ? 1 : 0];
+  CU(cudaGraphLaunch(gx, b->stream));
   CU(cudaStreamSynchronize(b->stream));
   b->launches += nk;
   b->steps++;
