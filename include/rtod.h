@@ -187,6 +187,39 @@ int rtod_batch_stats(const rtod_batch* b, int64_t out[4]);
 
 void rtod_batch_destroy(rtod_batch* b);
 
+/* ------------------------------------------------------------------------
+   Allocation-free detection of one window (no counterpart in RTOD).
+
+   For callers that must not allocate device memory at detection time: code
+   running inside a memory pool or allocator it does not own, real-time loops
+   where cudaMalloc's implicit synchronisation and latency are not allowed,
+   and hosts that only lend the library their own device buffers. All scratch
+   lives in one file-scope device array of RTOD_STATIC_SCRATCH_BYTES that
+   every GPU loading the library holds until the process exits; this call
+   performs no cudaMalloc, cudaFree or other allocating call.
+
+   pts      device pointer, n points point-major (n * dim floats): the window
+   out_ids  device pointer with room for n entries: the sorted offsets
+            (0 .. n-1) of the window's outliers
+   n_out    host pointer: number of outliers written
+   stream   the cudaStream_t to run on (NULL: the legacy default stream)
+   Predicate, grid and filter as rtod_create with opt = 2, cells_per_r = 2,
+   router and tuner off. n must be 1..RTOD_STATIC_MAX_POINTS and dim
+   1..RTOD_STATIC_MAX_DIM (RTOD_ERR_CAPACITY otherwise). The call returns
+   after its work on `stream` has finished.
+
+   The first call on a device looks up the device address of the scratch
+   array (cudaGetSymbolAddress, with that device current); make that first
+   call before any stream capture. All calls share the one array and it keeps
+   the previous call's contents (each call clears what must start at zero):
+   calls that overlap on the GPU, from several host threads or streams, race
+   and must not be issued. */
+#define RTOD_STATIC_MAX_POINTS 65536
+#define RTOD_STATIC_MAX_DIM 3
+#define RTOD_STATIC_SCRATCH_BYTES (4608u * 1024u)
+int rtod_detect_window_static(const float* pts, int64_t n, int32_t dim, double R, int32_t K, int32_t pred,
+                              int64_t* out_ids, int64_t* n_out, void* stream);
+
 /* Learned router state (rtod_config.router = 1). params (may be NULL)
    receives the network's rtod_mlp_param_count() parameters; info receives
    [0] training steps, [1] last training loss, [2] points routed to the

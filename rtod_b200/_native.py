@@ -68,6 +68,8 @@ SIGNATURES = [
     ("rtod_profile_run", _i32, [_vp, _vp, _i64, _i64, _vp, _i32]),
     ("rtod_kernel_name", ctypes.c_char_p, [_i32]),
     ("rtod_router_info", _i32, [_vp, _vp, _vp]),
+    ("rtod_detect_window_static", _i32, [_vp, _i64, _i32, ctypes.c_double, _i32, _i32, _vp,
+                                         ctypes.POINTER(_i64), _vp]),
     ("rtod_batch_create", _i32, [_vp, _i32, ctypes.POINTER(_vp)]),
     ("rtod_batch_push", _i32, [_vp, _i32, _vp, _i64]),
     ("rtod_batch_step", _i32, [_vp, _vp, _vp, _i64, ctypes.POINTER(_i64)]),

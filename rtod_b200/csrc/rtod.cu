@@ -1537,3 +1537,190 @@ RTOD_API int rtod_batch_stats(const rtod_batch* b, int64_t out[4]) {
   out[3] = (int64_t)b->groups.size();
   return RTOD_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free detection of one window (rtod_detect_window_static).
+//
+// Every buffer of the pipeline lives in one file-scope device array. Host code
+// only ever sees the array's device address through cudaGetSymbolAddress
+// (the symbol itself is a host-side stand-in). Layout, all 256-byte aligned:
+// Job, JobCtr, BatchState, block ranges, keys, last counts, bin counts, bin
+// starts, bin key minima and maxima, cell-ordered offsets, keys and
+// coordinates, queue, outlier bits, look-back words.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int64_t kStaticN = RTOD_STATIC_MAX_POINTS;
+constexpr int kStaticD = RTOD_STATIC_MAX_DIM;
+constexpr int64_t kStaticWp = ((kStaticN + 3) / 4) * 4 + 4;
+
+constexpr size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct StaticLayout {
+  size_t job, ctr, bs, blo, bhi, keys, prev, bcount, bstart, kmin, kmax, soff, sckey, sx, queue, flags, scan, cmp,
+      end;
+};
+
+constexpr StaticLayout make_layout() {
+  StaticLayout L{};
+  size_t o = 0;
+  L.job = o; o = al256(o + sizeof(Job));
+  L.ctr = o; o = al256(o + sizeof(JobCtr));
+  L.bs = o; o = al256(o + sizeof(BatchState));
+  L.blo = o; o = al256(o + sizeof(long long) * 6);  // blocks 0 and 1
+  L.bhi = o; o = al256(o + sizeof(long long) * 6);
+  L.keys = o; o = al256(o + sizeof(uint64_t) * kStaticN);
+  L.prev = o; o = al256(o + kStaticN);
+  L.bcount = o; o = al256(o + sizeof(uint32_t) * NB);
+  L.bstart = o; o = al256(o + sizeof(uint32_t) * (NB + 1));
+  L.kmin = o; o = al256(o + sizeof(unsigned long long) * NB);
+  L.kmax = o; o = al256(o + sizeof(unsigned long long) * NB);
+  L.soff = o; o = al256(o + sizeof(uint32_t) * kStaticN);
+  L.sckey = o; o = al256(o + sizeof(uint64_t) * kStaticN);
+  L.sx = o; o = al256(o + sizeof(float) * kStaticD * kStaticWp);
+  L.queue = o; o = al256(o + sizeof(uint32_t) * kStaticN);
+  L.flags = o; o = al256(o + sizeof(uint32_t) * (kStaticN / 32));
+  L.scan = o; o = al256(o + sizeof(unsigned long long) * SCAN_TILES);
+  L.cmp = o; o = al256(o + sizeof(unsigned long long) * ((kStaticN + CMP_TILE - 1) / CMP_TILE));
+  L.end = o;
+  return L;
+}
+constexpr StaticLayout kStatic = make_layout();
+static_assert(kStatic.end <= RTOD_STATIC_SCRATCH_BYTES, "static scratch too small for its layout");
+
+static __device__ __align__(256) unsigned char g_static_scratch[RTOD_STATIC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+unsigned char* g_static_addr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device (looked up once
+// per device, with that device current).
+int static_scratch(unsigned char** out) {
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(RTOD_ERR_NODEV, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_static_mu);
+  if (!g_static_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || !p)
+      return fail(RTOD_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+    g_static_addr[dev] = (unsigned char*)p;
+  }
+  *out = g_static_addr[dev];
+  return RTOD_OK;
+}
+
+}  // namespace
+
+RTOD_API int rtod_detect_window_static(const float* pts, int64_t n, int32_t dim, double R, int32_t K, int32_t pred,
+                                       int64_t* out_ids, int64_t* n_out, void* stream) {
+  if (!pts || !out_ids || !n_out) return fail(RTOD_ERR_ARG, "null argument");
+  if (n < 1 || n > kStaticN)
+    return fail(RTOD_ERR_CAPACITY, "window of %lld points: the allocation-free entry point takes 1..%lld",
+                (long long)n, (long long)kStaticN);
+  if (dim < 1 || dim > kStaticD)
+    return fail(RTOD_ERR_CAPACITY, "dim %d: the allocation-free entry point takes 1..%d", dim, kStaticD);
+  if (!(R >= 1e-18) || !(R <= 1e18) || !std::isfinite(R)) return fail(RTOD_ERR_CONFIG, "R must be finite and in [1e-18, 1e18]");
+  if (K < 0) return fail(RTOD_ERR_CONFIG, "K must be >= 0");
+  if (pred != RTOD_PRED_FP32_LE && pred != RTOD_PRED_F64_LT) return fail(RTOD_ERR_CONFIG, "unknown predicate %d", pred);
+  if (!is_device_ptr(pts) || !is_device_ptr(out_ids))
+    return fail(RTOD_ERR_ARG, "pts and out_ids must be device memory");
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  CU(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major != 10) return fail(RTOD_ERR_NODEV, "device %d is not sm_100", dev);
+  unsigned char* base = nullptr;
+  int r = static_scratch(&base);
+  if (r) return r;
+  cudaStream_t st = (cudaStream_t)stream;
+  auto at = [&](size_t off) { return (void*)(base + off); };
+
+  // Clear what must start at zero (the array keeps the previous call's contents).
+  CU(cudaMemsetAsync(at(kStatic.ctr), 0, sizeof(JobCtr), st));
+  CU(cudaMemsetAsync(at(kStatic.bs), 0, sizeof(BatchState), st));
+  CU(cudaMemsetAsync(at(kStatic.blo), 0x7f, sizeof(long long) * 6, st));
+  CU(cudaMemsetAsync(at(kStatic.bhi), 0x80, sizeof(long long) * 6, st));
+  CU(cudaMemsetAsync(at(kStatic.bcount), 0, sizeof(uint32_t) * NB, st));
+  CU(cudaMemsetAsync(at(kStatic.kmin), 0xff, sizeof(unsigned long long) * NB, st));
+  CU(cudaMemsetAsync(at(kStatic.kmax), 0, sizeof(unsigned long long) * NB, st));
+  CU(cudaMemsetAsync(at(kStatic.flags), 0, sizeof(uint32_t) * ((n + 31) / 32), st));
+  CU(cudaMemsetAsync(at(kStatic.scan), 0, sizeof(unsigned long long) * SCAN_TILES, st));
+  CU(cudaMemsetAsync(at(kStatic.cmp), 0, sizeof(unsigned long long) * ((kStaticN + CMP_TILE - 1) / CMP_TILE), st));
+
+  const int n_cells = 2;
+  Job jb{};
+  jb.W = n;
+  jb.S = n;  // one window, one slide block
+  jb.Wp = ((n + 3) / 4) * 4 + 4;
+  jb.cell = R * (1.0 + std::ldexp(1.0, -12)) / (double)n_cells;
+  jb.R = R;
+  jb.R2 = R * R;
+  {
+    volatile float rf = (float)R;
+    volatile float r2f = rf * rf;
+    jb.R2f = r2f;
+  }
+  jb.K = K;
+  jb.n = n_cells;
+  jb.filter = 1;
+  jb.ring = 0;
+  jb.pts = pts;
+  jb.keys = (const uint64_t*)at(kStatic.keys);
+  jb.stage = nullptr;
+  jb.blk_lo = (const long long*)at(kStatic.blo);
+  jb.blk_hi = (const long long*)at(kStatic.bhi);
+  jb.prev = (uint8_t*)at(kStatic.prev);
+  jb.bin_count = (uint32_t*)at(kStatic.bcount);
+  jb.bin_start = (uint32_t*)at(kStatic.bstart);
+  jb.kmin = (unsigned long long*)at(kStatic.kmin);
+  jb.kmax = (unsigned long long*)at(kStatic.kmax);
+  jb.s_off = (uint32_t*)at(kStatic.soff);
+  jb.s_ckey = (uint64_t*)at(kStatic.sckey);
+  jb.s_x = (float*)at(kStatic.sx);
+  jb.queue = (uint32_t*)at(kStatic.queue);
+  jb.feat = nullptr;
+  jb.flags = (uint32_t*)at(kStatic.flags);
+  jb.scan_status = (unsigned long long*)at(kStatic.scan);
+  jb.cmp_status = (unsigned long long*)at(kStatic.cmp);
+  jb.ctr = (JobCtr*)at(kStatic.ctr);
+  jb.rec_nout = nullptr;
+  jb.rec_undet = nullptr;
+  jb.rec_cap = 0;
+  // Pageable source: the copy has been staged when the call returns.
+  CU(cudaMemcpyAsync(at(kStatic.job), &jb, sizeof(Job), cudaMemcpyHostToDevice, st));
+
+  Batch b{};
+  b.jobs = (const Job*)at(kStatic.job);
+  b.njobs = 1;
+  b.bs = (BatchState*)at(kStatic.bs);
+  b.router = nullptr;
+  b.active = nullptr;
+  b.job_nout = nullptr;
+  b.out_ids = out_ids;
+  b.out_cap = n;
+  b.cmp_tiles = (n + CMP_TILE - 1) / CMP_TILE;
+
+  int sm = prop.multiProcessorCount;
+  const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sm * 8));
+  DISPATCH_D(dim, CU(launch_k(k_keys<D>, dim3(kx), 256, st, pts, (int64_t)0, n, jb.cell, (uint64_t*)at(kStatic.keys),
+                               (uint8_t*)at(kStatic.prev), b.bs, n, (long long*)at(kStatic.blo),
+                               (long long*)at(kStatic.bhi))));
+  const Geom g{n, n, dim, pred, 0, sm, 8, nullptr};
+  if ((r = launch_group(g, b, false, false, st, nullptr, nullptr))) return r;
+  BatchState s{};
+  CU(cudaMemcpyAsync(&s, at(kStatic.bs), sizeof(BatchState), cudaMemcpyDeviceToHost, st));
+  CU(cudaStreamSynchronize(st));
+  switch (s.err) {
+    case DERR_NONE: break;
+    case DERR_NONFINITE: return fail(RTOD_ERR_INPUT, "non-finite coordinate in the window");
+    case DERR_RANGE: return fail(RTOD_ERR_INPUT, "coordinate too large for the grid");
+    case DERR_CAPACITY: return fail(RTOD_ERR_CAPACITY, "outlier ID buffer too small");
+    case DERR_TIMEOUT: return fail(RTOD_ERR_TIMEOUT, "a bounded device-side wait ran out");
+    default: return fail(RTOD_ERR_CUDA, "device error %d", s.err);
+  }
+  *n_out = s.out_total;
+  return RTOD_OK;
+}
