@@ -51,6 +51,11 @@ extern "C" {
 #define RTOD_PRED_F64_LT 1  /* RTOD's double test: |dx| < R in 1-d, d^2 < R*R otherwise
                                (src/ods/optixScan.cu:170-190) */
 
+/* rtod_config.engine */
+#define RTOD_ENGINE_AUTO 0
+#define RTOD_ENGINE_WINDOW 1
+#define RTOD_ENGINE_SPAN 2
+
 typedef struct rtod_config {
   int64_t window;      /* W  (--window, src/ods/optixScan.cpp:166-171) */
   int64_t slide;       /* S  (--slide, :172-177); W % S == 0 (:1037) */
@@ -70,7 +75,13 @@ typedef struct rtod_config {
   int32_t device;      /* CUDA device ordinal */
   int32_t batch;       /* rtod_run: windows detected per launch (0 = auto); each window is
                           processed on its own, so results do not depend on it */
-  int32_t reserved[3];
+  int32_t engine;      /* rtod_run engine: RTOD_ENGINE_AUTO (span engine in 1-d without the
+                          router, else window engine; the tuner may choose either in 1-d),
+                          RTOD_ENGINE_WINDOW (one counting sort per window) or
+                          RTOD_ENGINE_SPAN (1-d only: one counting sort per batch of
+                          windows; falls back to the window engine when W/S > 2047).
+                          push/detect always use the window engine. Results are identical. */
+  int32_t reserved[2];
 } rtod_config;
 
 /* Per-slide stage times in ms, averaged over the slides of the last call,
@@ -130,13 +141,15 @@ int64_t rtod_slides_done(const rtod_handle* h);
 
 /* The resolved grid and launch parameters (after autotuning, if on):
    out[0] cells per R, out[1] warps per block of the range count,
-   out[2] hashed dimensions, out[3] windows per rtod_run launch.
+   out[2] hashed dimensions, out[3] windows per rtod_run launch, out[4] engine
+   of rtod_run (RTOD_ENGINE_WINDOW or RTOD_ENGINE_SPAN).
    With rtod_config.tuner = 1 the first rtod_run times candidate settings
-   (cells per R 1..3 or up to 6 in 1-d, 2/4/8 warps per block, 8..64 windows per launch and,
-   with the router on, its routing threshold and full-sweep size limit) on a
+   (in 1-d with engine = AUTO both engines, cells per R 1..3 or up to 6 in 1-d,
+   2/4/8 warps per block, 8..64 windows per launch and, with the router on and the
+   window engine, its routing threshold and full-sweep size limit) on a
    prefix of the stream and keeps the fastest; the choice is cached per
    configuration for the rest of the process. Results do not depend on it. */
-int rtod_get_tuning(const rtod_handle* h, int32_t out[4]);
+int rtod_get_tuning(const rtod_handle* h, int32_t out[5]);
 
 /* Counters since create: out[0] kernel launches issued by the library (a
    graph replay counts each of its kernels), out[1] graph replays, out[2]

@@ -26,6 +26,10 @@ class RtodError(RuntimeError):
         self.code = code
 
 
+ENGINE = {"auto": 0, "window": 1, "span": 2}
+ENGINE_NAME = {1: "window", 2: "span"}
+
+
 class Config(ctypes.Structure):
     _fields_ = [
         ("window", ctypes.c_int64), ("slide", ctypes.c_int64), ("R", ctypes.c_double),
@@ -33,7 +37,7 @@ class Config(ctypes.Structure):
         ("pred", ctypes.c_int32), ("router", ctypes.c_int32), ("tuner", ctypes.c_int32),
         ("cells_per_r", ctypes.c_int32), ("block_warps", ctypes.c_int32),
         ("use_graph", ctypes.c_int32), ("device", ctypes.c_int32), ("batch", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 3),
+        ("engine", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2),
     ]
 
 

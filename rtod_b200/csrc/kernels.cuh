@@ -88,6 +88,16 @@ struct BatchState {
   uint32_t done;        // finished k_compact tiles of the running batch
 };
 
+// Span engine counters (device), one per handle.
+struct SpanCtr {
+  uint32_t scan_ticket;  // tile tickets of the span's bin scan
+  uint32_t n_used;       // bins holding span points
+  int32_t pure;          // no two cells of the span share a bin
+  int32_t pad;
+};
+
+__device__ __forceinline__ void span_ctr_clear(SpanCtr* c) { c->n_used = 0; }
+
 struct Job {
   int64_t W, S, Wp;  // window, slide, padded SoA row stride (multiple of 4, >= W + 4)
   double cell;       // cell side: R * (1 + 2^-12) / n
@@ -136,6 +146,7 @@ struct Batch {
   int64_t* out_ids;  // outlier IDs of all jobs, concatenated in job order
   int64_t out_cap;
   int64_t cmp_tiles; // k_compact tiles over all jobs
+  SpanCtr* span;     // span engine counters, cleared by the last k_compact tile (null otherwise)
 };
 
 __device__ __forceinline__ void set_err(BatchState* bs, int32_t code) { atomicCAS(&bs->err, 0, code); }
@@ -466,22 +477,21 @@ struct Unroll {
   static constexpr int value = D <= 3 ? 4 : 2;
 };
 
-// Whether no two cells of the job's current window can share a bin: from the
-// per-slide-block coordinate ranges of a resident stream (a ring has none).
+// Whether no two cells of slide blocks [b0, b0 + nb) of a resident stream
+// can share a bin, from the per-block coordinate ranges (a ring has none).
 // The bin map is injective on boxes of at most 65536 cells (1-d),
 // 256 x 256 (2-d) or 16 x 64 x 64 (3-d). One warp computes it.
 template <int H>
-__device__ __forceinline__ bool window_pure(const Job& jb, int64_t lo) {
-  if (!jb.blk_lo) return false;
+__device__ __forceinline__ bool range_pure(const long long* blk_lo, const long long* blk_hi, int64_t b0,
+                                           int64_t nb) {
+  if (!blk_lo || nb > 4096) return false;
   const int lane = threadIdx.x & 31;
-  const int64_t b0 = lo / jb.S, nb = jb.W / jb.S;
-  if (nb > 4096) return false;
   long long mn[3] = {LLONG_MAX, LLONG_MAX, LLONG_MAX}, mx[3] = {LLONG_MIN, LLONG_MIN, LLONG_MIN};
   for (int64_t t = lane; t < nb; t += 32) {
 #pragma unroll
     for (int d = 0; d < H; ++d) {
-      mn[d] = min(mn[d], jb.blk_lo[(b0 + t) * 3 + d]);
-      mx[d] = max(mx[d], jb.blk_hi[(b0 + t) * 3 + d]);
+      mn[d] = min(mn[d], blk_lo[(b0 + t) * 3 + d]);
+      mx[d] = max(mx[d], blk_hi[(b0 + t) * 3 + d]);
     }
   }
   bool ok = true;
@@ -497,6 +507,12 @@ __device__ __forceinline__ bool window_pure(const Job& jb, int64_t lo) {
     ok &= span <= cap;
   }
   return ok;
+}
+
+// The same test for the job's current window.
+template <int H>
+__device__ __forceinline__ bool window_pure(const Job& jb, int64_t lo) {
+  return range_pure<H>(jb.blk_lo, jb.blk_hi, lo / jb.S, jb.W / jb.S);
 }
 
 
@@ -600,14 +616,11 @@ __global__ void __launch_bounds__(256) k_hist(Batch b) {
 // k_scan: exclusive scan of each job's NB bin counts. Grid (SCAN_TILES, jobs),
 // 256 threads; each thread owns 16 consecutive bins (four coalesced uint4).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_scan(Batch b) {
+__device__ __forceinline__ void scan_bins(const uint32_t* bin_count, uint32_t* bin_start,
+                                          unsigned long long* status, uint32_t* ticket, BatchState* bs) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t s_tile, s_prefix;
-  pdl_trigger();
-  pdl_wait();
-  if (!job_active(b)) return;
-  const Job& jb = b.jobs[blockIdx.y];
-  if (threadIdx.x == 0) s_tile = atomicAdd(&jb.ctr->scan_ticket, 1u);
+  if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
   __syncthreads();
   const uint32_t tile = s_tile;
   const uint32_t b0 = tile * SCAN_TILE + threadIdx.x * 16;
@@ -615,18 +628,18 @@ __global__ void __launch_bounds__(256) k_scan(Batch b) {
   uint32_t sum = 0;
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    v[q] = *reinterpret_cast<const uint4*>(jb.bin_count + b0 + 4 * q);
+    v[q] = *reinterpret_cast<const uint4*>(bin_count + b0 + 4 * q);
     sum += v[q].x + v[q].y + v[q].z + v[q].w;
   }
   uint32_t total;
   const uint32_t ex = block_exclusive_scan(sum, &total, sm);
   if (threadIdx.x < 32) {
-    const uint32_t pre = warp_lookback(jb.scan_status, tile, total, b.bs);
+    const uint32_t pre = warp_lookback(status, tile, total, bs);
     if (threadIdx.x == 0) {
       s_prefix = pre;
       if (tile == SCAN_TILES - 1) {
-        jb.bin_start[NB] = pre + total;
-        jb.ctr->scan_ticket = 0;
+        bin_start[NB] = pre + total;
+        *ticket = 0;
       }
     }
   }
@@ -639,8 +652,16 @@ __global__ void __launch_bounds__(256) k_scan(Batch b) {
     o.y = run; run += v[q].y;
     o.z = run; run += v[q].z;
     o.w = run; run += v[q].w;
-    *reinterpret_cast<uint4*>(jb.bin_start + b0 + 4 * q) = o;
+    *reinterpret_cast<uint4*>(bin_start + b0 + 4 * q) = o;
   }
+}
+
+__global__ void __launch_bounds__(256) k_scan(Batch b) {
+  pdl_trigger();
+  pdl_wait();
+  if (!job_active(b)) return;
+  const Job& jb = b.jobs[blockIdx.y];
+  scan_bins(jb.bin_count, jb.bin_start, jb.scan_status, &jb.ctr->scan_ticket, b.bs);
 }
 
 // ---------------------------------------------------------------------------
@@ -721,9 +742,11 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
   __shared__ uint32_t tbin[HIST_SLOTS];
   __shared__ uint32_t tcnt[HIST_SLOTS];
   __shared__ uint32_t tbase[HIST_SLOTS];
+  __shared__ unsigned long long s_routed[2];  // router statistics, flushed once per block
   pdl_trigger();
   pdl_wait();
   if (!job_active(b)) return;
+  if (ROUTE && threadIdx.x < 2) s_routed[threadIdx.x] = 0;
   constexpr int H = Hashed<D>::value;
   constexpr int U = Unroll<D>::value;
   const Job& jb = b.jobs[blockIdx.y];
@@ -866,11 +889,16 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
           }
         }
         if (lane == 0 && (need_e || need_s)) {
-          atomicAdd(&b.router->routed_early, (unsigned long long)__popc(need_e));
-          atomicAdd(&b.router->routed_sweep, (unsigned long long)__popc(need_s));
+          atomicAdd(&s_routed[0], (unsigned long long)__popc(need_e));
+          atomicAdd(&s_routed[1], (unsigned long long)__popc(need_s));
         }
       }
     }
+  }
+  if constexpr (ROUTE) {
+    __syncthreads();
+    if (threadIdx.x == 0 && s_routed[0]) atomicAdd(&b.router->routed_early, s_routed[0]);
+    if (threadIdx.x == 1 && s_routed[1]) atomicAdd(&b.router->routed_sweep, s_routed[1]);
   }
 }
 
@@ -1031,7 +1059,8 @@ __device__ __forceinline__ bool count_query(const Job& jb, uint32_t pos, int& to
   });
 }
 
-// Exact count of one queued point by one lane (full-sweep queue).
+// Exact count of one queued point by one lane (full-sweep queue): the
+// candidates are read 8 at a time, so that their loads are in flight together.
 template <int D, int PRED>
 __device__ __forceinline__ bool count_query_lane(const Job& jb, uint32_t pos, int& total) {
   constexpr int H = Hashed<D>::value;
@@ -1042,11 +1071,14 @@ __device__ __forceinline__ bool count_query_lane(const Job& jb, uint32_t pos, in
   unpack_key(jb.s_ckey[pos], H, k);
   total = 0;
   return for_each_run<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
-    for (uint32_t c = rs; c < re; ++c) {
-      float cx[D];
+    for (uint32_t c0 = rs; c0 < re; c0 += 8) {
+      float cx[8][D];
 #pragma unroll
-      for (int d = 0; d < D; ++d) cx[d] = jb.s_x[(int64_t)d * jb.Wp + c];
-      total += is_nbr<D, PRED>(qx, cx, jb.R2f, jb.R, jb.R2);
+      for (int e = 0; e < 8; ++e)
+#pragma unroll
+        for (int d = 0; d < D; ++d) cx[e][d] = c0 + e < re ? jb.s_x[(int64_t)d * jb.Wp + c0 + e] : 0.0f;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) total += (c0 + e < re) && is_nbr<D, PRED>(qx, cx[e], jb.R2f, jb.R, jb.R2);
       if (total > jb.K) return true;
     }
     return false;
@@ -1063,21 +1095,45 @@ __device__ __forceinline__ void record_count(const Job& jb, int64_t lo, uint32_t
   jb.prev[source_pos(jb, lo, i)] = (uint8_t)(total < 253 ? total : 253);
 }
 
+// Block-local buffer of router training samples and misroute count of
+// k_count, flushed to the router state once per block.
+constexpr int BLOCK_SAMPLES = 64;
+struct SampleBuf {
+  float s[BLOCK_SAMPLES][4];
+  uint32_t n;
+  uint32_t misrouted;
+};
+
 // Training sample of one routed point (one thread): its features and the
-// bucket of its exact capped count. Also counts misroutes.
-__device__ __forceinline__ void record_sample(const Job& jb, RouterState* rs, int64_t q, int total,
+// bucket of its exact capped count. Inliers (most points) are thinned to one
+// in INLIER_THIN by queue index so that the buckets are closer to balanced.
+__device__ __forceinline__ void record_sample(const Job& jb, SampleBuf& sb, int64_t q, int total,
                                               bool routed_early) {
   const int lab = count_bucket(total, jb.K);
-  if ((lab == 3) != routed_early) atomicAdd(&rs->misrouted, 1ull);
-  if (*(volatile uint32_t*)&rs->n_samples >= TRAIN_CAP) return;
-  // Most counted points are inliers: keep one inlier sample in INLIER_THIN so
-  // that the buckets are closer to balanced.
-  if (lab == 3 && (atomicAdd(&rs->inliers_seen, 1u) % INLIER_THIN) != 0) return;
-  const uint32_t s = atomicAdd(&rs->n_samples, 1u);
-  if (s >= TRAIN_CAP) return;
+  if ((lab == 3) != routed_early) atomicAdd(&sb.misrouted, 1u);
+  if (lab == 3 && (q % INLIER_THIN) != 0) return;
+  const uint32_t s = atomicAdd(&sb.n, 1u);
+  if (s >= BLOCK_SAMPLES) return;
 #pragma unroll
-  for (int j = 0; j < MLP_IN; ++j) rs->samples[s][j] = jb.feat[q * MLP_IN + j];
-  rs->samples[s][3] = (float)lab;
+  for (int j = 0; j < MLP_IN; ++j) sb.s[s][j] = jb.feat[q * MLP_IN + j];
+  sb.s[s][3] = (float)lab;
+}
+
+__device__ __forceinline__ void flush_samples(SampleBuf& sb, RouterState* rs) {
+  __syncthreads();
+  __shared__ uint32_t s_base;
+  const uint32_t n = min(sb.n, (uint32_t)BLOCK_SAMPLES);
+  if (threadIdx.x == 0) {
+    if (sb.misrouted) atomicAdd(&rs->misrouted, (unsigned long long)sb.misrouted);
+    s_base = (n && *(volatile uint32_t*)&rs->n_samples < TRAIN_CAP) ? atomicAdd(&rs->n_samples, n) : TRAIN_CAP;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t dst = s_base + i;
+    if (dst < TRAIN_CAP)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) rs->samples[dst][j] = sb.s[i][j];
+  }
 }
 
 // Per-job cleanup done by k_count: per-bin key ranges and compaction
@@ -1103,10 +1159,16 @@ __device__ __forceinline__ void reset_bins(const Job& jb) {
 // ---------------------------------------------------------------------------
 template <int D, int PRED, bool ROUTE>
 __global__ void __launch_bounds__(256) k_count(Batch b) {
+  __shared__ SampleBuf sb;
   pdl_trigger();
   pdl_wait();
   if (!job_active(b)) return;
   const Job& jb = b.jobs[blockIdx.y];
+  if (ROUTE && threadIdx.x == 0) {
+    sb.n = 0;
+    sb.misrouted = 0;
+  }
+  if (ROUTE) __syncthreads();
   reset_bins(jb);
   const int lane = threadIdx.x & 31;
   const int64_t lo = jb.ctr->lo;
@@ -1119,7 +1181,7 @@ __global__ void __launch_bounds__(256) k_count(Batch b) {
     const bool inlier = count_query<D, PRED>(jb, pos, total);
     if (lane == 0) {
       record_count(jb, lo, pos, inlier, total);
-      if constexpr (ROUTE) record_sample(jb, b.router, q, total, true);
+      if constexpr (ROUTE) record_sample(jb, sb, q, total, true);
     }
   }
   if constexpr (ROUTE) {
@@ -1132,9 +1194,10 @@ __global__ void __launch_bounds__(256) k_count(Batch b) {
         int total;
         const bool inlier = count_query_lane<D, PRED>(jb, pos, total);
         record_count(jb, lo, pos, inlier, total);
-        record_sample(jb, b.router, q, total, false);
+        record_sample(jb, sb, q, total, false);
       }
     }
+    flush_samples(sb, b.router);
   }
 }
 
@@ -1254,6 +1317,7 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
     bs->undet_total += tu;
     bs->slides += tn;
     bs->done = 0;
+    if (b.span) span_ctr_clear(b.span);
   }
 }
 

@@ -44,7 +44,7 @@ constexpr int OFF_B3 = OFF_W3 + MLP_B * MLP_H;    // 1312
 constexpr int MLP_P = OFF_B3 + MLP_B;             // 1316 parameters
 constexpr int TRAIN_CAP = 2048;                   // training samples buffered between steps
 constexpr int TRAIN_CHUNK = 128;                  // samples per chunk of k_train
-constexpr int TRAIN_MAX = 256;                    // samples used by one training step
+constexpr int TRAIN_MAX = 128;                    // samples used by one training step
 constexpr uint32_t INLIER_THIN = 16;              // inlier samples kept: one in 16
 constexpr int TQ0 = 32, TQ1 = 32, TQ2 = 16;       // routing table grid
 constexpr float F0_MAX = 1.5f, F1_MAX = 2.5f, F2_MIN = -1.0f, F2_MAX = 2.0f;
@@ -62,7 +62,6 @@ struct RouterState {
   uint32_t min_samples;  // train once at least this many samples are buffered
   float last_loss;
   uint32_t n_samples;  // samples buffered (atomic counter)
-  uint32_t inliers_seen;  // inlier samples offered (for thinning)
   float samples[TRAIN_CAP][4];  // f0, f1, f2, label
   // routing counters (since create)
   unsigned long long routed_early, routed_sweep, misrouted;
@@ -136,16 +135,20 @@ __device__ __forceinline__ float p_inlier(const float* z) {
 // summed over the samples in a fixed order by the thread that owns it.
 // grad (may be null) receives the mean-loss gradient; if adam, the parameters
 // take one Adam step. Returns the mean loss in *loss.
-// Shared memory: TRAIN_CHUNK * (3 + 32 + 32 + 32 + 32 + 4) floats.
+// Shared memory: TRAIN_CHUNK * (3 + 32 + 32 + 32 + 32 + 4) floats for the
+// per-sample rows, then a copy of the parameters (read by every sample).
 // ---------------------------------------------------------------------------
 constexpr int TRAIN_ROW = MLP_IN + 4 * MLP_H + MLP_B;  // x, h1, h2, d1, d2, d3 = 135
-constexpr size_t TRAIN_SMEM = sizeof(float) * TRAIN_CHUNK * TRAIN_ROW;
+constexpr size_t TRAIN_SMEM = sizeof(float) * (TRAIN_CHUNK * TRAIN_ROW + MLP_P);
 
 __device__ void mlp_train_block(float* P, float* m, float* v, float* b1t, float* b2t, float lr, float beta1,
                                 float beta2, float eps, const float* x, int xstride, const float* yf,
                                 int ystride, int n, float* grad, float* loss, bool adam, float* smem) {
   const int t = threadIdx.x;
   constexpr int PER = (MLP_P + 255) / 256;  // parameters owned per thread
+  float* PS = smem + TRAIN_CHUNK * TRAIN_ROW;
+  for (int i = t; i < MLP_P; i += blockDim.x) PS[i] = P[i];
+  __syncthreads();
   float g[PER];
 #pragma unroll
   for (int q = 0; q < PER; ++q) g[q] = 0.0f;
@@ -165,39 +168,49 @@ __device__ void mlp_train_block(float* P, float* m, float* v, float* b1t, float*
 #pragma unroll
       for (int j = 0; j < MLP_IN; ++j) xs[j] = x[(int64_t)s * xstride + j];
       const int lab = (int)yf[(int64_t)s * ystride];
-      float a1[MLP_H], a2[MLP_H];
+      // ReLU derivatives below use h > 0, which is the same test as a > 0.
+#pragma unroll 4
       for (int i = 0; i < MLP_H; ++i) {
-        float a = P[OFF_B1 + i];
-        for (int j = 0; j < MLP_IN; ++j) a = fmaf(P[OFF_W1 + i * MLP_IN + j], xs[j], a);
-        a1[i] = a;
+        float a = PS[OFF_B1 + i];
+#pragma unroll
+        for (int j = 0; j < MLP_IN; ++j) a = fmaf(PS[OFF_W1 + i * MLP_IN + j], xs[j], a);
         h1[i] = fmaxf(a, 0.0f);
       }
+#pragma unroll 2
       for (int i = 0; i < MLP_H; ++i) {
-        float a = P[OFF_B2 + i];
-        for (int j = 0; j < MLP_H; ++j) a = fmaf(P[OFF_W2 + i * MLP_H + j], h1[j], a);
-        a2[i] = a;
+        float a = PS[OFF_B2 + i];
+#pragma unroll 8
+        for (int j = 0; j < MLP_H; ++j) a = fmaf(PS[OFF_W2 + i * MLP_H + j], h1[j], a);
         h2[i] = fmaxf(a, 0.0f);
       }
       float z[MLP_B], mx = -INFINITY;
+#pragma unroll
       for (int k = 0; k < MLP_B; ++k) {
-        float a = P[OFF_B3 + k];
-        for (int j = 0; j < MLP_H; ++j) a = fmaf(P[OFF_W3 + k * MLP_H + j], h2[j], a);
+        float a = PS[OFF_B3 + k];
+#pragma unroll 8
+        for (int j = 0; j < MLP_H; ++j) a = fmaf(PS[OFF_W3 + k * MLP_H + j], h2[j], a);
         z[k] = a;
         mx = fmaxf(mx, a);
       }
       float se = 0.0f;
+#pragma unroll
       for (int k = 0; k < MLP_B; ++k) se += expf(z[k] - mx);
       lsum += -(z[lab] - mx - logf(se));
+#pragma unroll
       for (int k = 0; k < MLP_B; ++k) d3[k] = (expf(z[k] - mx) / se - (k == lab ? 1.0f : 0.0f)) * inv_n;
+#pragma unroll 4
       for (int j = 0; j < MLP_H; ++j) {
         float a = 0.0f;
-        for (int k = 0; k < MLP_B; ++k) a = fmaf(P[OFF_W3 + k * MLP_H + j], d3[k], a);
-        d2[j] = a2[j] > 0.0f ? a : 0.0f;
+#pragma unroll
+        for (int k = 0; k < MLP_B; ++k) a = fmaf(PS[OFF_W3 + k * MLP_H + j], d3[k], a);
+        d2[j] = h2[j] > 0.0f ? a : 0.0f;
       }
+#pragma unroll 2
       for (int j = 0; j < MLP_H; ++j) {
         float a = 0.0f;
-        for (int i = 0; i < MLP_H; ++i) a = fmaf(P[OFF_W2 + i * MLP_H + j], d2[i], a);
-        d1[j] = a1[j] > 0.0f ? a : 0.0f;
+#pragma unroll 8
+        for (int i = 0; i < MLP_H; ++i) a = fmaf(PS[OFF_W2 + i * MLP_H + j], d2[i], a);
+        d1[j] = h1[j] > 0.0f ? a : 0.0f;
       }
     }
     __syncthreads();
@@ -205,23 +218,19 @@ __device__ void mlp_train_block(float* P, float* m, float* v, float* b1t, float*
     for (int q = 0; q < PER; ++q) {
       const int p = t + q * 256;
       if (p >= MLP_P) break;
+      // gradient term of parameter p for one sample = row[a] * (b < 0 ? 1 : row[b])
+      int a, bb;
+      if (p < OFF_B1) { a = MLP_IN + 2 * MLP_H + p / MLP_IN; bb = p % MLP_IN; }
+      else if (p < OFF_W2) { a = MLP_IN + 2 * MLP_H + (p - OFF_B1); bb = -1; }
+      else if (p < OFF_B2) { a = MLP_IN + 3 * MLP_H + (p - OFF_W2) / MLP_H; bb = MLP_IN + (p - OFF_W2) % MLP_H; }
+      else if (p < OFF_W3) { a = MLP_IN + 3 * MLP_H + (p - OFF_B2); bb = -1; }
+      else if (p < OFF_B3) { a = MLP_IN + 4 * MLP_H + (p - OFF_W3) / MLP_H; bb = MLP_IN + MLP_H + (p - OFF_W3) % MLP_H; }
+      else { a = MLP_IN + 4 * MLP_H + (p - OFF_B3); bb = -1; }
       float acc = 0.0f;
-      for (int s = 0; s < cn; ++s) {
-        const float* row = smem + s * TRAIN_ROW;
-        const float* xs = row;
-        const float* h1 = xs + MLP_IN;
-        const float* h2 = h1 + MLP_H;
-        const float* d1 = h2 + MLP_H;
-        const float* d2 = d1 + MLP_H;
-        const float* d3 = d2 + MLP_H;
-        float term;
-        if (p < OFF_B1) term = d1[p / MLP_IN] * xs[p % MLP_IN];
-        else if (p < OFF_W2) term = d1[p - OFF_B1];
-        else if (p < OFF_B2) term = d2[(p - OFF_W2) / MLP_H] * h1[(p - OFF_W2) % MLP_H];
-        else if (p < OFF_W3) term = d2[p - OFF_B2];
-        else if (p < OFF_B3) term = d3[(p - OFF_W3) / MLP_H] * h2[(p - OFF_W3) % MLP_H];
-        else term = d3[p - OFF_B3];
-        acc += term;
+      if (bb >= 0) {
+        for (int s = 0; s < cn; ++s) acc = fmaf(smem[s * TRAIN_ROW + a], smem[s * TRAIN_ROW + bb], acc);
+      } else {
+        for (int s = 0; s < cn; ++s) acc += smem[s * TRAIN_ROW + a];
       }
       g[q] += acc;
     }
@@ -285,15 +294,18 @@ __global__ void __launch_bounds__(256) k_train(RouterState* rs) {
 
 // Routing table from the current parameters: one thread per grid cell.
 __global__ void __launch_bounds__(256) k_table(RouterState* rs) {
+  __shared__ float P[MLP_P];
   pdl_trigger();
   pdl_wait();
+  for (int i = threadIdx.x; i < MLP_P; i += blockDim.x) P[i] = rs->params[i];
+  __syncthreads();
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= TQ0 * TQ1 * TQ2) return;
   const int q2 = t % TQ2, q1 = (t / TQ2) % TQ1, q0 = t / (TQ2 * TQ1);
   const float x[MLP_IN] = {(q0 + 0.5f) * F0_MAX / TQ0, (q1 + 0.5f) * F1_MAX / TQ1,
                            F2_MIN + (q2 + 0.5f) * (F2_MAX - F2_MIN) / TQ2};
   float z[MLP_B];
-  mlp_forward(rs->params, x, z);
+  mlp_forward(P, x, z);
   rs->table[q0][q1][q2] = (uint8_t)fminf(255.0f, p_inlier(z) * 255.0f + 0.5f);
 }
 

@@ -21,6 +21,7 @@
 
 #include "../../include/rtod.h"
 #include "kernels.cuh"
+#include "span.cuh"
 
 #define RTOD_API extern "C" __attribute__((visibility("default")))
 
@@ -132,6 +133,26 @@ struct Scratch {
   unsigned long long* cmp_status = nullptr;
 };
 
+// Scratch of the span engine (one per handle): sized for spans of up to
+// nblk_cap slide blocks and pts_cap points.
+struct SpanScratch {
+  uint32_t* bin_count = nullptr;
+  uint32_t* bin_start = nullptr;
+  unsigned long long* kmin = nullptr;
+  unsigned long long* kmax = nullptr;
+  uint32_t* cnt = nullptr;
+  uint32_t* pre = nullptr;
+  uint32_t* used = nullptr;
+  uint32_t* s_off = nullptr;
+  float* s_x = nullptr;
+  unsigned long long* scan_status = nullptr;
+  SpanCtr* sc = nullptr;
+  int64_t nblk_cap = 0;
+  int64_t pts_cap = 0;
+  int64_t Wp = 0;
+  int64_t bytes = 0;
+};
+
 constexpr int kPipeKernels = 7;
 const char* kKernelNames[kPipeKernels] = {"k_keys",  "k_hist",    "k_scan", "k_scatter",
                                           "k_count", "k_compact", "k_train"};
@@ -161,7 +182,7 @@ void init_router(RouterState* r) {
   r->eps = 1e-8f;
   r->threshold = 0.5f;
   r->max_sweep = 64;
-  r->min_samples = 256;
+  r->min_samples = (uint32_t)TRAIN_MAX;
 }
 
 enum Mode { MODE_NONE = 0, MODE_RING = 1, MODE_RUN = 2 };
@@ -197,6 +218,8 @@ struct rtod_handle {
   int64_t device_bytes = 0;
 
   std::vector<Scratch> pool;  // allocated lazily up to batch_max
+  SpanScratch span;           // span engine scratch, allocated on first use
+  int engine = RTOD_ENGINE_WINDOW;  // engine of rtod_run (resolved from the config / tuner)
   JobCtr* ctr = nullptr;      // [batch_max]
   JobCtr* ctr_init = nullptr; // pinned host [batch_max]
   Job* jobs_dev = nullptr;    // [batch_max]
@@ -232,6 +255,8 @@ struct rtod_handle {
   cudaGraphExec_t graphs[2] = {nullptr, nullptr};  // without / with the router's training step
   int64_t graph_kernels[2] = {0, 0};
   Batch graph_batch{};
+  Span graph_span{};
+  bool graph_is_span = false;
   int graph_ring = -1;
   int64_t batches = 0;
 
@@ -268,6 +293,9 @@ int check_config(const rtod_config* c) {
       c->block_warps != 8)
     return fail(RTOD_ERR_CONFIG, "block_warps must be 0 (auto), 1, 2, 4 or 8");
   if (c->batch < 0 || c->batch > 256) return fail(RTOD_ERR_CONFIG, "batch must be 0..256");
+  if (c->engine < RTOD_ENGINE_AUTO || c->engine > RTOD_ENGINE_SPAN)
+    return fail(RTOD_ERR_CONFIG, "engine must be 0 (auto), 1 (window) or 2 (span)");
+  if (c->engine == RTOD_ENGINE_SPAN && c->dim != 1) return fail(RTOD_ERR_CONFIG, "the span engine needs dim = 1");
   return RTOD_OK;
 }
 
@@ -325,9 +353,93 @@ int scrub(rtod_handle* h) {
     CU(cudaMemsetAsync(s.scan_status, 0, SCAN_TILES * sizeof(unsigned long long), h->stream));
     CU(cudaMemsetAsync(s.cmp_status, 0, (size_t)cmp_tiles * sizeof(unsigned long long), h->stream));
   }
+  if (h->span.sc) {
+    SpanScratch& sp = h->span;
+    CU(cudaMemsetAsync(sp.bin_count, 0, NB * sizeof(uint32_t), h->stream));
+    CU(cudaMemsetAsync(sp.kmin, 0xff, NB * sizeof(unsigned long long), h->stream));
+    CU(cudaMemsetAsync(sp.kmax, 0, NB * sizeof(unsigned long long), h->stream));
+    CU(cudaMemsetAsync(sp.cnt, 0, (size_t)(sp.nblk_cap * NB) * sizeof(uint32_t), h->stream));
+    CU(cudaMemsetAsync(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long), h->stream));
+    CU(cudaMemsetAsync(sp.sc, 0, sizeof(SpanCtr), h->stream));
+  }
   CU(cudaMemsetAsync(h->ctr, 0, sizeof(JobCtr) * h->batch_max, h->stream));
   CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
   return RTOD_OK;
+}
+
+void free_span(rtod_handle* h) {
+  SpanScratch& sp = h->span;
+  dfree(sp.bin_count); dfree(sp.bin_start); dfree(sp.kmin); dfree(sp.kmax); dfree(sp.cnt); dfree(sp.pre);
+  dfree(sp.used); dfree(sp.s_off); dfree(sp.s_x); dfree(sp.scan_status); dfree(sp.sc);
+  h->device_bytes -= sp.bytes;
+  sp = SpanScratch{};
+}
+
+// Span scratch for spans of nblk slide blocks (nblk * S points).
+int ensure_span(rtod_handle* h, int64_t nblk) {
+  SpanScratch& sp = h->span;
+  const int64_t pts = nblk * h->S;
+  if (sp.sc && nblk <= sp.nblk_cap && pts <= sp.pts_cap) return RTOD_OK;
+  CU(cudaStreamSynchronize(h->stream));
+  free_span(h);
+  drop_graph(h);
+  const int64_t Wp = ((pts + 3) / 4) * 4 + 4;
+  int64_t bytes = 0;
+  bool ok = !dalloc(&sp.bin_count, NB, &bytes) && !dalloc(&sp.bin_start, NB + 1, &bytes) &&
+            !dalloc(&sp.kmin, NB, &bytes) && !dalloc(&sp.kmax, NB, &bytes) &&
+            !dalloc(&sp.cnt, (size_t)(nblk * NB), &bytes) && !dalloc(&sp.pre, (size_t)((nblk + 1) * NB), &bytes) &&
+            !dalloc(&sp.used, NB, &bytes) && !dalloc(&sp.s_off, (size_t)pts, &bytes) &&
+            !dalloc(&sp.s_x, (size_t)(Wp * h->D), &bytes) && !dalloc(&sp.scan_status, SCAN_TILES, &bytes) &&
+            !dalloc(&sp.sc, 1, &bytes);
+  sp.bytes = bytes;
+  h->device_bytes += bytes;
+  if (!ok) {
+    free_span(h);
+    return RTOD_ERR_CUDA;
+  }
+  sp.nblk_cap = nblk;
+  sp.pts_cap = pts;
+  sp.Wp = Wp;
+  CU(cudaMemset(sp.bin_count, 0, NB * sizeof(uint32_t)));
+  CU(cudaMemset(sp.kmin, 0xff, NB * sizeof(unsigned long long)));
+  CU(cudaMemset(sp.kmax, 0, NB * sizeof(unsigned long long)));
+  CU(cudaMemset(sp.cnt, 0, (size_t)(nblk * NB) * sizeof(uint32_t)));
+  CU(cudaMemset(sp.s_x, 0, (size_t)(Wp * h->D) * sizeof(float)));
+  CU(cudaMemset(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long)));
+  CU(cudaMemset(sp.sc, 0, sizeof(SpanCtr)));
+  return RTOD_OK;
+}
+
+// Span parameters of a batch of B windows over the resident stream.
+Span make_span(const rtod_handle* h, int B, const float* stream_pts) {
+  const SpanScratch& ss = h->span;
+  Span sp{};
+  sp.S = h->S;
+  sp.Wp = ss.Wp;
+  sp.wblk = (int32_t)(h->W / h->S);
+  sp.nblk = sp.wblk + B - 1;
+  sp.K = h->cfg.K;
+  sp.n = h->n;
+  sp.filter = h->filter;
+  sp.R = h->cfg.R;
+  sp.R2 = h->cfg.R * h->cfg.R;
+  sp.R2f = h->R2f;
+  sp.pts = stream_pts;
+  sp.keys = h->run_keys;
+  sp.blk_lo = h->run_blk_lo;
+  sp.blk_hi = h->run_blk_hi;
+  sp.bin_count = ss.bin_count;
+  sp.bin_start = ss.bin_start;
+  sp.kmin = ss.kmin;
+  sp.kmax = ss.kmax;
+  sp.cnt = ss.cnt;
+  sp.pre = ss.pre;
+  sp.used = ss.used;
+  sp.s_off = ss.s_off;
+  sp.s_x = ss.s_x;
+  sp.scan_status = ss.scan_status;
+  sp.sc = ss.sc;
+  return sp;
 }
 
 Job make_job(rtod_handle* h, int j, bool ring, const float* stream_pts) {
@@ -475,6 +587,37 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
   return RTOD_OK;
 }
 
+// Launches one batch of the span engine: hist prefix scan scatter classify
+// count compact. kev as for launch_group (kev[1] after hist + prefix, kev[4]
+// after classify + count).
+int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, cudaEvent_t* kev, int64_t* nk) {
+  const unsigned gy = (unsigned)b.njobs;
+  const int64_t npts = sp.nblk * sp.S;
+  const int64_t hx = std::max<int64_t>(1, std::min<int64_t>((npts + 1023) / 1024, (int64_t)g.sm_count * 8));
+  if (kev) CU(cudaEventRecord(kev[0], st));
+  CU(launch_k(k_span_hist<1>, dim3((unsigned)hx), 256, st, b, sp));
+  CU(launch_k(k_span_prefix, dim3(NB / 256), 256, st, b, sp));
+  if (kev) CU(cudaEventRecord(kev[1], st));
+  CU(launch_k(k_span_scan, dim3(SCAN_TILES), 256, st, b, sp));
+  if (kev) CU(cudaEventRecord(kev[2], st));
+  CU(launch_k(k_span_scatter<1>, dim3((unsigned)hx), 256, st, b, sp));
+  if (kev) CU(cudaEventRecord(kev[3], st));
+  CU(launch_k(k_span_classify, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
+  const int wpb = g.block_warps;
+  const int64_t cx = std::max<int64_t>(1, (int64_t)g.sm_count * (64 / wpb) / b.njobs);
+  if (g.pred == 0) {
+    CU(launch_k(k_span_count<1, 0>, dim3((unsigned)cx, gy), wpb * 32, st, b, sp));
+  } else {
+    CU(launch_k(k_span_count<1, 1>, dim3((unsigned)cx, gy), wpb * 32, st, b, sp));
+  }
+  if (kev) CU(cudaEventRecord(kev[4], st));
+  CU(launch_k(k_compact, dim3((unsigned)((g.Wmax + CMP_TILE - 1) / CMP_TILE), gy), 256, st, b));
+  if (kev) CU(cudaEventRecord(kev[5], st));
+  if (kev) CU(cudaEventRecord(kev[6], st));
+  if (nk) *nk = 7;
+  return RTOD_OK;
+}
+
 Geom geom_of(const rtod_handle* h) {
   return Geom{h->W, h->S, h->D, h->cfg.pred, h->cfg.router, h->sm_count, h->block_warps, h->router};
 }
@@ -483,25 +626,30 @@ constexpr int kTrainEvery = 8;  // batches between two router training steps
 
 bool train_now(rtod_handle* h) { return h->cfg.router && (h->batches++ % kTrainEvery) == 0; }
 
-int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev) {
+int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev, const Span* sp = nullptr) {
   int64_t nk = 0;
-  int r = launch_group(geom_of(h), b, ingest, train_now(h), h->stream, kev, &nk);
+  int r = sp ? launch_span(geom_of(h), b, *sp, h->stream, kev, &nk)
+             : launch_group(geom_of(h), b, ingest, train_now(h), h->stream, kev, &nk);
   h->launches += nk;
   return r;
 }
 
 // Runs one batch, replaying a captured graph when graphs are on (two graphs
 // with the router: with and without the training step).
-int run_batch(rtod_handle* h, const Batch& b, bool ingest) {
-  if (!h->cfg.use_graph) return launch_batch(h, b, ingest, nullptr);
-  const bool train = train_now(h);
+int run_batch(rtod_handle* h, const Batch& b, bool ingest, const Span* sp = nullptr) {
+  if (!h->cfg.use_graph) return launch_batch(h, b, ingest, nullptr, sp);
+  const bool train = sp ? false : train_now(h);
   cudaGraphExec_t& gx = h->graphs[train ? 1 : 0];
-  if (!gx || h->graph_ring != (int)ingest || std::memcmp(&h->graph_batch, &b, sizeof(Batch)) != 0) {
-    if (h->graph_ring != (int)ingest || std::memcmp(&h->graph_batch, &b, sizeof(Batch)) != 0) drop_graph(h);
+  const bool same = h->graph_ring == (int)ingest && std::memcmp(&h->graph_batch, &b, sizeof(Batch)) == 0 &&
+                    h->graph_is_span == (sp != nullptr) &&
+                    (!sp || std::memcmp(&h->graph_span, sp, sizeof(Span)) == 0);
+  if (!gx || !same) {
+    if (!same) drop_graph(h);
     cudaGraph_t g;
     CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int64_t nk = 0;
-    int r = launch_group(geom_of(h), b, ingest, train, h->stream, nullptr, &nk);
+    int r = sp ? launch_span(geom_of(h), b, *sp, h->stream, nullptr, &nk)
+               : launch_group(geom_of(h), b, ingest, train, h->stream, nullptr, &nk);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (r) return r;
     if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
@@ -510,6 +658,8 @@ int run_batch(rtod_handle* h, const Batch& b, bool ingest) {
     if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
     h->graph_batch = b;
     h->graph_ring = (int)ingest;
+    h->graph_is_span = sp != nullptr;
+    if (sp) h->graph_span = *sp;
     h->graph_kernels[train ? 1 : 0] = nk;
   }
   CU(cudaGraphLaunch(gx, h->stream));
@@ -615,6 +765,19 @@ int stage_stream(rtod_handle* h, const float* pts, int64_t used, const float** s
   return RTOD_OK;
 }
 
+// Whether rtod_run uses the span engine: one hashed dimension and at most
+// SPAN_MAX_BLOCKS slide blocks per window.
+bool use_span(const rtod_handle* h) {
+  return h->engine == RTOD_ENGINE_SPAN && h->D == 1 && h->W / h->S <= SPAN_MAX_BLOCKS;
+}
+
+// Largest batch of the span engine: spans of at most SPAN_MAX_BLOCKS blocks
+// and fewer than 2^31 points.
+int64_t span_batch_cap(const rtod_handle* h) {
+  const int64_t wblk = h->W / h->S;
+  return std::max<int64_t>(1, std::min<int64_t>(SPAN_MAX_BLOCKS, ((1ll << 31) - 1) / h->S) - wblk + 1);
+}
+
 int pick_batch(const rtod_handle* h, int64_t slides) {
   const int64_t b = h->cfg.batch ? h->cfg.batch : h->batch_max;
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, slides));
@@ -640,8 +803,11 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
   const float* src;
   if ((r = ensure_records(h, slides))) return r;
   if ((r = ensure_ids(h, std::max<int64_t>(1, std::min(ids_cap, slides * W))))) return r;
-  const int B = pick_batch(h, slides);
+  const bool span = use_span(h);
+  int B = pick_batch(h, slides);
+  if (span) B = (int)std::min<int64_t>(B, span_batch_cap(h));
   if ((r = ensure_pool(h, B))) return r;
+  if (span && (r = ensure_span(h, W / S + B - 1))) return r;
   if (e_begin) CU(cudaEventRecord(e_begin, h->stream));
   if ((r = stage_stream(h, pts, used, &src))) return r;
   if ((r = configure(h, MODE_RUN, B, S, src))) return r;  // first detected window: [S, W + S)
@@ -653,15 +819,26 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
   if (e_keys) CU(cudaEventRecord(e_keys, h->stream));
   const int64_t out_cap = std::min(ids_cap, h->ids_cap);
   const int64_t full = slides / B, rem = slides % B;
-  const Batch bfull = make_batch(h, B, out_cap);
+  Batch bfull = make_batch(h, B, out_cap);
+  const Span sfull = span ? make_span(h, B, src) : Span{};
+  if (span) bfull.span = h->span.sc;
   for (int64_t i = 0; i < full + (rem ? 1 : 0); ++i) {
-    const Batch b = i < full ? bfull : make_batch(h, (int)rem, out_cap);
+    Batch b = bfull;
+    Span sp = sfull;
+    if (i == full) {
+      b = make_batch(h, (int)rem, out_cap);
+      if (span) {
+        b.span = h->span.sc;
+        sp = make_span(h, (int)rem, src);
+      }
+    }
+    const Span* spp = span ? &sp : nullptr;
     if (kev) {
       cudaEvent_t* e = &(*kev)[(size_t)i * 8];
       CU(cudaEventRecord(e[0], h->stream));
-      r = launch_batch(h, b, false, e + 1);
+      r = launch_batch(h, b, false, e + 1, spp);
     } else {
-      r = i < full ? run_batch(h, b, false) : launch_batch(h, b, false, nullptr);
+      r = i < full ? run_batch(h, b, false, spp) : launch_batch(h, b, false, nullptr, spp);
     }
     if (r) return r;
   }
@@ -686,6 +863,7 @@ void free_all(rtod_handle* h) {
     dfree(s.cmp_status);
   }
   h->pool.clear();
+  free_span(h);
   dfree(h->ctr); dfree(h->jobs_dev); dfree(h->bs); dfree(h->router); dfree(h->ring); dfree(h->ring_keys);
   dfree(h->ring_prev); dfree(h->staging); dfree(h->run_buf); dfree(h->run_keys); dfree(h->run_prev);
   dfree(h->run_blk_lo); dfree(h->run_blk_hi);
@@ -713,6 +891,7 @@ struct Tuning {
   int batch = 32;
   float threshold = 0.5f;
   uint32_t max_sweep = 64;
+  int engine = RTOD_ENGINE_WINDOW;
 };
 
 struct TuneEntry {
@@ -734,6 +913,7 @@ int apply_tuning(rtod_handle* h, const Tuning& t) {
   h->cfg.batch = std::min(t.batch, h->batch_max);
   h->threshold = t.threshold;
   h->max_sweep = t.max_sweep;
+  h->engine = t.engine;
   if (h->router) {
     CU(cudaMemcpy((char*)h->router + offsetof(RouterState, threshold), &t.threshold, sizeof(float),
                   cudaMemcpyHostToDevice));
@@ -787,6 +967,7 @@ int autotune(rtod_handle* h, const float* pts, int64_t slides_total) {
   CU(cudaMemcpy(dev, pts, (size_t)(used * D) * sizeof(float), cudaMemcpyDefault));
   Tuning best;
   best.batch = std::min(32, h->batch_max);
+  best.engine = h->engine;
   int r = apply_tuning(h, best);
   if (r) return r;
   float best_ms;
@@ -802,6 +983,11 @@ int autotune(rtod_handle* h, const float* pts, int64_t slides_total) {
     }
     return RTOD_OK;
   };
+  if (h->D == 1 && h->cfg.engine == RTOD_ENGINE_AUTO) {
+    Tuning t = best;
+    t.engine = best.engine == RTOD_ENGINE_SPAN ? RTOD_ENGINE_WINDOW : RTOD_ENGINE_SPAN;
+    if ((r = trial(t))) return r;
+  }
   for (int n : {1, 3, 4, 6}) {
     if (n > 3 && h->D != 1) continue;
     Tuning t = best;
@@ -819,7 +1005,7 @@ int autotune(rtod_handle* h, const float* pts, int64_t slides_total) {
     t.batch = bt;
     if ((r = trial(t))) return r;
   }
-  if (h->cfg.router) {
+  if (h->cfg.router && best.engine == RTOD_ENGINE_WINDOW) {
     for (float th : {0.3f, 0.7f}) {
       Tuning t = best;
       t.threshold = th;
@@ -899,6 +1085,10 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
     h->R2f = r2f;
   }
   set_grid(h, cfg->cells_per_r ? cfg->cells_per_r : 2);
+  // Engine of rtod_run: the span engine by default in 1-d without the router.
+  h->engine = cfg->engine != RTOD_ENGINE_AUTO
+                  ? cfg->engine
+                  : ((cfg->dim == 1 && !cfg->router) ? RTOD_ENGINE_SPAN : RTOD_ENGINE_WINDOW);
   // Windows per rtod_run launch: up to 32, within ~1 GiB of scratch.
   const int64_t per_job = (int64_t)NB * 24 + h->W * (4 + 8 + 4 + 4) + h->Wp * h->D * 4 + h->W / 8;
   h->batch_max = (int)std::max<int64_t>(1, std::min<int64_t>(32, (1ll << 30) / per_job));
@@ -959,12 +1149,13 @@ RTOD_API int rtod_reset(rtod_handle* h) {
 
 RTOD_API int64_t rtod_slides_done(const rtod_handle* h) { return h ? h->slides_done : -1; }
 
-RTOD_API int rtod_get_tuning(const rtod_handle* h, int32_t out[4]) {
+RTOD_API int rtod_get_tuning(const rtod_handle* h, int32_t out[5]) {
   if (!h || !out) return fail(RTOD_ERR_ARG, "null argument");
   out[0] = h->n;
   out[1] = h->block_warps;
   out[2] = h->D < 3 ? h->D : 3;
   out[3] = (int32_t)(h->cfg.batch ? std::min(h->cfg.batch, h->batch_max) : h->batch_max);
+  out[4] = use_span(h) ? RTOD_ENGINE_SPAN : RTOD_ENGINE_WINDOW;
   return RTOD_OK;
 }
 

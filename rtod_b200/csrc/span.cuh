@@ -1,0 +1,477 @@
+// Span engine (one hashed dimension): one counting sort per batch of B
+// consecutive windows instead of one per window.
+//
+// The B windows of a batch, [lo0 + jS, lo0 + jS + W) for j < B, cover the
+// span [lo0, lo0 + W + (B-1)S): nblk = W/S + B - 1 slide blocks of S points,
+// and every window is a union of W/S whole blocks. The span is sorted once by
+// bin, and inside each bin by block (points of one block in any order):
+//
+//   position of a point of block t in bin b
+//     = bin_start[b] + pre[t][b] + (its claim among the block's points in b),
+//   pre[t][b] = points of bin b in blocks before t.
+//
+// So window j's points of bin b are the contiguous positions
+// [bin_start[b] + pre[j][b], bin_start[b] + pre[j + W/S][b]), and its count
+// of bin b is pre[j + W/S][b] - pre[j][b]: classification needs no per-point
+// work, and a queued point's candidates are 2n+1 such ranges.
+//
+// Kernels per batch: k_span_hist (per-block bin counts), k_span_prefix (pre,
+// list of bins in use), k_span_scan (bin_start), k_span_scatter (sorted
+// span), k_span_classify (per window and bin: safe or queued), k_span_count
+// (exact counts of the queued points, per window), then k_compact of the
+// window engine turns each window's outlier bits into sorted IDs.
+//
+// The safe-inlier rule is the window engine's (count > K in one cell, plus
+// the 1-d group rule), with "single cell" judged over the whole span: a bin
+// whose span holds two cells queues its points even in a window where it
+// holds one. That only queues more points; every result is an exact count.
+#pragma once
+
+#include "kernels.cuh"
+
+namespace rtod {
+
+constexpr int64_t SPAN_MAX_BLOCKS = 2047;  // slide blocks of one span (tables of (blocks + 1) x NB)
+
+struct Span {
+  int64_t S;       // slide = block size
+  int64_t Wp;      // row stride of s_x (multiple of 4, >= span points + 4)
+  int64_t nblk;    // blocks in the span: W/S + B - 1
+  int32_t wblk;    // blocks per window: W/S
+  int32_t K, n, filter;
+  double R, R2;
+  float R2f;
+  const float* pts;         // resident stream, point-major [N][D]
+  const uint64_t* keys;     // cell keys of the stream, by global index
+  const long long* blk_lo;  // per slide block cell coordinate range (span purity)
+  const long long* blk_hi;
+  uint32_t* bin_count;          // [NB] span points per bin
+  uint32_t* bin_start;          // [NB + 1]
+  unsigned long long* kmin;     // [NB] smallest / largest cell key of a bin over the span
+  unsigned long long* kmax;
+  uint32_t* cnt;    // [nblk][NB] points of block t in bin b (claims count them back to zero)
+  uint32_t* pre;    // [nblk + 1][NB] points of bin b in the blocks before t (bins in use only)
+  uint32_t* used;   // [NB] bins holding span points, n_used of them, in no particular order
+  uint32_t* s_off;  // [span] bin-ordered: offset from the span start
+  float* s_x;       // [D][Wp] bin-ordered coordinates
+  unsigned long long* scan_status;  // [SCAN_TILES]
+  SpanCtr* sc;
+};
+
+// First global index of the span: the window of the batch's first job.
+__device__ __forceinline__ int64_t span_lo(const Batch& b) { return b.jobs[0].ctr->lo; }
+
+// ---------------------------------------------------------------------------
+// k_span_hist: points per (block, bin) and per bin, and per-bin key ranges
+// unless the span is pure. Aggregated per warp, then per block in a
+// shared-memory table keyed by block * NB + bin, then one atomic per entry.
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
+  static_assert(Hashed<D>::value == 1, "span engine: one hashed dimension");
+  __shared__ uint32_t hkey[HIST_SLOTS];
+  __shared__ uint32_t hcnt[HIST_SLOTS];
+  __shared__ unsigned long long hmin[HIST_SLOTS], hmax[HIST_SLOTS];
+  __shared__ int s_pure;
+  pdl_trigger();
+  pdl_wait();
+  constexpr int U = 4;
+  const int64_t lo0 = span_lo(b);
+  const int64_t npts = sp.nblk * sp.S;
+  const int lane = threadIdx.x & 31;
+  if (threadIdx.x < 32) {
+    const bool pure = range_pure<1>(sp.blk_lo, sp.blk_hi, lo0 / sp.S, sp.nblk);
+    if (threadIdx.x == 0) {
+      s_pure = pure;
+      if (blockIdx.x == 0) sp.sc->pure = pure;
+    }
+  }
+  for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
+    hkey[t] = 0xffffffffu;
+    hcnt[t] = 0;
+    hmin[t] = EMPTY_KEY;
+    hmax[t] = 0;
+  }
+  __syncthreads();
+  const bool pure = s_pure;
+  const uint32_t S32 = (uint32_t)sp.S;
+  const int64_t chunk = (int64_t)blockDim.x * U;
+  for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < npts; c0 += (int64_t)gridDim.x * chunk) {
+    const int64_t w0 = c0 + (int64_t)(threadIdx.x >> 5) * 32 * U;
+    uint64_t key[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = w0 + u * 32 + lane;
+      key[u] = i < npts ? sp.keys[lo0 + i] : EMPTY_KEY;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = w0 + u * 32 + lane;
+      const bool valid = key[u] != EMPTY_KEY;
+      const uint32_t bin = (uint32_t)key[u] & NB_MASK;
+      const uint32_t comp = valid ? ((uint32_t)i / S32) * NB + bin : 0xffffffffu;
+      const unsigned peers = __match_any_sync(0xffffffffu, comp);
+      const int leader = __ffs(peers) - 1;
+      const uint64_t lkey = __shfl_sync(0xffffffffu, key[u], leader);
+      const bool mixed_grp = (__ballot_sync(0xffffffffu, key[u] != lkey) & peers) != 0;
+      int slot = -1;
+      if (valid && lane == leader) {
+        const uint32_t c = (uint32_t)__popc(peers);
+        uint32_t sl = (comp * 2654435761u) >> (32 - 8);
+#pragma unroll 1
+        for (int probe = 0; probe < 8; ++probe) {
+          const uint32_t old = atomicCAS(&hkey[sl], 0xffffffffu, comp);
+          if (old == 0xffffffffu || old == comp) {
+            atomicAdd(&hcnt[sl], c);
+            slot = (int)sl;
+            break;
+          }
+          sl = (sl + 1) & (HIST_SLOTS - 1);
+        }
+        if (slot < 0) {
+          atomicAdd(&sp.cnt[comp], c);
+          atomicAdd(&sp.bin_count[bin], c);
+        }
+      }
+      if (!pure) {
+        slot = __shfl_sync(0xffffffffu, slot, leader);
+        if (valid && (mixed_grp || lane == leader)) {
+          if (slot >= 0) {
+            atomicMin(&hmin[slot], (unsigned long long)key[u]);
+            atomicMax(&hmax[slot], (unsigned long long)key[u]);
+          } else {
+            atomicMin(&sp.kmin[bin], (unsigned long long)key[u]);
+            atomicMax(&sp.kmax[bin], (unsigned long long)key[u]);
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
+    const uint32_t comp = hkey[t];
+    if (comp != 0xffffffffu) {
+      const uint32_t bin = comp & NB_MASK;
+      atomicAdd(&sp.cnt[comp], hcnt[t]);
+      atomicAdd(&sp.bin_count[bin], hcnt[t]);
+      if (!pure) {
+        atomicMin(&sp.kmin[bin], hmin[t]);
+        atomicMax(&sp.kmax[bin], hmax[t]);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_span_prefix: one thread per bin; for a bin in use, appends it to the list
+// of bins in use and writes pre[t][b] for t = 0..nblk (8 loads in flight).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_span_prefix(Batch b, Span sp) {
+  pdl_trigger();
+  pdl_wait();
+  const uint32_t bin = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t c = bin < NB ? sp.bin_count[bin] : 0u;
+  const unsigned has = __ballot_sync(0xffffffffu, c != 0);
+  if (!has) return;
+  const int lane = threadIdx.x & 31;
+  uint32_t base = 0;
+  if (lane == 0) base = atomicAdd(&sp.sc->n_used, (uint32_t)__popc(has));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (c == 0) return;
+  sp.used[base + __popc(has & lanemask_lt())] = bin;
+  const uint32_t* __restrict__ cnt = sp.cnt + bin;
+  uint32_t* __restrict__ pre = sp.pre + bin;
+  uint32_t run = 0;
+  int64_t t = 0;
+  for (; t + 8 <= sp.nblk; t += 8) {
+    uint32_t v[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) v[e] = cnt[(t + e) * NB];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+      pre[(t + e) * NB] = run;
+      run += v[e];
+    }
+  }
+  for (; t < sp.nblk; ++t) {
+    const uint32_t v = cnt[t * NB];
+    pre[t * NB] = run;
+    run += v;
+  }
+  pre[sp.nblk * NB] = run;
+}
+
+// k_span_scan: bin_start of the span (exclusive scan of bin_count).
+__global__ void __launch_bounds__(256) k_span_scan(Batch b, Span sp) {
+  pdl_trigger();
+  pdl_wait();
+  scan_bins(sp.bin_count, sp.bin_start, sp.scan_status, &sp.sc->scan_ticket, b.bs);
+}
+
+// ---------------------------------------------------------------------------
+// k_span_scatter: the span in (bin, block) order. A block-local table
+// aggregates the points of one chunk per (block, bin); each entry claims its
+// positions with one atomicSub on cnt, which returns cnt to zero.
+// ---------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(256) k_span_scatter(Batch b, Span sp) {
+  __shared__ uint32_t tkey[HIST_SLOTS];
+  __shared__ uint32_t tcnt[HIST_SLOTS];
+  __shared__ uint32_t tbase[HIST_SLOTS];
+  pdl_trigger();
+  pdl_wait();
+  constexpr int U = 4;
+  const int64_t lo0 = span_lo(b);
+  const int64_t npts = sp.nblk * sp.S;
+  if (blockIdx.x == 0 && threadIdx.x < SCAN_TILES) sp.scan_status[threadIdx.x] = 0;
+  for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
+    tkey[t] = 0xffffffffu;
+    tcnt[t] = 0;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = lanemask_lt();
+  const uint32_t S32 = (uint32_t)sp.S;
+  const int64_t chunk = (int64_t)blockDim.x * U;
+  for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < npts; c0 += (int64_t)gridDim.x * chunk) {
+    const int64_t w0 = c0 + (int64_t)(threadIdx.x >> 5) * 32 * U;
+    uint64_t key[U];
+    uint32_t comp[U], goff[U];
+    int slot[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = w0 + u * 32 + lane;
+      key[u] = i < npts ? sp.keys[lo0 + i] : EMPTY_KEY;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int64_t i = w0 + u * 32 + lane;
+      const bool valid = key[u] != EMPTY_KEY;
+      comp[u] = valid ? ((uint32_t)i / S32) * NB + ((uint32_t)key[u] & NB_MASK) : 0xffffffffu;
+      const unsigned peers = __match_any_sync(0xffffffffu, comp[u]);
+      const int leader = __ffs(peers) - 1;
+      int sl_found = -1;
+      uint32_t off = 0;
+      if (valid && lane == leader) {
+        const uint32_t c = (uint32_t)__popc(peers);
+        uint32_t sl = (comp[u] * 2654435761u) >> (32 - 8);
+#pragma unroll 1
+        for (int probe = 0; probe < 8; ++probe) {
+          const uint32_t old = atomicCAS(&tkey[sl], 0xffffffffu, comp[u]);
+          if (old == 0xffffffffu || old == comp[u]) {
+            off = atomicAdd(&tcnt[sl], c);
+            sl_found = (int)sl;
+            break;
+          }
+          sl = (sl + 1) & (HIST_SLOTS - 1);
+        }
+        if (sl_found < 0) off = atomicSub(&sp.cnt[comp[u]], c) - c;  // table full: claim directly
+      }
+      slot[u] = __shfl_sync(0xffffffffu, sl_found, leader);
+      goff[u] = __shfl_sync(0xffffffffu, off, leader) + __popc(peers & lt);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
+      const uint32_t k = tkey[t];
+      if (k != 0xffffffffu) {
+        const uint32_t c = tcnt[t];
+        tbase[t] = atomicSub(&sp.cnt[k], c) - c;
+        tkey[t] = 0xffffffffu;
+        tcnt[t] = 0;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (comp[u] != 0xffffffffu) {
+        const int64_t i = w0 + u * 32 + lane;
+        const uint32_t bin = comp[u] & NB_MASK;
+        const uint32_t pos = sp.bin_start[bin] + sp.pre[comp[u]] + goff[u] + (slot[u] >= 0 ? tbase[slot[u]] : 0u);
+        sp.s_off[pos] = (uint32_t)i;
+#pragma unroll
+        for (int d = 0; d < D; ++d) sp.s_x[(int64_t)d * sp.Wp + pos] = sp.pts[(lo0 + i) * D + d];
+      }
+    }
+  }
+}
+
+// 1-d group rule of the window engine over window counts of the span: some
+// run of n-1 consecutive cells containing the cell of bin `bin` holds more
+// than K window points, every bin of the run holding nothing in the window
+// or only its expected cell over the whole span.
+__device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* p0, const uint32_t* p1,
+                                                uint32_t bin, bool pure) {
+  const int m = sp.n - 1;
+  if (m < 2 || bin < (uint32_t)(m - 1) || bin + m > NB - 1) return false;
+  constexpr int MMAX = 7;
+  uint32_t wc[2 * MMAX - 1];
+  bool ok[2 * MMAX - 1];
+  const unsigned long long key = sp.kmin[bin];
+#pragma unroll
+  for (int t = 0; t < 2 * MMAX - 1; ++t) {
+    wc[t] = 0;
+    ok[t] = false;
+    if (t < 2 * m - 1) {
+      const uint32_t j = bin - m + 1 + t;
+      const bool any = sp.bin_count[j] != 0;
+      wc[t] = any ? p1[j] - p0[j] : 0u;
+      const unsigned long long want = key + (unsigned long long)(t - (m - 1));
+      ok[t] = pure || wc[t] == 0 || (sp.kmin[j] == want && sp.kmax[j] == want);
+    }
+  }
+#pragma unroll
+  for (int g = 0; g < MMAX; ++g) {
+    if (g < m) {
+      bool all = true;
+      uint32_t sum = 0;
+#pragma unroll
+      for (int t = 0; t < MMAX; ++t)
+        if (t < m) {
+          all &= ok[g + t];
+          sum += wc[g + t];
+        }
+      if (all && sum > (uint32_t)sp.K) return true;
+    }
+  }
+  return false;
+}
+
+// ---------------------------------------------------------------------------
+// k_span_classify: one thread per (window, bin in use): the window's count of
+// the bin from pre; a bin that is not provably all-inlier queues its window
+// points (contiguous positions) in that window's queue.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
+  pdl_trigger();
+  pdl_wait();
+  const uint32_t nu = sp.sc->n_used;
+  const bool pure = sp.sc->pure;
+  const int64_t pairs = (int64_t)nu * b.njobs;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < pairs; e += stride) {
+    const int j = (int)(e / nu);
+    const uint32_t bin = sp.used[e - (int64_t)j * nu];
+    const uint32_t* p0 = sp.pre + (int64_t)j * NB;
+    const uint32_t* p1 = p0 + (int64_t)sp.wblk * NB;
+    const uint32_t a = p0[bin];
+    const uint32_t wc = p1[bin] - a;
+    if (wc == 0) continue;
+    bool safe = false;
+    if (sp.filter) {
+      const bool single = pure || sp.kmin[bin] == sp.kmax[bin];
+      safe = single && wc > (uint32_t)sp.K;
+      if (!safe && single && sp.n >= 3) safe = span_group_safe(sp, p0, p1, bin, pure);
+    }
+    if (safe) continue;
+    const Job& jb = b.jobs[j];
+    const uint32_t base = (uint32_t)atomicAdd(&jb.ctr->n_undet, (int)wc);
+    const uint32_t p = sp.bin_start[bin] + a;
+    for (uint32_t q = 0; q < wc; ++q) jb.queue[base + q] = p + q;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_span_count: grid (x, windows); one warp per queued point of its window.
+// Lane s < 2n+1 takes stencil cell key + d(s), d = 0, -1, +1, -2, +2, ...
+// (nearest first), and that bin's window range; a warp scan turns the range
+// lengths into offsets of one virtual candidate list, consumed 128 per step.
+// A point with at most K candidates is an outlier without any distance test.
+// Also clears the per-bin state of the bins in use for the next batch.
+// ---------------------------------------------------------------------------
+template <int D, int PRED>
+__global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
+  pdl_trigger();
+  pdl_wait();
+  const int j = blockIdx.y;
+  const Job& jb = b.jobs[j];
+  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (j == 0) {
+    const uint32_t nu = sp.sc->n_used;
+    for (int64_t u = gtid; u < nu; u += gstride) {
+      const uint32_t bin = sp.used[u];
+      sp.bin_count[bin] = 0;
+      sp.kmin[bin] = EMPTY_KEY;
+      sp.kmax[bin] = 0;
+    }
+  }
+  {
+    const int64_t tiles = (jb.W + CMP_TILE - 1) / CMP_TILE;
+    for (int64_t t = gtid; t < tiles; t += gstride) jb.cmp_status[t] = 0;
+  }
+  const int lane = threadIdx.x & 31;
+  const int64_t lo0 = span_lo(b);
+  const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
+  const uint32_t* p0 = sp.pre + (int64_t)j * NB;
+  const uint32_t* p1 = p0 + (int64_t)sp.wblk * NB;
+  const int slots = 2 * sp.n + 1;
+  const int64_t warp = gtid >> 5;
+  const int64_t nwarps = gstride >> 5;
+  const int64_t nq = jb.ctr->n_undet;
+  for (int64_t q = warp; q < nq; q += nwarps) {
+    const uint32_t pos = jb.queue[q];
+    const uint32_t i = sp.s_off[pos];
+    const uint64_t key = sp.keys[lo0 + i];
+    float qx[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) qx[d] = sp.s_x[(int64_t)d * sp.Wp + pos];
+    uint32_t rs = 0, len = 0;
+    if (lane < slots) {
+      const int dk = (lane & 1) ? -((lane + 1) >> 1) : (lane >> 1);
+      const uint32_t bin = (uint32_t)(key + (unsigned long long)(long long)dk) & NB_MASK;
+      const uint32_t b0 = sp.bin_start[bin], b1 = sp.bin_start[bin + 1];
+      if (b1 > b0) {
+        const uint32_t a = p0[bin];
+        rs = b0 + a;
+        len = p1[bin] - a;
+      }
+    }
+    uint32_t inc = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    const uint32_t off = inc - len;
+    const uint32_t T = __shfl_sync(0xffffffffu, inc, 31);
+    bool inlier = false;
+    if (T > (uint32_t)sp.K) {
+      int total = 0;
+      for (uint32_t v0 = 0; v0 < T && !inlier; v0 += 128) {
+        bool in[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const uint32_t v = v0 + 32 * e + lane;
+          // slot holding v: the last slot whose offset is <= v
+          int s = 0;
+#pragma unroll
+          for (int step = 16; step > 0; step >>= 1) {
+            const int cand = s + step;
+            const uint32_t oc = __shfl_sync(0xffffffffu, off, cand & 31);
+            if (cand < slots && oc <= v) s = cand;
+          }
+          const uint32_t base = __shfl_sync(0xffffffffu, rs, s);
+          const uint32_t os = __shfl_sync(0xffffffffu, off, s);
+          in[e] = false;
+          if (v < T) {
+            const uint32_t c = base + (v - os);
+            float cx[D];
+#pragma unroll
+            for (int d = 0; d < D; ++d) cx[d] = sp.s_x[(int64_t)d * sp.Wp + c];
+            in[e] = is_nbr<D, PRED>(qx, cx, sp.R2f, sp.R, sp.R2);
+          }
+        }
+        total += __popc(__ballot_sync(0xffffffffu, in[0])) + __popc(__ballot_sync(0xffffffffu, in[1])) +
+                 __popc(__ballot_sync(0xffffffffu, in[2])) + __popc(__ballot_sync(0xffffffffu, in[3]));
+        inlier = total > sp.K;
+      }
+    }
+    if (lane == 0 && !inlier) {
+      const int64_t w = (int64_t)i - shift;
+      atomicOr(&jb.flags[w >> 5], 1u << (w & 31));
+      atomicAdd(&jb.ctr->n_out, 1);
+    }
+  }
+}
+
+}  // namespace rtod

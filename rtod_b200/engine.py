@@ -54,6 +54,11 @@ class RunResult:
         return self.ids[self.offsets[j]:self.offsets[j + 1]]
 
 
+# Kernels of the span engine timed in each stage slot of rtod_profile_run.
+SPAN_STAGES = {"k_hist": "k_span_hist+k_span_prefix", "k_scan": "k_span_scan",
+               "k_scatter": "k_span_scatter", "k_count": "k_span_classify+k_span_count"}
+
+
 class Detector:
     """Sliding-window distance outlier detector on one CUDA device.
 
@@ -64,7 +69,7 @@ class Detector:
     def __init__(self, window: int, slide: int, R: float, K: int, dim: int = 1, opt: int = 2,
                  pred: str = "fp32_le", router: bool = False, tuner: bool = False,
                  cells_per_r: int = 0, block_warps: int = 0, use_graph: bool = True,
-                 batch: int = 0, device: int = 0):
+                 batch: int = 0, device: int = 0, engine: str = "auto"):
         cfg = Config()
         check(lib().rtod_config_init(ctypes.byref(cfg)))
         cfg.window, cfg.slide, cfg.R, cfg.K, cfg.dim, cfg.opt = window, slide, R, K, dim, opt
@@ -72,6 +77,7 @@ class Detector:
         cfg.router, cfg.tuner = int(router), int(tuner)
         cfg.cells_per_r, cfg.block_warps = cells_per_r, block_warps
         cfg.use_graph, cfg.device, cfg.batch = int(use_graph), device, batch
+        cfg.engine = _native.ENGINE[engine]
         self.cfg = cfg
         self.window, self.slide, self.R, self.K, self.dim = window, slide, R, K, dim
         self._h = ctypes.c_void_p()
@@ -160,12 +166,14 @@ class Detector:
         ms = (ctypes.c_double * 8)()
         check(lib().rtod_profile_run(self._h, ptr, n, max_slides, ms, 8))
         del keep
+        span = self.tuning["engine"] == "span"
         out = {}
         for i in range(8):
             name = lib().rtod_kernel_name(i)
             if name is None:
                 break
-            out[name.decode()] = ms[i]
+            name = name.decode()
+            out[SPAN_STAGES.get(name, name) if span else name] = ms[i]
         return out
 
     def reset(self) -> None:
@@ -187,9 +195,10 @@ class Detector:
 
     @property
     def tuning(self) -> dict:
-        a = (ctypes.c_int32 * 4)()
+        a = (ctypes.c_int32 * 5)()
         check(lib().rtod_get_tuning(self._h, a))
-        return {"cells_per_r": a[0], "block_warps": a[1], "hashed_dims": a[2], "batch": a[3]}
+        return {"cells_per_r": a[0], "block_warps": a[1], "hashed_dims": a[2], "batch": a[3],
+                "engine": _native.ENGINE_NAME.get(a[4], a[4])}
 
     def ring_slots(self, ids: np.ndarray) -> np.ndarray:
         """RTOD's outlier IDs (ring slots, optixScan.cpp:1097) for global indices."""

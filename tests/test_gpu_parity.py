@@ -29,11 +29,15 @@ def assert_same(res, off, ids):
 
 @pytest.mark.parametrize("path", golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
 @pytest.mark.parametrize("opt,graph,n", [(2, True, 0), (0, False, 0), (2, False, 1), (1, True, 3)])
-def test_run_matches_golden(rtod, path, opt, graph, n):
+@pytest.mark.parametrize("engine", ["window", "span"])
+def test_run_matches_golden(rtod, path, opt, graph, n, engine):
     meta, pts, off, ids = load_golden(path)
+    if engine == "span" and pts.shape[1] != 1:
+        pytest.skip("the span engine is 1-d only")
     with rtod.Detector(meta["W"], meta["S"], meta["R"], meta["K"], dim=pts.shape[1], opt=opt,
-                       pred=meta["pred"], use_graph=graph, cells_per_r=n) as det:
+                       pred=meta["pred"], use_graph=graph, cells_per_r=n, engine=engine) as det:
         assert_same(det.run(pts), off, ids)
+        assert det.tuning["engine"] == engine
 
 
 @pytest.mark.parametrize("path", golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
@@ -95,8 +99,10 @@ def test_full_size_properties(rtod):
     from rtod_b200 import datagen
     w = datagen.stock_like()
     runs = []
-    for kw in (dict(), dict(opt=0), dict(cells_per_r=1), dict(cells_per_r=3, use_graph=False),
-               dict(block_warps=2), dict(cells_per_r=4), dict(cells_per_r=7, batch=5)):
+    for kw in (dict(engine="window"), dict(opt=0), dict(cells_per_r=1), dict(cells_per_r=3, use_graph=False),
+               dict(block_warps=2), dict(cells_per_r=4), dict(cells_per_r=7, batch=5),
+               dict(engine="window", cells_per_r=4), dict(engine="window", cells_per_r=7, batch=5),
+               dict(engine="span", batch=64), dict(engine="span", batch=1), dict(engine="span", opt=0, batch=13)):
         with rtod.Detector(w.window, w.slide, w.R, w.K, **kw) as det:
             runs.append(det.run(w.points))
     base = runs[0]

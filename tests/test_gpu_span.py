@@ -1,0 +1,112 @@
+"""The span engine (one counting sort per batch of windows, 1-d) against the
+CPU oracle and against the window engine, on the cases where its layout
+differs from one sort per window: spans whose cells share bins, many slide
+blocks per window, batches of one window, every point an outlier, the grid
+filter off, the double predicate, and the fall-back to the window engine when
+a window holds more slide blocks than a span table allows. Bit-exact."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def rtod():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from rtod_b200 import build
+    build.build()
+    import rtod_b200
+    return rtod_b200
+
+
+def run(rtod, pts, W, S, R, K, slides, **kw):
+    pts = pts[:W + slides * S]
+    with rtod.Detector(W, S, R, K, dim=1, **kw) as det:
+        res = det.run(pts)
+        return res, det.tuning
+
+
+def check_vs_oracle(rtod, oracle_mod, pts, W, S, R, K, slides, pred="fp32_le", **kw):
+    off, ids, _ = oracle_mod.detect(pts[:W + slides * S], W, S, R, K, pred, engine="grid", threads=8)
+    res, tun = run(rtod, pts, W, S, R, K, slides, pred=pred, engine="span", **kw)
+    assert tun["engine"] == "span"
+    np.testing.assert_array_equal(res.offsets, off)
+    np.testing.assert_array_equal(res.ids, ids)
+    return res
+
+
+def test_cells_sharing_bins(rtod, oracle_mod):
+    """Span key range far above 65536 cells, so that bins hold several cells:
+    tight clusters (dense cells) among uniform points over a wide range."""
+    rng = np.random.default_rng(71)
+    n = 40_000
+    centres = rng.uniform(0, 5000, 60)
+    clustered = centres[rng.integers(0, 60, n)] + rng.normal(0, 5e-4, n)
+    uniform = rng.uniform(0, 5000, n)
+    pts = np.where(rng.random(n) < 0.6, clustered, uniform).astype(np.float32)[:, None]
+    R = 0.004  # cells of R/2 = 0.002: about 2.5 million cells over the range
+    for nc in (2, 5):
+        check_vs_oracle(rtod, oracle_mod, pts, 8000, 400, R, 20, 40, cells_per_r=nc, batch=16)
+
+
+def test_many_blocks_per_window(rtod, oracle_mod):
+    from rtod_b200 import datagen
+    pts = datagen.random_walk(30_000, 0.1, seed=72, jump_frac=0.005)
+    check_vs_oracle(rtod, oracle_mod, pts, 6000, 30, 0.3, 15, 300, batch=64)
+
+
+def test_batch_of_one_and_ragged_last_batch(rtod, oracle_mod):
+    from rtod_b200 import datagen
+    pts = datagen.random_walk(30_000, 0.1, seed=73, jump_frac=0.005)
+    check_vs_oracle(rtod, oracle_mod, pts, 5000, 500, 0.3, 12, 45, batch=1)
+    check_vs_oracle(rtod, oracle_mod, pts, 5000, 500, 0.3, 12, 45, batch=7)
+
+
+def test_all_outliers_and_filter_off(rtod, oracle_mod):
+    from rtod_b200 import datagen
+    pts = datagen.random_walk(20_000, 0.1, seed=74)
+    res = check_vs_oracle(rtod, oracle_mod, pts, 4000, 400, 0.3, 4000, 20)
+    assert res.offsets[-1] == 20 * 4000  # K >= W: every window point is an outlier
+    check_vs_oracle(rtod, oracle_mod, pts, 4000, 400, 0.3, 10, 20, opt=0)
+
+
+def test_double_predicate(rtod, oracle_mod):
+    from rtod_b200 import datagen
+    w = datagen.stock_like()
+    check_vs_oracle(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, 40, pred="f64_lt")
+
+
+def test_full_stream_span_equals_window(rtod):
+    """Whole stock-like stream: span and window engines, several grids."""
+    from rtod_b200 import datagen
+    w = datagen.stock_like()
+    base, _ = run(rtod, w.points, w.window, w.slide, w.R, w.K, w.slides, engine="window")
+    for kw in (dict(), dict(cells_per_r=1), dict(cells_per_r=3), dict(cells_per_r=6, batch=64),
+               dict(use_graph=False, batch=9)):
+        got, tun = run(rtod, w.points, w.window, w.slide, w.R, w.K, w.slides, engine="span", **kw)
+        assert tun["engine"] == "span"
+        np.testing.assert_array_equal(got.offsets, base.offsets)
+        np.testing.assert_array_equal(got.ids, base.ids)
+
+
+def test_too_many_blocks_falls_back_to_window_engine(rtod, oracle_mod):
+    from rtod_b200 import datagen
+    pts = datagen.random_walk(24_000, 0.1, seed=75, jump_frac=0.005)
+    W, S = 20_480, 10  # 2048 slide blocks per window
+    off, ids, _ = oracle_mod.detect(pts[:W + 5 * S], W, S, 0.3, 20, engine="grid", threads=8)
+    res, tun = run(rtod, pts, W, S, 0.3, 20, 5, engine="span")
+    assert tun["engine"] == "window"
+    np.testing.assert_array_equal(res.offsets, off)
+    np.testing.assert_array_equal(res.ids, ids)
+
+
+def test_engine_auto_with_tuner(rtod):
+    from rtod_b200 import datagen
+    w = datagen.stock_like()
+    base, _ = run(rtod, w.points, w.window, w.slide, w.R, w.K, 60, engine="window")
+    got, tun = run(rtod, w.points, w.window, w.slide, w.R, w.K, 60, tuner=True)
+    assert tun["engine"] in ("span", "window")
+    np.testing.assert_array_equal(got.offsets, base.offsets)
+    np.testing.assert_array_equal(got.ids, base.ids)
