@@ -176,7 +176,8 @@ def algorithmic_bytes(kernel: str, w, n_out_per_slide: float, undet_per_slide: f
         # read keys + points, write bin-ordered offsets + coordinates, once per batch
         "k_span_scatter": ((8 + 4 * d) + (4 + 4 * d)) * span_pts / batch,
         # per queued point: queue entry, offset, key, coordinates
-        "k_span_classify+k_span_count": undet_per_slide * (4 + 4 + 8 + 4 * d),
+        # per counted point: its offset and coordinates
+        "k_span_classify+k_span_count": undet_per_slide * (4 + 4 * d),
     }[kernel]
 
 

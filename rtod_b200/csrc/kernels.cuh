@@ -76,7 +76,7 @@ struct JobCtr {
   int32_t n_sweep;       // queued points of the full-sweep queue (router on)
   int32_t last_nout;     // outliers of the job's last detected window
   int32_t pure;          // current window: no two of its cells share a bin
-  int32_t pad;
+  int32_t n_pairs;       // span engine: groups listed for the window
 };
 
 // Per-handle state (device).
@@ -88,15 +88,20 @@ struct BatchState {
   uint32_t done;        // finished k_compact tiles of the running batch
 };
 
-// Span engine counters (device), one per handle.
+// Span engine counters (device), one per handle, and the per-bin arrays
+// that k_compact clears after each batch.
 struct SpanCtr {
   uint32_t scan_ticket;  // tile tickets of the span's bin scan
   uint32_t n_used;       // bins holding span points
   int32_t pure;          // no two cells of the span share a bin
   int32_t pad;
+  uint32_t* used;        // [NB] bins in use
+  uint32_t* bin_count;   // [NB]
+  unsigned long long* kmin;  // [NB]
+  unsigned long long* kmax;  // [NB]
 };
 
-__device__ __forceinline__ void span_ctr_clear(SpanCtr* c) { c->n_used = 0; }
+__device__ __forceinline__ void span_clear_bins(const SpanCtr* c);
 
 struct Job {
   int64_t W, S, Wp;  // window, slide, padded SoA row stride (multiple of 4, >= W + 4)
@@ -120,9 +125,10 @@ struct Job {
   uint32_t* s_off;        // [W] cell-ordered: window offset (global index - lo)
   uint64_t* s_ckey;       // [W] cell-ordered: cell key
   float* s_x;             // [D][Wp] cell-ordered coordinates
-  uint32_t* queue;        // [W] cell-ordered positions that need an exact count; with the
+  uint32_t* queue;        // [2W] cell-ordered positions that need an exact count; with the
                           // router on, the early-exit queue grows from the front and the
-                          // full-sweep queue from the back
+                          // full-sweep queue back from W - 1; the span engine keeps its
+                          // (first position, points) groups here, two words each
   float* feat;            // [W][3] router features, at the same index as the queue entry
   uint32_t* flags;        // [ceil(W / 32)] outlier bit per window offset
   unsigned long long* scan_status;  // [SCAN_TILES]
@@ -1260,6 +1266,7 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
       ++o;
     }
   }
+  if (b.span) span_clear_bins(b.span);  // span batches: every job has the same W (no early return above)
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) s_last = (atomicAdd(&bs->done, 1u) == (uint32_t)(b.cmp_tiles - 1));
@@ -1292,6 +1299,7 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
     c->n_out = 0;
     c->n_undet = 0;
     c->n_sweep = 0;
+    c->n_pairs = 0;
     c->cmp_ticket = 0;
   }
 #pragma unroll
@@ -1317,7 +1325,7 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
     bs->undet_total += tu;
     bs->slides += tn;
     bs->done = 0;
-    if (b.span) span_ctr_clear(b.span);
+    if (b.span) b.span->n_used = 0;
   }
 }
 

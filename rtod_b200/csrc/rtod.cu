@@ -323,7 +323,7 @@ int ensure_pool(rtod_handle* h, int jobs) {
     int64_t* c = &h->device_bytes;
     bool ok = !dalloc(&s.bin_count, NB, c) && !dalloc(&s.bin_start, NB + 1, c) && !dalloc(&s.kmin, NB, c) &&
               !dalloc(&s.kmax, NB, c) && !dalloc(&s.s_off, (size_t)W, c) && !dalloc(&s.s_ckey, (size_t)W, c) &&
-              !dalloc(&s.s_x, (size_t)(Wp * D), c) && !dalloc(&s.queue, (size_t)W, c) &&
+              !dalloc(&s.s_x, (size_t)(Wp * D), c) && !dalloc(&s.queue, (size_t)(2 * W), c) &&
               !dalloc(&s.feat, (size_t)(h->cfg.router ? W * MLP_IN : 1), c) &&
               !dalloc(&s.flags, (size_t)((W + 31) / 32), c) && !dalloc(&s.scan_status, SCAN_TILES, c) &&
               !dalloc(&s.cmp_status, (size_t)cmp_tiles, c);
@@ -360,7 +360,7 @@ int scrub(rtod_handle* h) {
     CU(cudaMemsetAsync(sp.kmax, 0, NB * sizeof(unsigned long long), h->stream));
     CU(cudaMemsetAsync(sp.cnt, 0, (size_t)(sp.nblk_cap * NB) * sizeof(uint32_t), h->stream));
     CU(cudaMemsetAsync(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long), h->stream));
-    CU(cudaMemsetAsync(sp.sc, 0, sizeof(SpanCtr), h->stream));
+    CU(cudaMemsetAsync(sp.sc, 0, offsetof(SpanCtr, used), h->stream));  // counters only
   }
   CU(cudaMemsetAsync(h->ctr, 0, sizeof(JobCtr) * h->batch_max, h->stream));
   CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
@@ -406,7 +406,12 @@ int ensure_span(rtod_handle* h, int64_t nblk) {
   CU(cudaMemset(sp.cnt, 0, (size_t)(nblk * NB) * sizeof(uint32_t)));
   CU(cudaMemset(sp.s_x, 0, (size_t)(Wp * h->D) * sizeof(float)));
   CU(cudaMemset(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long)));
-  CU(cudaMemset(sp.sc, 0, sizeof(SpanCtr)));
+  SpanCtr c{};
+  c.used = sp.used;
+  c.bin_count = sp.bin_count;
+  c.kmin = sp.kmin;
+  c.kmax = sp.kmax;
+  CU(cudaMemcpy(sp.sc, &c, sizeof(SpanCtr), cudaMemcpyHostToDevice));
   return RTOD_OK;
 }
 
@@ -421,6 +426,7 @@ Span make_span(const rtod_handle* h, int B, const float* stream_pts) {
   sp.K = h->cfg.K;
   sp.n = h->n;
   sp.filter = h->filter;
+  sp.cell = h->cell;
   sp.R = h->cfg.R;
   sp.R2 = h->cfg.R * h->cfg.R;
   sp.R2f = h->R2f;
@@ -1090,7 +1096,7 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
                   ? cfg->engine
                   : ((cfg->dim == 1 && !cfg->router) ? RTOD_ENGINE_SPAN : RTOD_ENGINE_WINDOW);
   // Windows per rtod_run launch: up to 32, within ~1 GiB of scratch.
-  const int64_t per_job = (int64_t)NB * 24 + h->W * (4 + 8 + 4 + 4) + h->Wp * h->D * 4 + h->W / 8;
+  const int64_t per_job = (int64_t)NB * 24 + h->W * (4 + 8 + 8 + 4) + h->Wp * h->D * 4 + h->W / 8;
   h->batch_max = (int)std::max<int64_t>(1, std::min<int64_t>(32, (1ll << 30) / per_job));
   if (cfg->batch) h->batch_max = cfg->batch;
 

@@ -17,9 +17,10 @@
 //
 // Kernels per batch: k_span_hist (per-block bin counts), k_span_prefix (pre,
 // list of bins in use), k_span_scan (bin_start), k_span_scatter (sorted
-// span), k_span_classify (per window and bin: safe or queued), k_span_count
-// (exact counts of the queued points, per window), then k_compact of the
-// window engine turns each window's outlier bits into sorted IDs.
+// span), k_span_classify (per window and bin in use: safe, or listed),
+// k_span_count (exact counts of the listed bins' window points), then
+// k_compact of the window engine turns each window's outlier bits into
+// sorted IDs and clears the per-bin state.
 //
 // The safe-inlier rule is the window engine's (count > K in one cell, plus
 // the 1-d group rule), with "single cell" judged over the whole span: a bin
@@ -39,7 +40,7 @@ struct Span {
   int64_t nblk;    // blocks in the span: W/S + B - 1
   int32_t wblk;    // blocks per window: W/S
   int32_t K, n, filter;
-  double R, R2;
+  double cell, R, R2;
   float R2f;
   const float* pts;         // resident stream, point-major [N][D]
   const uint64_t* keys;     // cell keys of the stream, by global index
@@ -337,111 +338,64 @@ __device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* 
 }
 
 // ---------------------------------------------------------------------------
-// k_span_classify: one thread per (window, bin in use): the window's count of
-// the bin from pre; a bin that is not provably all-inlier queues its window
-// points (contiguous positions) in that window's queue.
-// ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
-  pdl_trigger();
-  pdl_wait();
-  const uint32_t nu = sp.sc->n_used;
-  const bool pure = sp.sc->pure;
-  const int64_t pairs = (int64_t)nu * b.njobs;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < pairs; e += stride) {
-    const int j = (int)(e / nu);
-    const uint32_t bin = sp.used[e - (int64_t)j * nu];
-    const uint32_t* p0 = sp.pre + (int64_t)j * NB;
-    const uint32_t* p1 = p0 + (int64_t)sp.wblk * NB;
-    const uint32_t a = p0[bin];
-    const uint32_t wc = p1[bin] - a;
-    if (wc == 0) continue;
-    bool safe = false;
-    if (sp.filter) {
-      const bool single = pure || sp.kmin[bin] == sp.kmax[bin];
-      safe = single && wc > (uint32_t)sp.K;
-      if (!safe && single && sp.n >= 3) safe = span_group_safe(sp, p0, p1, bin, pure);
-    }
-    if (safe) continue;
-    const Job& jb = b.jobs[j];
-    const uint32_t base = (uint32_t)atomicAdd(&jb.ctr->n_undet, (int)wc);
-    const uint32_t p = sp.bin_start[bin] + a;
-    for (uint32_t q = 0; q < wc; ++q) jb.queue[base + q] = p + q;
-  }
-}
-
-// ---------------------------------------------------------------------------
-// k_span_count: grid (x, windows); one warp per queued point of its window.
-// Lane s < 2n+1 takes stencil cell key + d(s), d = 0, -1, +1, -2, +2, ...
-// (nearest first), and that bin's window range; a warp scan turns the range
-// lengths into offsets of one virtual candidate list, consumed 128 per step.
-// A point with at most K candidates is an outlier without any distance test.
-// Also clears the per-bin state of the bins in use for the next batch.
+// Exact counts of nq points of window j at bin-ordered positions
+// [p, p + nq), all of one cell, by one warp. Lane s < 2n+1 takes stencil cell
+// key + d(s), d = 0, -1, +1, -2, +2, ... (nearest first), and that bin's
+// window range; a warp scan turns the range lengths into offsets of one
+// virtual candidate list of T entries. With T <= K every point is an outlier
+// (its count cannot exceed T). Otherwise the list is read 256 candidates at a
+// time (8 per lane, kept in registers) and every undecided point of the group
+// (up to 32, one per lane) is tested against the chunk: per point, 8 tests per
+// lane and one warp reduction; a point is decided as soon as its count
+// exceeds K, and the chunks stop when every point is decided.
 // ---------------------------------------------------------------------------
 template <int D, int PRED>
-__global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
-  pdl_trigger();
-  pdl_wait();
-  const int j = blockIdx.y;
+__device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp, int j, uint32_t p,
+                                                 uint32_t nq, const uint32_t* p0, const uint32_t* p1) {
+  const int lane = threadIdx.x & 31;
   const Job& jb = b.jobs[j];
-  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (j == 0) {
-    const uint32_t nu = sp.sc->n_used;
-    for (int64_t u = gtid; u < nu; u += gstride) {
-      const uint32_t bin = sp.used[u];
-      sp.bin_count[bin] = 0;
-      sp.kmin[bin] = EMPTY_KEY;
-      sp.kmax[bin] = 0;
+  const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
+  float x0[D];
+#pragma unroll
+  for (int d = 0; d < D; ++d) x0[d] = sp.s_x[(int64_t)d * sp.Wp + p];
+  int32_t code;
+  const uint64_t key = cell_key<D>(x0, sp.cell, &code);  // the key k_keys gave these points
+  const int slots = 2 * sp.n + 1;
+  uint32_t rs = 0, len = 0;
+  if (lane < slots) {
+    const int dk = (lane & 1) ? -((lane + 1) >> 1) : (lane >> 1);
+    const uint32_t bin = (uint32_t)(key + (unsigned long long)(long long)dk) & NB_MASK;
+    const uint32_t b0 = sp.bin_start[bin], b1 = sp.bin_start[bin + 1];
+    if (b1 > b0) {
+      const uint32_t a = p0[bin];
+      rs = b0 + a;
+      len = p1[bin] - a;
     }
   }
-  {
-    const int64_t tiles = (jb.W + CMP_TILE - 1) / CMP_TILE;
-    for (int64_t t = gtid; t < tiles; t += gstride) jb.cmp_status[t] = 0;
+  uint32_t inc = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
   }
-  const int lane = threadIdx.x & 31;
-  const int64_t lo0 = span_lo(b);
-  const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
-  const uint32_t* p0 = sp.pre + (int64_t)j * NB;
-  const uint32_t* p1 = p0 + (int64_t)sp.wblk * NB;
-  const int slots = 2 * sp.n + 1;
-  const int64_t warp = gtid >> 5;
-  const int64_t nwarps = gstride >> 5;
-  const int64_t nq = jb.ctr->n_undet;
-  for (int64_t q = warp; q < nq; q += nwarps) {
-    const uint32_t pos = jb.queue[q];
-    const uint32_t i = sp.s_off[pos];
-    const uint64_t key = sp.keys[lo0 + i];
+  const uint32_t off = inc - len;
+  const uint32_t T = __shfl_sync(0xffffffffu, inc, 31);
+  int nout = 0;
+  for (uint32_t g = 0; g < nq; g += 32) {
+    const uint32_t q = g + lane;
+    const bool has = q < nq;
     float qx[D];
 #pragma unroll
-    for (int d = 0; d < D; ++d) qx[d] = sp.s_x[(int64_t)d * sp.Wp + pos];
-    uint32_t rs = 0, len = 0;
-    if (lane < slots) {
-      const int dk = (lane & 1) ? -((lane + 1) >> 1) : (lane >> 1);
-      const uint32_t bin = (uint32_t)(key + (unsigned long long)(long long)dk) & NB_MASK;
-      const uint32_t b0 = sp.bin_start[bin], b1 = sp.bin_start[bin + 1];
-      if (b1 > b0) {
-        const uint32_t a = p0[bin];
-        rs = b0 + a;
-        len = p1[bin] - a;
-      }
-    }
-    uint32_t inc = len;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += y;
-    }
-    const uint32_t off = inc - len;
-    const uint32_t T = __shfl_sync(0xffffffffu, inc, 31);
-    bool inlier = false;
+    for (int d = 0; d < D; ++d) qx[d] = has ? sp.s_x[(int64_t)d * sp.Wp + p + q] : 0.0f;
+    int cnt = 0;
+    unsigned live = __ballot_sync(0xffffffffu, has);
     if (T > (uint32_t)sp.K) {
-      int total = 0;
-      for (uint32_t v0 = 0; v0 < T && !inlier; v0 += 128) {
-        bool in[4];
+      for (uint32_t c0 = 0; c0 < T && live; c0 += 256) {
+        float cx[8][D];
+        bool cv[8];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const uint32_t v = v0 + 32 * e + lane;
+        for (int e = 0; e < 8; ++e) {
+          const uint32_t v = c0 + 32 * e + lane;
           // slot holding v: the last slot whose offset is <= v
           int s = 0;
 #pragma unroll
@@ -452,25 +406,139 @@ __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
           }
           const uint32_t base = __shfl_sync(0xffffffffu, rs, s);
           const uint32_t os = __shfl_sync(0xffffffffu, off, s);
-          in[e] = false;
-          if (v < T) {
-            const uint32_t c = base + (v - os);
-            float cx[D];
+          cv[e] = v < T;
+          const uint32_t c = base + (v - os);
 #pragma unroll
-            for (int d = 0; d < D; ++d) cx[d] = sp.s_x[(int64_t)d * sp.Wp + c];
-            in[e] = is_nbr<D, PRED>(qx, cx, sp.R2f, sp.R, sp.R2);
-          }
+          for (int d = 0; d < D; ++d) cx[e][d] = cv[e] ? sp.s_x[(int64_t)d * sp.Wp + c] : 0.0f;
         }
-        total += __popc(__ballot_sync(0xffffffffu, in[0])) + __popc(__ballot_sync(0xffffffffu, in[1])) +
-                 __popc(__ballot_sync(0xffffffffu, in[2])) + __popc(__ballot_sync(0xffffffffu, in[3]));
-        inlier = total > sp.K;
+        unsigned todo = live;
+        while (todo) {
+          const int qq = __ffs(todo) - 1;
+          todo &= todo - 1;
+          float y[D];
+#pragma unroll
+          for (int d = 0; d < D; ++d) y[d] = __shfl_sync(0xffffffffu, qx[d], qq);
+          unsigned m = 0;
+#pragma unroll
+          for (int e = 0; e < 8; ++e) m += (cv[e] && is_nbr<D, PRED>(y, cx[e], sp.R2f, sp.R, sp.R2)) ? 1u : 0u;
+          const unsigned tot = __reduce_add_sync(0xffffffffu, m);
+          if (lane == qq) cnt += (int)tot;
+        }
+        live &= __ballot_sync(0xffffffffu, cnt <= sp.K);
       }
     }
-    if (lane == 0 && !inlier) {
-      const int64_t w = (int64_t)i - shift;
+    const bool out = has && cnt <= sp.K;
+    if (out) {
+      const int64_t w = (int64_t)sp.s_off[p + q] - shift;
       atomicOr(&jb.flags[w >> 5], 1u << (w & 31));
-      atomicAdd(&jb.ctr->n_out, 1);
     }
+    nout += __popc(__ballot_sync(0xffffffffu, out));
+  }
+  if (lane == 0 && nout) atomicAdd(&jb.ctr->n_out, nout);
+}
+
+// ---------------------------------------------------------------------------
+// k_span_classify: one thread per (window, bin in use): the window's count of
+// the bin from pre; a bin that is not provably all-inlier in that window is
+// appended to the window's list of groups to count: (first position, points,
+// bit 31 set when the bin's span holds several cells), two words per group in
+// the job's queue. Appends are aggregated per warp and window.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
+  pdl_trigger();
+  pdl_wait();
+  const int lane = threadIdx.x & 31;
+  const uint32_t nu = sp.sc->n_used;
+  const bool pure = sp.sc->pure;
+  const int64_t pairs = (int64_t)nu * b.njobs;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t e_end = (pairs + 31) & ~31ll;  // whole warps stay in the loop together
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < e_end; e += stride) {
+    int j = -1;
+    uint32_t start = 0, wc = 0;
+    bool need = false, single = true;
+    if (e < pairs) {
+      j = (int)(e / nu);
+      const uint32_t bin = sp.used[e - (int64_t)j * nu];
+      const uint32_t* p0 = sp.pre + (int64_t)j * NB;
+      const uint32_t* p1 = p0 + (int64_t)sp.wblk * NB;
+      const uint32_t a = p0[bin];
+      wc = p1[bin] - a;
+      if (wc) {
+        single = pure || sp.kmin[bin] == sp.kmax[bin];
+        bool safe = false;
+        if (sp.filter) {
+          safe = single && wc > (uint32_t)sp.K;
+          if (!safe && single && sp.n >= 3) safe = span_group_safe(sp, p0, p1, bin, pure);
+        }
+        need = !safe;
+        start = sp.bin_start[bin] + a;
+      }
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, need ? j : -1);
+    if (need) {
+      const int leader = __ffs(peers) - 1;
+      const unsigned lt = lanemask_lt();
+      uint32_t base = 0;
+      const uint32_t pts = __reduce_add_sync(peers, wc);  // points of the peers' groups
+      JobCtr* c = b.jobs[j].ctr;
+      if (lane == leader) {
+        base = (uint32_t)atomicAdd(&c->n_pairs, __popc(peers));
+        atomicAdd(&c->n_undet, (int)pts);
+      }
+      base = __shfl_sync(peers, base, leader);
+      const uint32_t k = base + __popc(peers & lt);
+      uint32_t* q = b.jobs[j].queue;
+      q[2 * k] = start;
+      q[2 * k + 1] = wc | (single ? 0u : 0x80000000u);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_span_count: grid (x, windows); one warp per group of the window's list:
+// a bin of one cell as one group, a bin whose span holds several cells point
+// by point (each with its own stencil). Also clears the compaction look-back
+// words of its window.
+// ---------------------------------------------------------------------------
+template <int D, int PRED>
+__global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
+  pdl_trigger();
+  pdl_wait();
+  const int j = blockIdx.y;
+  const Job& jb = b.jobs[j];
+  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
+  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  {
+    const int64_t tiles = (jb.W + CMP_TILE - 1) / CMP_TILE;
+    for (int64_t t = gtid; t < tiles; t += gstride) jb.cmp_status[t] = 0;
+  }
+  const uint32_t* p0 = sp.pre + (int64_t)j * NB;
+  const uint32_t* p1 = p0 + (int64_t)sp.wblk * NB;
+  const int64_t ng = jb.ctr->n_pairs;
+  for (int64_t k = gtid >> 5; k < ng; k += gstride >> 5) {
+    const uint32_t st = jb.queue[2 * k];
+    const uint32_t w = jb.queue[2 * k + 1];
+    const uint32_t n = w & 0x7fffffffu;
+    if (!(w >> 31)) {
+      span_count_group<D, PRED>(b, sp, j, st, n, p0, p1);
+    } else {
+      for (uint32_t q = 0; q < n; ++q) span_count_group<D, PRED>(b, sp, j, st + q, 1, p0, p1);
+    }
+  }
+}
+
+// Clears the per-bin state of the span's bins in use (all k_compact blocks
+// share the work; the block that finishes last clears the count of bins).
+__device__ __forceinline__ void span_clear_bins(const SpanCtr* c) {
+  const int64_t nb = (int64_t)gridDim.x * gridDim.y;
+  const int64_t f = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+  const uint32_t nu = c->n_used;
+  for (int64_t u = f * blockDim.x + threadIdx.x; u < nu; u += nb * blockDim.x) {
+    const uint32_t bin = c->used[u];
+    c->bin_count[bin] = 0;
+    c->kmin[bin] = EMPTY_KEY;
+    c->kmax[bin] = 0;
   }
 }
 
