@@ -81,11 +81,12 @@ struct JobCtr {
 
 // Per-handle state (device).
 struct BatchState {
-  int64_t out_total;    // outlier IDs appended to out_ids so far
+  int64_t out_total;    // outliers found so far (IDs in out_ids, or pending in bitsets)
   int64_t slides;       // windows detected so far
   int64_t undet_total;  // queued points summed over windows
   int32_t err;          // DERR_*
-  uint32_t done;        // finished k_compact tiles of the running batch
+  uint32_t done;        // finished blocks of the running batch's last kernel
+  int64_t ids_done;     // outlier IDs written by the deferred compaction so far
 };
 
 // Span engine counters (device), one per handle, and the per-bin arrays
@@ -101,7 +102,6 @@ struct SpanCtr {
   unsigned long long* kmax;  // [NB]
 };
 
-__device__ __forceinline__ void span_clear_bins(const SpanCtr* c);
 
 struct Job {
   int64_t W, S, Wp;  // window, slide, padded SoA row stride (multiple of 4, >= W + 4)
@@ -1208,72 +1208,14 @@ __global__ void __launch_bounds__(256) k_count(Batch b) {
 }
 
 // ---------------------------------------------------------------------------
-// k_compact: outlier bits in window order -> sorted global indices, appended
-// to the batch output after the outliers of the earlier jobs. Grid
-// (max tiles per job, jobs); a tile covers CMP_TILE window offsets, one
-// 32-bit word per thread, tiles chained by decoupled look-back. The last
-// tile of the batch records per-slide counts, advances every job's window
-// and resets the per-job counters.
+// End of a batch, run by the block of the batch's last kernel that finishes
+// last (after a fence): per-slide records, window advance, per-job counter
+// reset and the batch totals. Every thread of the block calls it.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_compact(Batch b) {
-  __shared__ uint32_t sm[33];
-  __shared__ uint32_t s_tile, s_prefix, s_last;
-  __shared__ int64_t s_jobbase;
-  __shared__ int64_t s_red[3][8];
-  pdl_trigger();
-  pdl_wait();
-  const Job& jb = b.jobs[blockIdx.y];
-  const int64_t ntiles = (jb.W + CMP_TILE - 1) / CMP_TILE;
-  if (blockIdx.x >= ntiles) return;  // smaller job in a mixed batch
+__device__ void finish_batch(const Batch& b) {
+  __shared__ int64_t s_red[3][32];
   BatchState* bs = b.bs;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const bool act = job_active(b);
-  if (act && wid == 0) {
-    // Output base of this job: IDs of all earlier jobs of the batch come first.
-    int64_t part = 0;
-    for (int j = lane; j < (int)blockIdx.y; j += 32) part += b.jobs[j].ctr->n_out;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-    if (lane == 0) {
-      s_jobbase = bs->out_total + part;
-      s_tile = atomicAdd(&jb.ctr->cmp_ticket, 1u);
-    }
-  }
-  __syncthreads();
-  if (act) {
-    const uint32_t tile = s_tile;
-    const int64_t lo = jb.ctr->lo;
-    const int64_t wi = ((int64_t)tile * CMP_TILE >> 5) + threadIdx.x;  // bitset word
-    const int64_t nwords = (jb.W + 31) >> 5;
-    uint32_t bits = 0;
-    if (wi < nwords) {
-      bits = jb.flags[wi];
-      if (bits) jb.flags[wi] = 0;
-    }
-    uint32_t total;
-    const uint32_t ex = block_exclusive_scan(__popc(bits), &total, sm);
-    if (wid == 0) {
-      const uint32_t pre = warp_lookback(jb.cmp_status, tile, total, bs);
-      if (lane == 0) s_prefix = pre;
-    }
-    __syncthreads();
-    int64_t o = s_jobbase + s_prefix + ex;
-    while (bits) {
-      const int e = __ffs(bits) - 1;
-      bits &= bits - 1;
-      if (o < b.out_cap) b.out_ids[o] = lo + wi * 32 + e;
-      else set_err(bs, DERR_CAPACITY);
-      ++o;
-    }
-  }
-  if (b.span) span_clear_bins(b.span);  // span batches: every job has the same W (no early return above)
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) s_last = (atomicAdd(&bs->done, 1u) == (uint32_t)(b.cmp_tiles - 1));
-  __syncthreads();
-  if (!s_last) return;
-  // Last tile of the batch: per-slide records, window advance, counter reset
-  // (one job per thread) and the batch totals.
   __threadfence();
   int64_t add = 0, und = 0, nact = 0;
   for (int j = threadIdx.x; j < b.njobs; j += blockDim.x) {
@@ -1327,6 +1269,72 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
     bs->done = 0;
     if (b.span) b.span->n_used = 0;
   }
+}
+
+// ---------------------------------------------------------------------------
+// k_compact: outlier bits in window order -> sorted global indices, appended
+// to the batch output after the outliers of the earlier jobs. Grid
+// (max tiles per job, jobs); a tile covers CMP_TILE window offsets, one
+// 32-bit word per thread, tiles chained by decoupled look-back. The last
+// tile of the batch records per-slide counts, advances every job's window
+// and resets the per-job counters.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_compact(Batch b) {
+  __shared__ uint32_t sm[33];
+  __shared__ uint32_t s_tile, s_prefix, s_last;
+  __shared__ int64_t s_jobbase;
+  pdl_trigger();
+  pdl_wait();
+  const Job& jb = b.jobs[blockIdx.y];
+  const int64_t ntiles = (jb.W + CMP_TILE - 1) / CMP_TILE;
+  if (blockIdx.x >= ntiles) return;  // smaller job in a mixed batch
+  BatchState* bs = b.bs;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const bool act = job_active(b);
+  if (act && wid == 0) {
+    // Output base of this job: IDs of all earlier jobs of the batch come first.
+    int64_t part = 0;
+    for (int j = lane; j < (int)blockIdx.y; j += 32) part += b.jobs[j].ctr->n_out;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if (lane == 0) {
+      s_jobbase = bs->out_total + part;
+      s_tile = atomicAdd(&jb.ctr->cmp_ticket, 1u);
+    }
+  }
+  __syncthreads();
+  if (act) {
+    const uint32_t tile = s_tile;
+    const int64_t lo = jb.ctr->lo;
+    const int64_t wi = ((int64_t)tile * CMP_TILE >> 5) + threadIdx.x;  // bitset word
+    const int64_t nwords = (jb.W + 31) >> 5;
+    uint32_t bits = 0;
+    if (wi < nwords) {
+      bits = jb.flags[wi];
+      if (bits) jb.flags[wi] = 0;
+    }
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(__popc(bits), &total, sm);
+    if (wid == 0) {
+      const uint32_t pre = warp_lookback(jb.cmp_status, tile, total, bs);
+      if (lane == 0) s_prefix = pre;
+    }
+    __syncthreads();
+    int64_t o = s_jobbase + s_prefix + ex;
+    while (bits) {
+      const int e = __ffs(bits) - 1;
+      bits &= bits - 1;
+      if (o < b.out_cap) b.out_ids[o] = lo + wi * 32 + e;
+      else set_err(bs, DERR_CAPACITY);
+      ++o;
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = (atomicAdd(&bs->done, 1u) == (uint32_t)(b.cmp_tiles - 1));
+  __syncthreads();
+  if (!s_last) return;
+  finish_batch(b);
 }
 
 }  // namespace rtod

@@ -147,8 +147,11 @@ struct SpanScratch {
   float* s_x = nullptr;
   unsigned long long* scan_status = nullptr;
   SpanCtr* sc = nullptr;
+  uint32_t* bits = nullptr;   // [chunk][words] per-slide outlier bitsets
+  int64_t* base = nullptr;    // [chunk] output offsets of a chunk's slides
   int64_t nblk_cap = 0;
   int64_t pts_cap = 0;
+  int64_t chunk_cap = 0;
   int64_t Wp = 0;
   int64_t bytes = 0;
 };
@@ -265,6 +268,7 @@ struct rtod_handle {
   int64_t graph_replays = 0;
   int64_t undet_total = 0;
   bool tuned = false;
+  double flush_ms = 0;  // device ms of the span engine's deferred compaction in the last profiled run
   float threshold = 0.5f;
   uint32_t max_sweep = 64;
 };
@@ -361,6 +365,7 @@ int scrub(rtod_handle* h) {
     CU(cudaMemsetAsync(sp.cnt, 0, (size_t)(sp.nblk_cap * NB) * sizeof(uint32_t), h->stream));
     CU(cudaMemsetAsync(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long), h->stream));
     CU(cudaMemsetAsync(sp.sc, 0, offsetof(SpanCtr, used), h->stream));  // counters only
+    CU(cudaMemsetAsync(sp.bits, 0, (size_t)(sp.chunk_cap * ((h->W + 31) / 32)) * sizeof(uint32_t), h->stream));
   }
   CU(cudaMemsetAsync(h->ctr, 0, sizeof(JobCtr) * h->batch_max, h->stream));
   CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
@@ -371,15 +376,18 @@ void free_span(rtod_handle* h) {
   SpanScratch& sp = h->span;
   dfree(sp.bin_count); dfree(sp.bin_start); dfree(sp.kmin); dfree(sp.kmax); dfree(sp.cnt); dfree(sp.pre);
   dfree(sp.used); dfree(sp.s_off); dfree(sp.s_x); dfree(sp.scan_status); dfree(sp.sc);
+  dfree(sp.bits); dfree(sp.base);
   h->device_bytes -= sp.bytes;
   sp = SpanScratch{};
 }
 
-// Span scratch for spans of nblk slide blocks (nblk * S points).
-int ensure_span(rtod_handle* h, int64_t nblk) {
+// Span scratch for spans of nblk slide blocks (nblk * S points) and bitsets
+// of `chunk` slides.
+int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
   SpanScratch& sp = h->span;
   const int64_t pts = nblk * h->S;
-  if (sp.sc && nblk <= sp.nblk_cap && pts <= sp.pts_cap) return RTOD_OK;
+  const int64_t words = (h->W + 31) / 32;
+  if (sp.sc && nblk <= sp.nblk_cap && pts <= sp.pts_cap && chunk <= sp.chunk_cap) return RTOD_OK;
   CU(cudaStreamSynchronize(h->stream));
   free_span(h);
   drop_graph(h);
@@ -390,7 +398,8 @@ int ensure_span(rtod_handle* h, int64_t nblk) {
             !dalloc(&sp.cnt, (size_t)(nblk * NB), &bytes) && !dalloc(&sp.pre, (size_t)((nblk + 1) * NB), &bytes) &&
             !dalloc(&sp.used, NB, &bytes) && !dalloc(&sp.s_off, (size_t)pts, &bytes) &&
             !dalloc(&sp.s_x, (size_t)(Wp * h->D), &bytes) && !dalloc(&sp.scan_status, SCAN_TILES, &bytes) &&
-            !dalloc(&sp.sc, 1, &bytes);
+            !dalloc(&sp.sc, 1, &bytes) && !dalloc(&sp.bits, (size_t)(chunk * words), &bytes) &&
+            !dalloc(&sp.base, (size_t)chunk, &bytes);
   sp.bytes = bytes;
   h->device_bytes += bytes;
   if (!ok) {
@@ -399,7 +408,9 @@ int ensure_span(rtod_handle* h, int64_t nblk) {
   }
   sp.nblk_cap = nblk;
   sp.pts_cap = pts;
+  sp.chunk_cap = chunk;
   sp.Wp = Wp;
+  CU(cudaMemset(sp.bits, 0, (size_t)(chunk * words) * sizeof(uint32_t)));
   CU(cudaMemset(sp.bin_count, 0, NB * sizeof(uint32_t)));
   CU(cudaMemset(sp.kmin, 0xff, NB * sizeof(unsigned long long)));
   CU(cudaMemset(sp.kmax, 0, NB * sizeof(unsigned long long)));
@@ -415,8 +426,9 @@ int ensure_span(rtod_handle* h, int64_t nblk) {
   return RTOD_OK;
 }
 
-// Span parameters of a batch of B windows over the resident stream.
-Span make_span(const rtod_handle* h, int B, const float* stream_pts) {
+// Span parameters of a batch of B windows over the resident stream, with
+// bitsets of `chunk` slides.
+Span make_span(const rtod_handle* h, int B, const float* stream_pts, int64_t chunk) {
   const SpanScratch& ss = h->span;
   Span sp{};
   sp.S = h->S;
@@ -445,7 +457,19 @@ Span make_span(const rtod_handle* h, int B, const float* stream_pts) {
   sp.s_x = ss.s_x;
   sp.scan_status = ss.scan_status;
   sp.sc = ss.sc;
+  sp.bits = ss.bits;
+  sp.words = (h->W + 31) / 32;
+  sp.chunk = chunk;
   return sp;
+}
+
+// Slides per bitset chunk of the span engine: a multiple of the batch B,
+// within about 256 MiB of bitsets, and no more than the run needs.
+int64_t span_chunk(const rtod_handle* h, int B, int64_t slides) {
+  const int64_t row = ((h->W + 31) / 32) * 4;
+  const int64_t per_batch = std::max<int64_t>(1, (256ll << 20) / (row * B));
+  const int64_t batches = (slides + B - 1) / B;
+  return (int64_t)B * std::max<int64_t>(1, std::min(per_batch, batches));
 }
 
 Job make_job(rtod_handle* h, int j, bool ring, const float* stream_pts) {
@@ -594,8 +618,8 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
 }
 
 // Launches one batch of the span engine: hist prefix scan scatter classify
-// count compact. kev as for launch_group (kev[1] after hist + prefix, kev[4]
-// after classify + count).
+// count. kev as for launch_group (kev[1] after hist + prefix, kev[4] after
+// classify + count; the compaction of a chunk is timed by run_stream).
 int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, cudaEvent_t* kev, int64_t* nk) {
   const unsigned gy = (unsigned)b.njobs;
   const int64_t npts = sp.nblk * sp.S;
@@ -617,10 +641,28 @@ int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, 
     CU(launch_k(k_span_count<1, 1>, dim3((unsigned)cx, gy), wpb * 32, st, b, sp));
   }
   if (kev) CU(cudaEventRecord(kev[4], st));
-  CU(launch_k(k_compact, dim3((unsigned)((g.Wmax + CMP_TILE - 1) / CMP_TILE), gy), 256, st, b));
-  if (kev) CU(cudaEventRecord(kev[5], st));
+  if (kev) CU(cudaEventRecord(kev[5], st));  // no per-batch compaction: see span_flush
   if (kev) CU(cudaEventRecord(kev[6], st));
-  if (nk) *nk = 7;
+  if (nk) *nk = 6;
+  return RTOD_OK;
+}
+
+// Deferred compaction of span-engine slides [s0, s0 + n) (one bitset chunk).
+int span_flush(rtod_handle* h, const Span& sp, int64_t s0, int64_t n, int64_t out_cap) {
+  SpanOut o{};
+  o.bits = sp.bits;
+  o.words = sp.words;
+  o.chunk = sp.chunk;
+  o.W = h->W;
+  o.S = h->S;
+  o.rec_nout = h->rec_nout;
+  o.base = h->span.base;
+  o.out_ids = h->ids;
+  o.out_cap = out_cap;
+  o.bs = h->bs;
+  CU(launch_k(k_slide_base, dim3(1), 1024, h->stream, o, s0, n));
+  CU(launch_k(k_span_compact, dim3((unsigned)n), 1024, h->stream, o, s0));
+  h->launches += 2;
   return RTOD_OK;
 }
 
@@ -813,7 +855,8 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
   int B = pick_batch(h, slides);
   if (span) B = (int)std::min<int64_t>(B, span_batch_cap(h));
   if ((r = ensure_pool(h, B))) return r;
-  if (span && (r = ensure_span(h, W / S + B - 1))) return r;
+  const int64_t chunk = span ? span_chunk(h, B, slides) : 0;
+  if (span && (r = ensure_span(h, W / S + B - 1, chunk))) return r;
   if (e_begin) CU(cudaEventRecord(e_begin, h->stream));
   if ((r = stage_stream(h, pts, used, &src))) return r;
   if ((r = configure(h, MODE_RUN, B, S, src))) return r;  // first detected window: [S, W + S)
@@ -826,7 +869,10 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
   const int64_t out_cap = std::min(ids_cap, h->ids_cap);
   const int64_t full = slides / B, rem = slides % B;
   Batch bfull = make_batch(h, B, out_cap);
-  const Span sfull = span ? make_span(h, B, src) : Span{};
+  const Span sfull = span ? make_span(h, B, src, chunk) : Span{};
+  const int64_t chunk_batches = span ? chunk / B : 0;
+  EventSet chunk_es;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> chunk_ev;
   if (span) bfull.span = h->span.sc;
   for (int64_t i = 0; i < full + (rem ? 1 : 0); ++i) {
     Batch b = bfull;
@@ -835,7 +881,7 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
       b = make_batch(h, (int)rem, out_cap);
       if (span) {
         b.span = h->span.sc;
-        sp = make_span(h, (int)rem, src);
+        sp = make_span(h, (int)rem, src, chunk);
       }
     }
     const Span* spp = span ? &sp : nullptr;
@@ -847,6 +893,17 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
       r = i < full ? run_batch(h, b, false, spp) : launch_batch(h, b, false, nullptr, spp);
     }
     if (r) return r;
+    const bool last = i + 1 == full + (rem ? 1 : 0);
+    if (span && ((i + 1) % chunk_batches == 0 || last)) {
+      const int64_t s1 = std::min(slides, (i + 1) * (int64_t)B);
+      const int64_t s0 = ((s1 - 1) / chunk) * chunk;
+      if (kev) {
+        chunk_ev.emplace_back(chunk_es.make(), chunk_es.make());
+        CU(cudaEventRecord(chunk_ev.back().first, h->stream));
+      }
+      if ((r = span_flush(h, sfull, s0, s1 - s0, out_cap))) return r;
+      if (kev) CU(cudaEventRecord(chunk_ev.back().second, h->stream));
+    }
   }
   nout->resize((size_t)slides);
   nund->resize((size_t)slides);
@@ -854,6 +911,8 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
   CU(cudaMemcpyAsync(nout->data(), h->rec_nout, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaMemcpyAsync(nund->data(), h->rec_undet, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
+  h->flush_ms = 0;
+  for (const auto& pr : chunk_ev) h->flush_ms += elapsed(pr.first, pr.second);
   h->n_pushed = used;
   h->slides_done = slides;
   if ((r = check_device_error(h, *out_state))) return r;
@@ -1309,6 +1368,7 @@ RTOD_API int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_s
         bb += elapsed(e[2], e[4]);  // scan + scatter
         de += elapsed(e[4], e[7]);  // count + compact (+ router training)
       }
+      de += h->flush_ms;  // span engine: compaction once per chunk of slides
       times->prepare_cell = pc * inv;
       times->build_bvh = bb * inv;
       times->detect_outlier = de * inv;
@@ -1346,6 +1406,7 @@ RTOD_API int rtod_profile_run(rtod_handle* h, const float* pts, int64_t n, int64
     const cudaEvent_t* e = &kev[(size_t)i * 8];
     for (int k = 1; k < kPipeKernels && k < n_kernels; ++k) kernel_ms[k] += elapsed(e[k], e[k + 1]);
   }
+  if (n_kernels > 5) kernel_ms[5] += h->flush_ms;  // span engine: compaction once per chunk
   for (int i = 0; i < n_kernels; ++i) kernel_ms[i] /= (double)slides;
   return RTOD_OK;
 }

@@ -17,10 +17,11 @@
 //
 // Kernels per batch: k_span_hist (per-block bin counts), k_span_prefix (pre,
 // list of bins in use), k_span_scan (bin_start), k_span_scatter (sorted
-// span), k_span_classify (per window and bin in use: safe, or listed),
-// k_span_count (exact counts of the listed bins' window points), then
-// k_compact of the window engine turns each window's outlier bits into
-// sorted IDs and clears the per-bin state.
+// span), k_span_classify (per window and bin in use: safe, or listed) and
+// k_span_count (exact counts of the listed bins' window points into
+// per-slide outlier bitsets; its last block ends the batch). Once per chunk
+// of slides, k_slide_base and k_span_compact turn the bitsets into sorted
+// outlier IDs.
 //
 // The safe-inlier rule is the window engine's (count > K in one cell, plus
 // the 1-d group rule), with "single cell" judged over the whole span: a bin
@@ -57,6 +58,9 @@ struct Span {
   float* s_x;       // [D][Wp] bin-ordered coordinates
   unsigned long long* scan_status;  // [SCAN_TILES]
   SpanCtr* sc;
+  uint32_t* bits;   // [chunk][words] outlier bits per window offset, row = slide % chunk
+  int64_t words;    // ceil(W / 32)
+  int64_t chunk;    // slides per bitset chunk (a multiple of the batch)
 };
 
 // First global index of the span: the window of the batch's first job.
@@ -355,6 +359,7 @@ __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp,
   const int lane = threadIdx.x & 31;
   const Job& jb = b.jobs[j];
   const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
+  uint32_t* row = sp.bits + ((jb.ctr->lo - sp.S) / sp.S % sp.chunk) * sp.words;
   float x0[D];
 #pragma unroll
   for (int d = 0; d < D; ++d) x0[d] = sp.s_x[(int64_t)d * sp.Wp + p];
@@ -430,11 +435,25 @@ __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp,
     const bool out = has && cnt <= sp.K;
     if (out) {
       const int64_t w = (int64_t)sp.s_off[p + q] - shift;
-      atomicOr(&jb.flags[w >> 5], 1u << (w & 31));
+      atomicOr(&row[w >> 5], 1u << (w & 31));
     }
     nout += __popc(__ballot_sync(0xffffffffu, out));
   }
   if (lane == 0 && nout) atomicAdd(&jb.ctr->n_out, nout);
+}
+
+// Clears the per-bin state of the span's bins in use (all blocks of the
+// launch share the work; finish_batch then clears the count of bins).
+__device__ __forceinline__ void span_clear_bins(const SpanCtr* c) {
+  const int64_t nb = (int64_t)gridDim.x * gridDim.y;
+  const int64_t f = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
+  const uint32_t nu = c->n_used;
+  for (int64_t u = f * blockDim.x + threadIdx.x; u < nu; u += nb * blockDim.x) {
+    const uint32_t bin = c->used[u];
+    c->bin_count[bin] = 0;
+    c->kmin[bin] = EMPTY_KEY;
+    c->kmax[bin] = 0;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -498,21 +517,19 @@ __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
 // ---------------------------------------------------------------------------
 // k_span_count: grid (x, windows); one warp per group of the window's list:
 // a bin of one cell as one group, a bin whose span holds several cells point
-// by point (each with its own stencil). Also clears the compaction look-back
-// words of its window.
+// by point (each with its own stencil). Outliers set their bit in the slide's
+// bitset row. Then the blocks clear the per-bin state, and the block that
+// finishes last ends the batch (records, window advance, counters).
 // ---------------------------------------------------------------------------
 template <int D, int PRED>
 __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
+  __shared__ int s_last;
   pdl_trigger();
   pdl_wait();
   const int j = blockIdx.y;
   const Job& jb = b.jobs[j];
   const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
   const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  {
-    const int64_t tiles = (jb.W + CMP_TILE - 1) / CMP_TILE;
-    for (int64_t t = gtid; t < tiles; t += gstride) jb.cmp_status[t] = 0;
-  }
   const uint32_t* p0 = sp.pre + (int64_t)j * NB;
   const uint32_t* p1 = p0 + (int64_t)sp.wblk * NB;
   const int64_t ng = jb.ctr->n_pairs;
@@ -526,19 +543,74 @@ __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
       for (uint32_t q = 0; q < n; ++q) span_count_group<D, PRED>(b, sp, j, st + q, 1, p0, p1);
     }
   }
+  // The per-bin state is no longer read in this batch: clear it, then the
+  // block that finishes last ends the batch.
+  span_clear_bins(sp.sc);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&b.bs->done, 1u) == gridDim.x * gridDim.y - 1;
+  __syncthreads();
+  if (s_last) finish_batch(b);
 }
 
-// Clears the per-bin state of the span's bins in use (all k_compact blocks
-// share the work; the block that finishes last clears the count of bins).
-__device__ __forceinline__ void span_clear_bins(const SpanCtr* c) {
-  const int64_t nb = (int64_t)gridDim.x * gridDim.y;
-  const int64_t f = (int64_t)blockIdx.y * gridDim.x + blockIdx.x;
-  const uint32_t nu = c->n_used;
-  for (int64_t u = f * blockDim.x + threadIdx.x; u < nu; u += nb * blockDim.x) {
-    const uint32_t bin = c->used[u];
-    c->bin_count[bin] = 0;
-    c->kmin[bin] = EMPTY_KEY;
-    c->kmax[bin] = 0;
+// ---------------------------------------------------------------------------
+// Deferred compaction of a chunk of slides [s0, s0 + n): k_slide_base turns
+// the per-slide outlier counts into output offsets (one block), then
+// k_span_compact, one block per slide, turns the slide's bitset row into
+// sorted global indices at its offset and clears the row.
+// ---------------------------------------------------------------------------
+struct SpanOut {
+  uint32_t* bits;
+  int64_t words, chunk, W, S;
+  const int32_t* rec_nout;
+  int64_t* base;   // [chunk] output offset of each slide of the chunk
+  int64_t* out_ids;
+  int64_t out_cap;
+  BatchState* bs;
+};
+
+__global__ void __launch_bounds__(1024) k_slide_base(SpanOut o, int64_t s0, int64_t n) {
+  __shared__ uint32_t sm[33];
+  pdl_trigger();
+  pdl_wait();
+  int64_t run = o.bs->ids_done;
+  for (int64_t c = 0; c < n; c += blockDim.x) {
+    const int64_t i = c + threadIdx.x;
+    const uint32_t v = i < n ? (uint32_t)o.rec_nout[s0 + i] : 0u;
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(v, &total, sm);
+    if (i < n) o.base[i] = run + ex;
+    run += total;
+  }
+  if (threadIdx.x == 0) o.bs->ids_done = run;
+}
+
+__global__ void __launch_bounds__(1024) k_span_compact(SpanOut o, int64_t s0) {
+  __shared__ uint32_t sm[33];
+  pdl_trigger();
+  pdl_wait();
+  const int64_t s = s0 + blockIdx.x;
+  uint32_t* row = o.bits + (s % o.chunk) * o.words;
+  const int64_t lo = (s + 1) * o.S;
+  int64_t out = o.base[blockIdx.x];
+  for (int64_t c = 0; c < o.words; c += blockDim.x) {
+    const int64_t wi = c + threadIdx.x;
+    uint32_t bits = 0;
+    if (wi < o.words) {
+      bits = row[wi];
+      if (bits) row[wi] = 0;
+    }
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(__popc(bits), &total, sm);
+    int64_t q = out + ex;
+    while (bits) {
+      const int e = __ffs(bits) - 1;
+      bits &= bits - 1;
+      if (q < o.out_cap) o.out_ids[q] = lo + wi * 32 + e;
+      else set_err(o.bs, DERR_CAPACITY);
+      ++q;
+    }
+    out += total;
   }
 }
 
