@@ -117,8 +117,10 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
-// Scratch of one job (one window in flight).
+// Scratch of one job (one window in flight). The span engine uses only the
+// queue; the other arrays are allocated when the window engine first needs them.
 struct Scratch {
+  bool full = false;
   uint32_t* bin_count = nullptr;
   uint32_t* bin_start = nullptr;
   unsigned long long* kmin = nullptr;
@@ -155,6 +157,8 @@ struct SpanScratch {
   int64_t Wp = 0;
   int64_t bytes = 0;
 };
+
+constexpr int kMaxJobs = 256;  // windows per launch, either engine
 
 constexpr int kPipeKernels = 7;
 const char* kKernelNames[kPipeKernels] = {"k_keys",  "k_hist",    "k_scan", "k_scatter",
@@ -217,15 +221,16 @@ struct rtod_handle {
   double cell = 0;
   float R2f = 0;
   int block_warps = 8;
-  int batch_max = 32;
+  int batch_max = 32;       // windows per launch of the window engine
+  int span_batch_max = 256; // windows per launch of the span engine
   int64_t device_bytes = 0;
 
-  std::vector<Scratch> pool;  // allocated lazily up to batch_max
+  std::vector<Scratch> pool;  // allocated lazily, one per job of a batch
   SpanScratch span;           // span engine scratch, allocated on first use
   int engine = RTOD_ENGINE_WINDOW;  // engine of rtod_run (resolved from the config / tuner)
-  JobCtr* ctr = nullptr;      // [batch_max]
-  JobCtr* ctr_init = nullptr; // pinned host [batch_max]
-  Job* jobs_dev = nullptr;    // [batch_max]
+  JobCtr* ctr = nullptr;      // [kMaxJobs]
+  JobCtr* ctr_init = nullptr; // pinned host [kMaxJobs]
+  Job* jobs_dev = nullptr;    // [kMaxJobs]
   std::vector<Job> tab_host;  // last uploaded job table
   BatchState* bs = nullptr;
   RouterState* router = nullptr;
@@ -319,20 +324,30 @@ void drop_graph(rtod_handle* h) {
   h->graph_ring = -1;
 }
 
-int ensure_pool(rtod_handle* h, int jobs) {
+// Scratch for `jobs` jobs: the queue of each, and with `full` every array of
+// the window engine.
+int ensure_pool(rtod_handle* h, int jobs, bool full = true) {
   const int64_t W = h->W, Wp = h->Wp, D = h->D;
   const int64_t cmp_tiles = (W + CMP_TILE - 1) / CMP_TILE;
+  int64_t* c = &h->device_bytes;
   while ((int)h->pool.size() < jobs) {
     Scratch s;
-    int64_t* c = &h->device_bytes;
+    const bool ok = !dalloc(&s.queue, (size_t)(2 * W), c);
+    h->pool.push_back(s);
+    if (!ok) return RTOD_ERR_CUDA;
+  }
+  for (int j = 0; j < jobs && full; ++j) {
+    Scratch& s = h->pool[j];
+    if (s.full) continue;
     bool ok = !dalloc(&s.bin_count, NB, c) && !dalloc(&s.bin_start, NB + 1, c) && !dalloc(&s.kmin, NB, c) &&
               !dalloc(&s.kmax, NB, c) && !dalloc(&s.s_off, (size_t)W, c) && !dalloc(&s.s_ckey, (size_t)W, c) &&
-              !dalloc(&s.s_x, (size_t)(Wp * D), c) && !dalloc(&s.queue, (size_t)(2 * W), c) &&
+              !dalloc(&s.s_x, (size_t)(Wp * D), c) &&
               !dalloc(&s.feat, (size_t)(h->cfg.router ? W * MLP_IN : 1), c) &&
               !dalloc(&s.flags, (size_t)((W + 31) / 32), c) && !dalloc(&s.scan_status, SCAN_TILES, c) &&
               !dalloc(&s.cmp_status, (size_t)cmp_tiles, c);
-    h->pool.push_back(s);
     if (!ok) return RTOD_ERR_CUDA;
+    s.full = true;
+    drop_graph(h);
     CU(cudaMemset(s.bin_count, 0, NB * sizeof(uint32_t)));
     CU(cudaMemset(s.kmin, 0xff, NB * sizeof(unsigned long long)));
     CU(cudaMemset(s.kmax, 0, NB * sizeof(unsigned long long)));
@@ -350,6 +365,7 @@ int scrub(rtod_handle* h) {
   const int64_t W = h->W;
   const int64_t cmp_tiles = (W + CMP_TILE - 1) / CMP_TILE;
   for (Scratch& s : h->pool) {
+    if (!s.full) continue;
     CU(cudaMemsetAsync(s.bin_count, 0, NB * sizeof(uint32_t), h->stream));
     CU(cudaMemsetAsync(s.kmin, 0xff, NB * sizeof(unsigned long long), h->stream));
     CU(cudaMemsetAsync(s.kmax, 0, NB * sizeof(unsigned long long), h->stream));
@@ -367,7 +383,7 @@ int scrub(rtod_handle* h) {
     CU(cudaMemsetAsync(sp.sc, 0, offsetof(SpanCtr, used), h->stream));  // counters only
     CU(cudaMemsetAsync(sp.bits, 0, (size_t)(sp.chunk_cap * ((h->W + 31) / 32)) * sizeof(uint32_t), h->stream));
   }
-  CU(cudaMemsetAsync(h->ctr, 0, sizeof(JobCtr) * h->batch_max, h->stream));
+  CU(cudaMemsetAsync(h->ctr, 0, sizeof(JobCtr) * kMaxJobs, h->stream));
   CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
   return RTOD_OK;
 }
@@ -514,8 +530,8 @@ Job make_job(rtod_handle* h, int j, bool ring, const float* stream_pts) {
 // Uploads the job table for a mode (only when it changed, so that captured
 // graphs stay valid) and initialises the job counters: job j starts at
 // window lo = first_lo + j*S and advances by jobs*S per batch.
-int configure(rtod_handle* h, int mode, int jobs, int64_t first_lo, const float* stream_pts) {
-  int r = ensure_pool(h, jobs);
+int configure(rtod_handle* h, int mode, int jobs, int64_t first_lo, const float* stream_pts, bool full = true) {
+  int r = ensure_pool(h, jobs, full);
   if (r) return r;
   std::vector<Job> tab((size_t)jobs);
   for (int j = 0; j < jobs; ++j) tab[j] = make_job(h, j, mode == MODE_RING, stream_pts);
@@ -735,7 +751,7 @@ int reset_state(rtod_handle* h) {
   if (h->poisoned) {
     r = scrub(h);
   } else {
-    CU(cudaMemsetAsync(h->ctr, 0, sizeof(JobCtr) * h->batch_max, h->stream));
+    CU(cudaMemsetAsync(h->ctr, 0, sizeof(JobCtr) * kMaxJobs, h->stream));
     CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
     r = RTOD_OK;
   }
@@ -827,7 +843,12 @@ int64_t span_batch_cap(const rtod_handle* h) {
 }
 
 int pick_batch(const rtod_handle* h, int64_t slides) {
-  const int64_t b = h->cfg.batch ? h->cfg.batch : h->batch_max;
+  int64_t b;
+  if (use_span(h)) {
+    b = std::min<int64_t>(h->cfg.batch ? h->cfg.batch : 32, std::min<int64_t>(h->span_batch_max, span_batch_cap(h)));
+  } else {
+    b = h->cfg.batch ? std::min(h->cfg.batch, h->batch_max) : h->batch_max;
+  }
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, slides));
 }
 
@@ -852,14 +873,13 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
   if ((r = ensure_records(h, slides))) return r;
   if ((r = ensure_ids(h, std::max<int64_t>(1, std::min(ids_cap, slides * W))))) return r;
   const bool span = use_span(h);
-  int B = pick_batch(h, slides);
-  if (span) B = (int)std::min<int64_t>(B, span_batch_cap(h));
-  if ((r = ensure_pool(h, B))) return r;
+  const int B = pick_batch(h, slides);
+  if ((r = ensure_pool(h, B, !span))) return r;
   const int64_t chunk = span ? span_chunk(h, B, slides) : 0;
   if (span && (r = ensure_span(h, W / S + B - 1, chunk))) return r;
   if (e_begin) CU(cudaEventRecord(e_begin, h->stream));
   if ((r = stage_stream(h, pts, used, &src))) return r;
-  if ((r = configure(h, MODE_RUN, B, S, src))) return r;  // first detected window: [S, W + S)
+  if ((r = configure(h, MODE_RUN, B, S, src, !span))) return r;  // first detected window: [S, W + S)
   CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
   const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((used + 255) / 256, h->sm_count * 8));
   DISPATCH_D(h->D, CU(launch_k(k_keys<D>, dim3(kx), 256, h->stream, src, (int64_t)0, used, h->cell, h->run_keys,
@@ -975,7 +995,7 @@ bool same_problem(const rtod_config& a, const rtod_config& b) {
 int apply_tuning(rtod_handle* h, const Tuning& t) {
   set_grid(h, t.n);
   h->block_warps = t.block_warps;
-  h->cfg.batch = std::min(t.batch, h->batch_max);
+  h->cfg.batch = t.batch;
   h->threshold = t.threshold;
   h->max_sweep = t.max_sweep;
   h->engine = t.engine;
@@ -1031,7 +1051,7 @@ int autotune(rtod_handle* h, const float* pts, int64_t slides_total) {
   } fr{dev};
   CU(cudaMemcpy(dev, pts, (size_t)(used * D) * sizeof(float), cudaMemcpyDefault));
   Tuning best;
-  best.batch = std::min(32, h->batch_max);
+  best.batch = h->engine == RTOD_ENGINE_SPAN ? 32 : std::min(32, h->batch_max);
   best.engine = h->engine;
   int r = apply_tuning(h, best);
   if (r) return r;
@@ -1064,8 +1084,8 @@ int autotune(rtod_handle* h, const float* pts, int64_t slides_total) {
     t.block_warps = bw;
     if ((r = trial(t))) return r;
   }
-  for (int bt : {8, 16, 64}) {
-    if (bt > h->batch_max) continue;
+  for (int bt : {8, 16, 64, 128}) {
+    if (bt > (best.engine == RTOD_ENGINE_SPAN ? h->span_batch_max : h->batch_max)) continue;
     Tuning t = best;
     t.batch = bt;
     if ((r = trial(t))) return r;
@@ -1158,14 +1178,21 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
   const int64_t per_job = (int64_t)NB * 24 + h->W * (4 + 8 + 8 + 4) + h->Wp * h->D * 4 + h->W / 8;
   h->batch_max = (int)std::max<int64_t>(1, std::min<int64_t>(32, (1ll << 30) / per_job));
   if (cfg->batch) h->batch_max = cfg->batch;
+  // Span engine: per window of a batch, a queue (8W bytes), one block row of
+  // the two per-block tables (2 * 4 * NB bytes) and S points of span
+  // arrays; up to kMaxJobs windows within ~2 GiB.
+  {
+    const int64_t per_win = 8 * h->W + 8 * (int64_t)NB + h->S * (4 + 4 * h->D);
+    h->span_batch_max = (int)std::max<int64_t>(1, std::min<int64_t>(kMaxJobs, (2ll << 30) / per_win));
+  }
 
   int64_t* c = &h->device_bytes;
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
-  ok = ok && !dalloc(&h->ctr, (size_t)h->batch_max, c) && !dalloc(&h->jobs_dev, (size_t)h->batch_max, c) &&
+  ok = ok && !dalloc(&h->ctr, (size_t)kMaxJobs, c) && !dalloc(&h->jobs_dev, (size_t)kMaxJobs, c) &&
        !dalloc(&h->bs, 1, c) && !dalloc(&h->ring, (size_t)(h->W * h->D), c) &&
        !dalloc(&h->ring_keys, (size_t)h->W, c) && !dalloc(&h->ring_prev, (size_t)h->W, c) &&
        !dalloc(&h->staging, (size_t)(h->W * h->D), c);
-  ok = ok && cudaMallocHost((void**)&h->ctr_init, sizeof(JobCtr) * h->batch_max) == cudaSuccess;
+  ok = ok && cudaMallocHost((void**)&h->ctr_init, sizeof(JobCtr) * kMaxJobs) == cudaSuccess;
   ok = ok && !dalloc(&h->router, 1, c);
   if (ok) {
     RouterState* init = new (std::nothrow) RouterState;
@@ -1219,7 +1246,7 @@ RTOD_API int rtod_get_tuning(const rtod_handle* h, int32_t out[5]) {
   out[0] = h->n;
   out[1] = h->block_warps;
   out[2] = h->D < 3 ? h->D : 3;
-  out[3] = (int32_t)(h->cfg.batch ? std::min(h->cfg.batch, h->batch_max) : h->batch_max);
+  out[3] = pick_batch(h, INT64_MAX);
   out[4] = use_span(h) ? RTOD_ENGINE_SPAN : RTOD_ENGINE_WINDOW;
   return RTOD_OK;
 }
