@@ -76,7 +76,7 @@ struct JobCtr {
   int32_t n_sweep;       // queued points of the full-sweep queue (router on)
   int32_t last_nout;     // outliers of the job's last detected window
   int32_t pure;          // current window: no two of its cells share a bin
-  int32_t n_pairs;       // span engine: groups listed for the window
+  int32_t pad;
 };
 
 // Per-handle state (device).
@@ -95,7 +95,7 @@ struct SpanCtr {
   uint32_t scan_ticket;  // tile tickets of the span's bin scan
   uint32_t n_used;       // bins holding span points
   int32_t pure;          // no two cells of the span share a bin
-  int32_t pad;
+  uint32_t n_groups;     // groups listed for exact counts in the running batch
   uint32_t* used;        // [NB] bins in use
   uint32_t* bin_count;   // [NB]
   unsigned long long* kmin;  // [NB]
@@ -125,10 +125,9 @@ struct Job {
   uint32_t* s_off;        // [W] cell-ordered: window offset (global index - lo)
   uint64_t* s_ckey;       // [W] cell-ordered: cell key
   float* s_x;             // [D][Wp] cell-ordered coordinates
-  uint32_t* queue;        // [2W] cell-ordered positions that need an exact count; with the
+  uint32_t* queue;        // [W] cell-ordered positions that need an exact count; with the
                           // router on, the early-exit queue grows from the front and the
-                          // full-sweep queue back from W - 1; the span engine keeps its
-                          // (first position, points) groups here, two words each
+                          // full-sweep queue from the back
   float* feat;            // [W][3] router features, at the same index as the queue entry
   uint32_t* flags;        // [ceil(W / 32)] outlier bit per window offset
   unsigned long long* scan_status;  // [SCAN_TILES]
@@ -1241,7 +1240,6 @@ __device__ void finish_batch(const Batch& b) {
     c->n_out = 0;
     c->n_undet = 0;
     c->n_sweep = 0;
-    c->n_pairs = 0;
     c->cmp_ticket = 0;
   }
 #pragma unroll
@@ -1267,7 +1265,10 @@ __device__ void finish_batch(const Batch& b) {
     bs->undet_total += tu;
     bs->slides += tn;
     bs->done = 0;
-    if (b.span) b.span->n_used = 0;
+    if (b.span) {
+      b.span->n_used = 0;
+      b.span->n_groups = 0;
+    }
   }
 }
 

@@ -117,8 +117,8 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
   return ms;
 }
 
-// Scratch of one job (one window in flight). The span engine uses only the
-// queue; the other arrays are allocated when the window engine first needs them.
+// Scratch of one job (one window in flight) of the window engine, allocated
+// when that engine first runs the job (the span engine uses none of it).
 struct Scratch {
   bool full = false;
   uint32_t* bin_count = nullptr;
@@ -149,6 +149,7 @@ struct SpanScratch {
   float* s_x = nullptr;
   unsigned long long* scan_status = nullptr;
   SpanCtr* sc = nullptr;
+  uint4* groups = nullptr;    // [windows][min(W, NB)] listed groups of a batch
   uint32_t* bits = nullptr;   // [chunk][words] per-slide outlier bitsets
   int64_t* base = nullptr;    // [chunk] output offsets of a chunk's slides
   int64_t nblk_cap = 0;
@@ -324,24 +325,18 @@ void drop_graph(rtod_handle* h) {
   h->graph_ring = -1;
 }
 
-// Scratch for `jobs` jobs: the queue of each, and with `full` every array of
-// the window engine.
+// Pool entries for `jobs` jobs; with `full`, their window-engine scratch.
 int ensure_pool(rtod_handle* h, int jobs, bool full = true) {
   const int64_t W = h->W, Wp = h->Wp, D = h->D;
   const int64_t cmp_tiles = (W + CMP_TILE - 1) / CMP_TILE;
   int64_t* c = &h->device_bytes;
-  while ((int)h->pool.size() < jobs) {
-    Scratch s;
-    const bool ok = !dalloc(&s.queue, (size_t)(2 * W), c);
-    h->pool.push_back(s);
-    if (!ok) return RTOD_ERR_CUDA;
-  }
+  while ((int)h->pool.size() < jobs) h->pool.push_back(Scratch{});
   for (int j = 0; j < jobs && full; ++j) {
     Scratch& s = h->pool[j];
     if (s.full) continue;
     bool ok = !dalloc(&s.bin_count, NB, c) && !dalloc(&s.bin_start, NB + 1, c) && !dalloc(&s.kmin, NB, c) &&
               !dalloc(&s.kmax, NB, c) && !dalloc(&s.s_off, (size_t)W, c) && !dalloc(&s.s_ckey, (size_t)W, c) &&
-              !dalloc(&s.s_x, (size_t)(Wp * D), c) &&
+              !dalloc(&s.s_x, (size_t)(Wp * D), c) && !dalloc(&s.queue, (size_t)W, c) &&
               !dalloc(&s.feat, (size_t)(h->cfg.router ? W * MLP_IN : 1), c) &&
               !dalloc(&s.flags, (size_t)((W + 31) / 32), c) && !dalloc(&s.scan_status, SCAN_TILES, c) &&
               !dalloc(&s.cmp_status, (size_t)cmp_tiles, c);
@@ -392,7 +387,7 @@ void free_span(rtod_handle* h) {
   SpanScratch& sp = h->span;
   dfree(sp.bin_count); dfree(sp.bin_start); dfree(sp.kmin); dfree(sp.kmax); dfree(sp.cnt); dfree(sp.pre);
   dfree(sp.used); dfree(sp.s_off); dfree(sp.s_x); dfree(sp.scan_status); dfree(sp.sc);
-  dfree(sp.bits); dfree(sp.base);
+  dfree(sp.bits); dfree(sp.base); dfree(sp.groups);
   h->device_bytes -= sp.bytes;
   sp = SpanScratch{};
 }
@@ -415,7 +410,8 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
             !dalloc(&sp.used, NB, &bytes) && !dalloc(&sp.s_off, (size_t)pts, &bytes) &&
             !dalloc(&sp.s_x, (size_t)(Wp * h->D), &bytes) && !dalloc(&sp.scan_status, SCAN_TILES, &bytes) &&
             !dalloc(&sp.sc, 1, &bytes) && !dalloc(&sp.bits, (size_t)(chunk * words), &bytes) &&
-            !dalloc(&sp.base, (size_t)chunk, &bytes);
+            !dalloc(&sp.base, (size_t)chunk, &bytes) &&
+            !dalloc(&sp.groups, (size_t)((nblk - h->W / h->S + 1) * std::min<int64_t>(h->W, NB)), &bytes);
   sp.bytes = bytes;
   h->device_bytes += bytes;
   if (!ok) {
@@ -473,6 +469,7 @@ Span make_span(const rtod_handle* h, int B, const float* stream_pts, int64_t chu
   sp.s_x = ss.s_x;
   sp.scan_status = ss.scan_status;
   sp.sc = ss.sc;
+  sp.groups = ss.groups;
   sp.bits = ss.bits;
   sp.words = (h->W + 31) / 32;
   sp.chunk = chunk;
@@ -642,7 +639,7 @@ int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, 
   const int64_t hx = std::max<int64_t>(1, std::min<int64_t>((npts + 1023) / 1024, (int64_t)g.sm_count * 8));
   if (kev) CU(cudaEventRecord(kev[0], st));
   CU(launch_k(k_span_hist<1>, dim3((unsigned)hx), 256, st, b, sp));
-  CU(launch_k(k_span_prefix, dim3(NB / 256), 256, st, b, sp));
+  CU(launch_k(k_span_prefix, dim3(NB / 32), 256, st, b, sp));
   if (kev) CU(cudaEventRecord(kev[1], st));
   CU(launch_k(k_span_scan, dim3(SCAN_TILES), 256, st, b, sp));
   if (kev) CU(cudaEventRecord(kev[2], st));
@@ -650,11 +647,11 @@ int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, 
   if (kev) CU(cudaEventRecord(kev[3], st));
   CU(launch_k(k_span_classify, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
   const int wpb = g.block_warps;
-  const int64_t cx = std::max<int64_t>(1, (int64_t)g.sm_count * (64 / wpb) / b.njobs);
+  const int64_t cx = (int64_t)g.sm_count * (64 / wpb);
   if (g.pred == 0) {
-    CU(launch_k(k_span_count<1, 0>, dim3((unsigned)cx, gy), wpb * 32, st, b, sp));
+    CU(launch_k(k_span_count<1, 0>, dim3((unsigned)cx), wpb * 32, st, b, sp));
   } else {
-    CU(launch_k(k_span_count<1, 1>, dim3((unsigned)cx, gy), wpb * 32, st, b, sp));
+    CU(launch_k(k_span_count<1, 1>, dim3((unsigned)cx), wpb * 32, st, b, sp));
   }
   if (kev) CU(cudaEventRecord(kev[4], st));
   if (kev) CU(cudaEventRecord(kev[5], st));  // no per-batch compaction: see span_flush
@@ -1175,14 +1172,15 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
                   ? cfg->engine
                   : ((cfg->dim == 1 && !cfg->router) ? RTOD_ENGINE_SPAN : RTOD_ENGINE_WINDOW);
   // Windows per rtod_run launch: up to 32, within ~1 GiB of scratch.
-  const int64_t per_job = (int64_t)NB * 24 + h->W * (4 + 8 + 8 + 4) + h->Wp * h->D * 4 + h->W / 8;
+  const int64_t per_job = (int64_t)NB * 24 + h->W * (4 + 8 + 4 + 4) + h->Wp * h->D * 4 + h->W / 8;
   h->batch_max = (int)std::max<int64_t>(1, std::min<int64_t>(32, (1ll << 30) / per_job));
   if (cfg->batch) h->batch_max = cfg->batch;
-  // Span engine: per window of a batch, a queue (8W bytes), one block row of
-  // the two per-block tables (2 * 4 * NB bytes) and S points of span
-  // arrays; up to kMaxJobs windows within ~2 GiB.
+  // Span engine: per window of a batch, room for its listed groups (16 bytes
+  // each, at most min(W, NB)), one block row of the two per-block tables
+  // (2 * 4 * NB bytes) and S points of span arrays; up to kMaxJobs windows
+  // within ~2 GiB.
   {
-    const int64_t per_win = 8 * h->W + 8 * (int64_t)NB + h->S * (4 + 4 * h->D);
+    const int64_t per_win = 16 * std::min<int64_t>(h->W, NB) + 8 * (int64_t)NB + h->S * (4 + 4 * h->D);
     h->span_batch_max = (int)std::max<int64_t>(1, std::min<int64_t>(kMaxJobs, (2ll << 30) / per_win));
   }
 

@@ -58,6 +58,7 @@ struct Span {
   float* s_x;       // [D][Wp] bin-ordered coordinates
   unsigned long long* scan_status;  // [SCAN_TILES]
   SpanCtr* sc;
+  uint4* groups;    // [B * min(W, NB)] listed groups: first position, points, bin, window
   uint32_t* bits;   // [chunk][words] outlier bits per window offset, row = slide % chunk
   int64_t words;    // ceil(W / 32)
   int64_t chunk;    // slides per bitset chunk (a multiple of the batch)
@@ -168,27 +169,52 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
 }
 
 // ---------------------------------------------------------------------------
-// k_span_prefix: one thread per bin; for a bin in use, appends it to the list
-// of bins in use and writes pre[t][b] for t = 0..nblk (8 loads in flight).
+// k_span_prefix: 8 threads per bin (32 bins per block of 256); for a bin in
+// use, the first of them appends it to the list of bins in use, and each
+// sums one eighth of the blocks (its loads all in flight), an 8-lane scan
+// gives its offset, and it writes pre[t][b] for its blocks (pre[nblk][b] by
+// the last one).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_span_prefix(Batch b, Span sp) {
   pdl_trigger();
   pdl_wait();
-  const uint32_t bin = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t c = bin < NB ? sp.bin_count[bin] : 0u;
-  const unsigned has = __ballot_sync(0xffffffffu, c != 0);
-  if (!has) return;
   const int lane = threadIdx.x & 31;
+  const int sub = lane & 7;                                   // eighth of the blocks
+  const uint32_t bin = blockIdx.x * 32 + (threadIdx.x >> 3);  // grid NB / 32
+  const uint32_t c = sp.bin_count[bin];
+  if (!__any_sync(0xffffffffu, c != 0)) return;
+  const unsigned has = __ballot_sync(0xffffffffu, c != 0 && sub == 0);
   uint32_t base = 0;
-  if (lane == 0) base = atomicAdd(&sp.sc->n_used, (uint32_t)__popc(has));
+  if (lane == 0 && has) base = atomicAdd(&sp.sc->n_used, (uint32_t)__popc(has));
   base = __shfl_sync(0xffffffffu, base, 0);
-  if (c == 0) return;
-  sp.used[base + __popc(has & lanemask_lt())] = bin;
+  if (c != 0 && sub == 0) sp.used[base + __popc(has & lanemask_lt())] = bin;
+  const int64_t per = (sp.nblk + 7) >> 3;
+  const int64_t t0 = min((int64_t)sub * per, sp.nblk), t1 = min(t0 + per, sp.nblk);
   const uint32_t* __restrict__ cnt = sp.cnt + bin;
   uint32_t* __restrict__ pre = sp.pre + bin;
-  uint32_t run = 0;
-  int64_t t = 0;
-  for (; t + 8 <= sp.nblk; t += 8) {
+  uint32_t sum = 0;
+  if (c != 0) {
+    int64_t t = t0;
+    for (; t + 8 <= t1; t += 8) {
+      uint32_t v[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) v[e] = cnt[(t + e) * NB];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) sum += v[e];
+    }
+    for (; t < t1; ++t) sum += cnt[t * NB];
+  }
+  // exclusive scan over the 8 lanes of the bin
+  uint32_t inc = sum;
+#pragma unroll
+  for (int o = 1; o < 8; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o, 8);
+    if (sub >= o) inc += y;
+  }
+  if (c == 0) return;
+  uint32_t run = inc - sum;
+  int64_t t = t0;
+  for (; t + 8 <= t1; t += 8) {
     uint32_t v[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) v[e] = cnt[(t + e) * NB];
@@ -198,12 +224,12 @@ __global__ void __launch_bounds__(256) k_span_prefix(Batch b, Span sp) {
       run += v[e];
     }
   }
-  for (; t < sp.nblk; ++t) {
+  for (; t < t1; ++t) {
     const uint32_t v = cnt[t * NB];
     pre[t * NB] = run;
     run += v;
   }
-  pre[sp.nblk * NB] = run;
+  if (sub == 7) pre[sp.nblk * NB] = run;
 }
 
 // k_span_scan: bin_start of the span (exclusive scan of bin_count).
@@ -342,39 +368,38 @@ __device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* 
 }
 
 // ---------------------------------------------------------------------------
-// Exact counts of nq points of window j at bin-ordered positions
-// [p, p + nq), all of one cell, by one warp. Lane s < 2n+1 takes stencil cell
-// key + d(s), d = 0, -1, +1, -2, +2, ... (nearest first), and that bin's
-// window range; a warp scan turns the range lengths into offsets of one
-// virtual candidate list of T entries. With T <= K every point is an outlier
-// (its count cannot exceed T). Otherwise the list is read 256 candidates at a
-// time (8 per lane, kept in registers) and every undecided point of the group
-// (up to 32, one per lane) is tested against the chunk: per point, 8 tests per
-// lane and one warp reduction; a point is decided as soon as its count
-// exceeds K, and the chunks stop when every point is decided.
+// Exact counts of the nq points of window j in bin `bin` (bin-ordered
+// positions [p, p + nq)) by one warp. Whatever cell k of the bin a point is
+// in, its stencil cells k + d, |d| <= n, lie in bins bin + d (mod NB): lane
+// s < 2n+1 takes bin + d(s), d = 0, -1, +1, -2, +2, ... (nearest first), and
+// that bin's window range (points of other cells sharing those bins are
+// rejected by the distance test); a warp scan turns the range lengths into
+// offsets of one virtual candidate list of T entries. With T <= K every point
+// is an outlier (its count cannot exceed T). Otherwise the list is read 256
+// candidates at a time (8 per lane, kept in registers) and every undecided
+// point of the group (up to 32, one per lane) is tested against the chunk:
+// per point, 8 tests per lane and one warp reduction; a point is decided as
+// soon as its count exceeds K, and the chunks stop when every point is
+// decided.
 // ---------------------------------------------------------------------------
 template <int D, int PRED>
 __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp, int j, uint32_t p,
-                                                 uint32_t nq, const uint32_t* p0, const uint32_t* p1) {
+                                                 uint32_t nq, uint32_t bin, const uint32_t* p0,
+                                                 const uint32_t* p1) {
   const int lane = threadIdx.x & 31;
   const Job& jb = b.jobs[j];
   const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
   uint32_t* row = sp.bits + ((jb.ctr->lo - sp.S) / sp.S % sp.chunk) * sp.words;
-  float x0[D];
-#pragma unroll
-  for (int d = 0; d < D; ++d) x0[d] = sp.s_x[(int64_t)d * sp.Wp + p];
-  int32_t code;
-  const uint64_t key = cell_key<D>(x0, sp.cell, &code);  // the key k_keys gave these points
   const int slots = 2 * sp.n + 1;
   uint32_t rs = 0, len = 0;
   if (lane < slots) {
     const int dk = (lane & 1) ? -((lane + 1) >> 1) : (lane >> 1);
-    const uint32_t bin = (uint32_t)(key + (unsigned long long)(long long)dk) & NB_MASK;
-    const uint32_t b0 = sp.bin_start[bin], b1 = sp.bin_start[bin + 1];
+    const uint32_t sb = (bin + (uint32_t)dk) & NB_MASK;
+    const uint32_t b0 = sp.bin_start[sb], b1 = sp.bin_start[sb + 1];
     if (b1 > b0) {
-      const uint32_t a = p0[bin];
+      const uint32_t a = p0[sb];
       rs = b0 + a;
-      len = p1[bin] - a;
+      len = p1[sb] - a;
     }
   }
   uint32_t inc = len;
@@ -459,9 +484,9 @@ __device__ __forceinline__ void span_clear_bins(const SpanCtr* c) {
 // ---------------------------------------------------------------------------
 // k_span_classify: one thread per (window, bin in use): the window's count of
 // the bin from pre; a bin that is not provably all-inlier in that window is
-// appended to the window's list of groups to count: (first position, points,
-// bit 31 set when the bin's span holds several cells), two words per group in
-// the job's queue. Appends are aggregated per warp and window.
+// appended to the batch's list of groups to count (first position, points,
+// bin, window): one atomic per warp for the list, one per window present in
+// the warp for its count of listed points.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
   pdl_trigger();
@@ -474,19 +499,19 @@ __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
   const int64_t e_end = (pairs + 31) & ~31ll;  // whole warps stay in the loop together
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < e_end; e += stride) {
     int j = -1;
-    uint32_t start = 0, wc = 0;
-    bool need = false, single = true;
+    uint32_t start = 0, wc = 0, bin = 0;
+    bool need = false;
     if (e < pairs) {
       j = (int)(e / nu);
-      const uint32_t bin = sp.used[e - (int64_t)j * nu];
+      bin = sp.used[e - (int64_t)j * nu];
       const uint32_t* p0 = sp.pre + (int64_t)j * NB;
       const uint32_t* p1 = p0 + (int64_t)sp.wblk * NB;
       const uint32_t a = p0[bin];
       wc = p1[bin] - a;
       if (wc) {
-        single = pure || sp.kmin[bin] == sp.kmax[bin];
         bool safe = false;
         if (sp.filter) {
+          const bool single = pure || sp.kmin[bin] == sp.kmax[bin];
           safe = single && wc > (uint32_t)sp.K;
           if (!safe && single && sp.n >= 3) safe = span_group_safe(sp, p0, p1, bin, pure);
         }
@@ -494,54 +519,38 @@ __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
         start = sp.bin_start[bin] + a;
       }
     }
+    const unsigned nmask = __ballot_sync(0xffffffffu, need);
+    uint32_t gbase = 0;
+    if (lane == 0 && nmask) gbase = atomicAdd(&sp.sc->n_groups, (uint32_t)__popc(nmask));
+    gbase = __shfl_sync(0xffffffffu, gbase, 0);
     const unsigned peers = __match_any_sync(0xffffffffu, need ? j : -1);
     if (need) {
-      const int leader = __ffs(peers) - 1;
-      const unsigned lt = lanemask_lt();
-      uint32_t base = 0;
-      const uint32_t pts = __reduce_add_sync(peers, wc);  // points of the peers' groups
-      JobCtr* c = b.jobs[j].ctr;
-      if (lane == leader) {
-        base = (uint32_t)atomicAdd(&c->n_pairs, __popc(peers));
-        atomicAdd(&c->n_undet, (int)pts);
-      }
-      base = __shfl_sync(peers, base, leader);
-      const uint32_t k = base + __popc(peers & lt);
-      uint32_t* q = b.jobs[j].queue;
-      q[2 * k] = start;
-      q[2 * k + 1] = wc | (single ? 0u : 0x80000000u);
+      sp.groups[gbase + __popc(nmask & lanemask_lt())] = make_uint4(start, wc, bin, (uint32_t)j);
+      const uint32_t pts = __reduce_add_sync(peers, wc);
+      if (lane == __ffs(peers) - 1) atomicAdd(&b.jobs[j].ctr->n_undet, (int)pts);
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// k_span_count: grid (x, windows); one warp per group of the window's list:
-// a bin of one cell as one group, a bin whose span holds several cells point
-// by point (each with its own stencil). Outliers set their bit in the slide's
-// bitset row. Then the blocks clear the per-bin state, and the block that
-// finishes last ends the batch (records, window advance, counters).
+// k_span_count: one warp per listed group of the batch (warps stride over the
+// list). Outliers set their bit in the slide's bitset row. Then the blocks
+// clear the per-bin state, and the block that finishes last ends the batch
+// (records, window advance, counters).
 // ---------------------------------------------------------------------------
 template <int D, int PRED>
 __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
   __shared__ int s_last;
   pdl_trigger();
   pdl_wait();
-  const int j = blockIdx.y;
-  const Job& jb = b.jobs[j];
   const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
   const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t* p0 = sp.pre + (int64_t)j * NB;
-  const uint32_t* p1 = p0 + (int64_t)sp.wblk * NB;
-  const int64_t ng = jb.ctr->n_pairs;
+  const int64_t ng = sp.sc->n_groups;
   for (int64_t k = gtid >> 5; k < ng; k += gstride >> 5) {
-    const uint32_t st = jb.queue[2 * k];
-    const uint32_t w = jb.queue[2 * k + 1];
-    const uint32_t n = w & 0x7fffffffu;
-    if (!(w >> 31)) {
-      span_count_group<D, PRED>(b, sp, j, st, n, p0, p1);
-    } else {
-      for (uint32_t q = 0; q < n; ++q) span_count_group<D, PRED>(b, sp, j, st + q, 1, p0, p1);
-    }
+    const uint4 g = sp.groups[k];
+    const int j = (int)g.w;
+    const uint32_t* p0 = sp.pre + (int64_t)j * NB;
+    span_count_group<D, PRED>(b, sp, j, g.x, g.y, g.z, p0, p0 + (int64_t)sp.wblk * NB);
   }
   // The per-bin state is no longer read in this batch: clear it, then the
   // block that finishes last ends the batch.
