@@ -156,7 +156,16 @@ def ncu_traffic(kernel: str):
     return None
 
 
-def algorithmic_bytes(kernel: str, w, n_out_per_slide: float, undet_per_slide: float, batch: int) -> float:
+def used_bins(w, cells_per_r: int, batch: int) -> int:
+    """Bins of the 65536-bin table holding points of the first span of
+    `batch` windows (1-d cells of R(1+2^-12)/n, bin = cell mod 65536)."""
+    span = w.points[w.slide:w.slide + w.window + (batch - 1) * w.slide, 0].astype(np.float64)
+    cell = w.R * (1 + 2.0 ** -12) / cells_per_r
+    return int(np.unique(np.floor(span / cell).astype(np.int64) & 65535).size)
+
+
+def algorithmic_bytes(kernel: str, w, n_out_per_slide: float, undet_per_slide: float, batch: int,
+                      used_bins: int = 0) -> float:
     """Minimum DRAM bytes of each pipeline stage per slide (per window); the
     span engine's stages move their per-batch bytes once per `batch` windows."""
     W, S, d = w.window, w.slide, w.dim
@@ -175,9 +184,13 @@ def algorithmic_bytes(kernel: str, w, n_out_per_slide: float, undet_per_slide: f
         "k_span_scan": 4 * 65536 * 2 / batch,                 # read counts, write starts
         # read keys + points, write bin-ordered offsets + coordinates, once per batch
         "k_span_scatter": ((8 + 4 * d) + (4 + 4 * d)) * span_pts / batch,
-        # per queued point: queue entry, offset, key, coordinates
-        # per counted point: its offset and coordinates
-        "k_span_classify+k_span_count": undet_per_slide * (4 + 4 * d),
+        # per (window, bin in use): the bin's two prefix entries
+        "k_span_classify": 8 * used_bins,
+        # per counted point: its offset and coordinates (candidates are read
+        # per group of one bin and shared by its points: not counted)
+        "k_span_count": undet_per_slide * (4 + 4 * d),
+        # per slide: its bitset row, its outlier IDs
+        "k_slide_base+k_span_compact": W / 8 + 8 * n_out_per_slide,
     }[kernel]
 
 
@@ -319,9 +332,15 @@ def emit_ours(args, world, w, res):
     prof = r["prof"]
     dom = max(prof, key=prof.get)
     n_out = r["n_outliers"] / slides
-    alg = algorithmic_bytes(dom, w, n_out, r["undet"], r["tuning"]["batch"])
+    tun = r["tuning"]
+    ub = used_bins(w, tun["cells_per_r"], tun["batch"]) if w.dim == 1 else 0
+    alg = algorithmic_bytes(dom, w, n_out, r["undet"], tun["batch"], ub)
     peak, peak_kind = hbm_peak()
-    achieved = alg / (prof[dom] / 1e3) / 1e9
+    # per launch: pipeline kernels run once per batch of windows, the key
+    # kernel and the chunk compaction once per pass over the stream
+    per_launch = slides if dom in ("k_keys", "k_slide_base+k_span_compact") else tun["batch"]
+    launch_ms = prof[dom] * per_launch
+    achieved = alg * per_launch / (launch_ms / 1e3) / 1e9
     traffic = ncu_traffic(dom)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K,
@@ -335,8 +354,9 @@ def emit_ours(args, world, w, res):
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback",
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
-                     "algorithmic_bytes_per_launch": alg, "launch_ms": prof[dom],
-                     "kernel_ms_per_slide": prof},
+                     "algorithmic_bytes_per_launch": alg * per_launch, "windows_per_launch": per_launch,
+                     "launch_ms": launch_ms, "used_bins": ub,
+                     "stage_ms_per_slide": prof},
         "clocks": r["clocks"],
         "gpu_launches": r["launches"],
         "e2e": {"value": world * r["e2e_steps"] * slides * w.slide / r["e2e_s"], "unit": UNIT,

@@ -160,12 +160,15 @@ int rtod_get_stats(const rtod_handle* h, int64_t out[5]);
 
 /* Diagnostic run: like rtod_run on a fresh handle but launches every kernel
    individually with a CUDA event after each, and writes the average device
-   time per slide of each pipeline kernel, in order (keys, hist, scan,
+   time per slide of each pipeline stage, in order (keys, hist, scan,
    scatter, count, compact, and the router's training step), to
-   kernel_ms[0..n_kernels). A batch of B
-   windows shares one launch of each kernel; its time is divided by B. The
-   kernel names are given by rtod_kernel_name(i). Results are discarded. No
-   counterpart in RTOD (it times stages with gettimeofday, src/ods/timer.h). */
+   kernel_ms[0..n_kernels). A batch of B windows shares one launch of each
+   kernel; its time is divided by B. With the span engine the seven slots
+   hold its kernels: keys, k_span_hist + k_span_prefix, k_span_scan,
+   k_span_scatter, k_span_classify, k_span_count, and the compaction of each
+   chunk of slides (k_slide_base + k_span_compact).
+   The stage names are given by rtod_kernel_name(i). Results are discarded.
+   No counterpart in RTOD (it times stages with gettimeofday, src/ods/timer.h). */
 int rtod_profile_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides,
                      double* kernel_ms, int32_t n_kernels);
 

@@ -631,8 +631,9 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
 }
 
 // Launches one batch of the span engine: hist prefix scan scatter classify
-// count. kev as for launch_group (kev[1] after hist + prefix, kev[4] after
-// classify + count; the compaction of a chunk is timed by run_stream).
+// count. kev as for launch_group, with kev[1] after hist + prefix, kev[4]
+// after classify and kev[5] after count (the stage slots of count, compact
+// and train hold classify, count and the chunk compaction timed by run_stream).
 int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, cudaEvent_t* kev, int64_t* nk) {
   const unsigned gy = (unsigned)b.njobs;
   const int64_t npts = sp.nblk * sp.S;
@@ -646,6 +647,7 @@ int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, 
   CU(launch_k(k_span_scatter<1>, dim3((unsigned)hx), 256, st, b, sp));
   if (kev) CU(cudaEventRecord(kev[3], st));
   CU(launch_k(k_span_classify, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
+  if (kev) CU(cudaEventRecord(kev[4], st));
   const int wpb = g.block_warps;
   const int64_t cx = (int64_t)g.sm_count * (64 / wpb);
   if (g.pred == 0) {
@@ -653,9 +655,8 @@ int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, 
   } else {
     CU(launch_k(k_span_count<1, 1>, dim3((unsigned)cx), wpb * 32, st, b, sp));
   }
-  if (kev) CU(cudaEventRecord(kev[4], st));
-  if (kev) CU(cudaEventRecord(kev[5], st));  // no per-batch compaction: see span_flush
-  if (kev) CU(cudaEventRecord(kev[6], st));
+  if (kev) CU(cudaEventRecord(kev[5], st));
+  if (kev) CU(cudaEventRecord(kev[6], st));  // no per-batch compaction: see span_flush
   if (nk) *nk = 6;
   return RTOD_OK;
 }
@@ -861,7 +862,7 @@ int64_t count_slides(const rtod_handle* h, int64_t n, int64_t max_slides) {
 // batch: one before and one after each kernel (the last one after the
 // router's training step, or right after k_compact without router).
 int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap, cudaEvent_t e_begin,
-               cudaEvent_t e_keys, std::vector<cudaEvent_t>* kev, BatchState* out_state,
+               cudaEvent_t e_keys, cudaEvent_t e_end, std::vector<cudaEvent_t>* kev, BatchState* out_state,
                std::vector<int32_t>* nout, std::vector<int32_t>* nund) {
   const int64_t W = h->W, S = h->S;
   const int64_t used = W + slides * S;
@@ -878,6 +879,7 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
   if ((r = stage_stream(h, pts, used, &src))) return r;
   if ((r = configure(h, MODE_RUN, B, S, src, !span))) return r;  // first detected window: [S, W + S)
   CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
+  CU(cudaEventRecord(h->ev[1], h->stream));  // start of the key kernel (profile)
   const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((used + 255) / 256, h->sm_count * 8));
   DISPATCH_D(h->D, CU(launch_k(k_keys<D>, dim3(kx), 256, h->stream, src, (int64_t)0, used, h->cell, h->run_keys,
                                h->run_prev, h->bs, h->S, h->run_blk_lo, h->run_blk_hi)));
@@ -922,6 +924,7 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
       if (kev) CU(cudaEventRecord(chunk_ev.back().second, h->stream));
     }
   }
+  if (e_end) CU(cudaEventRecord(e_end, h->stream));
   nout->resize((size_t)slides);
   nund->resize((size_t)slides);
   CU(cudaMemcpyAsync(out_state, h->bs, sizeof(BatchState), cudaMemcpyDeviceToHost, h->stream));
@@ -1017,7 +1020,7 @@ int time_pass(rtod_handle* h, const float* dev_pts, int64_t slides, float* ms) {
     BatchState s{};
     std::vector<int32_t> nout, nund;
     CU(cudaEventRecord(a, h->stream));
-    r = run_stream(h, dev_pts, slides, slides * h->W, nullptr, nullptr, nullptr, &s, &nout, &nund);
+    r = run_stream(h, dev_pts, slides, slides * h->W, nullptr, nullptr, nullptr, nullptr, &s, &nout, &nund);
     if (r) return r;
     CU(cudaEventRecord(b, h->stream));
     CU(cudaStreamSynchronize(h->stream));
@@ -1369,9 +1372,8 @@ RTOD_API int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_s
   }
   BatchState s{};
   std::vector<int32_t> nout, nund;
-  int r = run_stream(h, pts, slides, ids_cap, t0, t1, stage ? &kev : nullptr, &s, &nout, &nund);
+  int r = run_stream(h, pts, slides, ids_cap, t0, t1, t2, stage ? &kev : nullptr, &s, &nout, &nund);
   if (r) return r;
-  CU(cudaEventRecord(t2, h->stream));
   for (int64_t j = 0; j < slides; ++j) out_offsets[j + 1] = out_offsets[j] + nout[j];
   if (out_offsets[slides] != s.out_total) return fail(RTOD_ERR_CUDA, "inconsistent outlier totals");
   CU(cudaEventRecord(d0, h->stream));
@@ -1398,9 +1400,9 @@ RTOD_API int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_s
       times->build_bvh = bb * inv;
       times->detect_outlier = de * inv;
     }
-    // Everything on the library stream: input copy, keys, all batches and the
-    // outlier copy-out (the per-slide counts read-back and its host wait are
-    // the only parts outside).
+    // Everything on the library stream from the input copy to the last
+    // kernel, plus the outlier copy-out (the per-slide counts read-back and
+    // its host wait are the only parts outside).
     times->total = (elapsed(t0, t2) + elapsed(d0, d1)) * inv;
     times->undetermined_per_slide = (double)s.undet_total * inv;
   }
@@ -1423,15 +1425,15 @@ RTOD_API int rtod_profile_run(rtod_handle* h, const float* pts, int64_t n, int64
   for (auto& e : kev) e = es.make();
   BatchState s{};
   std::vector<int32_t> nout, nund;
-  int r = run_stream(h, pts, slides, slides * h->W, t0, t1, &kev, &s, &nout, &nund);
+  int r = run_stream(h, pts, slides, slides * h->W, t0, t1, nullptr, &kev, &s, &nout, &nund);
   if (r) return r;
   for (int i = 0; i < n_kernels; ++i) kernel_ms[i] = 0;
-  kernel_ms[0] = elapsed(t0, t1);  // input copy (host streams only) + cell keys of the stream
+  kernel_ms[0] = elapsed(h->ev[1], t1);  // cell keys of the stream
   for (int64_t i = 0; i < nb; ++i) {
     const cudaEvent_t* e = &kev[(size_t)i * 8];
     for (int k = 1; k < kPipeKernels && k < n_kernels; ++k) kernel_ms[k] += elapsed(e[k], e[k + 1]);
   }
-  if (n_kernels > 5) kernel_ms[5] += h->flush_ms;  // span engine: compaction once per chunk
+  if (n_kernels > 6) kernel_ms[6] += h->flush_ms;  // span engine: compaction once per chunk
   for (int i = 0; i < n_kernels; ++i) kernel_ms[i] /= (double)slides;
   return RTOD_OK;
 }
