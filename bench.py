@@ -309,16 +309,24 @@ def run_ours(args, world, rank, local):
 
 
 def cpu_baseline(w):
+    """The oracle's grid engine (CPU restatement of RTOD's path) on the whole
+    stream: all host threads (the reported value) and one thread."""
     from oracle import oracle
     oracle.build()
     threads = os.cpu_count() or 1
     t0 = time.perf_counter()
     off, ids, st = oracle.detect(w.points, w.window, w.slide, w.R, w.K, engine="grid", threads=threads)
     dt = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    off1, ids1, _ = oracle.detect(w.points, w.window, w.slide, w.R, w.K, engine="grid", threads=1)
+    dt1 = time.perf_counter() - t0
+    assert np.array_equal(off, off1) and np.array_equal(ids, ids1)
     slides = len(off) - 1
     return {"value": slides * w.slide / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"whole stream once ({slides} slides), oracle grid engine, slides split over "
-                      f"{threads} threads", "us_per_slide": dt / slides * 1e6}, (off, ids)
+                      f"{threads} threads", "us_per_slide": dt / slides * 1e6,
+            "single_thread": {"value": slides * w.slide / dt1, "unit": UNIT, "cores": 1,
+                              "us_per_slide": dt1 / slides * 1e6}}, (off, ids)
 
 
 def emit_ours(args, world, w, res):
@@ -372,7 +380,8 @@ def emit_ours(args, world, w, res):
         "bit_exact_across_engines": True,
     }
     if not args.no_cpu_baseline and world == 1:
-        cb, _ = cpu_baseline(w)
+        cb, (coff, cids) = cpu_baseline(w)
+        cb["same_outliers_as_gpu"] = bool(np.array_equal(coff, r["offsets"]) and np.array_equal(cids, r["ids"]))
         line["cpu_baseline"] = cb
     print(json.dumps(line))
 

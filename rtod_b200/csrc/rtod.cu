@@ -269,7 +269,11 @@ struct rtod_handle {
   int graph_ring = -1;
   int64_t batches = 0;
 
-  cudaEvent_t ev[8] = {};
+  cudaEvent_t ev[16] = {};
+  cudaStream_t copy_stream = nullptr;     // host-stream pieces, overlapped with detection
+  std::vector<cudaEvent_t> piece_ev;      // one per piece
+  void* host_rb = nullptr;  // pinned read-back of the run's counters and per-slide records
+  size_t host_rb_bytes = 0;
   int64_t launches = 0;
   int64_t graph_replays = 0;
   int64_t undet_total = 0;
@@ -785,12 +789,13 @@ int ensure_records(rtod_handle* h, int64_t n) {
   return RTOD_OK;
 }
 
-// Device copy of a stream of `used` points (a host pointer is copied into the
-// handle's run buffer) plus room for its keys and router features.
-int stage_stream(rtod_handle* h, const float* pts, int64_t used, const float** src) {
+// Room for a stream of `used` points: the handle's run buffer for a host
+// stream (*host = true; run_stream copies it in), its keys and features.
+int stage_stream(rtod_handle* h, const float* pts, int64_t used, const float** src, bool* host) {
   const int64_t D = h->D;
   *src = pts;
-  if (!is_device_ptr(pts)) {
+  *host = !is_device_ptr(pts);
+  if (*host) {
     if (h->run_buf_cap < used * D) {
       if (h->run_buf) h->device_bytes -= h->run_buf_cap * 4;
       dfree(h->run_buf);
@@ -798,8 +803,7 @@ int stage_stream(rtod_handle* h, const float* pts, int64_t used, const float** s
       if (dalloc(&h->run_buf, (size_t)(used * D), &h->device_bytes)) return RTOD_ERR_CUDA;
       h->run_buf_cap = used * D;
     }
-    CU(cudaMemcpyAsync(h->run_buf, pts, (size_t)(used * D) * sizeof(float), cudaMemcpyHostToDevice, h->stream));
-    *src = h->run_buf;
+    *src = h->run_buf;  // filled piece by piece by run_stream
   }
   if (h->run_key_cap < used) {
     if (h->run_keys) h->device_bytes -= h->run_key_cap * 9;
@@ -876,14 +880,44 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
   const int64_t chunk = span ? span_chunk(h, B, slides) : 0;
   if (span && (r = ensure_span(h, W / S + B - 1, chunk))) return r;
   if (e_begin) CU(cudaEventRecord(e_begin, h->stream));
-  if ((r = stage_stream(h, pts, used, &src))) return r;
+  bool host = false;
+  if ((r = stage_stream(h, pts, used, &src, &host))) return r;
   if ((r = configure(h, MODE_RUN, B, S, src, !span))) return r;  // first detected window: [S, W + S)
   CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
+  // A host stream is copied in pieces on a second stream: piece i holds the
+  // points batch i needs beyond the earlier pieces ([0, W + B S) for the
+  // first), so detection of a batch overlaps the copy of the next pieces.
+  const int64_t nbatch = (slides + B - 1) / B;
+  auto piece_end = [&](int64_t i) { return std::min(used, W + (i + 1) * (int64_t)B * S); };
+  if (host) {
+    if (!h->copy_stream) CU(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    while ((int64_t)h->piece_ev.size() < nbatch) {
+      cudaEvent_t e;
+      CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      h->piece_ev.push_back(e);
+    }
+    if (e_begin) CU(cudaStreamWaitEvent(h->copy_stream, e_begin, 0));
+    const int64_t D = h->D;
+    for (int64_t i = 0; i < nbatch; ++i) {
+      const int64_t a = i ? piece_end(i - 1) : 0, e = piece_end(i);
+      CU(cudaMemcpyAsync(h->run_buf + a * D, pts + a * D, (size_t)((e - a) * D) * sizeof(float),
+                         cudaMemcpyHostToDevice, h->copy_stream));
+      CU(cudaEventRecord(h->piece_ev[(size_t)i], h->copy_stream));
+    }
+  }
+  const unsigned kgrid = (unsigned)h->sm_count * 8;
+  // cell keys of points [a, b) (and their slide blocks' coordinate ranges),
+  // after their piece has arrived
+  auto keys = [&](int64_t i, int64_t a, int64_t b) -> int {
+    if (host) CU(cudaStreamWaitEvent(h->stream, h->piece_ev[(size_t)i], 0));
+    const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((b - a + 255) / 256, kgrid));
+    DISPATCH_D(h->D, CU(launch_k(k_keys<D>, dim3(kx), 256, h->stream, src, a, b, h->cell, h->run_keys,
+                                 h->run_prev, h->bs, h->S, h->run_blk_lo, h->run_blk_hi)));
+    h->launches++;
+    return RTOD_OK;
+  };
   CU(cudaEventRecord(h->ev[1], h->stream));  // start of the key kernel (profile)
-  const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((used + 255) / 256, h->sm_count * 8));
-  DISPATCH_D(h->D, CU(launch_k(k_keys<D>, dim3(kx), 256, h->stream, src, (int64_t)0, used, h->cell, h->run_keys,
-                               h->run_prev, h->bs, h->S, h->run_blk_lo, h->run_blk_hi)));
-  h->launches++;
+  if ((r = keys(0, 0, host ? piece_end(0) : used))) return r;
   if (e_keys) CU(cudaEventRecord(e_keys, h->stream));
   const int64_t out_cap = std::min(ids_cap, h->ids_cap);
   const int64_t full = slides / B, rem = slides % B;
@@ -904,6 +938,7 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
       }
     }
     const Span* spp = span ? &sp : nullptr;
+    if (host && i > 0 && (r = keys(i, piece_end(i - 1), piece_end(i)))) return r;
     if (kev) {
       cudaEvent_t* e = &(*kev)[(size_t)i * 8];
       CU(cudaEventRecord(e[0], h->stream));
@@ -925,12 +960,26 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
     }
   }
   if (e_end) CU(cudaEventRecord(e_end, h->stream));
-  nout->resize((size_t)slides);
-  nund->resize((size_t)slides);
-  CU(cudaMemcpyAsync(out_state, h->bs, sizeof(BatchState), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaMemcpyAsync(nout->data(), h->rec_nout, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaMemcpyAsync(nund->data(), h->rec_undet, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+  // Counters and per-slide records through one pinned buffer: async copies
+  // and a single wait.
+  const size_t rb = sizeof(BatchState) + 2 * (size_t)slides * sizeof(int32_t);
+  if (rb > h->host_rb_bytes) {
+    if (h->host_rb) cudaFreeHost(h->host_rb);
+    h->host_rb = nullptr;
+    h->host_rb_bytes = 0;
+    CU(cudaMallocHost(&h->host_rb, rb));
+    h->host_rb_bytes = rb;
+  }
+  char* hb = (char*)h->host_rb;
+  int32_t* hno = (int32_t*)(hb + sizeof(BatchState));
+  int32_t* hnu = hno + slides;
+  CU(cudaMemcpyAsync(hb, h->bs, sizeof(BatchState), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaMemcpyAsync(hno, h->rec_nout, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+  CU(cudaMemcpyAsync(hnu, h->rec_undet, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
   CU(cudaStreamSynchronize(h->stream));
+  std::memcpy(out_state, hb, sizeof(BatchState));
+  nout->assign(hno, hno + slides);
+  nund->assign(hnu, hnu + slides);
   h->flush_ms = 0;
   for (const auto& pr : chunk_ev) h->flush_ms += elapsed(pr.first, pr.second);
   h->n_pushed = used;
@@ -955,8 +1004,15 @@ void free_all(rtod_handle* h) {
   dfree(h->rec_nout); dfree(h->rec_undet); dfree(h->ids);
   if (h->ctr_init) cudaFreeHost(h->ctr_init);
   h->ctr_init = nullptr;
+  if (h->host_rb) cudaFreeHost(h->host_rb);
+  h->host_rb = nullptr;
+  h->host_rb_bytes = 0;
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
+  for (auto e : h->piece_ev) cudaEventDestroy(e);
+  h->piece_ev.clear();
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  h->copy_stream = nullptr;
   if (h->stream) cudaStreamDestroy(h->stream);
 }
 
@@ -1361,7 +1417,7 @@ RTOD_API int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_s
     if (rt) return rt;
   }
   EventSet es;
-  cudaEvent_t t0 = es.make(), t1 = es.make(), t2 = es.make(), d0 = es.make(), d1 = es.make();
+  cudaEvent_t t0 = h->ev[8], t1 = h->ev[9], t2 = h->ev[10], d0 = h->ev[11], d1 = h->ev[12];
   // Stage split (only without graphs): events around every kernel of every batch.
   std::vector<cudaEvent_t> kev;
   const bool stage = times && !h->cfg.use_graph;
