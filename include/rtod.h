@@ -51,6 +51,11 @@ extern "C" {
 #define RTOD_PRED_F64_LT 1  /* RTOD's double test: |dx| < R in 1-d, d^2 < R*R otherwise
                                (src/ods/optixScan.cu:170-190) */
 
+/* rtod_config.coord: how coordinates are passed and stored. */
+#define RTOD_COORD_F32 0 /* float (default) */
+#define RTOD_COORD_F64 1 /* double, as RTOD stores them (double3 read with %lf, src/ods/optixScan.cpp:95-147);
+                            needs RTOD_PRED_F64_LT; pass points to the _f64 entry points */
+
 /* rtod_config.engine */
 #define RTOD_ENGINE_AUTO 0
 #define RTOD_ENGINE_WINDOW 1
@@ -81,7 +86,8 @@ typedef struct rtod_config {
                           RTOD_ENGINE_SPAN (1-d only: one counting sort per batch of
                           windows; falls back to the window engine when W/S > 2047).
                           push/detect always use the window engine. Results are identical. */
-  int32_t reserved[2];
+  int32_t coord;       /* RTOD_COORD_F32 or RTOD_COORD_F64 */
+  int32_t reserved[1];
 } rtod_config;
 
 /* Per-slide stage times in ms, averaged over the slides of the last call,
@@ -116,6 +122,12 @@ int rtod_create(const rtod_config* cfg, rtod_handle** out);
    rtod_detect before the next push. */
 int rtod_push_slide(rtod_handle* h, const float* pts, int64_t n);
 
+/* rtod_push_slide for a handle created with coord = RTOD_COORD_F64: n * dim
+   doubles, stored and compared as doubles (RTOD keeps double3 points and
+   tests them in double, src/ods/optixScan.cu:170-190). Each entry point
+   rejects a handle of the other coordinate type (RTOD_ERR_ARG). */
+int rtod_push_slide_f64(rtod_handle* h, const double* pts, int64_t n);
+
 /* Detects the outliers of the window produced by the last push and copies
    their sorted global indices to out_ids (host or device memory, room for
    cap entries); *n_out receives the count even when it exceeds cap (then
@@ -132,6 +144,12 @@ int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t* n_out, r
 int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides,
              int64_t* out_offsets, int64_t* out_ids, int64_t ids_cap, int64_t* slides_out,
              rtod_times* times);
+
+/* rtod_run for a handle created with coord = RTOD_COORD_F64 (n * dim
+   doubles). */
+int rtod_run_f64(rtod_handle* h, const double* pts, int64_t n, int64_t max_slides,
+                 int64_t* out_offsets, int64_t* out_ids, int64_t ids_cap, int64_t* slides_out,
+                 rtod_times* times);
 
 /* Clears the stream so that the handle can take a new first window. */
 int rtod_reset(rtod_handle* h);

@@ -40,8 +40,12 @@ def lib():
         L.oracle_detect.argtypes = [vp, i64, i32, i64, i64, f64, i32, i32, i32, i32, i64, vp, vp, i64, vp]
         L.oracle_window_counts.restype = i32
         L.oracle_window_counts.argtypes = [vp, i64, i32, i64, i64, f64, i32, vp]
+        L.oracle_detect_f64.restype = i64
+        L.oracle_detect_f64.argtypes = [vp, i64, i32, i64, i64, f64, i32, i32, i32, i32, i64, vp, vp, i64, vp]
         L.oracle_pred.restype = i32
         L.oracle_pred.argtypes = [vp, vp, i32, f64, i32]
+        L.oracle_pred_f64.restype = i32
+        L.oracle_pred_f64.argtypes = [vp, vp, i32, f64]
         L.oracle_mlp_param_count.restype = i32
         L.oracle_mlp_param_count.argtypes = [i32]
         L.oracle_mlp_forward.restype = i32
@@ -59,10 +63,12 @@ def _ptr(a: np.ndarray):
 
 
 def detect(points: np.ndarray, W: int, S: int, R: float, K: int, pred="fp32_le", engine="grid",
-           threads: int = 1, max_slides: int = 10000, ids_cap: int | None = None):
+           threads: int = 1, max_slides: int = 10000, ids_cap: int | None = None, f64: bool = False):
     """Per-slide sorted outlier indices in CSR form: (offsets, ids, stats).
-    stats = [undetermined points summed over slides, pair tests, slides]."""
-    pts = np.ascontiguousarray(points, dtype=np.float32)
+    stats = [undetermined points summed over slides, pair tests, slides].
+    f64: the points are kept as double (RTOD's storage) and compared with
+    RTOD's double predicate (pred must be "f64_lt")."""
+    pts = np.ascontiguousarray(points, dtype=np.float64 if f64 else np.float32)
     if pts.ndim == 1:
         pts = pts[:, None]
     n, d = pts.shape
@@ -74,7 +80,8 @@ def detect(points: np.ndarray, W: int, S: int, R: float, K: int, pred="fp32_le",
     off = np.zeros(slides + 1, np.int64)
     ids = np.zeros(ids_cap, np.int64)
     stats = np.zeros(3, np.int64)
-    r = lib().oracle_detect(_ptr(pts), n, d, W, S, float(R), K,
+    fn = lib().oracle_detect_f64 if f64 else lib().oracle_detect
+    r = fn(_ptr(pts), n, d, W, S, float(R), K,
                             PRED[pred] if isinstance(pred, str) else int(pred),
                             ENGINE[engine], threads, max_slides, _ptr(off), _ptr(ids), ids_cap,
                             _ptr(stats))
@@ -99,6 +106,13 @@ def pred(p, q, R: float, mode="fp32_le") -> bool:
     p = np.ascontiguousarray(p, dtype=np.float32).ravel()
     q = np.ascontiguousarray(q, dtype=np.float32).ravel()
     return bool(lib().oracle_pred(_ptr(p), _ptr(q), p.size, float(R), PRED[mode]))
+
+
+def pred_f64(p, q, R: float) -> bool:
+    """RTOD's double predicate on double coordinates."""
+    p = np.ascontiguousarray(p, dtype=np.float64).ravel()
+    q = np.ascontiguousarray(q, dtype=np.float64).ravel()
+    return bool(lib().oracle_pred_f64(_ptr(p), _ptr(q), p.size, float(R)))
 
 
 def mlp_param_count(B: int = 4) -> int:

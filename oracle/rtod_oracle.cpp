@@ -77,12 +77,14 @@ struct Pred {
     R2f = rf * rf;
   }
 
-  // Neighbour test between two points stored point-major (d floats each).
-  inline bool operator()(const float* p, const float* q) const {
+  // Neighbour test between two points stored point-major (d coordinates
+  // each, float or double; the FP32 predicate is only used with float).
+  template <typename T>
+  inline bool operator()(const T* p, const T* q) const {
     if (mode == PRED_FP32_LE) {
       float s = 0.0f;
       for (int i = 0; i < dim; ++i) {
-        float dx = p[i] - q[i];
+        float dx = (float)p[i] - (float)q[i];
         float t = dx * dx;
         s = (i == 0) ? t : s + t;
         if (s > R2f) return false;  // partial sums never decrease
@@ -104,21 +106,23 @@ struct Pred {
   }
 };
 
+template <typename T>
 struct Stream {
-  const float* pts;
+  const T* pts;
   int64_t n;
   int dim;
   int64_t W, S;
   int K;
   Pred pred;
-  const float* at(int64_t g) const { return pts + g * dim; }
+  const T* at(int64_t g) const { return pts + g * dim; }
 };
 
 // Brute-force count of window [lo, lo+W) neighbours of point g, stopping once
 // the count exceeds `cap` (check_outlier, optixScan.cpp:820-833).
-int count_brute(const Stream& s, int64_t lo, int64_t g, int cap, uint64_t* tests) {
+template <typename T>
+int count_brute(const Stream<T>& s, int64_t lo, int64_t g, int cap, uint64_t* tests) {
   int c = 0;
-  const float* p = s.at(g);
+  const T* p = s.at(g);
   for (int64_t q = lo; q < lo + s.W; ++q) {
     ++*tests;
     if (s.pred(p, s.at(q))) {
@@ -129,8 +133,9 @@ int count_brute(const Stream& s, int64_t lo, int64_t g, int cap, uint64_t* tests
 }
 
 // Grid filter state: a restatement of ScanState::cell_queue plus FixQueue.
+template <typename T>
 struct Grid {
-  const Stream& s;
+  const Stream<T>& s;
   int hd;                 // hashed dimensions (min(d, 3))
   double cell;            // cell side
   double mn[3];           // global per-dim minimum (read_data, optixScan.cpp:104-146)
@@ -139,7 +144,7 @@ struct Grid {
   int reach;              // neighbour-cell reach (cells) of the exact count
   std::unordered_map<int64_t, std::deque<int64_t>> cells;
 
-  Grid(const Stream& st, bool filter) : s(st) {
+  Grid(const Stream<T>& st, bool filter) : s(st) {
     hd = s.dim < 3 ? s.dim : 3;
     cell = s.pred.R / std::sqrt((double)hd) * (1.0 - std::ldexp(1.0, -16));
     double mx[3];
@@ -181,7 +186,7 @@ struct Grid {
   int count(int64_t g, uint64_t* tests) const {
     int64_t c[3], o[3] = {0, 0, 0};
     coords(g, c);
-    const float* p = s.at(g);
+    const T* p = s.at(g);
     int n = 0;
     int span = 2 * reach + 1;
     int total = 1;
@@ -213,7 +218,8 @@ struct SlideOut {
   int64_t undetermined = 0;
 };
 
-void run_brute(const Stream& s, int64_t j0, int64_t j1, std::vector<SlideOut>& out, uint64_t* tests) {
+template <typename T>
+void run_brute(const Stream<T>& s, int64_t j0, int64_t j1, std::vector<SlideOut>& out, uint64_t* tests) {
   for (int64_t j = j0; j < j1; ++j) {
     int64_t lo = (j + 1) * s.S;
     SlideOut& so = out[j];
@@ -223,10 +229,11 @@ void run_brute(const Stream& s, int64_t j0, int64_t j1, std::vector<SlideOut>& o
   }
 }
 
-void run_grid(const Stream& s, bool filter, int64_t j0, int64_t j1, std::vector<SlideOut>& out,
+template <typename T>
+void run_grid(const Stream<T>& s, bool filter, int64_t j0, int64_t j1, std::vector<SlideOut>& out,
               uint64_t* tests) {
   if (j0 >= j1) return;
-  Grid grid(s, filter);
+  Grid<T> grid(s, filter);
   // Window before slide j0 (detect_outlier's initial fill, optixScan.cpp:1029-1033).
   for (int64_t g = j0 * s.S; g < j0 * s.S + s.W; ++g) grid.insert(g);
   std::vector<int64_t> undet;
@@ -247,19 +254,16 @@ void run_grid(const Stream& s, bool filter, int64_t j0, int64_t j1, std::vector<
   }
 }
 
-bool finite_all(const float* p, int64_t n) {
+template <typename T>
+bool finite_all(const T* p, int64_t n) {
   for (int64_t i = 0; i < n; ++i)
     if (!std::isfinite(p[i])) return false;
   return true;
 }
 
-}  // namespace
-
-extern "C" {
-
 // Processes a whole stream the way detect_outlier does and writes, per slide,
 // the sorted global indices of the outliers in CSR form.
-//   pts          n points, point-major (n * dim floats)
+//   pts          n points, point-major (n * dim coordinates)
 //   engine       0 brute force, 1 grid filter (opt >= 1) , 2 grid without the
 //                all-inlier filter (opt 0)
 //   threads      >= 1; slides are split into contiguous ranges, one per thread
@@ -267,16 +271,17 @@ extern "C" {
 //   stats        [3]: undetermined points (sum over slides), pair tests, slides
 // Returns the number of slides (>= 0) or a negative error:
 //   -1 bad config, -2 output capacity, -5 non-finite input.
-int64_t oracle_detect(const float* pts, int64_t n, int32_t dim, int64_t W, int64_t S, double R,
-                      int32_t K, int32_t pred, int32_t engine, int32_t threads, int64_t max_slides,
-                      int64_t* out_offsets, int64_t* out_ids, int64_t ids_cap, int64_t* stats) {
+template <typename T>
+int64_t detect_impl(const T* pts, int64_t n, int32_t dim, int64_t W, int64_t S, double R, int32_t K,
+                    int32_t pred, int32_t engine, int32_t threads, int64_t max_slides, int64_t* out_offsets,
+                    int64_t* out_ids, int64_t ids_cap, int64_t* stats) {
   if (dim < 1 || dim > 8 || W < 1 || S < 1 || S > W || W % S != 0 || !(R > 0) || K < 0 ||
       (pred != PRED_FP32_LE && pred != PRED_F64_LT) || engine < 0 || engine > 2 || n < 0)
     return -1;
   if (!finite_all(pts, n * dim)) return -5;
   int64_t slides = n >= W ? (n - W) / S : 0;
   if (max_slides >= 0 && slides > max_slides) slides = max_slides;
-  Stream s{pts, n, dim, W, S, K, Pred(dim, pred, R)};
+  Stream<T> s{pts, n, dim, W, S, K, Pred(dim, pred, R)};
   std::vector<SlideOut> out((size_t)slides);
   if (threads < 1) threads = 1;
   if (threads > slides) threads = (int)std::max<int64_t>(1, slides);
@@ -315,12 +320,35 @@ int64_t oracle_detect(const float* pts, int64_t n, int32_t dim, int64_t W, int64
   return slides;
 }
 
+}  // namespace
+
+extern "C" {
+
+// detect_impl on float coordinates.
+int64_t oracle_detect(const float* pts, int64_t n, int32_t dim, int64_t W, int64_t S, double R,
+                      int32_t K, int32_t pred, int32_t engine, int32_t threads, int64_t max_slides,
+                      int64_t* out_offsets, int64_t* out_ids, int64_t ids_cap, int64_t* stats) {
+  return detect_impl(pts, n, dim, W, S, R, K, pred, engine, threads, max_slides, out_offsets, out_ids, ids_cap,
+                     stats);
+}
+
+// The same on double coordinates (RTOD stores double3 points,
+// src/ods/optixScan.cpp:95-147), with RTOD's double predicate only
+// (pred must be 1).
+int64_t oracle_detect_f64(const double* pts, int64_t n, int32_t dim, int64_t W, int64_t S, double R,
+                          int32_t K, int32_t pred, int32_t engine, int32_t threads, int64_t max_slides,
+                          int64_t* out_offsets, int64_t* out_ids, int64_t ids_cap, int64_t* stats) {
+  if (pred != PRED_F64_LT) return -1;
+  return detect_impl(pts, n, dim, W, S, R, K, pred, engine, threads, max_slides, out_offsets, out_ids, ids_cap,
+                     stats);
+}
+
 // Uncapped neighbour counts (self included) of every point of the window
 // [lo, lo+W) against that window, by brute force. counts[i] is point lo+i.
 int32_t oracle_window_counts(const float* pts, int64_t n, int32_t dim, int64_t lo, int64_t W,
                              double R, int32_t pred, int32_t* counts) {
   if (dim < 1 || dim > 8 || lo < 0 || W < 1 || lo + W > n || !(R > 0)) return -1;
-  Stream s{pts, n, dim, W, W, 0, Pred(dim, pred, R)};
+  Stream<float> s{pts, n, dim, W, W, 0, Pred(dim, pred, R)};
   for (int64_t i = 0; i < W; ++i) {
     int c = 0;
     const float* p = s.at(lo + i);
@@ -333,6 +361,11 @@ int32_t oracle_window_counts(const float* pts, int64_t n, int32_t dim, int64_t l
 // The predicate itself, for known-answer tests.
 int32_t oracle_pred(const float* p, const float* q, int32_t dim, double R, int32_t pred) {
   return Pred(dim, pred, R)(p, q) ? 1 : 0;
+}
+
+// RTOD's double predicate on double coordinates.
+int32_t oracle_pred_f64(const double* p, const double* q, int32_t dim, double R) {
+  return Pred(dim, PRED_F64_LT, R)(p, q) ? 1 : 0;
 }
 
 }  // extern "C"

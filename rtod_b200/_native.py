@@ -27,6 +27,7 @@ class RtodError(RuntimeError):
 
 
 ENGINE = {"auto": 0, "window": 1, "span": 2}
+COORD = {"f32": 0, "f64": 1}
 ENGINE_NAME = {1: "window", 2: "span"}
 
 
@@ -37,7 +38,7 @@ class Config(ctypes.Structure):
         ("pred", ctypes.c_int32), ("router", ctypes.c_int32), ("tuner", ctypes.c_int32),
         ("cells_per_r", ctypes.c_int32), ("block_warps", ctypes.c_int32),
         ("use_graph", ctypes.c_int32), ("device", ctypes.c_int32), ("batch", ctypes.c_int32),
-        ("engine", ctypes.c_int32), ("reserved", ctypes.c_int32 * 2),
+        ("engine", ctypes.c_int32), ("coord", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1),
     ]
 
 
@@ -62,9 +63,12 @@ SIGNATURES = [
     ("rtod_config_init", _i32, [ctypes.POINTER(Config)]),
     ("rtod_create", _i32, [ctypes.POINTER(Config), ctypes.POINTER(_vp)]),
     ("rtod_push_slide", _i32, [_vp, _vp, _i64]),
+    ("rtod_push_slide_f64", _i32, [_vp, _vp, _i64]),
     ("rtod_detect", _i32, [_vp, _vp, _i64, ctypes.POINTER(_i64), ctypes.POINTER(Times)]),
     ("rtod_run", _i32, [_vp, _vp, _i64, _i64, _vp, _vp, _i64, ctypes.POINTER(_i64),
                         ctypes.POINTER(Times)]),
+    ("rtod_run_f64", _i32, [_vp, _vp, _i64, _i64, _vp, _vp, _i64, ctypes.POINTER(_i64),
+                            ctypes.POINTER(Times)]),
     ("rtod_reset", _i32, [_vp]),
     ("rtod_slides_done", _i64, [_vp]),
     ("rtod_get_tuning", _i32, [_vp, _vp]),

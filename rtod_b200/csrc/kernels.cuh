@@ -112,9 +112,10 @@ struct Job {
   int32_t n;         // cells per R = stencil reach in cells
   int32_t filter;    // safe-inlier skip enabled
   int32_t ring;      // 1: ring source, 0: resident stream
-  const float* pts;       // ring: SoA [D][W] by slot; stream: point-major [N][D]
+  const void* pts;        // coordinates (float or double, the handle's type): ring: SoA
+                          // [D][W] by slot; stream: point-major [N][D]
   const uint64_t* keys;   // ring: [W] by slot; stream: [N] by global index
-  const float* stage;     // ring: the points k_ingest writes (point-major)
+  const void* stage;      // ring: the points k_ingest writes (point-major)
   const long long* blk_lo;  // stream: per slide block (S points), min cell coordinate per
   const long long* blk_hi;  //   hashed dimension ([blocks][3]); null for a ring
   uint8_t* prev;          // last capped count per source position (255 = safe, 254 = none)
@@ -124,7 +125,7 @@ struct Job {
   unsigned long long* kmax;   // [NB] largest cell key in a bin (0 when none)
   uint32_t* s_off;        // [W] cell-ordered: window offset (global index - lo)
   uint64_t* s_ckey;       // [W] cell-ordered: cell key
-  float* s_x;             // [D][Wp] cell-ordered coordinates
+  void* s_x;              // [D][Wp] cell-ordered coordinates (the handle's type)
   uint32_t* queue;        // [W] cell-ordered positions that need an exact count; with the
                           // router on, the early-exit queue grows from the front and the
                           // full-sweep queue from the back
@@ -210,10 +211,11 @@ struct Hashed {
   static constexpr int value = D < 3 ? D : 3;
 };
 
-// Cell key of one point; *code = DERR_NONFINITE for a non-finite coordinate,
-// DERR_RANGE for one too large for the grid (then the key is zero).
-template <int D>
-__device__ __forceinline__ uint64_t cell_key(const float* x, double cell, int32_t* code) {
+// Cell key of one point (float or double coordinates); *code =
+// DERR_NONFINITE for a non-finite coordinate, DERR_RANGE for one too large
+// for the grid (then the key is zero).
+template <int D, typename T>
+__device__ __forceinline__ uint64_t cell_key(const T* x, double cell, int32_t* code) {
   constexpr int H = Hashed<D>::value;
   const double lim = coord_limit(H);
   bool ok = true;
@@ -236,11 +238,14 @@ __device__ __forceinline__ uint64_t cell_key(const float* x, double cell, int32_
 // Neighbour predicates. PRED 0: FP32, each subtract, multiply and add
 // rounded on its own (no FMA contraction), summed left to right,
 // d2 <= fl32(fl32(R)^2). PRED 1: RTOD's double test
-// (src/ods/optixScan.cu:170-190): |dx| < R in 1-d, d^2 < R*R otherwise.
+// (src/ods/optixScan.cu:170-190): |dx| < R in 1-d, d^2 < R*R otherwise, on
+// float coordinates widened to double or on double coordinates (T = double,
+// used only with PRED 1).
 // ---------------------------------------------------------------------------
-template <int D, int PRED>
-__device__ __forceinline__ bool is_nbr(const float* q, const float* c, float R2f, double R, double R2) {
+template <int D, int PRED, typename T>
+__device__ __forceinline__ bool is_nbr(const T* q, const T* c, float R2f, double R, double R2) {
   if constexpr (PRED == 0) {
+    static_assert(sizeof(T) == sizeof(float), "the FP32 predicate runs on float coordinates");
     float s = 0.0f;
 #pragma unroll
     for (int i = 0; i < D; ++i) {
@@ -367,15 +372,33 @@ __device__ __forceinline__ int64_t source_pos(const Job& jb, int64_t lo, int64_t
   return jb.ring ? g % jb.W : g;
 }
 
-template <int D>
-__device__ __forceinline__ void load_point(const Job& jb, int64_t src, float* x) {
+template <int D, typename T>
+__device__ __forceinline__ void load_point(const Job& jb, int64_t src, T* x) {
+  const T* pts = static_cast<const T*>(jb.pts);
   if (jb.ring) {
 #pragma unroll
-    for (int d = 0; d < D; ++d) x[d] = jb.pts[(int64_t)d * jb.W + src];
+    for (int d = 0; d < D; ++d) x[d] = pts[(int64_t)d * jb.W + src];
   } else {
 #pragma unroll
-    for (int d = 0; d < D; ++d) x[d] = jb.pts[src * D + d];
+    for (int d = 0; d < D; ++d) x[d] = pts[src * D + d];
   }
+}
+
+// Coordinate row d of a job's cell-ordered SoA.
+template <typename T>
+__device__ __forceinline__ T* sx_row(const Job& jb, int d) {
+  return static_cast<T*>(jb.s_x) + (int64_t)d * jb.Wp;
+}
+
+// Four consecutive coordinates starting at a multiple of 4 (rows are
+// aligned to 16 bytes for float, 32 for double).
+__device__ __forceinline__ void load4(const float* p, float* v) {
+  const float4 t = *reinterpret_cast<const float4*>(p);
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void load4(const double* p, double* v) {
+  const double2 a = *reinterpret_cast<const double2*>(p), b = *reinterpret_cast<const double2*>(p + 2);
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
 }
 
 }  // namespace rtod
@@ -387,8 +410,8 @@ namespace rtod {
 // ---------------------------------------------------------------------------
 // k_keys: cell keys of a resident stream, global indices [g0, g1).
 // ---------------------------------------------------------------------------
-template <int D>
-__global__ void __launch_bounds__(256) k_keys(const float* pts, int64_t g0, int64_t g1, double cell,
+template <int D, typename T>
+__global__ void __launch_bounds__(256) k_keys(const T* pts, int64_t g0, int64_t g1, double cell,
                                               uint64_t* keys, uint8_t* prev, BatchState* bs, int64_t S,
                                               long long* blk_lo, long long* blk_hi) {
   pdl_trigger();
@@ -402,11 +425,11 @@ __global__ void __launch_bounds__(256) k_keys(const float* pts, int64_t g0, int6
     int64_t k[3] = {0, 0, 0};
     int64_t blk = -1;
     if (valid) {
-      float x[D];
+      T x[D];
 #pragma unroll
       for (int d = 0; d < D; ++d) x[d] = pts[g * D + d];
       int32_t code;
-      const uint64_t key = cell_key<D>(x, cell, &code);
+      const uint64_t key = cell_key<D, T>(x, cell, &code);
       keys[g] = key;
       prev[g] = 254;
       if (code) set_err(bs, code);
@@ -444,24 +467,25 @@ __global__ void __launch_bounds__(256) k_keys(const float* pts, int64_t g0, int6
 // (global indices [0, W)); otherwise the S newest points of the job's window
 // [lo, lo + W), i.e. [lo + W - S, lo + W). Slot = global index % W.
 // ---------------------------------------------------------------------------
-template <int D>
+template <int D, typename T>
 __global__ void __launch_bounds__(256) k_ingest(Batch b, int32_t fill) {
   pdl_trigger();
   pdl_wait();
   if (!job_active(b)) return;
   const Job& jb = b.jobs[blockIdx.y];
-  float* ring = const_cast<float*>(jb.pts);
+  T* ring = static_cast<T*>(const_cast<void*>(jb.pts));
+  const T* stage = static_cast<const T*>(jb.stage);
   uint64_t* keys = const_cast<uint64_t*>(jb.keys);
   const int64_t n_new = fill ? jb.W : jb.S;
   const int64_t base = fill ? 0 : jb.ctr->lo + jb.W - jb.S;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += stride) {
     const int64_t slot = (base + i) % jb.W;
-    float x[D];
+    T x[D];
 #pragma unroll
-    for (int d = 0; d < D; ++d) x[d] = jb.stage[i * D + d];
+    for (int d = 0; d < D; ++d) x[d] = stage[i * D + d];
     int32_t code;
-    const uint64_t key = cell_key<D>(x, jb.cell, &code);
+    const uint64_t key = cell_key<D, T>(x, jb.cell, &code);
     if (code) set_err(b.bs, code);
 #pragma unroll
     for (int d = 0; d < D; ++d) ring[(int64_t)d * jb.W + slot] = x[d];
@@ -741,7 +765,7 @@ __device__ __forceinline__ bool group_safe_1d(const Job& jb, uint64_t key, uint3
   return false;
 }
 
-template <int D, bool ROUTE>
+template <int D, bool ROUTE, typename T>
 __global__ void __launch_bounds__(256) k_scatter(Batch b) {
   // Block-local table: bin, points of the chunk in the bin, claimed base.
   __shared__ uint32_t tbin[HIST_SLOTS];
@@ -830,12 +854,12 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
         const uint32_t bs0 = jb.bin_start[bin[u]];
         const uint32_t bs1 = jb.bin_start[bin[u] + 1];
         pos = bs0 + goff[u] + (slot[u] >= 0 ? tbase[slot[u]] : 0u);
-        float x[D];
-        load_point<D>(jb, src[u], x);
+        T x[D];
+        load_point<D, T>(jb, src[u], x);
         jb.s_off[pos] = (uint32_t)i;
         jb.s_ckey[pos] = key[u];
 #pragma unroll
-        for (int d = 0; d < D; ++d) jb.s_x[(int64_t)d * jb.Wp + pos] = x[d];
+        for (int d = 0; d < D; ++d) sx_row<T>(jb, d)[pos] = x[d];
         cnt = bs1 - bs0;
         if (jb.filter) {
           safe = cnt > (uint32_t)jb.K && (pure || jb.kmin[bin[u]] == jb.kmax[bin[u]]);
@@ -911,24 +935,24 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
 // [rs, re), 128 per step: each lane loads 4 consecutive candidates per
 // dimension with one float4, the warp tallies them with ballot/popc.
 // Returns true once the running total exceeds K.
-template <int D, int PRED>
-__device__ __forceinline__ bool count_run(const Job& jb, const float* qx, uint32_t rs, uint32_t re,
+template <int D, int PRED, typename T>
+__device__ __forceinline__ bool count_run(const Job& jb, const T* qx, uint32_t rs, uint32_t re,
                                           int& total) {
   const int lane = threadIdx.x & 31;
   for (uint32_t b = rs & ~3u; b < re; b += 128) {
     const uint32_t c0 = b + 4 * lane;
     bool in[4] = {false, false, false, false};
     if (c0 < re) {
-      float4 v[D];
+      T v[D][4];
 #pragma unroll
-      for (int d = 0; d < D; ++d) v[d] = *reinterpret_cast<const float4*>(jb.s_x + (int64_t)d * jb.Wp + c0);
+      for (int d = 0; d < D; ++d) load4(sx_row<T>(jb, d) + c0, v[d]);
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        float cx[D];
+        T cx[D];
 #pragma unroll
-        for (int d = 0; d < D; ++d) cx[d] = (&v[d].x)[e];
+        for (int d = 0; d < D; ++d) cx[d] = v[d][e];
         const uint32_t c = c0 + e;
-        in[e] = c >= rs && c < re && is_nbr<D, PRED>(qx, cx, jb.R2f, jb.R, jb.R2);
+        in[e] = c >= rs && c < re && is_nbr<D, PRED, T>(qx, cx, jb.R2f, jb.R, jb.R2);
       }
     }
     total += __popc(__ballot_sync(0xffffffffu, in[0])) + __popc(__ballot_sync(0xffffffffu, in[1])) +
@@ -955,16 +979,16 @@ __constant__ uint8_t c_rows3[3][49] = {
     {24, 23, 25, 17, 31, 16, 18, 30, 32, 22, 26, 10, 38, 15, 19, 29, 33, 9, 11, 37, 39, 8, 12, 36, 40,
      21, 27, 3, 45, 14, 20, 28, 34, 2, 4, 44, 46, 7, 13, 35, 41, 1, 5, 43, 47, 0, 6, 42, 48}};
 
-template <int D, int PRED>
+template <int D, int PRED, typename T>
 __device__ __forceinline__ bool count_query_rows(const Job& jb, uint32_t pos, int& total, bool* ok) {
   constexpr int H = Hashed<D>::value;
   static_assert(H >= 2, "row-parallel count needs 2 or 3 hashed dimensions");
   const int lane = threadIdx.x & 31;
   const int n = jb.n, span = 2 * n + 1;
   const int rows = (H == 2) ? span : span * span;
-  float qx[D];
+  T qx[D];
 #pragma unroll
-  for (int d = 0; d < D; ++d) qx[d] = jb.s_x[(int64_t)d * jb.Wp + pos];
+  for (int d = 0; d < D; ++d) qx[d] = sx_row<T>(jb, d)[pos];
   int64_t k[3];
   unpack_key(jb.s_ckey[pos], H, k);
   uint32_t rs[2] = {0, 0}, len[2] = {0, 0};
@@ -996,7 +1020,7 @@ __device__ __forceinline__ bool count_query_rows(const Job& jb, uint32_t pos, in
   *ok = !__any_sync(0xffffffffu, wrap);
   if (!*ok) return false;
   // exclusive offsets of the 64 row slots (slot = lane + 32 t)
-  uint32_t off[2], T = 0;
+  uint32_t off[2], ncand = 0;
 #pragma unroll
   for (int t = 0; t < 2; ++t) {
     uint32_t inc = len[t];
@@ -1005,10 +1029,10 @@ __device__ __forceinline__ bool count_query_rows(const Job& jb, uint32_t pos, in
       const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
       if (lane >= o) inc += y;
     }
-    off[t] = T + inc - len[t];
-    T += __shfl_sync(0xffffffffu, inc, 31);
+    off[t] = ncand + inc - len[t];
+    ncand += __shfl_sync(0xffffffffu, inc, 31);
   }
-  for (uint32_t v0 = 0; v0 < T; v0 += 128) {
+  for (uint32_t v0 = 0; v0 < ncand; v0 += 128) {
     bool in[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
@@ -1028,12 +1052,12 @@ __device__ __forceinline__ bool count_query_rows(const Job& jb, uint32_t pos, in
       const uint32_t base1 = __shfl_sync(0xffffffffu, rs[1], lo_s & 31);
       const uint32_t oo0 = __shfl_sync(0xffffffffu, off[0], lo_s & 31);
       const uint32_t oo1 = __shfl_sync(0xffffffffu, off[1], lo_s & 31);
-      if (v < T) {
+      if (v < ncand) {
         const uint32_t c = (lo_s < 32 ? base0 : base1) + (v - (lo_s < 32 ? oo0 : oo1));
-        float cx[D];
+        T cx[D];
 #pragma unroll
-        for (int d = 0; d < D; ++d) cx[d] = jb.s_x[(int64_t)d * jb.Wp + c];
-        in[e] = is_nbr<D, PRED>(qx, cx, jb.R2f, jb.R, jb.R2);
+        for (int d = 0; d < D; ++d) cx[d] = sx_row<T>(jb, d)[c];
+        in[e] = is_nbr<D, PRED, T>(qx, cx, jb.R2f, jb.R, jb.R2);
       }
     }
     total += __popc(__ballot_sync(0xffffffffu, in[0])) + __popc(__ballot_sync(0xffffffffu, in[1])) +
@@ -1045,45 +1069,45 @@ __device__ __forceinline__ bool count_query_rows(const Job& jb, uint32_t pos, in
 
 // Exact count of one queued point by the whole warp: `total` receives the
 // count (capped just above K); returns true if it exceeded K.
-template <int D, int PRED>
+template <int D, int PRED, typename T>
 __device__ __forceinline__ bool count_query(const Job& jb, uint32_t pos, int& total) {
   constexpr int H = Hashed<D>::value;
   if constexpr (H >= 2) {
     bool ok;
-    const bool r = count_query_rows<D, PRED>(jb, pos, total, &ok);
+    const bool r = count_query_rows<D, PRED, T>(jb, pos, total, &ok);
     if (ok) return r;
   }
-  float qx[D];
+  T qx[D];
 #pragma unroll
-  for (int d = 0; d < D; ++d) qx[d] = jb.s_x[(int64_t)d * jb.Wp + pos];
+  for (int d = 0; d < D; ++d) qx[d] = sx_row<T>(jb, d)[pos];
   int64_t k[3];
   unpack_key(jb.s_ckey[pos], H, k);
   total = 0;
   return for_each_run<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
-    return count_run<D, PRED>(jb, qx, rs, re, total);
+    return count_run<D, PRED, T>(jb, qx, rs, re, total);
   });
 }
 
 // Exact count of one queued point by one lane (full-sweep queue): the
 // candidates are read 8 at a time, so that their loads are in flight together.
-template <int D, int PRED>
+template <int D, int PRED, typename T>
 __device__ __forceinline__ bool count_query_lane(const Job& jb, uint32_t pos, int& total) {
   constexpr int H = Hashed<D>::value;
-  float qx[D];
+  T qx[D];
 #pragma unroll
-  for (int d = 0; d < D; ++d) qx[d] = jb.s_x[(int64_t)d * jb.Wp + pos];
+  for (int d = 0; d < D; ++d) qx[d] = sx_row<T>(jb, d)[pos];
   int64_t k[3];
   unpack_key(jb.s_ckey[pos], H, k);
   total = 0;
   return for_each_run<H>(jb.bin_start, k, jb.n, [&](uint32_t rs, uint32_t re) {
     for (uint32_t c0 = rs; c0 < re; c0 += 8) {
-      float cx[8][D];
+      T cx[8][D];
 #pragma unroll
       for (int e = 0; e < 8; ++e)
 #pragma unroll
-        for (int d = 0; d < D; ++d) cx[e][d] = c0 + e < re ? jb.s_x[(int64_t)d * jb.Wp + c0 + e] : 0.0f;
+        for (int d = 0; d < D; ++d) cx[e][d] = c0 + e < re ? sx_row<T>(jb, d)[c0 + e] : T(0);
 #pragma unroll
-      for (int e = 0; e < 8; ++e) total += (c0 + e < re) && is_nbr<D, PRED>(qx, cx[e], jb.R2f, jb.R, jb.R2);
+      for (int e = 0; e < 8; ++e) total += (c0 + e < re) && is_nbr<D, PRED, T>(qx, cx[e], jb.R2f, jb.R, jb.R2);
       if (total > jb.K) return true;
     }
     return false;
@@ -1162,7 +1186,7 @@ __device__ __forceinline__ void reset_bins(const Job& jb) {
 //     32 points per warp, each lane sweeping its own (short) candidate list;
 //     every counted point becomes a training sample of the router.
 // ---------------------------------------------------------------------------
-template <int D, int PRED, bool ROUTE>
+template <int D, int PRED, bool ROUTE, typename T>
 __global__ void __launch_bounds__(256) k_count(Batch b) {
   __shared__ SampleBuf sb;
   pdl_trigger();
@@ -1183,7 +1207,7 @@ __global__ void __launch_bounds__(256) k_count(Batch b) {
   for (int64_t q = warp; q < nq; q += nwarps) {
     const uint32_t pos = jb.queue[q];
     int total;
-    const bool inlier = count_query<D, PRED>(jb, pos, total);
+    const bool inlier = count_query<D, PRED, T>(jb, pos, total);
     if (lane == 0) {
       record_count(jb, lo, pos, inlier, total);
       if constexpr (ROUTE) record_sample(jb, sb, q, total, true);
@@ -1197,7 +1221,7 @@ __global__ void __launch_bounds__(256) k_count(Batch b) {
         const int64_t q = jb.W - 1 - idx;
         const uint32_t pos = jb.queue[q];
         int total;
-        const bool inlier = count_query_lane<D, PRED>(jb, pos, total);
+        const bool inlier = count_query_lane<D, PRED, T>(jb, pos, total);
         record_count(jb, lo, pos, inlier, total);
         record_sample(jb, sb, q, total, false);
       }

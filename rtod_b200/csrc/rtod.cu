@@ -69,6 +69,24 @@ int fail(int code, const char* fmt, ...) {
     DISPATCH_D(D_, { constexpr int PRED = 1; __VA_ARGS__; }); \
   }
 
+// Dimension x coordinate type (T = float, or double for a handle storing
+// double coordinates).
+#define DISPATCH_DT(F64_, D_, ...)                        \
+  if (F64_) {                                             \
+    DISPATCH_D(D_, { using T = double; __VA_ARGS__; });   \
+  } else {                                                \
+    DISPATCH_D(D_, { using T = float; __VA_ARGS__; });    \
+  }
+
+// Dimension x predicate x coordinate type: double coordinates always use
+// RTOD's double predicate.
+#define DISPATCH_DPT(F64_, D_, P_, ...)                                           \
+  if (F64_) {                                                                     \
+    DISPATCH_D(D_, { constexpr int PRED = 1; using T = double; __VA_ARGS__; });   \
+  } else {                                                                        \
+    DISPATCH_DP(D_, P_, { using T = float; __VA_ARGS__; });                       \
+  }
+
 bool is_device_ptr(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -127,7 +145,7 @@ struct Scratch {
   unsigned long long* kmax = nullptr;
   uint32_t* s_off = nullptr;
   uint64_t* s_ckey = nullptr;
-  float* s_x = nullptr;
+  unsigned char* s_x = nullptr;  // coordinates, the handle's type
   uint32_t* queue = nullptr;
   float* feat = nullptr;
   uint32_t* flags = nullptr;
@@ -146,7 +164,7 @@ struct SpanScratch {
   uint32_t* pre = nullptr;
   uint32_t* used = nullptr;
   uint32_t* s_off = nullptr;
-  float* s_x = nullptr;
+  unsigned char* s_x = nullptr;  // coordinates, the handle's type
   unsigned long long* scan_status = nullptr;
   SpanCtr* sc = nullptr;
   uint4* groups = nullptr;    // [windows][min(W, NB)] listed groups of a batch
@@ -236,13 +254,15 @@ struct rtod_handle {
   BatchState* bs = nullptr;
   RouterState* router = nullptr;
 
-  float* ring = nullptr;  // SoA [D][W]
+  int f64 = 0;   // coordinates stored as double (RTOD_COORD_F64)
+  int esz = 4;   // bytes per coordinate
+  unsigned char* ring = nullptr;  // SoA [D][W] coordinates
   uint64_t* ring_keys = nullptr;
   uint8_t* ring_prev = nullptr;
-  float* staging = nullptr;  // W * D floats
+  unsigned char* staging = nullptr;  // W * D coordinates
 
-  float* run_buf = nullptr;
-  int64_t run_buf_cap = 0;  // floats
+  unsigned char* run_buf = nullptr;
+  int64_t run_buf_cap = 0;  // coordinates
   uint64_t* run_keys = nullptr;
   uint8_t* run_prev = nullptr;
   int64_t run_key_cap = 0;
@@ -310,6 +330,10 @@ int check_config(const rtod_config* c) {
   if (c->engine < RTOD_ENGINE_AUTO || c->engine > RTOD_ENGINE_SPAN)
     return fail(RTOD_ERR_CONFIG, "engine must be 0 (auto), 1 (window) or 2 (span)");
   if (c->engine == RTOD_ENGINE_SPAN && c->dim != 1) return fail(RTOD_ERR_CONFIG, "the span engine needs dim = 1");
+  if (c->coord != RTOD_COORD_F32 && c->coord != RTOD_COORD_F64)
+    return fail(RTOD_ERR_CONFIG, "coord must be RTOD_COORD_F32 or RTOD_COORD_F64");
+  if (c->coord == RTOD_COORD_F64 && c->pred != RTOD_PRED_F64_LT)
+    return fail(RTOD_ERR_CONFIG, "double coordinates need the double predicate (RTOD_PRED_F64_LT)");
   return RTOD_OK;
 }
 
@@ -340,7 +364,7 @@ int ensure_pool(rtod_handle* h, int jobs, bool full = true) {
     if (s.full) continue;
     bool ok = !dalloc(&s.bin_count, NB, c) && !dalloc(&s.bin_start, NB + 1, c) && !dalloc(&s.kmin, NB, c) &&
               !dalloc(&s.kmax, NB, c) && !dalloc(&s.s_off, (size_t)W, c) && !dalloc(&s.s_ckey, (size_t)W, c) &&
-              !dalloc(&s.s_x, (size_t)(Wp * D), c) && !dalloc(&s.queue, (size_t)W, c) &&
+              !dalloc(&s.s_x, (size_t)(Wp * D * h->esz), c) && !dalloc(&s.queue, (size_t)W, c) &&
               !dalloc(&s.feat, (size_t)(h->cfg.router ? W * MLP_IN : 1), c) &&
               !dalloc(&s.flags, (size_t)((W + 31) / 32), c) && !dalloc(&s.scan_status, SCAN_TILES, c) &&
               !dalloc(&s.cmp_status, (size_t)cmp_tiles, c);
@@ -350,7 +374,7 @@ int ensure_pool(rtod_handle* h, int jobs, bool full = true) {
     CU(cudaMemset(s.bin_count, 0, NB * sizeof(uint32_t)));
     CU(cudaMemset(s.kmin, 0xff, NB * sizeof(unsigned long long)));
     CU(cudaMemset(s.kmax, 0, NB * sizeof(unsigned long long)));
-    CU(cudaMemset(s.s_x, 0, (size_t)(Wp * D) * sizeof(float)));
+    CU(cudaMemset(s.s_x, 0, (size_t)(Wp * D * h->esz)));
     CU(cudaMemset(s.flags, 0, (size_t)((W + 31) / 32) * sizeof(uint32_t)));
     CU(cudaMemset(s.scan_status, 0, SCAN_TILES * sizeof(unsigned long long)));
     CU(cudaMemset(s.cmp_status, 0, (size_t)cmp_tiles * sizeof(unsigned long long)));
@@ -412,7 +436,7 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
             !dalloc(&sp.kmin, NB, &bytes) && !dalloc(&sp.kmax, NB, &bytes) &&
             !dalloc(&sp.cnt, (size_t)(nblk * NB), &bytes) && !dalloc(&sp.pre, (size_t)((nblk + 1) * NB), &bytes) &&
             !dalloc(&sp.used, NB, &bytes) && !dalloc(&sp.s_off, (size_t)pts, &bytes) &&
-            !dalloc(&sp.s_x, (size_t)(Wp * h->D), &bytes) && !dalloc(&sp.scan_status, SCAN_TILES, &bytes) &&
+            !dalloc(&sp.s_x, (size_t)(Wp * h->D * h->esz), &bytes) && !dalloc(&sp.scan_status, SCAN_TILES, &bytes) &&
             !dalloc(&sp.sc, 1, &bytes) && !dalloc(&sp.bits, (size_t)(chunk * words), &bytes) &&
             !dalloc(&sp.base, (size_t)chunk, &bytes) &&
             !dalloc(&sp.groups, (size_t)((nblk - h->W / h->S + 1) * std::min<int64_t>(h->W, NB)), &bytes);
@@ -431,7 +455,7 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
   CU(cudaMemset(sp.kmin, 0xff, NB * sizeof(unsigned long long)));
   CU(cudaMemset(sp.kmax, 0, NB * sizeof(unsigned long long)));
   CU(cudaMemset(sp.cnt, 0, (size_t)(nblk * NB) * sizeof(uint32_t)));
-  CU(cudaMemset(sp.s_x, 0, (size_t)(Wp * h->D) * sizeof(float)));
+  CU(cudaMemset(sp.s_x, 0, (size_t)(Wp * h->D * h->esz)));
   CU(cudaMemset(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long)));
   SpanCtr c{};
   c.used = sp.used;
@@ -444,7 +468,7 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
 
 // Span parameters of a batch of B windows over the resident stream, with
 // bitsets of `chunk` slides.
-Span make_span(const rtod_handle* h, int B, const float* stream_pts, int64_t chunk) {
+Span make_span(const rtod_handle* h, int B, const void* stream_pts, int64_t chunk) {
   const SpanScratch& ss = h->span;
   Span sp{};
   sp.S = h->S;
@@ -489,7 +513,7 @@ int64_t span_chunk(const rtod_handle* h, int B, int64_t slides) {
   return (int64_t)B * std::max<int64_t>(1, std::min(per_batch, batches));
 }
 
-Job make_job(rtod_handle* h, int j, bool ring, const float* stream_pts) {
+Job make_job(rtod_handle* h, int j, bool ring, const void* stream_pts) {
   Job jb{};
   jb.W = h->W;
   jb.S = h->S;
@@ -531,7 +555,7 @@ Job make_job(rtod_handle* h, int j, bool ring, const float* stream_pts) {
 // Uploads the job table for a mode (only when it changed, so that captured
 // graphs stay valid) and initialises the job counters: job j starts at
 // window lo = first_lo + j*S and advances by jobs*S per batch.
-int configure(rtod_handle* h, int mode, int jobs, int64_t first_lo, const float* stream_pts, bool full = true) {
+int configure(rtod_handle* h, int mode, int jobs, int64_t first_lo, const void* stream_pts, bool full = true) {
   int r = ensure_pool(h, jobs, full);
   if (r) return r;
   std::vector<Job> tab((size_t)jobs);
@@ -571,6 +595,7 @@ struct Geom {
   int64_t Wmax, Smax;
   int D, pred, route, sm_count, block_warps;
   RouterState* router;
+  int f64 = 0;  // double coordinates
 };
 
 // Launches one batch: [ingest] hist scan scatter count compact [train].
@@ -584,7 +609,7 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
   int64_t launched = 0;
   if (ingest) {
     const int64_t gx = std::max<int64_t>(1, std::min<int64_t>((g.Smax + 255) / 256, g.sm_count * 4));
-    DISPATCH_D(g.D, CU(launch_k(k_ingest<D>, dim3((unsigned)gx, gy), 256, st, b, 0)));
+    DISPATCH_DT(g.f64, g.D, CU(launch_k(k_ingest<D, T>, dim3((unsigned)gx, gy), 256, st, b, 0)));
     launched++;
   }
   if (kev) CU(cudaEventRecord(kev[0], st));
@@ -596,17 +621,19 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
   CU(launch_k(k_scan, dim3(SCAN_TILES, gy), 256, st, b));
   if (kev) CU(cudaEventRecord(kev[2], st));
   if (g.route) {
-    DISPATCH_D(g.D, CU(launch_k(k_scatter<D, true>, dim3((unsigned)wx, gy), 256, st, b)));
+    DISPATCH_DT(g.f64, g.D, CU(launch_k(k_scatter<D, true, T>, dim3((unsigned)wx, gy), 256, st, b)));
   } else {
-    DISPATCH_D(g.D, CU(launch_k(k_scatter<D, false>, dim3((unsigned)wx, gy), 256, st, b)));
+    DISPATCH_DT(g.f64, g.D, CU(launch_k(k_scatter<D, false, T>, dim3((unsigned)wx, gy), 256, st, b)));
   }
   if (kev) CU(cudaEventRecord(kev[3], st));
   const int wpb = g.block_warps;
   const int64_t cx = std::max<int64_t>(1, (int64_t)g.sm_count * (64 / wpb) / nj);
   if (g.route) {
-    DISPATCH_DP(g.D, g.pred, CU(launch_k(k_count<D, PRED, true>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
+    DISPATCH_DPT(g.f64, g.D, g.pred,
+                 CU(launch_k(k_count<D, PRED, true, T>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
   } else {
-    DISPATCH_DP(g.D, g.pred, CU(launch_k(k_count<D, PRED, false>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
+    DISPATCH_DPT(g.f64, g.D, g.pred,
+                 CU(launch_k(k_count<D, PRED, false, T>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
   }
   if (kev) CU(cudaEventRecord(kev[4], st));
   CU(launch_k(k_compact, dim3((unsigned)((W + CMP_TILE - 1) / CMP_TILE), gy), 256, st, b));
@@ -639,7 +666,6 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
 // after classify and kev[5] after count (the stage slots of count, compact
 // and train hold classify, count and the chunk compaction timed by run_stream).
 int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, cudaEvent_t* kev, int64_t* nk) {
-  const unsigned gy = (unsigned)b.njobs;
   const int64_t npts = sp.nblk * sp.S;
   const int64_t hx = std::max<int64_t>(1, std::min<int64_t>((npts + 1023) / 1024, (int64_t)g.sm_count * 8));
   if (kev) CU(cudaEventRecord(kev[0], st));
@@ -648,16 +674,22 @@ int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, 
   if (kev) CU(cudaEventRecord(kev[1], st));
   CU(launch_k(k_span_scan, dim3(SCAN_TILES), 256, st, b, sp));
   if (kev) CU(cudaEventRecord(kev[2], st));
-  CU(launch_k(k_span_scatter<1>, dim3((unsigned)hx), 256, st, b, sp));
+  if (g.f64) {
+    CU(launch_k(k_span_scatter<1, double>, dim3((unsigned)hx), 256, st, b, sp));
+  } else {
+    CU(launch_k(k_span_scatter<1, float>, dim3((unsigned)hx), 256, st, b, sp));
+  }
   if (kev) CU(cudaEventRecord(kev[3], st));
   CU(launch_k(k_span_classify, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
   if (kev) CU(cudaEventRecord(kev[4], st));
   const int wpb = g.block_warps;
   const int64_t cx = (int64_t)g.sm_count * (64 / wpb);
-  if (g.pred == 0) {
-    CU(launch_k(k_span_count<1, 0>, dim3((unsigned)cx), wpb * 32, st, b, sp));
+  if (g.f64) {
+    CU(launch_k(k_span_count<1, 1, double>, dim3((unsigned)cx), wpb * 32, st, b, sp));
+  } else if (g.pred == 0) {
+    CU(launch_k(k_span_count<1, 0, float>, dim3((unsigned)cx), wpb * 32, st, b, sp));
   } else {
-    CU(launch_k(k_span_count<1, 1>, dim3((unsigned)cx), wpb * 32, st, b, sp));
+    CU(launch_k(k_span_count<1, 1, float>, dim3((unsigned)cx), wpb * 32, st, b, sp));
   }
   if (kev) CU(cudaEventRecord(kev[5], st));
   if (kev) CU(cudaEventRecord(kev[6], st));  // no per-batch compaction: see span_flush
@@ -685,7 +717,7 @@ int span_flush(rtod_handle* h, const Span& sp, int64_t s0, int64_t n, int64_t ou
 }
 
 Geom geom_of(const rtod_handle* h) {
-  return Geom{h->W, h->S, h->D, h->cfg.pred, h->cfg.router, h->sm_count, h->block_warps, h->router};
+  return Geom{h->W, h->S, h->D, h->cfg.pred, h->cfg.router, h->sm_count, h->block_warps, h->router, h->f64};
 }
 
 constexpr int kTrainEvery = 8;  // batches between two router training steps
@@ -791,16 +823,16 @@ int ensure_records(rtod_handle* h, int64_t n) {
 
 // Room for a stream of `used` points: the handle's run buffer for a host
 // stream (*host = true; run_stream copies it in), its keys and features.
-int stage_stream(rtod_handle* h, const float* pts, int64_t used, const float** src, bool* host) {
+int stage_stream(rtod_handle* h, const void* pts, int64_t used, const void** src, bool* host) {
   const int64_t D = h->D;
   *src = pts;
   *host = !is_device_ptr(pts);
   if (*host) {
     if (h->run_buf_cap < used * D) {
-      if (h->run_buf) h->device_bytes -= h->run_buf_cap * 4;
+      if (h->run_buf) h->device_bytes -= h->run_buf_cap * h->esz;
       dfree(h->run_buf);
       h->run_buf_cap = 0;
-      if (dalloc(&h->run_buf, (size_t)(used * D), &h->device_bytes)) return RTOD_ERR_CUDA;
+      if (dalloc(&h->run_buf, (size_t)(used * D * h->esz), &h->device_bytes)) return RTOD_ERR_CUDA;
       h->run_buf_cap = used * D;
     }
     *src = h->run_buf;  // filled piece by piece by run_stream
@@ -865,13 +897,13 @@ int64_t count_slides(const rtod_handle* h, int64_t n, int64_t max_slides) {
 // batches of B consecutive windows. kev (may be null) gets 8 events per
 // batch: one before and one after each kernel (the last one after the
 // router's training step, or right after k_compact without router).
-int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap, cudaEvent_t e_begin,
+int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap, cudaEvent_t e_begin,
                cudaEvent_t e_keys, cudaEvent_t e_end, std::vector<cudaEvent_t>* kev, BatchState* out_state,
                std::vector<int32_t>* nout, std::vector<int32_t>* nund) {
   const int64_t W = h->W, S = h->S;
   const int64_t used = W + slides * S;
   int r;
-  const float* src;
+  const void* src;
   if ((r = ensure_records(h, slides))) return r;
   if ((r = ensure_ids(h, std::max<int64_t>(1, std::min(ids_cap, slides * W))))) return r;
   const bool span = use_span(h);
@@ -900,7 +932,8 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
     const int64_t D = h->D;
     for (int64_t i = 0; i < nbatch; ++i) {
       const int64_t a = i ? piece_end(i - 1) : 0, e = piece_end(i);
-      CU(cudaMemcpyAsync(h->run_buf + a * D, pts + a * D, (size_t)((e - a) * D) * sizeof(float),
+      const int64_t es = h->esz;
+      CU(cudaMemcpyAsync(h->run_buf + a * D * es, (const unsigned char*)pts + a * D * es, (size_t)((e - a) * D * es),
                          cudaMemcpyHostToDevice, h->copy_stream));
       CU(cudaEventRecord(h->piece_ev[(size_t)i], h->copy_stream));
     }
@@ -911,8 +944,8 @@ int run_stream(rtod_handle* h, const float* pts, int64_t slides, int64_t ids_cap
   auto keys = [&](int64_t i, int64_t a, int64_t b) -> int {
     if (host) CU(cudaStreamWaitEvent(h->stream, h->piece_ev[(size_t)i], 0));
     const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((b - a + 255) / 256, kgrid));
-    DISPATCH_D(h->D, CU(launch_k(k_keys<D>, dim3(kx), 256, h->stream, src, a, b, h->cell, h->run_keys,
-                                 h->run_prev, h->bs, h->S, h->run_blk_lo, h->run_blk_hi)));
+    DISPATCH_DT(h->f64, h->D, CU(launch_k(k_keys<D, T>, dim3(kx), 256, h->stream, (const T*)src, a, b, h->cell,
+                                          h->run_keys, h->run_prev, h->bs, h->S, h->run_blk_lo, h->run_blk_hi)));
     h->launches++;
     return RTOD_OK;
   };
@@ -1066,7 +1099,7 @@ int apply_tuning(rtod_handle* h, const Tuning& t) {
 }
 
 // Device ms of one pass over `slides` slides of a device-resident stream.
-int time_pass(rtod_handle* h, const float* dev_pts, int64_t slides, float* ms) {
+int time_pass(rtod_handle* h, const void* dev_pts, int64_t slides, float* ms) {
   EventSet es;
   cudaEvent_t a = es.make(), b = es.make();
   float best = 1e30f;
@@ -1086,7 +1119,7 @@ int time_pass(rtod_handle* h, const float* dev_pts, int64_t slides, float* ms) {
   return RTOD_OK;
 }
 
-int autotune(rtod_handle* h, const float* pts, int64_t slides_total) {
+int autotune(rtod_handle* h, const void* pts, int64_t slides_total) {
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     for (const auto& e : g_tune_cache)
@@ -1099,13 +1132,13 @@ int autotune(rtod_handle* h, const float* pts, int64_t slides_total) {
   const int64_t slides = std::min<int64_t>(slides_total, 96);
   const int64_t used = W + slides * S;
   // A private device copy of the prefix, so that trials never touch the caller's stream buffers.
-  float* dev = nullptr;
-  CU(cudaMalloc((void**)&dev, (size_t)(used * D) * sizeof(float)));
+  void* dev = nullptr;
+  CU(cudaMalloc(&dev, (size_t)(used * D * h->esz)));
   struct Free {
-    float* p;
+    void* p;
     ~Free() { cudaFree(p); }
   } fr{dev};
-  CU(cudaMemcpy(dev, pts, (size_t)(used * D) * sizeof(float), cudaMemcpyDefault));
+  CU(cudaMemcpy(dev, pts, (size_t)(used * D * h->esz), cudaMemcpyDefault));
   Tuning best;
   best.batch = h->engine == RTOD_ENGINE_SPAN ? 32 : std::min(32, h->batch_max);
   best.engine = h->engine;
@@ -1219,6 +1252,8 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
   h->W = cfg->window;
   h->S = cfg->slide;
   h->D = cfg->dim;
+  h->f64 = cfg->coord == RTOD_COORD_F64;
+  h->esz = h->f64 ? 8 : 4;
   h->Wp = ((h->W + 3) / 4) * 4 + 4;  // padded SoA row: float4 loads stay in bounds
   {
     volatile float rf = (float)cfg->R;
@@ -1246,9 +1281,9 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
   int64_t* c = &h->device_bytes;
   bool ok = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess;
   ok = ok && !dalloc(&h->ctr, (size_t)kMaxJobs, c) && !dalloc(&h->jobs_dev, (size_t)kMaxJobs, c) &&
-       !dalloc(&h->bs, 1, c) && !dalloc(&h->ring, (size_t)(h->W * h->D), c) &&
+       !dalloc(&h->bs, 1, c) && !dalloc(&h->ring, (size_t)(h->W * h->D * h->esz), c) &&
        !dalloc(&h->ring_keys, (size_t)h->W, c) && !dalloc(&h->ring_prev, (size_t)h->W, c) &&
-       !dalloc(&h->staging, (size_t)(h->W * h->D), c);
+       !dalloc(&h->staging, (size_t)(h->W * h->D * h->esz), c);
   ok = ok && cudaMallocHost((void**)&h->ctr_init, sizeof(JobCtr) * kMaxJobs) == cudaSuccess;
   ok = ok && !dalloc(&h->router, 1, c);
   if (ok) {
@@ -1320,8 +1355,19 @@ RTOD_API int rtod_get_stats(const rtod_handle* h, int64_t out[5]) {
 
 RTOD_API const char* rtod_kernel_name(int32_t i) { return (i >= 0 && i < kPipeKernels) ? kKernelNames[i] : nullptr; }
 
-RTOD_API int rtod_push_slide(rtod_handle* h, const float* pts, int64_t n) {
+namespace {
+
+// The coordinate type of a call must be the handle's.
+int check_coord(const rtod_handle* h, bool f64) {
+  if (h->f64 != (int)f64)
+    return fail(RTOD_ERR_ARG, h->f64 ? "this handle stores double coordinates: use the _f64 entry points"
+                                     : "this handle stores float coordinates: use the float entry points");
+  return RTOD_OK;
+}
+
+int push_impl(rtod_handle* h, const void* pts, int64_t n, bool f64) {
   if (!h || !pts) return fail(RTOD_ERR_ARG, "null argument");
+  if (int r = check_coord(h, f64)) return r;
   if (h->poisoned) return fail(RTOD_ERR_STATE, "handle is in an error state; call rtod_reset");
   CU(cudaSetDevice(h->device));
   const int64_t W = h->W, S = h->S, D = h->D;
@@ -1333,14 +1379,14 @@ RTOD_API int rtod_push_slide(rtod_handle* h, const float* pts, int64_t n) {
     if (n != S) return fail(RTOD_ERR_STATE, "a slide push must hold exactly S=%lld points", (long long)S);
   }
   CU(cudaEventRecord(h->ev[4], h->stream));
-  CU(cudaMemcpyAsync(h->staging, pts, (size_t)(n * D) * sizeof(float), cudaMemcpyDefault, h->stream));
+  CU(cudaMemcpyAsync(h->staging, pts, (size_t)(n * D * h->esz), cudaMemcpyDefault, h->stream));
   CU(cudaEventRecord(h->ev[5], h->stream));
   if (h->n_pushed == 0) {
     int r = configure(h, MODE_RING, 1, S, nullptr);  // first detected window: [S, W + S)
     if (r) return r;
     const Batch b = make_batch(h, 1, h->ids_cap);
     const int64_t gx = std::max<int64_t>(1, std::min<int64_t>((W + 255) / 256, h->sm_count * 8));
-    DISPATCH_D(h->D, CU(launch_k(k_ingest<D>, dim3((unsigned)gx, 1), 256, h->stream, b, 1)));
+    DISPATCH_DT(h->f64, h->D, CU(launch_k(k_ingest<D, T>, dim3((unsigned)gx, 1), 256, h->stream, b, 1)));
     h->launches++;
     BatchState s;
     CU(cudaMemcpyAsync(&s, h->bs, sizeof s, cudaMemcpyDeviceToHost, h->stream));
@@ -1353,6 +1399,13 @@ RTOD_API int rtod_push_slide(rtod_handle* h, const float* pts, int64_t n) {
   h->n_pushed += n;
   return RTOD_OK;
 }
+
+}  // namespace
+
+RTOD_API int rtod_push_slide(rtod_handle* h, const float* pts, int64_t n) { return push_impl(h, pts, n, false); }
+
+RTOD_API int rtod_push_slide_f64(rtod_handle* h, const double* pts, int64_t n) { return push_impl(h, pts, n, true); }
+
 
 RTOD_API int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t* n_out, rtod_times* times) {
   if (!h || !n_out || (cap > 0 && !out_ids)) return fail(RTOD_ERR_ARG, "null argument");
@@ -1400,10 +1453,13 @@ RTOD_API int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t*
   return RTOD_OK;
 }
 
-RTOD_API int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides, int64_t* out_offsets,
-                      int64_t* out_ids, int64_t ids_cap, int64_t* slides_out, rtod_times* times) {
+namespace {
+
+int run_impl(rtod_handle* h, const void* pts, int64_t n, int64_t max_slides, int64_t* out_offsets,
+             int64_t* out_ids, int64_t ids_cap, int64_t* slides_out, rtod_times* times, bool f64) {
   if (!h || !pts || !out_offsets || !slides_out || (ids_cap > 0 && !out_ids))
     return fail(RTOD_ERR_ARG, "null argument");
+  if (int r = check_coord(h, f64)) return r;
   if (h->poisoned) return fail(RTOD_ERR_STATE, "handle is in an error state; call rtod_reset");
   if (h->n_pushed != 0) return fail(RTOD_ERR_STATE, "rtod_run needs a fresh handle (call rtod_reset)");
   if (n < 0 || ids_cap < 0) return fail(RTOD_ERR_ARG, "negative size");
@@ -1465,9 +1521,23 @@ RTOD_API int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_s
   return RTOD_OK;
 }
 
+}  // namespace
+
+RTOD_API int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides, int64_t* out_offsets,
+                      int64_t* out_ids, int64_t ids_cap, int64_t* slides_out, rtod_times* times) {
+  return run_impl(h, pts, n, max_slides, out_offsets, out_ids, ids_cap, slides_out, times, false);
+}
+
+RTOD_API int rtod_run_f64(rtod_handle* h, const double* pts, int64_t n, int64_t max_slides, int64_t* out_offsets,
+                          int64_t* out_ids, int64_t ids_cap, int64_t* slides_out, rtod_times* times) {
+  return run_impl(h, pts, n, max_slides, out_offsets, out_ids, ids_cap, slides_out, times, true);
+}
+
+
 RTOD_API int rtod_profile_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides, double* kernel_ms,
                               int32_t n_kernels) {
   if (!h || !pts || !kernel_ms || n_kernels < 1) return fail(RTOD_ERR_ARG, "null argument");
+  if (int r = check_coord(h, false)) return r;
   if (h->poisoned) return fail(RTOD_ERR_STATE, "handle is in an error state; call rtod_reset");
   if (h->n_pushed != 0) return fail(RTOD_ERR_STATE, "rtod_profile_run needs a fresh handle");
   CU(cudaSetDevice(h->device));
@@ -1696,6 +1766,7 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
     int r = check_config(&cfgs[i]);
     if (r) return r;
     if (cfgs[i].device != cfgs[0].device) return fail(RTOD_ERR_CONFIG, "all streams must use one device");
+    if (cfgs[i].coord != RTOD_COORD_F32) return fail(RTOD_ERR_CONFIG, "the multi-stream API takes float coordinates");
   }
   rtod_batch* b = new (std::nothrow) rtod_batch();
   if (!b) return fail(RTOD_ERR_ARG, "out of host memory");
@@ -2046,7 +2117,7 @@ RTOD_API int rtod_detect_window_static(const float* pts, int64_t n, int32_t dim,
 
   int sm = prop.multiProcessorCount;
   const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sm * 8));
-  DISPATCH_D(dim, CU(launch_k(k_keys<D>, dim3(kx), 256, st, pts, (int64_t)0, n, jb.cell, (uint64_t*)at(kStatic.keys),
+  DISPATCH_D(dim, CU(launch_k(k_keys<D, float>, dim3(kx), 256, st, pts, (int64_t)0, n, jb.cell, (uint64_t*)at(kStatic.keys),
                                (uint8_t*)at(kStatic.prev), b.bs, n, (long long*)at(kStatic.blo),
                                (long long*)at(kStatic.bhi))));
   const Geom g{n, n, dim, pred, 0, sm, 8, nullptr};

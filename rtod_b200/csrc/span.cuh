@@ -43,7 +43,7 @@ struct Span {
   int32_t K, n, filter;
   double cell, R, R2;
   float R2f;
-  const float* pts;         // resident stream, point-major [N][D]
+  const void* pts;          // resident stream, point-major [N][D] (the handle's coordinate type)
   const uint64_t* keys;     // cell keys of the stream, by global index
   const long long* blk_lo;  // per slide block cell coordinate range (span purity)
   const long long* blk_hi;
@@ -55,7 +55,7 @@ struct Span {
   uint32_t* pre;    // [nblk + 1][NB] points of bin b in the blocks before t (bins in use only)
   uint32_t* used;   // [NB] bins holding span points, n_used of them, in no particular order
   uint32_t* s_off;  // [span] bin-ordered: offset from the span start
-  float* s_x;       // [D][Wp] bin-ordered coordinates
+  void* s_x;        // [D][Wp] bin-ordered coordinates (the handle's coordinate type)
   unsigned long long* scan_status;  // [SCAN_TILES]
   SpanCtr* sc;
   uint4* groups;    // [B * min(W, NB)] listed groups: first position, points, bin, window
@@ -244,7 +244,7 @@ __global__ void __launch_bounds__(256) k_span_scan(Batch b, Span sp) {
 // aggregates the points of one chunk per (block, bin); each entry claims its
 // positions with one atomicSub on cnt, which returns cnt to zero.
 // ---------------------------------------------------------------------------
-template <int D>
+template <int D, typename T>
 __global__ void __launch_bounds__(256) k_span_scatter(Batch b, Span sp) {
   __shared__ uint32_t tkey[HIST_SLOTS];
   __shared__ uint32_t tcnt[HIST_SLOTS];
@@ -320,7 +320,8 @@ __global__ void __launch_bounds__(256) k_span_scatter(Batch b, Span sp) {
         const uint32_t pos = sp.bin_start[bin] + sp.pre[comp[u]] + goff[u] + (slot[u] >= 0 ? tbase[slot[u]] : 0u);
         sp.s_off[pos] = (uint32_t)i;
 #pragma unroll
-        for (int d = 0; d < D; ++d) sp.s_x[(int64_t)d * sp.Wp + pos] = sp.pts[(lo0 + i) * D + d];
+        for (int d = 0; d < D; ++d)
+          static_cast<T*>(sp.s_x)[(int64_t)d * sp.Wp + pos] = static_cast<const T*>(sp.pts)[(lo0 + i) * D + d];
       }
     }
   }
@@ -374,21 +375,22 @@ __device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* 
 // s < 2n+1 takes bin + d(s), d = 0, -1, +1, -2, +2, ... (nearest first), and
 // that bin's window range (points of other cells sharing those bins are
 // rejected by the distance test); a warp scan turns the range lengths into
-// offsets of one virtual candidate list of T entries. With T <= K every point
-// is an outlier (its count cannot exceed T). Otherwise the list is read 256
-// candidates at a time (8 per lane, kept in registers) and every undecided
-// point of the group (up to 32, one per lane) is tested against the chunk:
-// per point, 8 tests per lane and one warp reduction; a point is decided as
-// soon as its count exceeds K, and the chunks stop when every point is
-// decided.
+// offsets of one virtual candidate list of ncand entries. With ncand <= K
+// every point is an outlier (its count cannot exceed ncand). Otherwise the
+// list is read 256 candidates at a time (8 per lane, kept in registers) and
+// every undecided point of the group (up to 32, one per lane) is tested
+// against the chunk: per point, 8 tests per lane and one warp reduction; a
+// point is decided as soon as its count exceeds K, and the chunks stop when
+// every point is decided.
 // ---------------------------------------------------------------------------
-template <int D, int PRED>
+template <int D, int PRED, typename T>
 __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp, int j, uint32_t p,
                                                  uint32_t nq, uint32_t bin, const uint32_t* p0,
                                                  const uint32_t* p1) {
   const int lane = threadIdx.x & 31;
   const Job& jb = b.jobs[j];
   const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
+  const T* sx = static_cast<const T*>(sp.s_x);
   uint32_t* row = sp.bits + ((jb.ctr->lo - sp.S) / sp.S % sp.chunk) * sp.words;
   const int slots = 2 * sp.n + 1;
   uint32_t rs = 0, len = 0;
@@ -409,19 +411,19 @@ __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp,
     if (lane >= o) inc += y;
   }
   const uint32_t off = inc - len;
-  const uint32_t T = __shfl_sync(0xffffffffu, inc, 31);
+  const uint32_t ncand = __shfl_sync(0xffffffffu, inc, 31);
   int nout = 0;
   for (uint32_t g = 0; g < nq; g += 32) {
     const uint32_t q = g + lane;
     const bool has = q < nq;
-    float qx[D];
+    T qx[D];
 #pragma unroll
-    for (int d = 0; d < D; ++d) qx[d] = has ? sp.s_x[(int64_t)d * sp.Wp + p + q] : 0.0f;
+    for (int d = 0; d < D; ++d) qx[d] = has ? sx[(int64_t)d * sp.Wp + p + q] : T(0);
     int cnt = 0;
     unsigned live = __ballot_sync(0xffffffffu, has);
-    if (T > (uint32_t)sp.K) {
-      for (uint32_t c0 = 0; c0 < T && live; c0 += 256) {
-        float cx[8][D];
+    if (ncand > (uint32_t)sp.K) {
+      for (uint32_t c0 = 0; c0 < ncand && live; c0 += 256) {
+        T cx[8][D];
         bool cv[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
@@ -436,21 +438,21 @@ __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp,
           }
           const uint32_t base = __shfl_sync(0xffffffffu, rs, s);
           const uint32_t os = __shfl_sync(0xffffffffu, off, s);
-          cv[e] = v < T;
+          cv[e] = v < ncand;
           const uint32_t c = base + (v - os);
 #pragma unroll
-          for (int d = 0; d < D; ++d) cx[e][d] = cv[e] ? sp.s_x[(int64_t)d * sp.Wp + c] : 0.0f;
+          for (int d = 0; d < D; ++d) cx[e][d] = cv[e] ? sx[(int64_t)d * sp.Wp + c] : T(0);
         }
         unsigned todo = live;
         while (todo) {
           const int qq = __ffs(todo) - 1;
           todo &= todo - 1;
-          float y[D];
+          T y[D];
 #pragma unroll
           for (int d = 0; d < D; ++d) y[d] = __shfl_sync(0xffffffffu, qx[d], qq);
           unsigned m = 0;
 #pragma unroll
-          for (int e = 0; e < 8; ++e) m += (cv[e] && is_nbr<D, PRED>(y, cx[e], sp.R2f, sp.R, sp.R2)) ? 1u : 0u;
+          for (int e = 0; e < 8; ++e) m += (cv[e] && is_nbr<D, PRED, T>(y, cx[e], sp.R2f, sp.R, sp.R2)) ? 1u : 0u;
           const unsigned tot = __reduce_add_sync(0xffffffffu, m);
           if (lane == qq) cnt += (int)tot;
         }
@@ -538,7 +540,7 @@ __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
 // clear the per-bin state, and the block that finishes last ends the batch
 // (records, window advance, counters).
 // ---------------------------------------------------------------------------
-template <int D, int PRED>
+template <int D, int PRED, typename T>
 __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
   __shared__ int s_last;
   pdl_trigger();
@@ -550,7 +552,7 @@ __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
     const uint4 g = sp.groups[k];
     const int j = (int)g.w;
     const uint32_t* p0 = sp.pre + (int64_t)j * NB;
-    span_count_group<D, PRED>(b, sp, j, g.x, g.y, g.z, p0, p0 + (int64_t)sp.wblk * NB);
+    span_count_group<D, PRED, T>(b, sp, j, g.x, g.y, g.z, p0, p0 + (int64_t)sp.wblk * NB);
   }
   // The per-bin state is no longer read in this batch: clear it, then the
   // block that finishes last ends the batch.

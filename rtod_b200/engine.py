@@ -20,18 +20,19 @@ from . import _native
 from ._native import Config, Times, check, lib
 
 
-def _as_points(points, dim: int):
-    """(pointer, n, keepalive) for a point-major float32 array: a numpy array
-    (host) or a CUDA tensor exposing data_ptr() (device)."""
+def _as_points(points, dim: int, f64: bool = False):
+    """(pointer, n, keepalive) for a point-major float32 (float64 with f64)
+    array: a numpy array (host) or a CUDA tensor exposing data_ptr() (device)."""
     if hasattr(points, "data_ptr") and hasattr(points, "is_cuda"):
         t = points
-        if t.dtype.__repr__() != "torch.float32" or not t.is_contiguous():
-            raise TypeError("device points must be a contiguous float32 tensor")
+        want = "torch.float64" if f64 else "torch.float32"
+        if t.dtype.__repr__() != want or not t.is_contiguous():
+            raise TypeError(f"device points must be a contiguous {want[6:]} tensor")
         n = t.numel() // dim
         if n * dim != t.numel():
             raise ValueError(f"tensor size {t.numel()} is not a multiple of dim={dim}")
         return ctypes.c_void_p(t.data_ptr()), n, t
-    a = np.ascontiguousarray(points, dtype=np.float32)
+    a = np.ascontiguousarray(points, dtype=np.float64 if f64 else np.float32)
     if a.ndim == 1 and dim == 1:
         a = a[:, None]
     if a.ndim != 2 or a.shape[1] != dim:
@@ -70,7 +71,7 @@ class Detector:
     def __init__(self, window: int, slide: int, R: float, K: int, dim: int = 1, opt: int = 2,
                  pred: str = "fp32_le", router: bool = False, tuner: bool = False,
                  cells_per_r: int = 0, block_warps: int = 0, use_graph: bool = True,
-                 batch: int = 0, device: int = 0, engine: str = "auto"):
+                 batch: int = 0, device: int = 0, engine: str = "auto", coord: str = "f32"):
         cfg = Config()
         check(lib().rtod_config_init(ctypes.byref(cfg)))
         cfg.window, cfg.slide, cfg.R, cfg.K, cfg.dim, cfg.opt = window, slide, R, K, dim, opt
@@ -79,6 +80,8 @@ class Detector:
         cfg.cells_per_r, cfg.block_warps = cells_per_r, block_warps
         cfg.use_graph, cfg.device, cfg.batch = int(use_graph), device, batch
         cfg.engine = _native.ENGINE[engine]
+        cfg.coord = _native.COORD[coord]
+        self.f64 = coord == "f64"
         self.cfg = cfg
         self.window, self.slide, self.R, self.K, self.dim = window, slide, R, K, dim
         self._h = ctypes.c_void_p()
@@ -105,8 +108,9 @@ class Detector:
     # -- streaming --------------------------------------------------------
     def push(self, points) -> None:
         """Appends W points (first call) or S points (each later call)."""
-        ptr, n, keep = _as_points(points, self.dim)
-        check(lib().rtod_push_slide(self._h, ptr, n))
+        ptr, n, keep = _as_points(points, self.dim, self.f64)
+        push = lib().rtod_push_slide_f64 if self.f64 else lib().rtod_push_slide
+        check(push(self._h, ptr, n))
         del keep
 
     def detect(self, times: bool = False):
@@ -124,7 +128,7 @@ class Detector:
         """Processes a whole stream (host array or CUDA tensor) like RTOD's
         detect_outlier: fill with the first W points, then detect up to
         max_slides slides (RTOD caps the loop at 10000, optixScan.cpp:1045)."""
-        ptr, n, keep = _as_points(points, self.dim)
+        ptr, n, keep = _as_points(points, self.dim, self.f64)
         slides = max(0, (n - self.window) // self.slide) if n >= self.window else 0
         if max_slides is not None and max_slides >= 0:
             slides = min(slides, max_slides)
@@ -146,7 +150,8 @@ class Detector:
             out_ptr = ctypes.c_void_p(out_ids.data_ptr())
         ns = ctypes.c_int64()
         t = Times()
-        check(lib().rtod_run(self._h, ptr, n, -1 if max_slides is None else max_slides,
+        fn = lib().rtod_run_f64 if self.f64 else lib().rtod_run
+        check(fn(self._h, ptr, n, -1 if max_slides is None else max_slides,
                              off.ctypes.data_as(ctypes.c_void_p), out_ptr, ids_cap,
                              ctypes.byref(ns), ctypes.byref(t) if times else None))
         del keep

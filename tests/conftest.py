@@ -24,7 +24,14 @@ def load_golden(path):
 
 
 def golden_cases():
-    return sorted(glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+    """Fixtures with float32 points."""
+    return sorted(p for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz"))
+                  if not os.path.basename(p).startswith("dbl_"))
+
+
+def golden_cases_f64():
+    """Fixtures with double points (double storage, RTOD's double predicate)."""
+    return sorted(glob.glob(os.path.join(GOLDEN_DIR, "dbl_*.npz")))
 
 
 @pytest.fixture(scope="session")

@@ -15,6 +15,10 @@ Predicates:
            d2 <= fl32(fl32(R)^2)
   f64_lt   RTOD's own double test: |dx| < R in 1-d, sum of dx^2 < R*R otherwise
 
+Double storage (files dbl_*.npz): points kept as float64, as RTOD keeps
+them (double3 read with %lf, src/ods/optixScan.cpp:95-147), compared with
+f64_lt on the doubles themselves.
+
 Run:  python tests/golden/make_golden.py   (writes tests/golden/*.npz)
 """
 from __future__ import annotations
@@ -57,13 +61,27 @@ def window_counts(X: np.ndarray, R: float, pred: str) -> np.ndarray:
     return (s < R * R).sum(axis=1)
 
 
-def detect(points: np.ndarray, W: int, S: int, R: float, K: int, pred: str):
+def window_counts_f64(X: np.ndarray, R: float) -> np.ndarray:
+    """f64_lt counts on double coordinates (no rounding to float32)."""
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    if X.shape[1] == 1:
+        return (np.abs(X[:, None, 0] - X[None, :, 0]) < R).sum(axis=1)
+    s = None
+    for i in range(X.shape[1]):
+        dx = X[:, None, i] - X[None, :, i]
+        t = dx * dx
+        s = t if s is None else (s + t)
+    return (s < R * R).sum(axis=1)
+
+
+def detect(points: np.ndarray, W: int, S: int, R: float, K: int, pred: str, counts=None):
+    counts = counts or (lambda X: window_counts(X, R, pred))
     n = points.shape[0]
     slides = max(0, (n - W) // S) if n >= W else 0
     offsets, ids, undet = [0], [], []
     for j in range(slides):
         lo = (j + 1) * S
-        c = window_counts(points[lo:lo + W], R, pred)
+        c = counts(points[lo:lo + W])
         out = lo + np.nonzero(c <= K)[0]
         ids.extend(out.tolist())
         offsets.append(len(ids))
@@ -84,6 +102,49 @@ def save(name: str, points: np.ndarray, W: int, S: int, R: float, K: int, pred: 
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), points=points, offsets=off, ids=ids,
                         meta=np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8))
     return off, ids
+
+
+def save_f64(name: str, points: np.ndarray, W: int, S: int, R: float, K: int, expected=None,
+             note: str = ""):
+    """A double-storage fixture (f64_lt on float64 points)."""
+    points = np.ascontiguousarray(points, dtype=np.float64)
+    if points.ndim == 1:
+        points = points[:, None]
+    off, ids = detect(points, W, S, R, K, "f64_lt", counts=lambda X: window_counts_f64(X, R))
+    if expected is not None:
+        got = [ids[off[j]:off[j + 1]].tolist() for j in range(len(off) - 1)]
+        assert got == expected, f"{name}: brute force {got} != hand-derived {expected}"
+    meta = dict(name=name, W=W, S=S, R=R, K=K, pred="f64_lt", pred_id=1, coord="f64", note=note,
+                hand_derived=expected is not None)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), points=points, offsets=off, ids=ids,
+                        meta=np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8))
+    return off, ids
+
+
+def double_storage():
+    # KAT: a pair 1e-12 inside R = 0.1 in double. As doubles they are
+    # neighbours (|dx| < R); rounded to float32, 0.1 - 1e-12 becomes
+    # fl32(0.1) > 0.1 and the pair is not. W = 2, S = 2, K = 1: the window
+    # {2, 3} holds the pair -> no outliers with double storage.
+    pts = np.array([50.0, 70.0, 0.0, 0.1 - 1e-12], np.float64)
+    f32 = window_counts(pts[2:, None].astype(np.float32), 0.1, "f64_lt")
+    assert f32.tolist() == [1, 1], "the pair must split when stored as float32"
+    save_f64("dbl_kat_pair_inside_R", pts, 2, 2, 0.1, 1, expected=[[]],
+             note="1e-12 inside R: neighbours only when stored as double")
+    # KAT, 3-d: d^2 = 3 * 0.1^2 - tiny < R^2 = 0.03 + 1e-15 in double only.
+    R = float(np.sqrt(0.03 + 1e-15))
+    a = np.array([1.0, 2.0, 3.0])
+    b = a + 0.1
+    pre = np.array([[40.0, 40.0, 40.0], [60.0, 60.0, 60.0]])
+    pts = np.concatenate([pre, np.stack([a, b])])
+    save_f64("dbl_kat_3d", pts, 2, 2, R, 1, note="3-d pair near R in double")
+    # Seeded streams whose values are not float32-representable.
+    rw = datagen.random_walk(3000, 0.1, seed=21, jump_frac=0.01).astype(np.float64)
+    rw = rw + np.random.default_rng(21).uniform(-1e-9, 1e-9, rw.shape)
+    save_f64("dbl_walk1d", rw, 1000, 100, 0.15, 8)
+    s3 = datagen.sensor_3d(2500, seed=23).astype(np.float64)
+    s3 = s3 + np.random.default_rng(23).uniform(-1e-9, 1e-9, s3.shape)
+    save_f64("dbl_sensor3d", s3, 1000, 250, 1.9, 12)
 
 
 def known_answers():
@@ -163,6 +224,7 @@ def seeded_streams():
 if __name__ == "__main__":
     known_answers()
     seeded_streams()
+    double_storage()
     for fn in sorted(os.listdir(HERE)):
         if fn.endswith(".npz"):
             z = np.load(os.path.join(HERE, fn))

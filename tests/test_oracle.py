@@ -4,7 +4,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import golden_cases, load_golden
+from conftest import golden_cases, golden_cases_f64, load_golden
 
 
 @pytest.mark.parametrize("path", golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
@@ -15,6 +15,23 @@ def test_oracle_matches_golden(oracle_mod, path, engine):
                                 engine=engine)
     np.testing.assert_array_equal(o, off)
     np.testing.assert_array_equal(i, ids)
+
+
+@pytest.mark.parametrize("path", golden_cases_f64(), ids=lambda p: os.path.basename(p)[:-4])
+@pytest.mark.parametrize("engine", ["brute", "grid", "grid_nofilter"])
+def test_oracle_double_storage_matches_golden(oracle_mod, path, engine):
+    meta, pts, off, ids = load_golden(path)
+    assert pts.dtype == np.float64 and meta["coord"] == "f64"
+    o, i, _ = oracle_mod.detect(pts, meta["W"], meta["S"], meta["R"], meta["K"], "f64_lt", engine=engine,
+                                f64=True)
+    np.testing.assert_array_equal(o, off)
+    np.testing.assert_array_equal(i, ids)
+
+
+def test_oracle_double_storage_differs_from_float_storage(oracle_mod):
+    """The pair 1e-12 inside R: neighbours as doubles, not once rounded to float32."""
+    assert oracle_mod.pred_f64([0.0], [0.1 - 1e-12], 0.1)
+    assert not oracle_mod.pred(np.float32([0.0]), np.float32([0.1 - 1e-12]), 0.1, "f64_lt")
 
 
 def test_oracle_threads_agree(oracle_mod):
