@@ -162,11 +162,12 @@ int64_t rtod_slides_done(const rtod_handle* h);
    out[2] hashed dimensions, out[3] windows per rtod_run launch, out[4] engine
    of rtod_run (RTOD_ENGINE_WINDOW or RTOD_ENGINE_SPAN).
    With rtod_config.tuner = 1 the first rtod_run times candidate settings
-   (in 1-d with engine = AUTO both engines, cells per R 1..3 or up to 6 in 1-d,
-   2/4/8 warps per block, 8..64 windows per launch and, with the router on and the
-   window engine, its routing threshold and full-sweep size limit) on a
-   prefix of the stream and keeps the fastest; the choice is cached per
-   configuration for the rest of the process. Results do not depend on it. */
+   (in 1-d with engine = AUTO both engines, cells per R 1..3 or up to 6 in
+   1-d, 2/4/8 warps per block, 8..256 windows per launch (up to 32 with the
+   window engine) and, with the router on and the window engine, its routing
+   threshold and full-sweep size limit) on the first 256 slides of the
+   stream and keeps the fastest; the choice is cached per configuration for
+   the rest of the process. Results do not depend on it. */
 int rtod_get_tuning(const rtod_handle* h, int32_t out[5]);
 
 /* Counters since create: out[0] kernel launches issued by the library (a

@@ -1129,7 +1129,7 @@ int autotune(rtod_handle* h, const void* pts, int64_t slides_total) {
       }
   }
   const int64_t W = h->W, S = h->S, D = h->D;
-  const int64_t slides = std::min<int64_t>(slides_total, 96);
+  const int64_t slides = std::min<int64_t>(slides_total, 256);
   const int64_t used = W + slides * S;
   // A private device copy of the prefix, so that trials never touch the caller's stream buffers.
   void* dev = nullptr;
@@ -1173,7 +1173,7 @@ int autotune(rtod_handle* h, const void* pts, int64_t slides_total) {
     t.block_warps = bw;
     if ((r = trial(t))) return r;
   }
-  for (int bt : {8, 16, 64, 128}) {
+  for (int bt : {8, 16, 64, 128, 256}) {
     if (bt > (best.engine == RTOD_ENGINE_SPAN ? h->span_batch_max : h->batch_max)) continue;
     Tuning t = best;
     t.batch = bt;
