@@ -180,8 +180,9 @@ def algorithmic_bytes(kernel: str, w, n_out_per_slide: float, undet_per_slide: f
         "k_keys": 4 * d * S + 8 * S,                          # per slide: read points, write keys
         "k_train": 2048 * 16 + 3 * 1316 * 4 * 2,              # samples + params/moments (per batch)
         # span engine: read the span's keys once per batch
-        "k_span_hist+k_span_prefix": 8 * span_pts / batch,
-        "k_span_scan": 4 * 65536 * 2 / batch,                 # read counts, write starts
+        "k_span_hist": 8 * span_pts / batch,
+        # read counts, write starts; per bin in use, its per-block counts and prefixes
+        "k_span_scan+k_span_prefix": (4 * 65536 * 2 + 8 * used_bins * (W // S + batch)) / batch,
         # read keys + points, write bin-ordered offsets + coordinates, once per batch
         "k_span_scatter": ((8 + 4 * d) + (4 + 4 * d)) * span_pts / batch,
         # per (window, bin in use): the bin's two prefix entries

@@ -105,7 +105,7 @@ struct SpanCtr {
 
 struct Job {
   int64_t W, S, Wp;  // window, slide, padded SoA row stride (multiple of 4, >= W + 4)
-  double cell;       // cell side: R * (1 + 2^-12) / n
+  double inv_cell;   // 1 / cell, cell side = R * (1 + 2^-12) / n
   double R, R2;
   float R2f;         // fl32(fl32(R)^2)
   int32_t K;
@@ -160,15 +160,17 @@ __device__ __forceinline__ void set_err(BatchState* bs, int32_t code) { atomicCA
 __device__ __forceinline__ bool job_active(const Batch& b) { return !b.active || b.active[blockIdx.y]; }
 
 // ---------------------------------------------------------------------------
-// Grid cells. Cell coordinate k_i = floor(x_i / cell) in double precision,
-// for the first h = min(D, 3) dimensions. With cell = R(1+2^-12)/n and
-// |x/cell| below the limits below, any pair accepted by either predicate has
-// |k_i(p) - k_i(q)| <= n (the stencil), and for D <= 3, n >= 2 two points of
-// one cell are always neighbours (so a cell with more than K points is
-// all-inlier). The limits keep the double rounding of x/cell below 2^-16 cells.
+// Grid cells. Cell coordinate k_i = floor(x_i * inv_cell) in double
+// precision (inv_cell = fl(1 / cell)), for the first h = min(D, 3)
+// dimensions. With cell = R(1+2^-12)/n and |x/cell| below the limits below,
+// any pair accepted by either predicate has |k_i(p) - k_i(q)| <= n (the
+// stencil), and for D <= 3, n >= 2 two points of one cell are always
+// neighbours (so a cell with more than K points is all-inlier). The product
+// x * inv_cell is within a relative 1.5 * 2^-52 of x / cell, so the limits
+// keep its error below 2^-16 cells.
 // ---------------------------------------------------------------------------
 __host__ __device__ __forceinline__ double coord_limit(int h) {
-  return h == 1 ? 68719476736.0 /* 2^36 */ : (h == 2 ? 1073741824.0 /* 2^30 */ : 1048576.0 /* 2^20 */);
+  return h == 1 ? 34359738368.0 /* 2^35 */ : (h == 2 ? 1073741824.0 /* 2^30 */ : 1048576.0 /* 2^20 */);
 }
 
 __device__ __forceinline__ uint64_t pack_key(const int64_t* k, int h) {
@@ -215,7 +217,7 @@ struct Hashed {
 // DERR_NONFINITE for a non-finite coordinate, DERR_RANGE for one too large
 // for the grid (then the key is zero).
 template <int D, typename T>
-__device__ __forceinline__ uint64_t cell_key(const T* x, double cell, int32_t* code) {
+__device__ __forceinline__ uint64_t cell_key(const T* x, double inv_cell, int32_t* code) {
   constexpr int H = Hashed<D>::value;
   const double lim = coord_limit(H);
   bool ok = true;
@@ -225,7 +227,7 @@ __device__ __forceinline__ uint64_t cell_key(const T* x, double cell, int32_t* c
   bool inr = true;
 #pragma unroll
   for (int d = 0; d < H; ++d) {
-    const double q = floor(__ddiv_rn((double)x[d], cell));
+    const double q = floor(__dmul_rn((double)x[d], inv_cell));
     inr &= (q > -lim) && (q < lim);
     k[d] = inr ? (int64_t)q : 0;
   }
@@ -411,7 +413,7 @@ namespace rtod {
 // k_keys: cell keys of a resident stream, global indices [g0, g1).
 // ---------------------------------------------------------------------------
 template <int D, typename T>
-__global__ void __launch_bounds__(256) k_keys(const T* pts, int64_t g0, int64_t g1, double cell,
+__global__ void __launch_bounds__(256) k_keys(const T* pts, int64_t g0, int64_t g1, double inv_cell,
                                               uint64_t* keys, uint8_t* prev, BatchState* bs, int64_t S,
                                               long long* blk_lo, long long* blk_hi) {
   pdl_trigger();
@@ -429,7 +431,7 @@ __global__ void __launch_bounds__(256) k_keys(const T* pts, int64_t g0, int64_t 
 #pragma unroll
       for (int d = 0; d < D; ++d) x[d] = pts[g * D + d];
       int32_t code;
-      const uint64_t key = cell_key<D, T>(x, cell, &code);
+      const uint64_t key = cell_key<D, T>(x, inv_cell, &code);
       keys[g] = key;
       prev[g] = 254;
       if (code) set_err(bs, code);
@@ -485,7 +487,7 @@ __global__ void __launch_bounds__(256) k_ingest(Batch b, int32_t fill) {
 #pragma unroll
     for (int d = 0; d < D; ++d) x[d] = stage[i * D + d];
     int32_t code;
-    const uint64_t key = cell_key<D, T>(x, jb.cell, &code);
+    const uint64_t key = cell_key<D, T>(x, jb.inv_cell, &code);
     if (code) set_err(b.bs, code);
 #pragma unroll
     for (int d = 0; d < D; ++d) ring[(int64_t)d * jb.W + slot] = x[d];

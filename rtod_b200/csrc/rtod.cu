@@ -478,7 +478,6 @@ Span make_span(const rtod_handle* h, int B, const void* stream_pts, int64_t chun
   sp.K = h->cfg.K;
   sp.n = h->n;
   sp.filter = h->filter;
-  sp.cell = h->cell;
   sp.R = h->cfg.R;
   sp.R2 = h->cfg.R * h->cfg.R;
   sp.R2f = h->R2f;
@@ -518,7 +517,7 @@ Job make_job(rtod_handle* h, int j, bool ring, const void* stream_pts) {
   jb.W = h->W;
   jb.S = h->S;
   jb.Wp = h->Wp;
-  jb.cell = h->cell;
+  jb.inv_cell = 1.0 / h->cell;
   jb.R = h->cfg.R;
   jb.R2 = h->cfg.R * h->cfg.R;
   jb.R2f = h->R2f;
@@ -661,18 +660,19 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
   return RTOD_OK;
 }
 
-// Launches one batch of the span engine: hist prefix scan scatter classify
-// count. kev as for launch_group, with kev[1] after hist + prefix, kev[4]
-// after classify and kev[5] after count (the stage slots of count, compact
-// and train hold classify, count and the chunk compaction timed by run_stream).
+// Launches one batch of the span engine: hist scan prefix scatter classify
+// count. kev as for launch_group, with kev[1] after hist, kev[2] after scan +
+// prefix, kev[4] after classify and kev[5] after count (the stage slots of
+// count, compact and train hold classify, count and the chunk compaction
+// timed by run_stream).
 int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, cudaEvent_t* kev, int64_t* nk) {
   const int64_t npts = sp.nblk * sp.S;
   const int64_t hx = std::max<int64_t>(1, std::min<int64_t>((npts + 1023) / 1024, (int64_t)g.sm_count * 8));
   if (kev) CU(cudaEventRecord(kev[0], st));
   CU(launch_k(k_span_hist<1>, dim3((unsigned)hx), 256, st, b, sp));
-  CU(launch_k(k_span_prefix, dim3(NB / 32), 256, st, b, sp));
   if (kev) CU(cudaEventRecord(kev[1], st));
   CU(launch_k(k_span_scan, dim3(SCAN_TILES), 256, st, b, sp));
+  CU(launch_k(k_span_prefix, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
   if (kev) CU(cudaEventRecord(kev[2], st));
   if (g.f64) {
     CU(launch_k(k_span_scatter<1, double>, dim3((unsigned)hx), 256, st, b, sp));
@@ -944,7 +944,7 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
   auto keys = [&](int64_t i, int64_t a, int64_t b) -> int {
     if (host) CU(cudaStreamWaitEvent(h->stream, h->piece_ev[(size_t)i], 0));
     const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((b - a + 255) / 256, kgrid));
-    DISPATCH_DT(h->f64, h->D, CU(launch_k(k_keys<D, T>, dim3(kx), 256, h->stream, (const T*)src, a, b, h->cell,
+    DISPATCH_DT(h->f64, h->D, CU(launch_k(k_keys<D, T>, dim3(kx), 256, h->stream, (const T*)src, a, b, 1.0 / h->cell,
                                           h->run_keys, h->run_prev, h->bs, h->S, h->run_blk_lo, h->run_blk_hi)));
     h->launches++;
     return RTOD_OK;
@@ -2067,7 +2067,7 @@ RTOD_API int rtod_detect_window_static(const float* pts, int64_t n, int32_t dim,
   jb.W = n;
   jb.S = n;  // one window, one slide block
   jb.Wp = ((n + 3) / 4) * 4 + 4;
-  jb.cell = R * (1.0 + std::ldexp(1.0, -12)) / (double)n_cells;
+  jb.inv_cell = 1.0 / (R * (1.0 + std::ldexp(1.0, -12)) / (double)n_cells);
   jb.R = R;
   jb.R2 = R * R;
   {
@@ -2117,7 +2117,7 @@ RTOD_API int rtod_detect_window_static(const float* pts, int64_t n, int32_t dim,
 
   int sm = prop.multiProcessorCount;
   const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sm * 8));
-  DISPATCH_D(dim, CU(launch_k(k_keys<D, float>, dim3(kx), 256, st, pts, (int64_t)0, n, jb.cell, (uint64_t*)at(kStatic.keys),
+  DISPATCH_D(dim, CU(launch_k(k_keys<D, float>, dim3(kx), 256, st, pts, (int64_t)0, n, jb.inv_cell, (uint64_t*)at(kStatic.keys),
                                (uint8_t*)at(kStatic.prev), b.bs, n, (long long*)at(kStatic.blo),
                                (long long*)at(kStatic.bhi))));
   const Geom g{n, n, dim, pred, 0, sm, 8, nullptr};

@@ -15,8 +15,8 @@
 // of bin b is pre[j + W/S][b] - pre[j][b]: classification needs no per-point
 // work, and a queued point's candidates are 2n+1 such ranges.
 //
-// Kernels per batch: k_span_hist (per-block bin counts), k_span_prefix (pre,
-// list of bins in use), k_span_scan (bin_start), k_span_scatter (sorted
+// Kernels per batch: k_span_hist (per-block bin counts), k_span_scan
+// (bin_start, list of bins in use), k_span_prefix (pre), k_span_scatter (sorted
 // span), k_span_classify (per window and bin in use: safe, or listed) and
 // k_span_count (exact counts of the listed bins' window points into
 // per-slide outlier bitsets; its last block ends the batch). Once per chunk
@@ -41,7 +41,7 @@ struct Span {
   int64_t nblk;    // blocks in the span: W/S + B - 1
   int32_t wblk;    // blocks per window: W/S
   int32_t K, n, filter;
-  double cell, R, R2;
+  double R, R2;
   float R2f;
   const void* pts;          // resident stream, point-major [N][D] (the handle's coordinate type)
   const uint64_t* keys;     // cell keys of the stream, by global index
@@ -169,74 +169,82 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
 }
 
 // ---------------------------------------------------------------------------
-// k_span_prefix: 8 threads per bin (32 bins per block of 256); for a bin in
-// use, the first of them appends it to the list of bins in use, and each
-// sums one eighth of the blocks (its loads all in flight), an 8-lane scan
-// gives its offset, and it writes pre[t][b] for its blocks (pre[nblk][b] by
-// the last one).
+// k_span_prefix: one warp per bin in use (the list k_span_scan built),
+// striding over the list: lane l sums blocks [l*per, (l+1)*per), per =
+// ceil(nblk / 32), 8 loads in flight per step (kept in registers when per
+// <= 8, the usual case), a warp scan gives its offset, and it writes
+// pre[t][b] for its blocks (pre[nblk][b] by the last lane).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_span_prefix(Batch b, Span sp) {
   pdl_trigger();
   pdl_wait();
   const int lane = threadIdx.x & 31;
-  const int sub = lane & 7;                                   // eighth of the blocks
-  const uint32_t bin = blockIdx.x * 32 + (threadIdx.x >> 3);  // grid NB / 32
-  const uint32_t c = sp.bin_count[bin];
-  if (!__any_sync(0xffffffffu, c != 0)) return;
-  const unsigned has = __ballot_sync(0xffffffffu, c != 0 && sub == 0);
-  uint32_t base = 0;
-  if (lane == 0 && has) base = atomicAdd(&sp.sc->n_used, (uint32_t)__popc(has));
-  base = __shfl_sync(0xffffffffu, base, 0);
-  if (c != 0 && sub == 0) sp.used[base + __popc(has & lanemask_lt())] = bin;
-  const int64_t per = (sp.nblk + 7) >> 3;
-  const int64_t t0 = min((int64_t)sub * per, sp.nblk), t1 = min(t0 + per, sp.nblk);
-  const uint32_t* __restrict__ cnt = sp.cnt + bin;
-  uint32_t* __restrict__ pre = sp.pre + bin;
-  uint32_t sum = 0;
-  if (c != 0) {
-    int64_t t = t0;
-    for (; t + 8 <= t1; t += 8) {
-      uint32_t v[8];
+  const uint32_t nu = sp.sc->n_used;
+  const int64_t per = (sp.nblk + 31) / 32;
+  const int64_t t0 = min((int64_t)lane * per, sp.nblk), t1 = min(t0 + per, sp.nblk);
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  for (int64_t u = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < nu; u += warps) {
+    const uint32_t bin = sp.used[u];
+    const uint32_t* __restrict__ cnt = sp.cnt + bin;
+    uint32_t* __restrict__ pre = sp.pre + bin;
+    uint32_t v[8];
+    uint32_t sum = 0;
+    for (int64_t t = t0; t < t1; t += 8) {
 #pragma unroll
-      for (int e = 0; e < 8; ++e) v[e] = cnt[(t + e) * NB];
+      for (int e = 0; e < 8; ++e) v[e] = t + e < t1 ? cnt[(t + e) * NB] : 0u;
 #pragma unroll
       for (int e = 0; e < 8; ++e) sum += v[e];
     }
-    for (; t < t1; ++t) sum += cnt[t * NB];
-  }
-  // exclusive scan over the 8 lanes of the bin
-  uint32_t inc = sum;
+    uint32_t inc = sum;
 #pragma unroll
-  for (int o = 1; o < 8; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o, 8);
-    if (sub >= o) inc += y;
-  }
-  if (c == 0) return;
-  uint32_t run = inc - sum;
-  int64_t t = t0;
-  for (; t + 8 <= t1; t += 8) {
-    uint32_t v[8];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) v[e] = cnt[(t + e) * NB];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      pre[(t + e) * NB] = run;
-      run += v[e];
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
     }
+    uint32_t run = inc - sum;
+    for (int64_t t = t0; t < t1; t += 8) {
+      if (per > 8) {  // values of this step are no longer in registers
+#pragma unroll
+        for (int e = 0; e < 8; ++e) v[e] = t + e < t1 ? cnt[(t + e) * NB] : 0u;
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        if (t + e < t1) pre[(t + e) * NB] = run;
+        run += v[e];
+      }
+    }
+    if (lane == 31) pre[sp.nblk * NB] = run;
   }
-  for (; t < t1; ++t) {
-    const uint32_t v = cnt[t * NB];
-    pre[t * NB] = run;
-    run += v;
-  }
-  if (sub == 7) pre[sp.nblk * NB] = run;
 }
 
-// k_span_scan: bin_start of the span (exclusive scan of bin_count).
+// k_span_scan: bin_start of the span (exclusive scan of bin_count) and the
+// list of bins in use (each thread appends its non-empty bins of 16).
 __global__ void __launch_bounds__(256) k_span_scan(Batch b, Span sp) {
+  __shared__ uint32_t sm[33];
+  __shared__ uint32_t s_base;
   pdl_trigger();
   pdl_wait();
   scan_bins(sp.bin_count, sp.bin_start, sp.scan_status, &sp.sc->scan_ticket, b.bs);
+  // this block's 4096 bins (scan_bins took a tile by ticket; any split of the
+  // bins over the blocks will do here)
+  const uint32_t b0 = blockIdx.x * SCAN_TILE + threadIdx.x * 16;
+  uint32_t c[16];
+  uint32_t nz = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const uint4 v = *reinterpret_cast<const uint4*>(sp.bin_count + b0 + 4 * q);
+    c[4 * q] = v.x; c[4 * q + 1] = v.y; c[4 * q + 2] = v.z; c[4 * q + 3] = v.w;
+  }
+#pragma unroll
+  for (int e = 0; e < 16; ++e) nz += c[e] != 0;
+  uint32_t total;
+  const uint32_t ex = block_exclusive_scan(nz, &total, sm);
+  if (threadIdx.x == 0) s_base = total ? atomicAdd(&sp.sc->n_used, total) : 0u;
+  __syncthreads();
+  uint32_t o = s_base + ex;
+#pragma unroll
+  for (int e = 0; e < 16; ++e)
+    if (c[e]) sp.used[o++] = b0 + e;
 }
 
 // ---------------------------------------------------------------------------
@@ -568,7 +576,8 @@ __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
 // Deferred compaction of a chunk of slides [s0, s0 + n): k_slide_base turns
 // the per-slide outlier counts into output offsets (one block), then
 // k_span_compact, one block per slide, turns the slide's bitset row into
-// sorted global indices at its offset and clears the row.
+// sorted global indices at its offset (4 words per thread, one block scan
+// per 4096 words) and clears the row.
 // ---------------------------------------------------------------------------
 struct SpanOut {
   uint32_t* bits;
@@ -600,26 +609,35 @@ __global__ void __launch_bounds__(1024) k_span_compact(SpanOut o, int64_t s0) {
   __shared__ uint32_t sm[33];
   pdl_trigger();
   pdl_wait();
+  constexpr int WPT = 4;  // bitset words per thread and step
   const int64_t s = s0 + blockIdx.x;
   uint32_t* row = o.bits + (s % o.chunk) * o.words;
   const int64_t lo = (s + 1) * o.S;
   int64_t out = o.base[blockIdx.x];
-  for (int64_t c = 0; c < o.words; c += blockDim.x) {
-    const int64_t wi = c + threadIdx.x;
-    uint32_t bits = 0;
-    if (wi < o.words) {
-      bits = row[wi];
-      if (bits) row[wi] = 0;
+  const int64_t step = (int64_t)blockDim.x * WPT;
+  for (int64_t c = 0; c < o.words; c += step) {
+    const int64_t w0 = c + (int64_t)threadIdx.x * WPT;
+    uint32_t bits[WPT];
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int e = 0; e < WPT; ++e) {
+      bits[e] = w0 + e < o.words ? row[w0 + e] : 0u;
+      cnt += __popc(bits[e]);
     }
     uint32_t total;
-    const uint32_t ex = block_exclusive_scan(__popc(bits), &total, sm);
+    const uint32_t ex = block_exclusive_scan(cnt, &total, sm);
     int64_t q = out + ex;
-    while (bits) {
-      const int e = __ffs(bits) - 1;
-      bits &= bits - 1;
-      if (q < o.out_cap) o.out_ids[q] = lo + wi * 32 + e;
-      else set_err(o.bs, DERR_CAPACITY);
-      ++q;
+#pragma unroll
+    for (int e = 0; e < WPT; ++e) {
+      uint32_t b = bits[e];
+      if (b) row[w0 + e] = 0;
+      while (b) {
+        const int f = __ffs(b) - 1;
+        b &= b - 1;
+        if (q < o.out_cap) o.out_ids[q] = lo + (w0 + e) * 32 + f;
+        else set_err(o.bs, DERR_CAPACITY);
+        ++q;
+      }
     }
     out += total;
   }
