@@ -423,16 +423,18 @@ def run_reference(args, world, rank):
 
 def run_ncu_case(args, local):
     """Profiler pass of the headline workload with the settings the autotuner
-    picks on it (span engine, 4 cells per R, 2-warp count blocks, 128 windows
-    per launch): one pass outside the profiler range, then two passes inside
-    it (cudaProfilerStart/Stop: run ncu with --profile-from-start off)."""
+    picks on it in plain runs (span engine, 4 cells per R, 2-warp count
+    blocks, up to 256 windows per launch; under ncu the tuner's own timings
+    would be distorted): one pass outside the profiler range, then two
+    passes inside it (cudaProfilerStart/Stop: run ncu with
+    --profile-from-start off)."""
     import torch
     from rtod_b200 import Detector
     w = workload()
     torch.cuda.set_device(local)
     pts = torch.from_numpy(w.points).to(f"cuda:{local}")
     with Detector(w.window, w.slide, w.R, w.K, dim=w.dim, device=local, engine="span", cells_per_r=4,
-                  block_warps=2, batch=128) as det:
+                  block_warps=2, batch=256) as det:
         r = det.run(pts)
         torch.cuda.synchronize()
         torch.cuda.profiler.start()
@@ -441,7 +443,8 @@ def run_ncu_case(args, local):
             r = det.run(pts)
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
-    print(json.dumps({"mode": "ncu", "slides": r.slides, "outliers": int(r.offsets[-1])}))
+        tuning = det.tuning
+    print(json.dumps({"mode": "ncu", "slides": r.slides, "outliers": int(r.offsets[-1]), "tuning": tuning}))
 
 
 def main():

@@ -734,9 +734,11 @@ __device__ __forceinline__ bool for_each_run(const uint32_t* bin_start, const in
 // ---------------------------------------------------------------------------
 // 1-d group filter. With cells of R(1+2^-12)/n, any n-1 consecutive cells
 // span less than R (with the same margin argument as one cell for n = 2),
-// so a point is an inlier if some run of n-1 consecutive cells containing its
-// cell holds more than K points, provided every bin of the run holds exactly
-// its expected cell (or nothing). Returns true when such a run exists.
+// and every point of the 2n-3 cells within n-2 of a cell lies within
+// (n-1)/n (1+2^-12) R < R of every point of that cell. So a point is an
+// inlier if those 2n-3 cells, or some run of n-1 consecutive cells containing
+// its cell, hold more than K points, provided every bin involved holds
+// exactly its expected cell (or nothing). Returns true when that holds.
 __device__ __forceinline__ bool group_safe_1d(const Job& jb, uint64_t key, uint32_t b, bool pure) {
   const int m = jb.n - 1;
   if (m < 2 || b < (uint32_t)(m - 1) || b + m > NB - 1) return false;
@@ -753,6 +755,13 @@ __device__ __forceinline__ bool group_safe_1d(const Job& jb, uint64_t key, uint3
       const unsigned long long want = key + (unsigned long long)(t - (m - 1));
       ok[t] = pure || bs[t + 1] == bs[t] || (jb.kmin[j] == want && jb.kmax[j] == want);
     }
+  }
+  {  // the whole neighbourhood of 2n-3 cells: bins b-m+1 .. b+m-1
+    bool all = true;
+#pragma unroll
+    for (int t = 0; t < 2 * MMAX - 1; ++t)
+      if (t < 2 * m - 1) all &= ok[t];
+    if (all && bs[2 * m - 1] - bs[0] > (uint32_t)jb.K) return true;
   }
 #pragma unroll
   for (int g = 0; g < MMAX; ++g) {

@@ -335,10 +335,12 @@ __global__ void __launch_bounds__(256) k_span_scatter(Batch b, Span sp) {
   }
 }
 
-// 1-d group rule of the window engine over window counts of the span: some
-// run of n-1 consecutive cells containing the cell of bin `bin` holds more
-// than K window points, every bin of the run holding nothing in the window
-// or only its expected cell over the whole span.
+// 1-d group rule of the window engine over window counts of the span: the
+// 2n-3 cells within n-2 of the cell of bin `bin` (all within R of every
+// point of that cell), or some run of n-1 consecutive cells containing it
+// (all within R of each other), hold more than K window points, every bin
+// involved holding nothing in the window or only its expected cell over the
+// whole span.
 __device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* p0, const uint32_t* p1,
                                                 uint32_t bin, bool pure) {
   const int m = sp.n - 1;
@@ -358,6 +360,17 @@ __device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* 
       const unsigned long long want = key + (unsigned long long)(t - (m - 1));
       ok[t] = pure || wc[t] == 0 || (sp.kmin[j] == want && sp.kmax[j] == want);
     }
+  }
+  {  // the whole neighbourhood of 2n-3 cells
+    bool all = true;
+    uint32_t sum = 0;
+#pragma unroll
+    for (int t = 0; t < 2 * MMAX - 1; ++t)
+      if (t < 2 * m - 1) {
+        all &= ok[t];
+        sum += wc[t];
+      }
+    if (all && sum > (uint32_t)sp.K) return true;
   }
 #pragma unroll
   for (int g = 0; g < MMAX; ++g) {
@@ -382,9 +395,12 @@ __device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* 
 // in, its stencil cells k + d, |d| <= n, lie in bins bin + d (mod NB): lane
 // s < 2n+1 takes bin + d(s), d = 0, -1, +1, -2, +2, ... (nearest first), and
 // that bin's window range (points of other cells sharing those bins are
-// rejected by the distance test); a warp scan turns the range lengths into
-// offsets of one virtual candidate list of ncand entries. With ncand <= K
-// every point is an outlier (its count cannot exceed ncand). Otherwise the
+// rejected by the distance test). In a pure span the bins with |d| <= n-2
+// hold only cells whose points all lie within R of the group's points: their
+// window counts add up to `given` without tests (given > K: all inliers).
+// A warp scan turns the other ranges' lengths into offsets of one virtual
+// candidate list of ncand entries. With given + ncand <= K every point is an
+// outlier (its count cannot exceed that). Otherwise the
 // list is read 256 candidates at a time (8 per lane, kept in registers) and
 // every undecided point of the group (up to 32, one per lane) is tested
 // against the chunk: per point, 8 tests per lane and one warp reduction; a
@@ -394,16 +410,21 @@ __device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* 
 template <int D, int PRED, typename T>
 __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp, int j, uint32_t p,
                                                  uint32_t nq, uint32_t bin, const uint32_t* p0,
-                                                 const uint32_t* p1) {
+                                                 const uint32_t* p1, bool pure) {
   const int lane = threadIdx.x & 31;
   const Job& jb = b.jobs[j];
   const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
   const T* sx = static_cast<const T*>(sp.s_x);
   uint32_t* row = sp.bits + ((jb.ctr->lo - sp.S) / sp.S % sp.chunk) * sp.words;
   const int slots = 2 * sp.n + 1;
+  // In a pure span the cells within n-2 of the group's cell (|d| <= n-2) lie
+  // within R of every point of it: their window points count without tests.
+  const int inner = (pure && D == 1) ? sp.n - 2 : -1;
   uint32_t rs = 0, len = 0;
+  bool sure = false;
   if (lane < slots) {
     const int dk = (lane & 1) ? -((lane + 1) >> 1) : (lane >> 1);
+    sure = (dk < 0 ? -dk : dk) <= inner;
     const uint32_t sb = (bin + (uint32_t)dk) & NB_MASK;
     const uint32_t b0 = sp.bin_start[sb], b1 = sp.bin_start[sb + 1];
     if (b1 > b0) {
@@ -412,6 +433,9 @@ __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp,
       len = p1[sb] - a;
     }
   }
+  const uint32_t given = __reduce_add_sync(0xffffffffu, sure ? len : 0u);
+  if (given > (uint32_t)sp.K) return;  // every point of the group is an inlier
+  if (sure) len = 0;
   uint32_t inc = len;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -427,9 +451,9 @@ __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp,
     T qx[D];
 #pragma unroll
     for (int d = 0; d < D; ++d) qx[d] = has ? sx[(int64_t)d * sp.Wp + p + q] : T(0);
-    int cnt = 0;
+    int cnt = (int)given;
     unsigned live = __ballot_sync(0xffffffffu, has);
-    if (ncand > (uint32_t)sp.K) {
+    if (given + ncand > (uint32_t)sp.K) {
       for (uint32_t c0 = 0; c0 < ncand && live; c0 += 256) {
         T cx[8][D];
         bool cv[8];
@@ -556,11 +580,12 @@ __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
   const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
   const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t ng = sp.sc->n_groups;
+  const bool pure = sp.sc->pure;
   for (int64_t k = gtid >> 5; k < ng; k += gstride >> 5) {
     const uint4 g = sp.groups[k];
     const int j = (int)g.w;
     const uint32_t* p0 = sp.pre + (int64_t)j * NB;
-    span_count_group<D, PRED, T>(b, sp, j, g.x, g.y, g.z, p0, p0 + (int64_t)sp.wblk * NB);
+    span_count_group<D, PRED, T>(b, sp, j, g.x, g.y, g.z, p0, p0 + (int64_t)sp.wblk * NB, pure);
   }
   // The per-bin state is no longer read in this batch: clear it, then the
   // block that finishes last ends the batch.
