@@ -342,12 +342,13 @@ def emit_ours(args, world, w, res):
     dom = max(prof, key=prof.get)
     n_out = r["n_outliers"] / slides
     tun = r["tuning"]
-    ub = used_bins(w, tun["cells_per_r"], tun["batch"]) if w.dim == 1 else 0
-    alg = algorithmic_bytes(dom, w, n_out, r["undet"], tun["batch"], ub)
+    batch = min(tun["batch"], slides)  # windows per launch of the pipeline kernels
+    ub = used_bins(w, tun["cells_per_r"], batch) if w.dim == 1 else 0
+    alg = algorithmic_bytes(dom, w, n_out, r["undet"], batch, ub)
     peak, peak_kind = hbm_peak()
     # per launch: pipeline kernels run once per batch of windows, the key
     # kernel and the chunk compaction once per pass over the stream
-    per_launch = slides if dom in ("k_keys", "k_slide_base+k_span_compact") else tun["batch"]
+    per_launch = slides if dom in ("k_keys", "k_slide_base+k_span_compact") else batch
     launch_ms = prof[dom] * per_launch
     achieved = alg * per_launch / (launch_ms / 1e3) / 1e9
     traffic = ncu_traffic(dom)
