@@ -80,11 +80,11 @@ typedef struct rtod_config {
   int32_t device;      /* CUDA device ordinal */
   int32_t batch;       /* rtod_run: windows detected per launch (0 = auto); each window is
                           processed on its own, so results do not depend on it */
-  int32_t engine;      /* rtod_run engine: RTOD_ENGINE_AUTO (span engine in 1-d without the
-                          router, else window engine; the tuner may choose either in 1-d),
+  int32_t engine;      /* rtod_run engine: RTOD_ENGINE_AUTO (span engine without the
+                          router, else window engine; the tuner may choose either),
                           RTOD_ENGINE_WINDOW (one counting sort per window) or
-                          RTOD_ENGINE_SPAN (1-d only: one counting sort per batch of
-                          windows; falls back to the window engine when W/S > 2047).
+                          RTOD_ENGINE_SPAN (one counting sort per batch of windows;
+                          falls back to the window engine when W/S > 2047).
                           push/detect always use the window engine. Results are identical. */
   int32_t coord;       /* RTOD_COORD_F32 or RTOD_COORD_F64 */
   int32_t reserved[1];

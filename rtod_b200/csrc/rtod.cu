@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <cstddef>
@@ -329,7 +330,6 @@ int check_config(const rtod_config* c) {
   if (c->batch < 0 || c->batch > 256) return fail(RTOD_ERR_CONFIG, "batch must be 0..256");
   if (c->engine < RTOD_ENGINE_AUTO || c->engine > RTOD_ENGINE_SPAN)
     return fail(RTOD_ERR_CONFIG, "engine must be 0 (auto), 1 (window) or 2 (span)");
-  if (c->engine == RTOD_ENGINE_SPAN && c->dim != 1) return fail(RTOD_ERR_CONFIG, "the span engine needs dim = 1");
   if (c->coord != RTOD_COORD_F32 && c->coord != RTOD_COORD_F64)
     return fail(RTOD_ERR_CONFIG, "coord must be RTOD_COORD_F32 or RTOD_COORD_F64");
   if (c->coord == RTOD_COORD_F64 && c->pred != RTOD_PRED_F64_LT)
@@ -478,6 +478,21 @@ Span make_span(const rtod_handle* h, int B, const void* stream_pts, int64_t chun
   sp.K = h->cfg.K;
   sp.n = h->n;
   sp.filter = h->filter;
+  sp.h = h->D < 3 ? h->D : 3;
+  // cells within R of every point of the centre cell: sum (|d_i| + 1)^2 < n^2
+  sp.n_sure = 0;
+  if (h->D <= 3) {
+    const int n = h->n, H = sp.h;
+    for (int d0 = -n; d0 <= n; ++d0)
+      for (int d1 = (H >= 2 ? -n : 0); d1 <= (H >= 2 ? n : 0); ++d1)
+        for (int d2 = (H >= 3 ? -n : 0); d2 <= (H >= 3 ? n : 0); ++d2) {
+          const int q = (std::abs(d0) + 1) * (std::abs(d0) + 1) + (H >= 2 ? (std::abs(d1) + 1) * (std::abs(d1) + 1) : 0) +
+                        (H >= 3 ? (std::abs(d2) + 1) * (std::abs(d2) + 1) : 0);
+          if (q >= n * n || sp.n_sure >= 16) continue;
+          const int delta = H == 1 ? d0 : (H == 2 ? d1 + 256 * d0 : d2 + 64 * d1 + 4096 * d0);
+          sp.sure_delta[sp.n_sure++] = delta;
+        }
+  }
   sp.R = h->cfg.R;
   sp.R2 = h->cfg.R * h->cfg.R;
   sp.R2f = h->R2f;
@@ -669,28 +684,18 @@ int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, 
   const int64_t npts = sp.nblk * sp.S;
   const int64_t hx = std::max<int64_t>(1, std::min<int64_t>((npts + 1023) / 1024, (int64_t)g.sm_count * 8));
   if (kev) CU(cudaEventRecord(kev[0], st));
-  CU(launch_k(k_span_hist<1>, dim3((unsigned)hx), 256, st, b, sp));
+  DISPATCH_D(g.D, CU(launch_k(k_span_hist<D>, dim3((unsigned)hx), 256, st, b, sp)));
   if (kev) CU(cudaEventRecord(kev[1], st));
   CU(launch_k(k_span_scan, dim3(SCAN_TILES), 256, st, b, sp));
   CU(launch_k(k_span_prefix, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
   if (kev) CU(cudaEventRecord(kev[2], st));
-  if (g.f64) {
-    CU(launch_k(k_span_scatter<1, double>, dim3((unsigned)hx), 256, st, b, sp));
-  } else {
-    CU(launch_k(k_span_scatter<1, float>, dim3((unsigned)hx), 256, st, b, sp));
-  }
+  DISPATCH_DT(g.f64, g.D, CU(launch_k(k_span_scatter<D, T>, dim3((unsigned)hx), 256, st, b, sp)));
   if (kev) CU(cudaEventRecord(kev[3], st));
   CU(launch_k(k_span_classify, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
   if (kev) CU(cudaEventRecord(kev[4], st));
   const int wpb = g.block_warps;
   const int64_t cx = (int64_t)g.sm_count * (64 / wpb);
-  if (g.f64) {
-    CU(launch_k(k_span_count<1, 1, double>, dim3((unsigned)cx), wpb * 32, st, b, sp));
-  } else if (g.pred == 0) {
-    CU(launch_k(k_span_count<1, 0, float>, dim3((unsigned)cx), wpb * 32, st, b, sp));
-  } else {
-    CU(launch_k(k_span_count<1, 1, float>, dim3((unsigned)cx), wpb * 32, st, b, sp));
-  }
+  DISPATCH_DPT(g.f64, g.D, g.pred, CU(launch_k(k_span_count<D, PRED, T>, dim3((unsigned)cx), wpb * 32, st, b, sp)));
   if (kev) CU(cudaEventRecord(kev[5], st));
   if (kev) CU(cudaEventRecord(kev[6], st));  // no per-batch compaction: see span_flush
   if (nk) *nk = 6;
@@ -863,10 +868,10 @@ int stage_stream(rtod_handle* h, const void* pts, int64_t used, const void** src
   return RTOD_OK;
 }
 
-// Whether rtod_run uses the span engine: one hashed dimension and at most
-// SPAN_MAX_BLOCKS slide blocks per window.
+// Whether rtod_run uses the span engine: at most SPAN_MAX_BLOCKS slide
+// blocks per window.
 bool use_span(const rtod_handle* h) {
-  return h->engine == RTOD_ENGINE_SPAN && h->D == 1 && h->W / h->S <= SPAN_MAX_BLOCKS;
+  return h->engine == RTOD_ENGINE_SPAN && h->W / h->S <= SPAN_MAX_BLOCKS;
 }
 
 // Largest batch of the span engine: spans of at most SPAN_MAX_BLOCKS blocks
@@ -1157,24 +1162,29 @@ int autotune(rtod_handle* h, const void* pts, int64_t slides_total) {
     }
     return RTOD_OK;
   };
-  if (h->D == 1 && h->cfg.engine == RTOD_ENGINE_AUTO) {
-    Tuning t = best;
-    t.engine = best.engine == RTOD_ENGINE_SPAN ? RTOD_ENGINE_WINDOW : RTOD_ENGINE_SPAN;
-    if ((r = trial(t))) return r;
+  // engine x cells per R (the best cell width differs between the engines)
+  {
+    const Tuning start = best;
+    for (int e : {RTOD_ENGINE_SPAN, RTOD_ENGINE_WINDOW}) {
+      if (h->cfg.engine != RTOD_ENGINE_AUTO && e != start.engine) continue;
+      for (int n : {1, 2, 3, 4, 6}) {
+        if (n > 3 && h->D != 1) continue;
+        if (e == start.engine && n == start.n) continue;  // the starting point, timed above
+        Tuning t = start;
+        t.engine = e;
+        t.n = n;
+        if ((r = trial(t))) return r;
+      }
+    }
   }
-  for (int n : {1, 3, 4, 6}) {
-    if (n > 3 && h->D != 1) continue;
-    Tuning t = best;
-    t.n = n;
-    if ((r = trial(t))) return r;
-  }
-  for (int bw : {2, 4}) {
+  for (int bw : {2, 4, 8}) {
+    if (bw == best.block_warps) continue;
     Tuning t = best;
     t.block_warps = bw;
     if ((r = trial(t))) return r;
   }
-  for (int bt : {8, 16, 64, 128, 256}) {
-    if (bt > (best.engine == RTOD_ENGINE_SPAN ? h->span_batch_max : h->batch_max)) continue;
+  for (int bt : {8, 16, 32, 64, 128, 256}) {
+    if (bt == best.batch || bt > (best.engine == RTOD_ENGINE_SPAN ? h->span_batch_max : h->batch_max)) continue;
     Tuning t = best;
     t.batch = bt;
     if ((r = trial(t))) return r;
@@ -1261,10 +1271,9 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
     h->R2f = r2f;
   }
   set_grid(h, cfg->cells_per_r ? cfg->cells_per_r : 2);
-  // Engine of rtod_run: the span engine by default in 1-d without the router.
-  h->engine = cfg->engine != RTOD_ENGINE_AUTO
-                  ? cfg->engine
-                  : ((cfg->dim == 1 && !cfg->router) ? RTOD_ENGINE_SPAN : RTOD_ENGINE_WINDOW);
+  // Engine of rtod_run: the span engine by default without the router.
+  h->engine = cfg->engine != RTOD_ENGINE_AUTO ? cfg->engine
+                                               : (!cfg->router ? RTOD_ENGINE_SPAN : RTOD_ENGINE_WINDOW);
   // Windows per rtod_run launch: up to 32, within ~1 GiB of scratch.
   const int64_t per_job = (int64_t)NB * 24 + h->W * (4 + 8 + 4 + 4) + h->Wp * h->D * 4 + h->W / 8;
   h->batch_max = (int)std::max<int64_t>(1, std::min<int64_t>(32, (1ll << 30) / per_job));

@@ -1,5 +1,5 @@
-// Span engine (one hashed dimension): one counting sort per batch of B
-// consecutive windows instead of one per window.
+// Span engine: one counting sort per batch of B consecutive windows instead
+// of one per window.
 //
 // The B windows of a batch, [lo0 + jS, lo0 + jS + W) for j < B, cover the
 // span [lo0, lo0 + W + (B-1)S): nblk = W/S + B - 1 slide blocks of S points,
@@ -13,7 +13,8 @@
 // So window j's points of bin b are the contiguous positions
 // [bin_start[b] + pre[j][b], bin_start[b] + pre[j + W/S][b]), and its count
 // of bin b is pre[j + W/S][b] - pre[j][b]: classification needs no per-point
-// work, and a queued point's candidates are 2n+1 such ranges.
+// work, and a queued point's candidates are (2n+1)^h such ranges (h = hashed
+// dimensions, min(D, 3)); all points of a bin share them.
 //
 // Kernels per batch: k_span_hist (per-block bin counts), k_span_scan
 // (bin_start, list of bins in use), k_span_prefix (pre), k_span_scatter (sorted
@@ -24,9 +25,11 @@
 // outlier IDs.
 //
 // The safe-inlier rule is the window engine's (count > K in one cell, plus
-// the 1-d group rule), with "single cell" judged over the whole span: a bin
-// whose span holds two cells queues its points even in a window where it
-// holds one. That only queues more points; every result is an exact count.
+// the 1-d group rule) and, for 2-3 hashed dimensions in a pure span, the
+// cells within R of every point of a cell; "single cell" is judged over the
+// whole span: a bin whose span holds two cells queues its points even in a
+// window where it holds one. That only queues more points; every result is
+// an exact count.
 #pragma once
 
 #include "kernels.cuh"
@@ -41,6 +44,9 @@ struct Span {
   int64_t nblk;    // blocks in the span: W/S + B - 1
   int32_t wblk;    // blocks per window: W/S
   int32_t K, n, filter;
+  int32_t h;       // hashed dimensions (1..3)
+  int32_t n_sure;  // stencil cells within R of every point of the centre cell (pure spans, D <= 3)
+  int32_t sure_delta[16];  // their bin offsets
   double R, R2;
   float R2f;
   const void* pts;          // resident stream, point-major [N][D] (the handle's coordinate type)
@@ -74,7 +80,7 @@ __device__ __forceinline__ int64_t span_lo(const Batch& b) { return b.jobs[0].ct
 // ---------------------------------------------------------------------------
 template <int D>
 __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
-  static_assert(Hashed<D>::value == 1, "span engine: one hashed dimension");
+  constexpr int H = Hashed<D>::value;
   __shared__ uint32_t hkey[HIST_SLOTS];
   __shared__ uint32_t hcnt[HIST_SLOTS];
   __shared__ unsigned long long hmin[HIST_SLOTS], hmax[HIST_SLOTS];
@@ -86,7 +92,7 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
   const int64_t npts = sp.nblk * sp.S;
   const int lane = threadIdx.x & 31;
   if (threadIdx.x < 32) {
-    const bool pure = range_pure<1>(sp.blk_lo, sp.blk_hi, lo0 / sp.S, sp.nblk);
+    const bool pure = range_pure<H>(sp.blk_lo, sp.blk_hi, lo0 / sp.S, sp.nblk);
     if (threadIdx.x == 0) {
       s_pure = pure;
       if (blockIdx.x == 0) sp.sc->pure = pure;
@@ -114,7 +120,7 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
     for (int u = 0; u < U; ++u) {
       const int64_t i = w0 + u * 32 + lane;
       const bool valid = key[u] != EMPTY_KEY;
-      const uint32_t bin = (uint32_t)key[u] & NB_MASK;
+      const uint32_t bin = valid ? bin_of_key(key[u], H) : 0u;
       const uint32_t comp = valid ? ((uint32_t)i / S32) * NB + bin : 0xffffffffu;
       const unsigned peers = __match_any_sync(0xffffffffu, comp);
       const int leader = __ffs(peers) - 1;
@@ -254,6 +260,7 @@ __global__ void __launch_bounds__(256) k_span_scan(Batch b, Span sp) {
 // ---------------------------------------------------------------------------
 template <int D, typename T>
 __global__ void __launch_bounds__(256) k_span_scatter(Batch b, Span sp) {
+  constexpr int H = Hashed<D>::value;
   __shared__ uint32_t tkey[HIST_SLOTS];
   __shared__ uint32_t tcnt[HIST_SLOTS];
   __shared__ uint32_t tbase[HIST_SLOTS];
@@ -286,7 +293,7 @@ __global__ void __launch_bounds__(256) k_span_scatter(Batch b, Span sp) {
     for (int u = 0; u < U; ++u) {
       const int64_t i = w0 + u * 32 + lane;
       const bool valid = key[u] != EMPTY_KEY;
-      comp[u] = valid ? ((uint32_t)i / S32) * NB + ((uint32_t)key[u] & NB_MASK) : 0xffffffffu;
+      comp[u] = valid ? ((uint32_t)i / S32) * NB + bin_of_key(key[u], H) : 0xffffffffu;
       const unsigned peers = __match_any_sync(0xffffffffu, comp[u]);
       const int leader = __ffs(peers) - 1;
       int sl_found = -1;
@@ -389,61 +396,99 @@ __device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* 
   return false;
 }
 
+// Stencil slot s of 2n+1 cells per hashed dimension: offsets d in [-n, n]^h
+// (1-d: 0, -1, +1, -2, +2, ..., nearest first; otherwise row-major) and the
+// bin offset of the cell k + d (bins are linear in the cell coordinates mod
+// NB: d, d1 + 256 d0, d2 + 64 d1 + 4096 d0).
+template <int H>
+__device__ __forceinline__ int slot_cell(int s, int n, int* d) {
+  if constexpr (H == 1) {
+    d[0] = (s & 1) ? -((s + 1) >> 1) : (s >> 1);
+    return d[0];
+  } else {
+    const int w = 2 * n + 1;
+#pragma unroll
+    for (int i = H - 1; i >= 0; --i) {
+      d[i] = s % w - n;
+      s /= w;
+    }
+    return H == 2 ? d[1] + 256 * d[0] : d[2] + 64 * d[1] + 4096 * d[0];
+  }
+}
+
+// Whether every point of cell k + d lies within R of every point of cell k:
+// sum of (|d_i| + 1)^2 < n^2 (cells of R(1+2^-12)/n; the margin is at least
+// 1/n^2 - 2^-11 of R^2, far above the predicates' rounding).
+template <int H>
+__device__ __forceinline__ bool slot_sure(const int* d, int n) {
+  int q = 0;
+#pragma unroll
+  for (int i = 0; i < H; ++i) {
+    const int a = (d[i] < 0 ? -d[i] : d[i]) + 1;
+    q += a * a;
+  }
+  return q < n * n;
+}
+
 // ---------------------------------------------------------------------------
 // Exact counts of the nq points of window j in bin `bin` (bin-ordered
 // positions [p, p + nq)) by one warp. Whatever cell k of the bin a point is
-// in, its stencil cells k + d, |d| <= n, lie in bins bin + d (mod NB): lane
-// s < 2n+1 takes bin + d(s), d = 0, -1, +1, -2, +2, ... (nearest first), and
-// that bin's window range (points of other cells sharing those bins are
-// rejected by the distance test). In a pure span the bins with |d| <= n-2
-// hold only cells whose points all lie within R of the group's points: their
-// window counts add up to `given` without tests (given > K: all inliers).
-// A warp scan turns the other ranges' lengths into offsets of one virtual
-// candidate list of ncand entries. With given + ncand <= K every point is an
-// outlier (its count cannot exceed that). Otherwise the
-// list is read 256 candidates at a time (8 per lane, kept in registers) and
-// every undecided point of the group (up to 32, one per lane) is tested
-// against the chunk: per point, 8 tests per lane and one warp reduction; a
-// point is decided as soon as its count exceeds K, and the chunks stop when
-// every point is decided.
+// in, its stencil cells k + d lie in bins bin + delta(d) (mod NB), so the
+// stencil is the same for all of them: (2n+1)^h slots, taken 32 at a time
+// (lane s of a round takes slot r0 + s and that bin's window range; points
+// of other cells sharing those bins are rejected by the distance test). In
+// a pure span (D <= 3) the "sure" slots hold only cells whose points all lie
+// within R of the group's points: their window counts add up to `given`
+// without tests (given > K: all inliers; given plus every other candidate
+// <= K: all outliers). In each round a warp scan turns the other ranges'
+// lengths into offsets of one virtual candidate list, read 256 candidates
+// at a time (8 per lane, kept in registers); every undecided point of the
+// group (up to 32, one per lane) is tested against the chunk: per point, 8
+// tests per lane and one warp reduction; a point is decided as soon as its
+// count exceeds K, and the rounds stop when every point is decided.
 // ---------------------------------------------------------------------------
 template <int D, int PRED, typename T>
 __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp, int j, uint32_t p,
                                                  uint32_t nq, uint32_t bin, const uint32_t* p0,
                                                  const uint32_t* p1, bool pure) {
+  constexpr int H = Hashed<D>::value;
   const int lane = threadIdx.x & 31;
   const Job& jb = b.jobs[j];
   const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
   const T* sx = static_cast<const T*>(sp.s_x);
   uint32_t* row = sp.bits + ((jb.ctr->lo - sp.S) / sp.S % sp.chunk) * sp.words;
-  const int slots = 2 * sp.n + 1;
-  // In a pure span the cells within n-2 of the group's cell (|d| <= n-2) lie
-  // within R of every point of it: their window points count without tests.
-  const int inner = (pure && D == 1) ? sp.n - 2 : -1;
-  uint32_t rs = 0, len = 0;
-  bool sure = false;
-  if (lane < slots) {
-    const int dk = (lane & 1) ? -((lane + 1) >> 1) : (lane >> 1);
-    sure = (dk < 0 ? -dk : dk) <= inner;
-    const uint32_t sb = (bin + (uint32_t)dk) & NB_MASK;
+  const int w = 2 * sp.n + 1;
+  const int slots = H == 1 ? w : (H == 2 ? w * w : w * w * w);
+  const bool can_sure = pure && D <= 3;
+  // window range of slot s; sure: counts without tests
+  auto slot = [&](int s, uint32_t& rs, uint32_t& len, bool& sure) {
+    rs = 0;
+    len = 0;
+    sure = false;
+    if (s >= slots) return;
+    int d[3] = {0, 0, 0};
+    const int delta = slot_cell<H>(s, sp.n, d);
+    sure = can_sure && slot_sure<H>(d, sp.n);
+    const uint32_t sb = (bin + (uint32_t)delta) & NB_MASK;
     const uint32_t b0 = sp.bin_start[sb], b1 = sp.bin_start[sb + 1];
     if (b1 > b0) {
       const uint32_t a = p0[sb];
       rs = b0 + a;
       len = p1[sb] - a;
     }
+  };
+  const bool one = slots <= 32;  // one round: its ranges stay in registers
+  uint32_t given = 0, total = 0, rs1 = 0, len1 = 0;
+  for (int r0 = 0; r0 < slots; r0 += 32) {
+    uint32_t rs, len;
+    bool sure;
+    slot(r0 + lane, rs, len, sure);
+    given += __reduce_add_sync(0xffffffffu, sure ? len : 0u);
+    total += __reduce_add_sync(0xffffffffu, len);
+    rs1 = rs;
+    len1 = sure ? 0u : len;
   }
-  const uint32_t given = __reduce_add_sync(0xffffffffu, sure ? len : 0u);
   if (given > (uint32_t)sp.K) return;  // every point of the group is an inlier
-  if (sure) len = 0;
-  uint32_t inc = len;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-    if (lane >= o) inc += y;
-  }
-  const uint32_t off = inc - len;
-  const uint32_t ncand = __shfl_sync(0xffffffffu, inc, 31);
   int nout = 0;
   for (uint32_t g = 0; g < nq; g += 32) {
     const uint32_t q = g + lane;
@@ -453,20 +498,34 @@ __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp,
     for (int d = 0; d < D; ++d) qx[d] = has ? sx[(int64_t)d * sp.Wp + p + q] : T(0);
     int cnt = (int)given;
     unsigned live = __ballot_sync(0xffffffffu, has);
-    if (given + ncand > (uint32_t)sp.K) {
+    for (int r0 = 0; r0 < slots && live && total > (uint32_t)sp.K; r0 += 32) {
+      uint32_t rs = rs1, len = len1;
+      if (!one) {
+        bool sure;
+        slot(r0 + lane, rs, len, sure);
+        if (sure) len = 0;
+      }
+      uint32_t inc = len;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+      }
+      const uint32_t off = inc - len;
+      const uint32_t ncand = __shfl_sync(0xffffffffu, inc, 31);
       for (uint32_t c0 = 0; c0 < ncand && live; c0 += 256) {
         T cx[8][D];
         bool cv[8];
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
           const uint32_t v = c0 + 32 * e + lane;
-          // slot holding v: the last slot whose offset is <= v
+          // lane holding v's range: the last lane whose offset is <= v
           int s = 0;
 #pragma unroll
           for (int step = 16; step > 0; step >>= 1) {
             const int cand = s + step;
             const uint32_t oc = __shfl_sync(0xffffffffu, off, cand & 31);
-            if (cand < slots && oc <= v) s = cand;
+            if (oc <= v) s = cand;
           }
           const uint32_t base = __shfl_sync(0xffffffffu, rs, s);
           const uint32_t os = __shfl_sync(0xffffffffu, off, s);
@@ -493,8 +552,8 @@ __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp,
     }
     const bool out = has && cnt <= sp.K;
     if (out) {
-      const int64_t w = (int64_t)sp.s_off[p + q] - shift;
-      atomicOr(&row[w >> 5], 1u << (w & 31));
+      const int64_t w2 = (int64_t)sp.s_off[p + q] - shift;
+      atomicOr(&row[w2 >> 5], 1u << (w2 & 31));
     }
     nout += __popc(__ballot_sync(0xffffffffu, out));
   }
@@ -517,10 +576,12 @@ __device__ __forceinline__ void span_clear_bins(const SpanCtr* c) {
 
 // ---------------------------------------------------------------------------
 // k_span_classify: one thread per (window, bin in use): the window's count of
-// the bin from pre; a bin that is not provably all-inlier in that window is
-// appended to the batch's list of groups to count (first position, points,
-// bin, window): one atomic per warp for the list, one per window present in
-// the warp for its count of listed points.
+// the bin from pre; a bin that is not provably all-inlier in that window
+// (more than K window points in its single cell, in the 1-d group rule's
+// cells, or, in a pure span of 2-3 hashed dimensions, in the cells within R
+// of every point of its cell) is appended to the batch's list of groups to
+// count (first position, points, bin, window): one atomic per warp for the
+// list, one per window present in the warp for its count of listed points.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
   pdl_trigger();
@@ -547,7 +608,16 @@ __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
         if (sp.filter) {
           const bool single = pure || sp.kmin[bin] == sp.kmax[bin];
           safe = single && wc > (uint32_t)sp.K;
-          if (!safe && single && sp.n >= 3) safe = span_group_safe(sp, p0, p1, bin, pure);
+          if (!safe && single && sp.h == 1 && sp.n >= 3) safe = span_group_safe(sp, p0, p1, bin, pure);
+          if (!safe && pure && sp.h > 1 && sp.n_sure > 1) {
+            // the sure neighbourhood: cells within R of every point of this one
+            uint32_t sum = 0;
+            for (int t = 0; t < sp.n_sure; ++t) {
+              const uint32_t nb = (bin + (uint32_t)sp.sure_delta[t]) & NB_MASK;
+              if (sp.bin_count[nb]) sum += p1[nb] - p0[nb];
+            }
+            safe = sum > (uint32_t)sp.K;
+          }
         }
         need = !safe;
         start = sp.bin_start[bin] + a;

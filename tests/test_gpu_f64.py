@@ -33,8 +33,6 @@ def det(rtod, W, S, R, K, dim, **kw):
 @pytest.mark.parametrize("engine,graph", [("window", True), ("window", False), ("span", True)])
 def test_run_matches_double_golden(rtod, path, engine, graph):
     meta, pts, off, ids = load_golden(path)
-    if engine == "span" and pts.shape[1] != 1:
-        pytest.skip("the span engine is 1-d only")
     with det(rtod, meta["W"], meta["S"], meta["R"], meta["K"], pts.shape[1], engine=engine,
              use_graph=graph) as d:
         r = d.run(pts)

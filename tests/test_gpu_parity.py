@@ -32,8 +32,6 @@ def assert_same(res, off, ids):
 @pytest.mark.parametrize("engine", ["window", "span"])
 def test_run_matches_golden(rtod, path, opt, graph, n, engine):
     meta, pts, off, ids = load_golden(path)
-    if engine == "span" and pts.shape[1] != 1:
-        pytest.skip("the span engine is 1-d only")
     with rtod.Detector(meta["W"], meta["S"], meta["R"], meta["K"], dim=pts.shape[1], opt=opt,
                        pred=meta["pred"], use_graph=graph, cells_per_r=n, engine=engine) as det:
         assert_same(det.run(pts), off, ids)

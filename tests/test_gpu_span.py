@@ -1,9 +1,10 @@
-"""The span engine (one counting sort per batch of windows, 1-d) against the
-CPU oracle and against the window engine, on the cases where its layout
-differs from one sort per window: spans whose cells share bins, many slide
-blocks per window, batches of one window, every point an outlier, the grid
-filter off, the double predicate, and the fall-back to the window engine when
-a window holds more slide blocks than a span table allows. Bit-exact."""
+"""The span engine (one counting sort per batch of windows) against the CPU
+oracle and against the window engine, on the cases where its layout differs
+from one sort per window: spans whose cells share bins, many slide blocks per
+window, batches of one window, every point an outlier, the grid filter off,
+the double predicate, 2-d/3-d/8-d stencils (one or several rounds of 32
+cells), and the fall-back to the window engine when a window holds more
+slide blocks than a span table allows. Bit-exact."""
 import numpy as np
 import pytest
 
@@ -23,7 +24,8 @@ def rtod():
 
 def run(rtod, pts, W, S, R, K, slides, **kw):
     pts = pts[:W + slides * S]
-    with rtod.Detector(W, S, R, K, dim=1, **kw) as det:
+    dim = pts.shape[1] if pts.ndim == 2 else 1
+    with rtod.Detector(W, S, R, K, dim=dim, **kw) as det:
         res = det.run(pts)
         return res, det.tuning
 
@@ -110,3 +112,31 @@ def test_engine_auto_with_tuner(rtod):
     assert tun["engine"] in ("span", "window")
     np.testing.assert_array_equal(got.offsets, base.offsets)
     np.testing.assert_array_equal(got.ids, base.ids)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3])
+def test_sensor_3d_stencils(rtod, oracle_mod, n):
+    """3-d: 27 stencil cells (one round), 125 and 343 (several rounds); n >= 2
+    enables the single-cell rule and, with n = 3, the neighbourhood rule."""
+    from rtod_b200 import datagen
+    w = datagen.sensor_like()
+    check_vs_oracle(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, 60, cells_per_r=n, batch=32)
+
+
+@pytest.mark.parametrize("d,n", [(2, 1), (2, 2), (2, 3), (8, 1), (8, 2)])
+def test_other_dims(rtod, oracle_mod, d, n):
+    from rtod_b200 import datagen
+    pts = datagen.random_walk(30_000, 0.1, seed=60 + d, dim=d)
+    check_vs_oracle(rtod, oracle_mod, pts, 6000, 600, 0.25 * d ** 0.5, 20, 15, cells_per_r=n, batch=8)
+
+
+def test_sensor_3d_sparse_and_shared_bins(rtod, oracle_mod):
+    """3-d points over a range wider than the 16 x 64 x 64 bin box (bins
+    shared by several cells, no pure span), with tight clusters."""
+    rng = np.random.default_rng(81)
+    n = 20_000
+    centres = rng.uniform(-400, 400, (40, 3))
+    pts = np.where(rng.random((n, 1)) < 0.7, centres[rng.integers(0, 40, n)] + rng.normal(0, 0.05, (n, 3)),
+                   rng.uniform(-400, 400, (n, 3))).astype(np.float32)
+    for nc in (2, 3):
+        check_vs_oracle(rtod, oracle_mod, pts, 4000, 400, 0.5, 10, 30, cells_per_r=nc, batch=16)
