@@ -52,8 +52,9 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", choices=["bench", "ncu"], default="bench",
-                    help="ncu: passes of the headline workload inside a cudaProfilerStart/Stop range")
+    ap.add_argument("--mode", choices=["bench", "ncu", "replica-check"], default="bench",
+                    help="ncu: passes of the headline workload inside a cudaProfilerStart/Stop range; "
+                         "replica-check: the multi-rank plumbing on host ranks (gloo), no GPU")
     return ap.parse_args()
 
 
@@ -62,6 +63,39 @@ def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     return world, rank, local
+
+
+class Ranks:
+    """Replica plumbing: one process per GPU, each detecting its own copy of
+    the workload; no collective on the data path. Only barriers and the
+    maximum of the device-timed durations cross ranks (backend "nccl" on
+    GPUs, "gloo" on the host)."""
+
+    def __init__(self, world: int, backend: str, device: str):
+        import datetime
+        import torch.distributed as dist
+        self.world, self.device, self.dist = world, device, dist
+        if world > 1:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+
+    def barrier(self):
+        import torch
+        if self.device.startswith("cuda"):
+            torch.cuda.synchronize()
+        if self.world > 1:
+            self.dist.barrier()
+
+    def reduce(self, x: float, op: str = "max") -> float:
+        import torch
+        if self.world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX if op == "max" else self.dist.ReduceOp.MIN)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
 
 
 def workload():
@@ -200,12 +234,10 @@ def algorithmic_bytes(kernel: str, w, n_out_per_slide: float, undet_per_slide: f
 # ---------------------------------------------------------------------------
 def run_ours(args, world, rank, local):
     import torch
-    import torch.distributed as dist
     from rtod_b200 import Detector
 
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    ranks = Ranks(world, "nccl", f"cuda:{local}")
     w = workload()
     slides = w.slides
     cap = slides * w.window // 4
@@ -213,17 +245,8 @@ def run_ours(args, world, rank, local):
     out_dev = torch.empty(cap, dtype=torch.int64, device=f"cuda:{local}")
     flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
 
-    def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier = ranks.barrier
+    max_over_ranks = ranks.reduce
 
     def measure(kw, steps, full):
         """Device-timed passes of one engine configuration; with full=True also
@@ -302,8 +325,7 @@ def run_ours(args, world, rank, local):
     for name, r in results.items():
         assert np.array_equal(r["offsets"], base["offsets"]), name
         assert np.array_equal(r["ids"], base["ids"]), name
-    if world > 1:
-        dist.destroy_process_group()
+    ranks.close()
     if rank != 0:
         return None
     return w, results
@@ -448,11 +470,40 @@ def run_ncu_case(args, local):
     print(json.dumps({"mode": "ncu", "slides": r.slides, "outliers": int(r.offsets[-1]), "tuning": tuning}))
 
 
+def run_replica_check(world, rank):
+    """The replica path of this file on host ranks (gloo): every rank detects
+    the same slides of the small random walk with the oracle (the CPU
+    restatement), the time is the maximum over ranks, the value counts the
+    points of all ranks, the outliers must agree on every rank, and rank 0
+    alone prints."""
+    from oracle import oracle
+    from rtod_b200 import datagen
+    ranks = Ranks(world, "gloo", "cpu")
+    w = datagen.small_walk()
+    slides = 20
+    ranks.barrier()
+    t0 = time.perf_counter()
+    off, ids, _ = oracle.detect(w.points[:w.window + slides * w.slide], w.window, w.slide, w.R, w.K,
+                                engine="grid")
+    dt = ranks.reduce(time.perf_counter() - t0, "max")
+    ranks.barrier()
+    digest = float(np.sum(ids * 2654435761 % 1000003)) + float(off[-1]) * 1e6
+    same = ranks.reduce(digest, "max") == ranks.reduce(digest, "min")
+    ranks.close()
+    if rank == 0:
+        print(json.dumps({"mode": "replica-check", "n_ranks": world, "slides": slides,
+                          "value": world * slides * w.slide / dt, "unit": UNIT, "s_max": dt,
+                          "outliers": int(off[-1]), "identical_on_all_ranks": same}))
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_env()
     if args.mode == "ncu":
         run_ncu_case(args, local)
+        return
+    if args.mode == "replica-check":
+        run_replica_check(world, rank)
         return
     if args.impl == "reference":
         run_reference(args, world, rank)
