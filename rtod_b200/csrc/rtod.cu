@@ -287,6 +287,12 @@ struct rtod_handle {
   Batch graph_batch{};
   Span graph_span{};
   bool graph_is_span = false;
+  // A whole rtod_run of a device-resident stream with the span engine, as one
+  // graph (memsets, counter upload, keys, batches, compaction), replayed while
+  // its key (stream, slides, batch and span parameters) stays the same.
+  cudaGraphExec_t run_graph = nullptr;
+  std::vector<unsigned char> run_graph_key;
+  int64_t run_graph_kernels = 0;
   int graph_ring = -1;
   int64_t batches = 0;
 
@@ -351,6 +357,8 @@ void drop_graph(rtod_handle* h) {
     g = nullptr;
   }
   h->graph_ring = -1;
+  if (h->run_graph) cudaGraphExecDestroy(h->run_graph);
+  h->run_graph = nullptr;
 }
 
 // Pool entries for `jobs` jobs; with `full`, their window-engine scratch.
@@ -569,7 +577,8 @@ Job make_job(rtod_handle* h, int j, bool ring, const void* stream_pts) {
 // Uploads the job table for a mode (only when it changed, so that captured
 // graphs stay valid) and initialises the job counters: job j starts at
 // window lo = first_lo + j*S and advances by jobs*S per batch.
-int configure(rtod_handle* h, int mode, int jobs, int64_t first_lo, const void* stream_pts, bool full = true) {
+int configure(rtod_handle* h, int mode, int jobs, int64_t first_lo, const void* stream_pts, bool full = true,
+              bool copy_ctr = true) {
   int r = ensure_pool(h, jobs, full);
   if (r) return r;
   std::vector<Job> tab((size_t)jobs);
@@ -586,8 +595,9 @@ int configure(rtod_handle* h, int mode, int jobs, int64_t first_lo, const void* 
     h->ctr_init[j].lo_step = (int64_t)jobs * h->S;
   }
   // Pinned source; every public call ends with a stream sync, so the buffer
-  // is never rewritten while a copy from it is pending.
-  CU(cudaMemcpyAsync(h->ctr, h->ctr_init, sizeof(JobCtr) * jobs, cudaMemcpyHostToDevice, h->stream));
+  // is never rewritten while a copy from it is pending (without copy_ctr the
+  // caller enqueues the copy).
+  if (copy_ctr) CU(cudaMemcpyAsync(h->ctr, h->ctr_init, sizeof(JobCtr) * jobs, cudaMemcpyHostToDevice, h->stream));
   h->mode = mode;
   return RTOD_OK;
 }
@@ -828,7 +838,8 @@ int ensure_records(rtod_handle* h, int64_t n) {
 
 // Room for a stream of `used` points: the handle's run buffer for a host
 // stream (*host = true; run_stream copies it in), its keys and features.
-int stage_stream(rtod_handle* h, const void* pts, int64_t used, const void** src, bool* host) {
+int stage_stream(rtod_handle* h, const void* pts, int64_t used, const void** src, bool* host,
+                 bool memsets = true) {
   const int64_t D = h->D;
   *src = pts;
   *host = !is_device_ptr(pts);
@@ -862,9 +873,12 @@ int stage_stream(rtod_handle* h, const void* pts, int64_t used, const void** src
       return RTOD_ERR_CUDA;
     h->run_blk_cap = blocks;
   }
-  // +inf / -inf patterns for the atomic min / max of k_keys
-  CU(cudaMemsetAsync(h->run_blk_lo, 0x7f, (size_t)(blocks * 3) * sizeof(long long), h->stream));
-  CU(cudaMemsetAsync(h->run_blk_hi, 0x80, (size_t)(blocks * 3) * sizeof(long long), h->stream));
+  // +inf / -inf patterns for the atomic min / max of k_keys (without memsets
+  // the caller enqueues them)
+  if (memsets) {
+    CU(cudaMemsetAsync(h->run_blk_lo, 0x7f, (size_t)(blocks * 3) * sizeof(long long), h->stream));
+    CU(cudaMemsetAsync(h->run_blk_hi, 0x80, (size_t)(blocks * 3) * sizeof(long long), h->stream));
+  }
   return RTOD_OK;
 }
 
@@ -918,9 +932,10 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
   if (span && (r = ensure_span(h, W / S + B - 1, chunk))) return r;
   if (e_begin) CU(cudaEventRecord(e_begin, h->stream));
   bool host = false;
-  if ((r = stage_stream(h, pts, used, &src, &host))) return r;
-  if ((r = configure(h, MODE_RUN, B, S, src, !span))) return r;  // first detected window: [S, W + S)
-  CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
+  if ((r = stage_stream(h, pts, used, &src, &host, false))) return r;
+  // first detected window: [S, W + S)
+  if ((r = configure(h, MODE_RUN, B, S, src, !span, false))) return r;
+  const int64_t blocks = used / S + 1;
   // A host stream is copied in pieces on a second stream: piece i holds the
   // points batch i needs beyond the earlier pieces ([0, W + B S) for the
   // first), so detection of a batch overlaps the copy of the next pieces.
@@ -954,9 +969,6 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
     h->launches++;
     return RTOD_OK;
   };
-  CU(cudaEventRecord(h->ev[1], h->stream));  // start of the key kernel (profile)
-  if ((r = keys(0, 0, host ? piece_end(0) : used))) return r;
-  if (e_keys) CU(cudaEventRecord(e_keys, h->stream));
   const int64_t out_cap = std::min(ids_cap, h->ids_cap);
   const int64_t full = slides / B, rem = slides % B;
   Batch bfull = make_batch(h, B, out_cap);
@@ -965,37 +977,84 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
   EventSet chunk_es;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> chunk_ev;
   if (span) bfull.span = h->span.sc;
-  for (int64_t i = 0; i < full + (rem ? 1 : 0); ++i) {
-    Batch b = bfull;
-    Span sp = sfull;
-    if (i == full) {
-      b = make_batch(h, (int)rem, out_cap);
-      if (span) {
-        b.span = h->span.sc;
-        sp = make_span(h, (int)rem, src, chunk);
+  // a whole run as one graph: span engine, device-resident stream, no stage events
+  const bool whole = span && !host && h->cfg.use_graph && !kev;
+  // Everything from the scratch resets to the last compaction.
+  auto enqueue = [&]() -> int {
+    // +inf / -inf patterns for the atomic min / max of k_keys
+    CU(cudaMemsetAsync(h->run_blk_lo, 0x7f, (size_t)(blocks * 3) * sizeof(long long), h->stream));
+    CU(cudaMemsetAsync(h->run_blk_hi, 0x80, (size_t)(blocks * 3) * sizeof(long long), h->stream));
+    CU(cudaMemcpyAsync(h->ctr, h->ctr_init, sizeof(JobCtr) * B, cudaMemcpyHostToDevice, h->stream));
+    CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
+    if (!whole) CU(cudaEventRecord(h->ev[1], h->stream));  // start of the key kernel (profile)
+    int rr;
+    if ((rr = keys(0, 0, host ? piece_end(0) : used))) return rr;
+    if (e_keys && !whole) CU(cudaEventRecord(e_keys, h->stream));
+    for (int64_t i = 0; i < full + (rem ? 1 : 0); ++i) {
+      Batch b = bfull;
+      Span sp = sfull;
+      if (i == full) {
+        b = make_batch(h, (int)rem, out_cap);
+        if (span) {
+          b.span = h->span.sc;
+          sp = make_span(h, (int)rem, src, chunk);
+        }
       }
-    }
-    const Span* spp = span ? &sp : nullptr;
-    if (host && i > 0 && (r = keys(i, piece_end(i - 1), piece_end(i)))) return r;
-    if (kev) {
-      cudaEvent_t* e = &(*kev)[(size_t)i * 8];
-      CU(cudaEventRecord(e[0], h->stream));
-      r = launch_batch(h, b, false, e + 1, spp);
-    } else {
-      r = i < full ? run_batch(h, b, false, spp) : launch_batch(h, b, false, nullptr, spp);
-    }
-    if (r) return r;
-    const bool last = i + 1 == full + (rem ? 1 : 0);
-    if (span && ((i + 1) % chunk_batches == 0 || last)) {
-      const int64_t s1 = std::min(slides, (i + 1) * (int64_t)B);
-      const int64_t s0 = ((s1 - 1) / chunk) * chunk;
+      const Span* spp = span ? &sp : nullptr;
+      if (host && i > 0 && (rr = keys(i, piece_end(i - 1), piece_end(i)))) return rr;
       if (kev) {
-        chunk_ev.emplace_back(chunk_es.make(), chunk_es.make());
-        CU(cudaEventRecord(chunk_ev.back().first, h->stream));
+        cudaEvent_t* e = &(*kev)[(size_t)i * 8];
+        CU(cudaEventRecord(e[0], h->stream));
+        rr = launch_batch(h, b, false, e + 1, spp);
+      } else {
+        rr = (i < full && !whole) ? run_batch(h, b, false, spp) : launch_batch(h, b, false, nullptr, spp);
       }
-      if ((r = span_flush(h, sfull, s0, s1 - s0, out_cap))) return r;
-      if (kev) CU(cudaEventRecord(chunk_ev.back().second, h->stream));
+      if (rr) return rr;
+      const bool last = i + 1 == full + (rem ? 1 : 0);
+      if (span && ((i + 1) % chunk_batches == 0 || last)) {
+        const int64_t s1 = std::min(slides, (i + 1) * (int64_t)B);
+        const int64_t s0 = ((s1 - 1) / chunk) * chunk;
+        if (kev) {
+          chunk_ev.emplace_back(chunk_es.make(), chunk_es.make());
+          CU(cudaEventRecord(chunk_ev.back().first, h->stream));
+        }
+        if ((rr = span_flush(h, sfull, s0, s1 - s0, out_cap))) return rr;
+        if (kev) CU(cudaEventRecord(chunk_ev.back().second, h->stream));
+      }
     }
+    return RTOD_OK;
+  };
+  if (whole) {
+    // key of the captured run: stream, sizes and the batch / span parameters
+    std::vector<unsigned char> key(sizeof(void*) + 4 * sizeof(int64_t) + sizeof(Batch) + sizeof(Span));
+    unsigned char* k = key.data();
+    const int64_t ints[4] = {slides, out_cap, chunk, (int64_t)B};
+    std::memcpy(k, &src, sizeof(void*));
+    std::memcpy(k + sizeof(void*), ints, sizeof ints);
+    std::memcpy(k + sizeof(void*) + sizeof ints, &bfull, sizeof(Batch));
+    std::memcpy(k + sizeof(void*) + sizeof ints + sizeof(Batch), &sfull, sizeof(Span));
+    if (!h->run_graph || key != h->run_graph_key) {
+      if (h->run_graph) cudaGraphExecDestroy(h->run_graph);
+      h->run_graph = nullptr;
+      const int64_t l0 = h->launches;
+      cudaGraph_t g;
+      CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      r = enqueue();
+      cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+      if (r) return r;
+      if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+      e = cudaGraphInstantiate(&h->run_graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
+      h->run_graph_key = key;
+      h->run_graph_kernels = h->launches - l0;
+      h->launches = l0;
+    }
+    CU(cudaGraphLaunch(h->run_graph, h->stream));
+    h->launches += h->run_graph_kernels;
+    h->graph_replays++;
+  } else {
+    if ((r = enqueue())) return r;
   }
   if (e_end) CU(cudaEventRecord(e_end, h->stream));
   // Counters and per-slide records through one pinned buffer: async copies
