@@ -97,6 +97,28 @@ bool is_device_ptr(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Whether kernels on `device` can read and write p directly: memory of that
+// device, managed memory, or pinned (page-locked) host memory.
+bool device_addressable(const void* p, int device) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (a.type == cudaMemoryTypeManaged || a.type == cudaMemoryTypeHost) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == device;
+}
+
+// Pinned (page-locked) host memory.
+bool pinned_host_ptr(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
 template <typename T>
 int dalloc(T** p, size_t count, int64_t* counter) {
   *p = nullptr;
@@ -298,6 +320,7 @@ struct rtod_handle {
 
   cudaEvent_t ev[16] = {};
   cudaStream_t copy_stream = nullptr;     // host-stream pieces, overlapped with detection
+  cudaEvent_t fork_ev = nullptr;          // the copy stream's start on the library stream
   std::vector<cudaEvent_t> piece_ev;      // one per piece
   void* host_rb = nullptr;  // pinned read-back of the run's counters and per-slide records
   size_t host_rb_bytes = 0;
@@ -602,13 +625,13 @@ int configure(rtod_handle* h, int mode, int jobs, int64_t first_lo, const void* 
   return RTOD_OK;
 }
 
-Batch make_batch(rtod_handle* h, int njobs, int64_t out_cap) {
+Batch make_batch(rtod_handle* h, int njobs, int64_t out_cap, int64_t* out_ids = nullptr) {
   Batch b{};
   b.jobs = h->jobs_dev;
   b.njobs = njobs;
   b.bs = h->bs;
   b.router = h->router;
-  b.out_ids = h->ids;
+  b.out_ids = out_ids ? out_ids : h->ids;
   b.out_cap = out_cap;
   b.cmp_tiles = (int64_t)njobs * ((h->W + CMP_TILE - 1) / CMP_TILE);
   return b;
@@ -713,7 +736,7 @@ int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, 
 }
 
 // Deferred compaction of span-engine slides [s0, s0 + n) (one bitset chunk).
-int span_flush(rtod_handle* h, const Span& sp, int64_t s0, int64_t n, int64_t out_cap) {
+int span_flush(rtod_handle* h, const Span& sp, int64_t s0, int64_t n, int64_t out_cap, int64_t* out_ids) {
   SpanOut o{};
   o.bits = sp.bits;
   o.words = sp.words;
@@ -722,7 +745,7 @@ int span_flush(rtod_handle* h, const Span& sp, int64_t s0, int64_t n, int64_t ou
   o.S = h->S;
   o.rec_nout = h->rec_nout;
   o.base = h->span.base;
-  o.out_ids = h->ids;
+  o.out_ids = out_ids;
   o.out_cap = out_cap;
   o.bs = h->bs;
   CU(launch_k(k_slide_base, dim3(1), 1024, h->stream, o, s0, n));
@@ -839,10 +862,11 @@ int ensure_records(rtod_handle* h, int64_t n) {
 // Room for a stream of `used` points: the handle's run buffer for a host
 // stream (*host = true; run_stream copies it in), its keys and features.
 int stage_stream(rtod_handle* h, const void* pts, int64_t used, const void** src, bool* host,
-                 bool memsets = true) {
+                 bool memsets = true, bool* pinned = nullptr) {
   const int64_t D = h->D;
   *src = pts;
   *host = !is_device_ptr(pts);
+  if (pinned) *pinned = *host && pinned_host_ptr(pts);
   if (*host) {
     if (h->run_buf_cap < used * D) {
       if (h->run_buf) h->device_bytes -= h->run_buf_cap * h->esz;
@@ -918,21 +942,28 @@ int64_t count_slides(const rtod_handle* h, int64_t n, int64_t max_slides) {
 // router's training step, or right after k_compact without router).
 int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap, cudaEvent_t e_begin,
                cudaEvent_t e_keys, cudaEvent_t e_end, std::vector<cudaEvent_t>* kev, BatchState* out_state,
-               std::vector<int32_t>* nout, std::vector<int32_t>* nund) {
+               std::vector<int32_t>* nout, std::vector<int32_t>* nund, int64_t* out_ids = nullptr,
+               bool* direct = nullptr) {
   const int64_t W = h->W, S = h->S;
   const int64_t used = W + slides * S;
   int r;
   const void* src;
   if ((r = ensure_records(h, slides))) return r;
-  if ((r = ensure_ids(h, std::max<int64_t>(1, std::min(ids_cap, slides * W))))) return r;
+  // Outlier IDs go straight to the caller's buffer when it is memory of this
+  // device; otherwise to the handle's buffer and out in one copy by the
+  // caller (one bulk copy beats scattered device writes into host memory).
+  const bool to_user = out_ids && ids_cap > 0 && is_device_ptr(out_ids) && device_addressable(out_ids, h->device);
+  if (direct) *direct = to_user;
+  if (!to_user && (r = ensure_ids(h, std::max<int64_t>(1, std::min(ids_cap, slides * W))))) return r;
+  int64_t* const dst = to_user ? out_ids : h->ids;
   const bool span = use_span(h);
   const int B = pick_batch(h, slides);
   if ((r = ensure_pool(h, B, !span))) return r;
   const int64_t chunk = span ? span_chunk(h, B, slides) : 0;
   if (span && (r = ensure_span(h, W / S + B - 1, chunk))) return r;
   if (e_begin) CU(cudaEventRecord(e_begin, h->stream));
-  bool host = false;
-  if ((r = stage_stream(h, pts, used, &src, &host, false))) return r;
+  bool host = false, pinned = false;
+  if ((r = stage_stream(h, pts, used, &src, &host, false, &pinned))) return r;
   // first detected window: [S, W + S)
   if ((r = configure(h, MODE_RUN, B, S, src, !span, false))) return r;
   const int64_t blocks = used / S + 1;
@@ -943,21 +974,26 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
   auto piece_end = [&](int64_t i) { return std::min(used, W + (i + 1) * (int64_t)B * S); };
   if (host) {
     if (!h->copy_stream) CU(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    if (!h->fork_ev) CU(cudaEventCreateWithFlags(&h->fork_ev, cudaEventDisableTiming));
     while ((int64_t)h->piece_ev.size() < nbatch) {
       cudaEvent_t e;
       CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       h->piece_ev.push_back(e);
     }
-    if (e_begin) CU(cudaStreamWaitEvent(h->copy_stream, e_begin, 0));
-    const int64_t D = h->D;
+  }
+  // the pieces, on the copy stream forked from the library stream
+  auto copy_pieces = [&]() -> int {
+    CU(cudaEventRecord(h->fork_ev, h->stream));
+    CU(cudaStreamWaitEvent(h->copy_stream, h->fork_ev, 0));
+    const int64_t D = h->D, es = h->esz;
     for (int64_t i = 0; i < nbatch; ++i) {
       const int64_t a = i ? piece_end(i - 1) : 0, e = piece_end(i);
-      const int64_t es = h->esz;
       CU(cudaMemcpyAsync(h->run_buf + a * D * es, (const unsigned char*)pts + a * D * es, (size_t)((e - a) * D * es),
                          cudaMemcpyHostToDevice, h->copy_stream));
       CU(cudaEventRecord(h->piece_ev[(size_t)i], h->copy_stream));
     }
-  }
+    return RTOD_OK;
+  };
   const unsigned kgrid = (unsigned)h->sm_count * 8;
   // cell keys of points [a, b) (and their slide blocks' coordinate ranges),
   // after their piece has arrived
@@ -969,16 +1005,17 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
     h->launches++;
     return RTOD_OK;
   };
-  const int64_t out_cap = std::min(ids_cap, h->ids_cap);
+  const int64_t out_cap = to_user ? ids_cap : std::min(ids_cap, h->ids_cap);
   const int64_t full = slides / B, rem = slides % B;
-  Batch bfull = make_batch(h, B, out_cap);
+  Batch bfull = make_batch(h, B, out_cap, dst);
   const Span sfull = span ? make_span(h, B, src, chunk) : Span{};
   const int64_t chunk_batches = span ? chunk / B : 0;
   EventSet chunk_es;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> chunk_ev;
   if (span) bfull.span = h->span.sc;
-  // a whole run as one graph: span engine, device-resident stream, no stage events
-  const bool whole = span && !host && h->cfg.use_graph && !kev;
+  // a whole run as one graph: span engine, a device-resident or pinned host
+  // stream (a graph's copy may not read pageable memory), no stage events
+  const bool whole = span && (!host || pinned) && h->cfg.use_graph && !kev;
   // Everything from the scratch resets to the last compaction.
   auto enqueue = [&]() -> int {
     // +inf / -inf patterns for the atomic min / max of k_keys
@@ -986,15 +1023,16 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
     CU(cudaMemsetAsync(h->run_blk_hi, 0x80, (size_t)(blocks * 3) * sizeof(long long), h->stream));
     CU(cudaMemcpyAsync(h->ctr, h->ctr_init, sizeof(JobCtr) * B, cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
-    if (!whole) CU(cudaEventRecord(h->ev[1], h->stream));  // start of the key kernel (profile)
     int rr;
+    if (host && (rr = copy_pieces())) return rr;
+    if (!whole) CU(cudaEventRecord(h->ev[1], h->stream));  // start of the key kernel (profile)
     if ((rr = keys(0, 0, host ? piece_end(0) : used))) return rr;
     if (e_keys && !whole) CU(cudaEventRecord(e_keys, h->stream));
     for (int64_t i = 0; i < full + (rem ? 1 : 0); ++i) {
       Batch b = bfull;
       Span sp = sfull;
       if (i == full) {
-        b = make_batch(h, (int)rem, out_cap);
+        b = make_batch(h, (int)rem, out_cap, dst);
         if (span) {
           b.span = h->span.sc;
           sp = make_span(h, (int)rem, src, chunk);
@@ -1018,7 +1056,7 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
           chunk_ev.emplace_back(chunk_es.make(), chunk_es.make());
           CU(cudaEventRecord(chunk_ev.back().first, h->stream));
         }
-        if ((rr = span_flush(h, sfull, s0, s1 - s0, out_cap))) return rr;
+        if ((rr = span_flush(h, sfull, s0, s1 - s0, out_cap, dst))) return rr;
         if (kev) CU(cudaEventRecord(chunk_ev.back().second, h->stream));
       }
     }
@@ -1029,7 +1067,7 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
     std::vector<unsigned char> key(sizeof(void*) + 4 * sizeof(int64_t) + sizeof(Batch) + sizeof(Span));
     unsigned char* k = key.data();
     const int64_t ints[4] = {slides, out_cap, chunk, (int64_t)B};
-    std::memcpy(k, &src, sizeof(void*));
+    std::memcpy(k, &pts, sizeof(void*));  // the caller's stream (host pieces are copied from it)
     std::memcpy(k + sizeof(void*), ints, sizeof ints);
     std::memcpy(k + sizeof(void*) + sizeof ints, &bfull, sizeof(Batch));
     std::memcpy(k + sizeof(void*) + sizeof ints + sizeof(Batch), &sfull, sizeof(Span));
@@ -1108,6 +1146,8 @@ void free_all(rtod_handle* h) {
     if (e) cudaEventDestroy(e);
   for (auto e : h->piece_ev) cudaEventDestroy(e);
   h->piece_ev.clear();
+  if (h->fork_ev) cudaEventDestroy(h->fork_ev);
+  h->fork_ev = nullptr;
   if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   h->copy_stream = nullptr;
   if (h->stream) cudaStreamDestroy(h->stream);
@@ -1552,12 +1592,14 @@ int run_impl(rtod_handle* h, const void* pts, int64_t n, int64_t max_slides, int
   }
   BatchState s{};
   std::vector<int32_t> nout, nund;
-  int r = run_stream(h, pts, slides, ids_cap, t0, t1, t2, stage ? &kev : nullptr, &s, &nout, &nund);
+  bool direct = false;
+  int r = run_stream(h, pts, slides, ids_cap, t0, t1, t2, stage ? &kev : nullptr, &s, &nout, &nund, out_ids,
+                     &direct);
   if (r) return r;
   for (int64_t j = 0; j < slides; ++j) out_offsets[j + 1] = out_offsets[j] + nout[j];
   if (out_offsets[slides] != s.out_total) return fail(RTOD_ERR_CUDA, "inconsistent outlier totals");
   CU(cudaEventRecord(d0, h->stream));
-  if (s.out_total > 0)
+  if (!direct && s.out_total > 0)  // the IDs are in the handle's buffer
     CU(cudaMemcpyAsync(out_ids, h->ids, (size_t)s.out_total * sizeof(int64_t), cudaMemcpyDefault, h->stream));
   CU(cudaEventRecord(d1, h->stream));
   CU(cudaStreamSynchronize(h->stream));
