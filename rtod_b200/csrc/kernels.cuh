@@ -1,4 +1,8 @@
-// Device code of the detector pipeline (sm_100a), batched over jobs.
+// Device code of the detector pipeline (sm_100a), batched over jobs: the
+// window engine (one counting sort per window; push/detect, the
+// multi-stream API, and rtod_run when chosen). span.cuh holds the span
+// engine of rtod_run (one counting sort per batch of consecutive windows),
+// which shares this file's cell keys, predicates, scans and finish_batch.
 //
 // A job is the detection of one window of one stream. Every kernel takes a
 // Batch (a table of jobs) and uses blockIdx.y as the job index, so one launch
@@ -37,9 +41,9 @@
 //
 // Scratch arrays clean up after themselves for the next batch: k_scatter
 // hands bin counts back to zero (it claims positions with atomicSub),
-// k_count resets the per-bin key ranges and the compaction look-back words, k_compact
-// clears the outlier bits it read, and the last k_compact block resets the
-// per-job counters. Consecutive kernels use programmatic dependent launch:
+// k_count resets the per-bin key ranges and the compaction look-back words,
+// k_compact clears the outlier bits it read, and its last block ends the
+// batch (finish_batch: per-slide records, window advance, per-job counters). Consecutive kernels use programmatic dependent launch:
 // each kernel lets the next one launch early and waits (griddepcontrol.wait)
 // for its predecessor to complete before touching shared data.
 #pragma once
