@@ -213,8 +213,8 @@ def algorithmic_bytes(kernel: str, w, n_out_per_slide: float, undet_per_slide: f
         "k_compact": W / 8 + 8 * n_out_per_slide,             # read the outlier bits, write IDs
         "k_keys": 4 * d * S + 8 * S,                          # per slide: read points, write keys
         "k_train": 2048 * 16 + 3 * 1316 * 4 * 2,              # samples + params/moments (per batch)
-        # span engine: read the span's keys once per batch
-        "k_span_hist": 8 * span_pts / batch,
+        # span engine: read the span's points, write their keys, once per batch
+        "k_span_hist": (4 * d + 8) * span_pts / batch,
         # read counts, write starts; per bin in use, its per-block counts and prefixes
         "k_span_scan+k_span_prefix": (4 * 65536 * 2 + 8 * used_bins * (W // S + batch)) / batch,
         # read keys + points, write bin-ordered offsets + coordinates, once per batch
@@ -225,7 +225,7 @@ def algorithmic_bytes(kernel: str, w, n_out_per_slide: float, undet_per_slide: f
         # per group of one bin and shared by its points: not counted)
         "k_span_count": undet_per_slide * (4 + 4 * d),
         # per slide: its bitset row, its outlier IDs
-        "k_slide_base+k_span_compact": W / 8 + 8 * n_out_per_slide,
+        "k_span_compact": W / 8 + 8 * n_out_per_slide,
     }[kernel]
 
 
@@ -370,7 +370,7 @@ def emit_ours(args, world, w, res):
     peak, peak_kind = hbm_peak()
     # per launch: pipeline kernels run once per batch of windows, the key
     # kernel and the chunk compaction once per pass over the stream
-    per_launch = slides if dom in ("k_keys", "k_slide_base+k_span_compact") else batch
+    per_launch = slides if dom in ("k_keys", "k_span_compact") else batch
     launch_ms = prof[dom] * per_launch
     achieved = alg * per_launch / (launch_ms / 1e3) / 1e9
     traffic = ncu_traffic(dom)

@@ -183,9 +183,10 @@ int rtod_get_stats(const rtod_handle* h, int64_t out[5]);
    scatter, count, compact, and the router's training step), to
    kernel_ms[0..n_kernels). A batch of B windows shares one launch of each
    kernel; its time is divided by B. With the span engine the seven slots
-   hold its kernels: keys, k_span_hist, k_span_scan + k_span_prefix,
-   k_span_scatter, k_span_classify, k_span_count, and the compaction of each
-   chunk of slides (k_slide_base + k_span_compact).
+   hold its kernels: keys (none: k_span_hist computes them), k_span_hist,
+   k_span_scan + k_span_prefix, k_span_scatter, k_span_classify,
+   k_span_count, and the compaction of each chunk of slides
+   (k_span_compact).
    The stage names are given by rtod_kernel_name(i). Results are discarded.
    No counterpart in RTOD (it times stages with gettimeofday, src/ods/timer.h). */
 int rtod_profile_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides,

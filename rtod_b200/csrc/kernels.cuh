@@ -90,7 +90,6 @@ struct BatchState {
   int64_t undet_total;  // queued points summed over windows
   int32_t err;          // DERR_*
   uint32_t done;        // finished blocks of the running batch's last kernel
-  int64_t ids_done;     // outlier IDs written by the deferred compaction so far
 };
 
 // Span engine counters (device), one per handle, and the per-bin arrays
@@ -98,8 +97,10 @@ struct BatchState {
 struct SpanCtr {
   uint32_t scan_ticket;  // tile tickets of the span's bin scan
   uint32_t n_used;       // bins holding span points
-  int32_t pure;          // no two cells of the span share a bin
+  int32_t pure;          // the span's cells and their sure neighbours map to distinct bins (k_span_scan)
   uint32_t n_groups;     // groups listed for exact counts in the running batch
+  long long cmin[3];     // per hashed dimension, the span's cell coordinate range (k_span_hist)
+  long long cmax[3];
   uint32_t* used;        // [NB] bins in use
   uint32_t* bin_count;   // [NB]
   unsigned long long* kmin;  // [NB]
@@ -140,6 +141,7 @@ struct Job {
   JobCtr* ctr;
   int32_t* rec_nout;      // per-slide outlier counts, indexed (lo - S) / S; may be null
   int32_t* rec_undet;
+  int64_t* rec_base;      // per-slide output offset of its outlier IDs (span batches)
   int64_t rec_cap;
 };
 
@@ -513,12 +515,29 @@ struct Unroll {
 };
 
 // Whether no two cells of slide blocks [b0, b0 + nb) of a resident stream
-// can share a bin, from the per-block coordinate ranges (a ring has none).
-// The bin map is injective on boxes of at most 65536 cells (1-d),
-// 256 x 256 (2-d) or 16 x 64 x 64 (3-d). One warp computes it.
+// can share a bin, nor a cell share one with a neighbour within margin/2 of
+// another, from the per-block coordinate ranges (a ring has none). The bin
+// map is injective on boxes of at most 65536 cells (1-d), 256 x 256 (2-d)
+// or 16 x 64 x 64 (3-d). One warp computes it.
+// Whether cells within [mn_d - margin/2, mx_d + margin/2] per dimension map
+// to distinct bins: then no two cells of the range share a bin, and a
+// neighbour k + d (|d_i| <= margin/2) of a cell k of the range lies in a bin
+// that holds cell k + d or nothing.
+template <int H>
+__device__ __forceinline__ bool box_pure(const long long* mn, const long long* mx, int margin) {
+  bool ok = true;
+#pragma unroll
+  for (int d = 0; d < H; ++d) {
+    const long long span = mx[d] - mn[d] + 1 + margin;
+    const long long cap = H == 1 ? 65536 : (H == 2 ? 256 : (d == 0 ? 16 : 64));
+    ok &= span <= cap;
+  }
+  return ok;
+}
+
 template <int H>
 __device__ __forceinline__ bool range_pure(const long long* blk_lo, const long long* blk_hi, int64_t b0,
-                                           int64_t nb) {
+                                           int64_t nb, int margin) {
   if (!blk_lo || nb > 4096) return false;
   const int lane = threadIdx.x & 31;
   long long mn[3] = {LLONG_MAX, LLONG_MAX, LLONG_MAX}, mx[3] = {LLONG_MIN, LLONG_MIN, LLONG_MIN};
@@ -529,7 +548,6 @@ __device__ __forceinline__ bool range_pure(const long long* blk_lo, const long l
       mx[d] = max(mx[d], blk_hi[(b0 + t) * 3 + d]);
     }
   }
-  bool ok = true;
 #pragma unroll
   for (int d = 0; d < H; ++d) {
 #pragma unroll
@@ -537,17 +555,15 @@ __device__ __forceinline__ bool range_pure(const long long* blk_lo, const long l
       mn[d] = min(mn[d], __shfl_xor_sync(0xffffffffu, mn[d], o));
       mx[d] = max(mx[d], __shfl_xor_sync(0xffffffffu, mx[d], o));
     }
-    const long long span = mx[d] - mn[d] + 1;
-    const long long cap = H == 1 ? 65536 : (H == 2 ? 256 : (d == 0 ? 16 : 64));
-    ok &= span <= cap;
   }
-  return ok;
+  return box_pure<H>(mn, mx, margin);
 }
 
-// The same test for the job's current window.
+// The same test for the job's current window, with room for the 1-d group
+// rule's neighbours (cells within n-2).
 template <int H>
 __device__ __forceinline__ bool window_pure(const Job& jb, int64_t lo) {
-  return range_pure<H>(jb.blk_lo, jb.blk_hi, lo / jb.S, jb.W / jb.S);
+  return range_pure<H>(jb.blk_lo, jb.blk_hi, lo / jb.S, jb.W / jb.S, 2 * max(jb.n - 2, 0));
 }
 
 
@@ -1247,16 +1263,44 @@ __global__ void __launch_bounds__(256) k_count(Batch b) {
 
 // ---------------------------------------------------------------------------
 // End of a batch, run by the block of the batch's last kernel that finishes
-// last (after a fence): per-slide records, window advance, per-job counter
-// reset and the batch totals. Every thread of the block calls it.
+// last (after a fence): per-slide records (outlier count, counted points and,
+// where kept, the slide's output offset in window order), window advance,
+// per-job counter reset and the batch totals. Every thread of the block
+// calls it.
 // ---------------------------------------------------------------------------
 __device__ void finish_batch(const Batch& b) {
   __shared__ int64_t s_red[3][32];
+  __shared__ int64_t s_scan[33];
   BatchState* bs = b.bs;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (int)(blockDim.x >> 5);
   __threadfence();
+  // jobs in contiguous runs per thread, so that an exclusive scan over the
+  // threads gives each slide its output offset in window order
+  const int per = (b.njobs + (int)blockDim.x - 1) / (int)blockDim.x;
+  const int j0 = min(b.njobs, (int)threadIdx.x * per), j1 = min(b.njobs, j0 + per);
+  int64_t mine = 0;
+  for (int j = j0; j < j1; ++j)
+    if (!b.active || b.active[j]) mine += *(volatile int32_t*)&b.jobs[j].ctr->n_out;
+  int64_t inc = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) s_scan[wid] = inc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t run = bs->out_total;  // IDs of the earlier batches
+    for (int w = 0; w < nw; ++w) {
+      const int64_t t = s_scan[w];
+      s_scan[w] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+  int64_t base = s_scan[wid] + inc - mine;
   int64_t add = 0, und = 0, nact = 0;
-  for (int j = threadIdx.x; j < b.njobs; j += blockDim.x) {
+  for (int j = j0; j < j1; ++j) {
     if (b.active && !b.active[j]) {
       if (b.job_nout) b.job_nout[j] = 0;
       continue;
@@ -1269,7 +1313,9 @@ __device__ void finish_batch(const Batch& b) {
     if (J.rec_nout && slide >= 0 && slide < J.rec_cap) {
       J.rec_nout[slide] = nout;
       J.rec_undet[slide] = nund;
+      if (J.rec_base) J.rec_base[slide] = base;
     }
+    base += nout;
     add += nout;
     und += nund;
     nact += 1;
@@ -1307,6 +1353,10 @@ __device__ void finish_batch(const Batch& b) {
     if (b.span) {
       b.span->n_used = 0;
       b.span->n_groups = 0;
+      for (int d = 0; d < 3; ++d) {
+        b.span->cmin[d] = LLONG_MAX;
+        b.span->cmax[d] = LLONG_MIN;
+      }
     }
   }
 }

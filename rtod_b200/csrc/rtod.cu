@@ -192,7 +192,6 @@ struct SpanScratch {
   SpanCtr* sc = nullptr;
   uint4* groups = nullptr;    // [windows][min(W, NB)] listed groups of a batch
   uint32_t* bits = nullptr;   // [chunk][words] per-slide outlier bitsets
-  int64_t* base = nullptr;    // [chunk] output offsets of a chunk's slides
   int64_t nblk_cap = 0;
   int64_t pts_cap = 0;
   int64_t chunk_cap = 0;
@@ -294,6 +293,7 @@ struct rtod_handle {
   int64_t run_blk_cap = 0;
   int32_t* rec_nout = nullptr;
   int32_t* rec_undet = nullptr;
+  int64_t* rec_base = nullptr;  // per-slide output offsets (span engine)
   int64_t rec_cap = 0;
   int64_t* ids = nullptr;
   int64_t ids_cap = 0;
@@ -434,7 +434,13 @@ int scrub(rtod_handle* h) {
     CU(cudaMemsetAsync(sp.kmax, 0, NB * sizeof(unsigned long long), h->stream));
     CU(cudaMemsetAsync(sp.cnt, 0, (size_t)(sp.nblk_cap * NB) * sizeof(uint32_t), h->stream));
     CU(cudaMemsetAsync(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long), h->stream));
-    CU(cudaMemsetAsync(sp.sc, 0, offsetof(SpanCtr, used), h->stream));  // counters only
+    SpanCtr c{};  // counters back to their starting values
+    for (int d = 0; d < 3; ++d) {
+      c.cmin[d] = LLONG_MAX;
+      c.cmax[d] = LLONG_MIN;
+    }
+    CU(cudaStreamSynchronize(h->stream));
+    CU(cudaMemcpy(sp.sc, &c, offsetof(SpanCtr, used), cudaMemcpyHostToDevice));
     CU(cudaMemsetAsync(sp.bits, 0, (size_t)(sp.chunk_cap * ((h->W + 31) / 32)) * sizeof(uint32_t), h->stream));
   }
   CU(cudaMemsetAsync(h->ctr, 0, sizeof(JobCtr) * kMaxJobs, h->stream));
@@ -446,7 +452,7 @@ void free_span(rtod_handle* h) {
   SpanScratch& sp = h->span;
   dfree(sp.bin_count); dfree(sp.bin_start); dfree(sp.kmin); dfree(sp.kmax); dfree(sp.cnt); dfree(sp.pre);
   dfree(sp.used); dfree(sp.s_off); dfree(sp.s_x); dfree(sp.scan_status); dfree(sp.sc);
-  dfree(sp.bits); dfree(sp.base); dfree(sp.groups);
+  dfree(sp.bits); dfree(sp.groups);
   h->device_bytes -= sp.bytes;
   sp = SpanScratch{};
 }
@@ -469,7 +475,6 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
             !dalloc(&sp.used, NB, &bytes) && !dalloc(&sp.s_off, (size_t)pts, &bytes) &&
             !dalloc(&sp.s_x, (size_t)(Wp * h->D * h->esz), &bytes) && !dalloc(&sp.scan_status, SCAN_TILES, &bytes) &&
             !dalloc(&sp.sc, 1, &bytes) && !dalloc(&sp.bits, (size_t)(chunk * words), &bytes) &&
-            !dalloc(&sp.base, (size_t)chunk, &bytes) &&
             !dalloc(&sp.groups, (size_t)((nblk - h->W / h->S + 1) * std::min<int64_t>(h->W, NB)), &bytes);
   sp.bytes = bytes;
   h->device_bytes += bytes;
@@ -489,6 +494,10 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
   CU(cudaMemset(sp.s_x, 0, (size_t)(Wp * h->D * h->esz)));
   CU(cudaMemset(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long)));
   SpanCtr c{};
+  for (int d = 0; d < 3; ++d) {
+    c.cmin[d] = LLONG_MAX;
+    c.cmax[d] = LLONG_MIN;
+  }
   c.used = sp.used;
   c.bin_count = sp.bin_count;
   c.kmin = sp.kmin;
@@ -529,8 +538,7 @@ Span make_span(const rtod_handle* h, int B, const void* stream_pts, int64_t chun
   sp.R2f = h->R2f;
   sp.pts = stream_pts;
   sp.keys = h->run_keys;
-  sp.blk_lo = h->run_blk_lo;
-  sp.blk_hi = h->run_blk_hi;
+  sp.inv_cell = 1.0 / h->cell;
   sp.bin_count = ss.bin_count;
   sp.bin_start = ss.bin_start;
   sp.kmin = ss.kmin;
@@ -593,6 +601,7 @@ Job make_job(rtod_handle* h, int j, bool ring, const void* stream_pts) {
   jb.ctr = h->ctr + j;
   jb.rec_nout = ring ? nullptr : h->rec_nout;
   jb.rec_undet = ring ? nullptr : h->rec_undet;
+  jb.rec_base = ring ? nullptr : h->rec_base;
   jb.rec_cap = ring ? 0 : h->rec_cap;
   return jb;
 }
@@ -717,7 +726,7 @@ int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, 
   const int64_t npts = sp.nblk * sp.S;
   const int64_t hx = std::max<int64_t>(1, std::min<int64_t>((npts + 1023) / 1024, (int64_t)g.sm_count * 8));
   if (kev) CU(cudaEventRecord(kev[0], st));
-  DISPATCH_D(g.D, CU(launch_k(k_span_hist<D>, dim3((unsigned)hx), 256, st, b, sp)));
+  DISPATCH_DT(g.f64, g.D, CU(launch_k(k_span_hist<D, T>, dim3((unsigned)hx), 256, st, b, sp)));
   if (kev) CU(cudaEventRecord(kev[1], st));
   CU(launch_k(k_span_scan, dim3(SCAN_TILES), 256, st, b, sp));
   CU(launch_k(k_span_prefix, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
@@ -743,14 +752,12 @@ int span_flush(rtod_handle* h, const Span& sp, int64_t s0, int64_t n, int64_t ou
   o.chunk = sp.chunk;
   o.W = h->W;
   o.S = h->S;
-  o.rec_nout = h->rec_nout;
-  o.base = h->span.base;
+  o.rec_base = h->rec_base;
   o.out_ids = out_ids;
   o.out_cap = out_cap;
   o.bs = h->bs;
-  CU(launch_k(k_slide_base, dim3(1), 1024, h->stream, o, s0, n));
   CU(launch_k(k_span_compact, dim3((unsigned)n), 1024, h->stream, o, s0));
-  h->launches += 2;
+  h->launches += 1;
   return RTOD_OK;
 }
 
@@ -849,11 +856,13 @@ int ensure_ids(rtod_handle* h, int64_t cap) {
 
 int ensure_records(rtod_handle* h, int64_t n) {
   if (n <= h->rec_cap) return RTOD_OK;
-  if (h->rec_nout) h->device_bytes -= h->rec_cap * 8;
+  if (h->rec_nout) h->device_bytes -= h->rec_cap * 16;
   dfree(h->rec_nout);
   dfree(h->rec_undet);
+  dfree(h->rec_base);
   h->rec_cap = 0;
-  if (dalloc(&h->rec_nout, (size_t)n, &h->device_bytes) || dalloc(&h->rec_undet, (size_t)n, &h->device_bytes))
+  if (dalloc(&h->rec_nout, (size_t)n, &h->device_bytes) || dalloc(&h->rec_undet, (size_t)n, &h->device_bytes) ||
+      dalloc(&h->rec_base, (size_t)n, &h->device_bytes))
     return RTOD_ERR_CUDA;
   h->rec_cap = n;
   return RTOD_OK;
@@ -996,9 +1005,11 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
   };
   const unsigned kgrid = (unsigned)h->sm_count * 8;
   // cell keys of points [a, b) (and their slide blocks' coordinate ranges),
-  // after their piece has arrived
+  // after their piece has arrived; the span engine computes them in
+  // k_span_hist
   auto keys = [&](int64_t i, int64_t a, int64_t b) -> int {
     if (host) CU(cudaStreamWaitEvent(h->stream, h->piece_ev[(size_t)i], 0));
+    if (span) return RTOD_OK;
     const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((b - a + 255) / 256, kgrid));
     DISPATCH_DT(h->f64, h->D, CU(launch_k(k_keys<D, T>, dim3(kx), 256, h->stream, (const T*)src, a, b, 1.0 / h->cell,
                                           h->run_keys, h->run_prev, h->bs, h->S, h->run_blk_lo, h->run_blk_hi)));
@@ -1018,9 +1029,10 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
   const bool whole = span && (!host || pinned) && h->cfg.use_graph && !kev;
   // Everything from the scratch resets to the last compaction.
   auto enqueue = [&]() -> int {
-    // +inf / -inf patterns for the atomic min / max of k_keys
-    CU(cudaMemsetAsync(h->run_blk_lo, 0x7f, (size_t)(blocks * 3) * sizeof(long long), h->stream));
-    CU(cudaMemsetAsync(h->run_blk_hi, 0x80, (size_t)(blocks * 3) * sizeof(long long), h->stream));
+    if (!span) {  // +inf / -inf patterns for the atomic min / max of k_keys
+      CU(cudaMemsetAsync(h->run_blk_lo, 0x7f, (size_t)(blocks * 3) * sizeof(long long), h->stream));
+      CU(cudaMemsetAsync(h->run_blk_hi, 0x80, (size_t)(blocks * 3) * sizeof(long long), h->stream));
+    }
     CU(cudaMemcpyAsync(h->ctr, h->ctr_init, sizeof(JobCtr) * B, cudaMemcpyHostToDevice, h->stream));
     CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
     int rr;
@@ -1136,7 +1148,7 @@ void free_all(rtod_handle* h) {
   dfree(h->ctr); dfree(h->jobs_dev); dfree(h->bs); dfree(h->router); dfree(h->ring); dfree(h->ring_keys);
   dfree(h->ring_prev); dfree(h->staging); dfree(h->run_buf); dfree(h->run_keys); dfree(h->run_prev);
   dfree(h->run_blk_lo); dfree(h->run_blk_hi);
-  dfree(h->rec_nout); dfree(h->rec_undet); dfree(h->ids);
+  dfree(h->rec_nout); dfree(h->rec_undet); dfree(h->rec_base); dfree(h->ids);
   if (h->ctr_init) cudaFreeHost(h->ctr_init);
   h->ctr_init = nullptr;
   if (h->host_rb) cudaFreeHost(h->host_rb);
@@ -2210,6 +2222,7 @@ RTOD_API int rtod_detect_window_static(const float* pts, int64_t n, int32_t dim,
   jb.ctr = (JobCtr*)at(kStatic.ctr);
   jb.rec_nout = nullptr;
   jb.rec_undet = nullptr;
+  jb.rec_base = nullptr;
   jb.rec_cap = 0;
   // Pageable source: the copy has been staged when the call returns.
   CU(cudaMemcpyAsync(at(kStatic.job), &jb, sizeof(Job), cudaMemcpyHostToDevice, st));

@@ -21,8 +21,7 @@
 // span), k_span_classify (per window and bin in use: safe, or listed) and
 // k_span_count (exact counts of the listed bins' window points into
 // per-slide outlier bitsets; its last block ends the batch). Once per chunk
-// of slides, k_slide_base and k_span_compact turn the bitsets into sorted
-// outlier IDs.
+// of slides, k_span_compact turns the bitsets into sorted outlier IDs.
 //
 // The safe-inlier rule is the window engine's (count > K in one cell, plus
 // the 1-d group rule) and, for 2-3 hashed dimensions in a pure span, the
@@ -50,9 +49,8 @@ struct Span {
   double R, R2;
   float R2f;
   const void* pts;          // resident stream, point-major [N][D] (the handle's coordinate type)
-  const uint64_t* keys;     // cell keys of the stream, by global index
-  const long long* blk_lo;  // per slide block cell coordinate range (span purity)
-  const long long* blk_hi;
+  uint64_t* keys;           // cell keys of the stream, by global index (written by k_span_hist)
+  double inv_cell;          // 1 / cell side
   uint32_t* bin_count;          // [NB] span points per bin
   uint32_t* bin_start;          // [NB + 1]
   unsigned long long* kmin;     // [NB] smallest / largest cell key of a bin over the span
@@ -74,30 +72,28 @@ struct Span {
 __device__ __forceinline__ int64_t span_lo(const Batch& b) { return b.jobs[0].ctr->lo; }
 
 // ---------------------------------------------------------------------------
-// k_span_hist: points per (block, bin) and per bin, and per-bin key ranges
-// unless the span is pure. Aggregated per warp, then per block in a
-// shared-memory table keyed by block * NB + bin, then one atomic per entry.
+// k_span_hist: the cell key of every span point (from its coordinates,
+// stored for k_span_scatter), the span's cell-coordinate range (its purity
+// is decided by k_span_scan), points per (block, bin) and per bin, and the
+// per-bin key range (a bin holds one cell iff min == max). Aggregated per
+// warp, then per block in a shared-memory table keyed by block * NB + bin,
+// then one atomic per entry.
 // ---------------------------------------------------------------------------
-template <int D>
+template <int D, typename T>
 __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
   constexpr int H = Hashed<D>::value;
   __shared__ uint32_t hkey[HIST_SLOTS];
   __shared__ uint32_t hcnt[HIST_SLOTS];
   __shared__ unsigned long long hmin[HIST_SLOTS], hmax[HIST_SLOTS];
-  __shared__ int s_pure;
+  __shared__ long long s_cr[2][3][8];  // per warp: the cell-coordinate range
   pdl_trigger();
   pdl_wait();
   constexpr int U = 4;
   const int64_t lo0 = span_lo(b);
   const int64_t npts = sp.nblk * sp.S;
   const int lane = threadIdx.x & 31;
-  if (threadIdx.x < 32) {
-    const bool pure = range_pure<H>(sp.blk_lo, sp.blk_hi, lo0 / sp.S, sp.nblk);
-    if (threadIdx.x == 0) {
-      s_pure = pure;
-      if (blockIdx.x == 0) sp.sc->pure = pure;
-    }
-  }
+  const T* pts = static_cast<const T*>(sp.pts);
+  long long cmn[3] = {LLONG_MAX, LLONG_MAX, LLONG_MAX}, cmx[3] = {LLONG_MIN, LLONG_MIN, LLONG_MIN};
   for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
     hkey[t] = 0xffffffffu;
     hcnt[t] = 0;
@@ -105,7 +101,6 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
     hmax[t] = 0;
   }
   __syncthreads();
-  const bool pure = s_pure;
   const uint32_t S32 = (uint32_t)sp.S;
   const int64_t chunk = (int64_t)blockDim.x * U;
   for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < npts; c0 += (int64_t)gridDim.x * chunk) {
@@ -114,7 +109,23 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t i = w0 + u * 32 + lane;
-      key[u] = i < npts ? sp.keys[lo0 + i] : EMPTY_KEY;
+      key[u] = EMPTY_KEY;
+      if (i < npts) {
+        T x[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) x[d] = pts[(lo0 + i) * D + d];
+        int32_t code;
+        key[u] = cell_key<D, T>(x, sp.inv_cell, &code);
+        if (code) set_err(b.bs, code);
+        sp.keys[lo0 + i] = key[u];
+        int64_t k[3];
+        unpack_key(key[u], H, k);
+#pragma unroll
+        for (int d = 0; d < H; ++d) {
+          cmn[d] = min(cmn[d], (long long)k[d]);
+          cmx[d] = max(cmx[d], (long long)k[d]);
+        }
+      }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -145,31 +156,52 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
           atomicAdd(&sp.bin_count[bin], c);
         }
       }
-      if (!pure) {
-        slot = __shfl_sync(0xffffffffu, slot, leader);
-        if (valid && (mixed_grp || lane == leader)) {
-          if (slot >= 0) {
-            atomicMin(&hmin[slot], (unsigned long long)key[u]);
-            atomicMax(&hmax[slot], (unsigned long long)key[u]);
-          } else {
-            atomicMin(&sp.kmin[bin], (unsigned long long)key[u]);
-            atomicMax(&sp.kmax[bin], (unsigned long long)key[u]);
-          }
+      // key range of the bin: the leader alone when the group's keys agree
+      slot = __shfl_sync(0xffffffffu, slot, leader);
+      if (valid && (mixed_grp || lane == leader)) {
+        if (slot >= 0) {
+          atomicMin(&hmin[slot], (unsigned long long)key[u]);
+          atomicMax(&hmax[slot], (unsigned long long)key[u]);
+        } else {
+          atomicMin(&sp.kmin[bin], (unsigned long long)key[u]);
+          atomicMax(&sp.kmax[bin], (unsigned long long)key[u]);
         }
       }
     }
   }
+#pragma unroll
+  for (int d = 0; d < H; ++d) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      cmn[d] = min(cmn[d], __shfl_xor_sync(0xffffffffu, cmn[d], o));
+      cmx[d] = max(cmx[d], __shfl_xor_sync(0xffffffffu, cmx[d], o));
+    }
+    if (lane == 0) {
+      s_cr[0][d][threadIdx.x >> 5] = cmn[d];
+      s_cr[1][d][threadIdx.x >> 5] = cmx[d];
+    }
+  }
   __syncthreads();
+  if (threadIdx.x < H) {
+    const int d = threadIdx.x;
+    long long mn = LLONG_MAX, mx = LLONG_MIN;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      mn = min(mn, s_cr[0][d][w]);
+      mx = max(mx, s_cr[1][d][w]);
+    }
+    if (mn <= mx) {
+      atomicMin(&sp.sc->cmin[d], mn);
+      atomicMax(&sp.sc->cmax[d], mx);
+    }
+  }
   for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
     const uint32_t comp = hkey[t];
     if (comp != 0xffffffffu) {
       const uint32_t bin = comp & NB_MASK;
       atomicAdd(&sp.cnt[comp], hcnt[t]);
       atomicAdd(&sp.bin_count[bin], hcnt[t]);
-      if (!pure) {
-        atomicMin(&sp.kmin[bin], hmin[t]);
-        atomicMax(&sp.kmax[bin], hmax[t]);
-      }
+      atomicMin(&sp.kmin[bin], hmin[t]);
+      atomicMax(&sp.kmax[bin], hmax[t]);
     }
   }
 }
@@ -223,8 +255,9 @@ __global__ void __launch_bounds__(256) k_span_prefix(Batch b, Span sp) {
   }
 }
 
-// k_span_scan: bin_start of the span (exclusive scan of bin_count) and the
-// list of bins in use (each thread appends its non-empty bins of 16).
+// k_span_scan: bin_start of the span (exclusive scan of bin_count), the list
+// of bins in use (each thread appends its non-empty bins of 16) and the
+// span's purity.
 __global__ void __launch_bounds__(256) k_span_scan(Batch b, Span sp) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t s_base;
@@ -243,6 +276,15 @@ __global__ void __launch_bounds__(256) k_span_scan(Batch b, Span sp) {
   }
 #pragma unroll
   for (int e = 0; e < 16; ++e) nz += c[e] != 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    // pure: the span's cells, widened by the sure / group-rule neighbours
+    // (within n-2), map to distinct bins
+    const int margin = 2 * max(sp.n - 2, 0);
+    const long long* mn = sp.sc->cmin;
+    const long long* mx = sp.sc->cmax;
+    sp.sc->pure = sp.h == 1 ? box_pure<1>(mn, mx, margin)
+                            : (sp.h == 2 ? box_pure<2>(mn, mx, margin) : box_pure<3>(mn, mx, margin));
+  }
   uint32_t total;
   const uint32_t ex = block_exclusive_scan(nz, &total, sm);
   if (threadIdx.x == 0) s_base = total ? atomicAdd(&sp.sc->n_used, total) : 0u;
@@ -668,37 +710,19 @@ __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
 }
 
 // ---------------------------------------------------------------------------
-// Deferred compaction of a chunk of slides [s0, s0 + n): k_slide_base turns
-// the per-slide outlier counts into output offsets (one block), then
-// k_span_compact, one block per slide, turns the slide's bitset row into
-// sorted global indices at its offset (4 words per thread, one block scan
-// per 4096 words) and clears the row.
+// Deferred compaction of a chunk of slides [s0, s0 + n): k_span_compact, one
+// block per slide, turns the slide's bitset row into sorted global indices
+// at the slide's output offset (recorded by finish_batch; 4 words per
+// thread, one block scan per 4096 words) and clears the row.
 // ---------------------------------------------------------------------------
 struct SpanOut {
   uint32_t* bits;
   int64_t words, chunk, W, S;
-  const int32_t* rec_nout;
-  int64_t* base;   // [chunk] output offset of each slide of the chunk
+  const int64_t* rec_base;  // per-slide output offsets
   int64_t* out_ids;
   int64_t out_cap;
   BatchState* bs;
 };
-
-__global__ void __launch_bounds__(1024) k_slide_base(SpanOut o, int64_t s0, int64_t n) {
-  __shared__ uint32_t sm[33];
-  pdl_trigger();
-  pdl_wait();
-  int64_t run = o.bs->ids_done;
-  for (int64_t c = 0; c < n; c += blockDim.x) {
-    const int64_t i = c + threadIdx.x;
-    const uint32_t v = i < n ? (uint32_t)o.rec_nout[s0 + i] : 0u;
-    uint32_t total;
-    const uint32_t ex = block_exclusive_scan(v, &total, sm);
-    if (i < n) o.base[i] = run + ex;
-    run += total;
-  }
-  if (threadIdx.x == 0) o.bs->ids_done = run;
-}
 
 __global__ void __launch_bounds__(1024) k_span_compact(SpanOut o, int64_t s0) {
   __shared__ uint32_t sm[33];
@@ -708,7 +732,7 @@ __global__ void __launch_bounds__(1024) k_span_compact(SpanOut o, int64_t s0) {
   const int64_t s = s0 + blockIdx.x;
   uint32_t* row = o.bits + (s % o.chunk) * o.words;
   const int64_t lo = (s + 1) * o.S;
-  int64_t out = o.base[blockIdx.x];
+  int64_t out = o.rec_base[s];
   const int64_t step = (int64_t)blockDim.x * WPT;
   for (int64_t c = 0; c < o.words; c += step) {
     const int64_t w0 = c + (int64_t)threadIdx.x * WPT;

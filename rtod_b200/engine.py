@@ -58,7 +58,7 @@ class RunResult:
 # Kernels of the span engine timed in each stage slot of rtod_profile_run.
 SPAN_STAGES = {"k_hist": "k_span_hist", "k_scan": "k_span_scan+k_span_prefix",
                "k_scatter": "k_span_scatter", "k_count": "k_span_classify", "k_compact": "k_span_count",
-               "k_train": "k_slide_base+k_span_compact"}
+               "k_train": "k_span_compact"}
 
 
 class Detector:

@@ -140,3 +140,30 @@ def test_sensor_3d_sparse_and_shared_bins(rtod, oracle_mod):
                    rng.uniform(-400, 400, (n, 3))).astype(np.float32)
     for nc in (2, 3):
         check_vs_oracle(rtod, oracle_mod, pts, 4000, 400, 0.5, 10, 30, cells_per_r=nc, batch=16)
+
+
+@pytest.mark.parametrize("engine", ["span", "window"])
+def test_aliased_neighbour_bin_at_range_limit(rtod, oracle_mod, engine):
+    """Two clusters 65535 cells apart: the cell next to cluster A shares its
+    bin with cluster B while the span's cell range is just 65536. A's points
+    (fewer than K per window) are outliers; counting B's bin as A's
+    neighbour cell would make them inliers."""
+    R, n = 1.0, 4
+    cell = R * (1 + 2.0 ** -12) / n
+    kA = 30_000
+    rng = np.random.default_rng(91)
+    m = 12_000
+    is_a = rng.random(m) < 0.2
+    xa = (kA + 0.25 + 0.5 * rng.random(m)) * cell           # cell kA
+    xb = (kA + 65_535 + 0.25 + 0.5 * rng.random(m)) * cell  # cell kA + 65535: bin kA - 1
+    pts = np.where(is_a, xa, xb).astype(np.float32)[:, None]
+    res = check_vs_oracle(rtod, oracle_mod, pts, 1000, 100, R, 300, 20, cells_per_r=n, batch=8) \
+        if engine == "span" else None
+    if engine == "window":
+        off, ids, _ = oracle_mod.detect(pts[:1000 + 20 * 100], 1000, 100, R, 300, engine="grid", threads=8)
+        r, tun = run(rtod, pts, 1000, 100, R, 300, 20, cells_per_r=n, engine="window")
+        np.testing.assert_array_equal(r.offsets, off)
+        np.testing.assert_array_equal(r.ids, ids)
+        res = r
+    # every cluster-A point of every window is an outlier
+    assert res.offsets[-1] == sum(int(is_a[(j + 1) * 100:(j + 1) * 100 + 1000].sum()) for j in range(20))
