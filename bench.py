@@ -32,6 +32,7 @@ import os
 import statistics
 import subprocess
 import sys
+import threading
 import time
 
 import numpy as np
@@ -117,6 +118,9 @@ def workload_config(w, extra=None):
 # clocks during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples every 50 ms while the
+    timed region runs; entering waits (up to 5 s) for the first sample so
+    that short regions are covered too."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -124,26 +128,38 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
+        self.lines = []
+        self.first = threading.Event()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line)
+            self.first.set()
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.gpu)],
+                 "-lms", "50", "-i", str(self.gpu)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+            return self
+        self.reader = threading.Thread(target=self._read, daemon=True)
+        self.reader.start()
+        self.first.wait(5.0)
         return self
 
     def __exit__(self, *exc):
-        self.out = ""
         if self.proc:
             self.proc.terminate()
             try:
-                self.out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                self.out, _ = self.proc.communicate()
+                self.proc.wait()
+            self.reader.join(timeout=5)
+        self.out = "".join(self.lines)
 
     def summary(self):
         rows = [r for r in csv.reader(io.StringIO(self.out or "")) if len(r) >= 9]

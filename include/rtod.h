@@ -61,6 +61,19 @@ extern "C" {
 #define RTOD_ENGINE_WINDOW 1
 #define RTOD_ENGINE_SPAN 2
 
+/* rtod_config.count: how the window engine counts the points of a cell
+   that are not provably inliers (the range count of RTOD's intersection
+   program, src/ods/optixScan.cu:158-199). Results are identical. */
+#define RTOD_COUNT_AUTO 0  /* group counts in more than 3 dimensions (no cell is ever all-inlier
+                              there) with the router off when a window (in the multi-stream API:
+                              the windows of the streams of that dimension and predicate) holds
+                              at least 4096 points per SM, point counts otherwise; the tuner
+                              may choose either */
+#define RTOD_COUNT_POINT 1 /* one warp per point, early exit at K+1 (with the router: early-exit
+                              and full-sweep queues) */
+#define RTOD_COUNT_GROUP 2 /* one warp per part of up to 32 points of a cell bin: they share the
+                              stencil's candidates, read once per part; the router is not used */
+
 typedef struct rtod_config {
   int64_t window;      /* W  (--window, src/ods/optixScan.cpp:166-171) */
   int64_t slide;       /* S  (--slide, :172-177); W % S == 0 (:1037) */
@@ -87,7 +100,8 @@ typedef struct rtod_config {
                           falls back to the window engine when W/S > 2047).
                           push/detect always use the window engine. Results are identical. */
   int32_t coord;       /* RTOD_COORD_F32 or RTOD_COORD_F64 */
-  int32_t reserved[1];
+  int32_t count;       /* RTOD_COUNT_*: window-engine count (push/detect, the multi-stream
+                          API, rtod_run with the window engine) */
 } rtod_config;
 
 /* Per-slide stage times in ms, averaged over the slides of the last call,
@@ -160,7 +174,8 @@ int64_t rtod_slides_done(const rtod_handle* h);
 /* The resolved grid and launch parameters (after autotuning, if on):
    out[0] cells per R, out[1] warps per block of the range count,
    out[2] hashed dimensions, out[3] windows per rtod_run launch, out[4] engine
-   of rtod_run (RTOD_ENGINE_WINDOW or RTOD_ENGINE_SPAN).
+   of rtod_run (RTOD_ENGINE_WINDOW or RTOD_ENGINE_SPAN). The window engine's
+   count mode is read with rtod_get_count_mode.
    With rtod_config.tuner = 1 the first rtod_run times candidate settings
    (in 1-d with engine = AUTO both engines, cells per R 1..3 or up to 6 in
    1-d, 2/4/8 warps per block, 8..256 windows per launch (up to 32 with the
@@ -169,6 +184,9 @@ int64_t rtod_slides_done(const rtod_handle* h);
    stream and keeps the fastest; the choice is cached per configuration for
    the rest of the process. Results do not depend on it. */
 int rtod_get_tuning(const rtod_handle* h, int32_t out[5]);
+
+/* The resolved window-engine count (RTOD_COUNT_POINT or RTOD_COUNT_GROUP). */
+int rtod_get_count_mode(const rtod_handle* h, int32_t* mode);
 
 /* Counters since create: out[0] kernel launches issued by the library (a
    graph replay counts each of its kernels), out[1] graph replays, out[2]

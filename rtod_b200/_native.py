@@ -28,6 +28,8 @@ class RtodError(RuntimeError):
 
 ENGINE = {"auto": 0, "window": 1, "span": 2}
 COORD = {"f32": 0, "f64": 1}
+COUNT = {"auto": 0, "point": 1, "group": 2}
+COUNT_NAME = {1: "point", 2: "group"}
 ENGINE_NAME = {1: "window", 2: "span"}
 
 
@@ -38,7 +40,7 @@ class Config(ctypes.Structure):
         ("pred", ctypes.c_int32), ("router", ctypes.c_int32), ("tuner", ctypes.c_int32),
         ("cells_per_r", ctypes.c_int32), ("block_warps", ctypes.c_int32),
         ("use_graph", ctypes.c_int32), ("device", ctypes.c_int32), ("batch", ctypes.c_int32),
-        ("engine", ctypes.c_int32), ("coord", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1),
+        ("engine", ctypes.c_int32), ("coord", ctypes.c_int32), ("count", ctypes.c_int32),
     ]
 
 
@@ -72,6 +74,7 @@ SIGNATURES = [
     ("rtod_reset", _i32, [_vp]),
     ("rtod_slides_done", _i64, [_vp]),
     ("rtod_get_tuning", _i32, [_vp, _vp]),
+    ("rtod_get_count_mode", _i32, [_vp, ctypes.POINTER(_i32)]),
     ("rtod_get_stats", _i32, [_vp, _vp]),
     ("rtod_profile_run", _i32, [_vp, _vp, _i64, _i64, _vp, _i32]),
     ("rtod_kernel_name", ctypes.c_char_p, [_i32]),

@@ -15,7 +15,7 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "librtod.so")
 SOURCES = ["rtod.cu"]
-HEADERS = ["kernels.cuh", "router.cuh", "batch.cuh"]
+HEADERS = ["kernels.cuh", "router.cuh", "span.cuh", "group.cuh"]
 
 
 def nvcc() -> str:

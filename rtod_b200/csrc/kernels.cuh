@@ -80,7 +80,7 @@ struct JobCtr {
   int32_t n_sweep;       // queued points of the full-sweep queue (router on)
   int32_t last_nout;     // outliers of the job's last detected window
   int32_t pure;          // current window: no two of its cells share a bin
-  int32_t pad;
+  int32_t n_groups;      // parts of bins listed for a group count (group mode)
 };
 
 // Per-handle state (device).
@@ -117,6 +117,7 @@ struct Job {
   int32_t n;         // cells per R = stencil reach in cells
   int32_t filter;    // safe-inlier skip enabled
   int32_t ring;      // 1: ring source, 0: resident stream
+  int32_t gpts;      // group mode: points per listed part of a bin (power of two, >= 32)
   const void* pts;        // coordinates (float or double, the handle's type): ring: SoA
                           // [D][W] by slot; stream: point-major [N][D]
   const uint64_t* keys;   // ring: [W] by slot; stream: [N] by global index
@@ -412,6 +413,7 @@ __device__ __forceinline__ void load4(const double* p, double* v) {
 }  // namespace rtod
 
 #include "router.cuh"
+#include "group.cuh"
 
 namespace rtod {
 
@@ -796,7 +798,7 @@ __device__ __forceinline__ bool group_safe_1d(const Job& jb, uint64_t key, uint3
   return false;
 }
 
-template <int D, bool ROUTE, typename T>
+template <int D, bool ROUTE, typename T, bool GROUP = false>
 __global__ void __launch_bounds__(256) k_scatter(Batch b) {
   // Block-local table: bin, points of the chunk in the bin, claimed base.
   __shared__ uint32_t tbin[HIST_SLOTS];
@@ -880,9 +882,9 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
       const bool valid = src[u] >= 0;
       const int64_t i = w0 + u * 32 + lane;
       bool safe = false;
-      uint32_t pos = 0, cnt = 0;
+      uint32_t pos = 0, cnt = 0, bs0 = 0;
       if (valid) {
-        const uint32_t bs0 = jb.bin_start[bin[u]];
+        bs0 = jb.bin_start[bin[u]];
         const uint32_t bs1 = jb.bin_start[bin[u] + 1];
         pos = bs0 + goff[u] + (slot[u] >= 0 ? tbase[slot[u]] : 0u);
         T x[D];
@@ -901,6 +903,25 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
         if (safe) jb.prev[src[u]] = 255;
       }
       const bool need = valid && !safe;
+      if constexpr (GROUP) {
+        // Group mode: a bin that needs counting (safety is decided per bin, so
+        // every point of it does) is listed as parts of jb.gpts points, each
+        // by the point at the part's first position.
+        const bool emit = need && ((pos - bs0) & (uint32_t)(jb.gpts - 1)) == 0;
+        const unsigned em = __ballot_sync(0xffffffffu, emit);
+        if (em) {
+          const uint32_t pts = __reduce_add_sync(0xffffffffu, emit && pos == bs0 ? cnt : 0u);
+          const int ql = __ffs(em) - 1;
+          uint32_t gb = 0;
+          if (lane == ql) {
+            gb = atomicAdd(reinterpret_cast<uint32_t*>(&jb.ctr->n_groups), (uint32_t)__popc(em));
+            if (pts) atomicAdd(&jb.ctr->n_undet, (int)pts);
+          }
+          gb = __shfl_sync(0xffffffffu, gb, ql);
+          if (emit) jb.queue[gb + __popc(em & lt)] = pos;
+        }
+        continue;
+      }
       bool sweep = false;
       float f[MLP_IN] = {0.0f, 0.0f, 0.0f};
       if constexpr (ROUTE) {
@@ -1217,7 +1238,7 @@ __device__ __forceinline__ void reset_bins(const Job& jb) {
 //     32 points per warp, each lane sweeping its own (short) candidate list;
 //     every counted point becomes a training sample of the router.
 // ---------------------------------------------------------------------------
-template <int D, int PRED, bool ROUTE, typename T>
+template <int D, int PRED, bool ROUTE, typename T, bool GROUP = false>
 __global__ void __launch_bounds__(256) k_count(Batch b) {
   __shared__ SampleBuf sb;
   pdl_trigger();
@@ -1234,6 +1255,31 @@ __global__ void __launch_bounds__(256) k_count(Batch b) {
   const int64_t lo = jb.ctr->lo;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  if constexpr (GROUP) {
+    // one warp per listed part of a bin: its points share the stencil (count_group)
+    constexpr int H = Hashed<D>::value;
+    const int64_t ng = jb.ctr->n_groups;
+    const bool can_sure = jb.ctr->pure && D <= 3;
+    int nout = 0;
+    for (int64_t g = warp; g < ng; g += nwarps) {
+      const uint32_t p = jb.queue[g];
+      const uint32_t bin = bin_of_key(jb.s_ckey[p], H);
+      const uint32_t nq = min((uint32_t)jb.gpts, jb.bin_start[bin + 1] - p);
+      const GroupArgs ga{p, nq, bin, jb.n, jb.K, jb.R2f, jb.R, jb.R2, jb.Wp, can_sure};
+      nout += count_group<D, PRED, T>(
+          static_cast<const T*>(jb.s_x), ga,
+          [&](uint32_t sb2, uint32_t& rs, uint32_t& len) {
+            rs = jb.bin_start[sb2];
+            len = jb.bin_start[sb2 + 1] - rs;
+          },
+          [&](uint32_t pos) {
+            const uint32_t i = jb.s_off[pos];
+            atomicOr(&jb.flags[i >> 5], 1u << (i & 31));
+          });
+    }
+    if (lane == 0 && nout) atomicAdd(&jb.ctr->n_out, nout);
+    return;
+  }
   const int64_t nq = jb.ctr->n_undet;
   for (int64_t q = warp; q < nq; q += nwarps) {
     const uint32_t pos = jb.queue[q];
@@ -1325,6 +1371,7 @@ __device__ void finish_batch(const Batch& b) {
     c->n_out = 0;
     c->n_undet = 0;
     c->n_sweep = 0;
+    c->n_groups = 0;
     c->cmp_ticket = 0;
   }
 #pragma unroll

@@ -269,6 +269,7 @@ struct rtod_handle {
   std::vector<Scratch> pool;  // allocated lazily, one per job of a batch
   SpanScratch span;           // span engine scratch, allocated on first use
   int engine = RTOD_ENGINE_WINDOW;  // engine of rtod_run (resolved from the config / tuner)
+  int group = 0;                    // window-engine count: 1 = group counts (resolved from the config / tuner)
   JobCtr* ctr = nullptr;      // [kMaxJobs]
   JobCtr* ctr_init = nullptr; // pinned host [kMaxJobs]
   Job* jobs_dev = nullptr;    // [kMaxJobs]
@@ -363,6 +364,8 @@ int check_config(const rtod_config* c) {
     return fail(RTOD_ERR_CONFIG, "coord must be RTOD_COORD_F32 or RTOD_COORD_F64");
   if (c->coord == RTOD_COORD_F64 && c->pred != RTOD_PRED_F64_LT)
     return fail(RTOD_ERR_CONFIG, "double coordinates need the double predicate (RTOD_PRED_F64_LT)");
+  if (c->count < RTOD_COUNT_AUTO || c->count > RTOD_COUNT_GROUP)
+    return fail(RTOD_ERR_CONFIG, "count must be 0 (auto), 1 (point) or 2 (group)");
   return RTOD_OK;
 }
 
@@ -566,6 +569,26 @@ int64_t span_chunk(const rtod_handle* h, int B, int64_t slides) {
   return (int64_t)B * std::max<int64_t>(1, std::min(per_batch, batches));
 }
 
+// Points per listed part of a bin in group mode, for a launch counting
+// `points` points: parts short enough that there are about 16 per SM (a
+// part is one warp's work), and long enough (up to 1024) that a warp's
+// lanes are refilled from the part's other points while it walks the
+// candidates.
+int32_t group_part(int64_t points, int sm_count) {
+  const int64_t fill = points / ((int64_t)sm_count * 16);
+  int32_t p = 32;
+  while (p < 1024 && 2 * (int64_t)p <= fill) p *= 2;
+  return p;
+}
+
+// Whether RTOD_COUNT_AUTO picks group counts for a launch of `points`
+// points: in more than 3 dimensions (no cell is ever all-inlier, so every
+// point is counted and a bin's points are many) when the parts hold at
+// least 256 points. Measured on 8-d Gaussian blobs: shorter parts (a single
+// window of 162k points, 64-point parts) are slower than point counts, while
+// 64 streams of 1.6M points in all (512-point parts) gain a quarter.
+bool auto_group(int D, int64_t points, int sm_count) { return D > 3 && group_part(points, sm_count) >= 256; }
+
 Job make_job(rtod_handle* h, int j, bool ring, const void* stream_pts) {
   Job jb{};
   jb.W = h->W;
@@ -579,6 +602,7 @@ Job make_job(rtod_handle* h, int j, bool ring, const void* stream_pts) {
   jb.n = h->n;
   jb.filter = h->filter;
   jb.ring = ring ? 1 : 0;
+  jb.gpts = 32;
   jb.pts = ring ? h->ring : stream_pts;
   jb.keys = ring ? h->ring_keys : h->run_keys;
   jb.stage = h->staging;
@@ -614,7 +638,10 @@ int configure(rtod_handle* h, int mode, int jobs, int64_t first_lo, const void* 
   int r = ensure_pool(h, jobs, full);
   if (r) return r;
   std::vector<Job> tab((size_t)jobs);
-  for (int j = 0; j < jobs; ++j) tab[j] = make_job(h, j, mode == MODE_RING, stream_pts);
+  for (int j = 0; j < jobs; ++j) {
+    tab[j] = make_job(h, j, mode == MODE_RING, stream_pts);
+    tab[j].gpts = group_part(h->W * jobs, h->sm_count);
+  }
   if (tab.size() != h->tab_host.size() ||
       std::memcmp(tab.data(), h->tab_host.data(), sizeof(Job) * tab.size()) != 0) {
     CU(cudaMemcpy(h->jobs_dev, tab.data(), sizeof(Job) * jobs, cudaMemcpyHostToDevice));
@@ -651,7 +678,8 @@ struct Geom {
   int64_t Wmax, Smax;
   int D, pred, route, sm_count, block_warps;
   RouterState* router;
-  int f64 = 0;  // double coordinates
+  int f64 = 0;    // double coordinates
+  int group = 0;  // group counts (route is then 0)
 };
 
 // Launches one batch: [ingest] hist scan scatter count compact [train].
@@ -678,6 +706,8 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
   if (kev) CU(cudaEventRecord(kev[2], st));
   if (g.route) {
     DISPATCH_DT(g.f64, g.D, CU(launch_k(k_scatter<D, true, T>, dim3((unsigned)wx, gy), 256, st, b)));
+  } else if (g.group) {
+    DISPATCH_DT(g.f64, g.D, CU(launch_k(k_scatter<D, false, T, true>, dim3((unsigned)wx, gy), 256, st, b)));
   } else {
     DISPATCH_DT(g.f64, g.D, CU(launch_k(k_scatter<D, false, T>, dim3((unsigned)wx, gy), 256, st, b)));
   }
@@ -687,6 +717,9 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
   if (g.route) {
     DISPATCH_DPT(g.f64, g.D, g.pred,
                  CU(launch_k(k_count<D, PRED, true, T>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
+  } else if (g.group) {
+    DISPATCH_DPT(g.f64, g.D, g.pred,
+                 CU(launch_k(k_count<D, PRED, false, T, true>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
   } else {
     DISPATCH_DPT(g.f64, g.D, g.pred,
                  CU(launch_k(k_count<D, PRED, false, T>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
@@ -762,7 +795,8 @@ int span_flush(rtod_handle* h, const Span& sp, int64_t s0, int64_t n, int64_t ou
 }
 
 Geom geom_of(const rtod_handle* h) {
-  return Geom{h->W, h->S, h->D, h->cfg.pred, h->cfg.router, h->sm_count, h->block_warps, h->router, h->f64};
+  return Geom{h->W, h->S, h->D, h->cfg.pred, h->cfg.router && !h->group, h->sm_count, h->block_warps,
+              h->router, h->f64, h->group};
 }
 
 constexpr int kTrainEvery = 8;  // batches between two router training steps
@@ -1182,6 +1216,7 @@ struct Tuning {
   float threshold = 0.5f;
   uint32_t max_sweep = 64;
   int engine = RTOD_ENGINE_WINDOW;
+  int group = 0;
 };
 
 struct TuneEntry {
@@ -1194,7 +1229,8 @@ std::vector<TuneEntry> g_tune_cache;
 
 bool same_problem(const rtod_config& a, const rtod_config& b) {
   return a.window == b.window && a.slide == b.slide && a.R == b.R && a.K == b.K && a.dim == b.dim &&
-         a.opt == b.opt && a.pred == b.pred && a.router == b.router && a.device == b.device;
+         a.opt == b.opt && a.pred == b.pred && a.router == b.router && a.device == b.device &&
+         a.engine == b.engine && a.coord == b.coord && a.count == b.count;
 }
 
 int apply_tuning(rtod_handle* h, const Tuning& t) {
@@ -1204,6 +1240,7 @@ int apply_tuning(rtod_handle* h, const Tuning& t) {
   h->threshold = t.threshold;
   h->max_sweep = t.max_sweep;
   h->engine = t.engine;
+  h->group = t.group;
   if (h->router) {
     CU(cudaMemcpy((char*)h->router + offsetof(RouterState, threshold), &t.threshold, sizeof(float),
                   cudaMemcpyHostToDevice));
@@ -1258,6 +1295,7 @@ int autotune(rtod_handle* h, const void* pts, int64_t slides_total) {
   Tuning best;
   best.batch = h->engine == RTOD_ENGINE_SPAN ? 32 : std::min(32, h->batch_max);
   best.engine = h->engine;
+  best.group = h->group;
   int r = apply_tuning(h, best);
   if (r) return r;
   float best_ms;
@@ -1288,6 +1326,11 @@ int autotune(rtod_handle* h, const void* pts, int64_t slides_total) {
       }
     }
   }
+  if (best.engine == RTOD_ENGINE_WINDOW && h->cfg.count == RTOD_COUNT_AUTO) {
+    Tuning t = best;
+    t.group = !best.group;
+    if ((r = trial(t))) return r;
+  }
   for (int bw : {2, 4, 8}) {
     if (bw == best.block_warps) continue;
     Tuning t = best;
@@ -1300,7 +1343,7 @@ int autotune(rtod_handle* h, const void* pts, int64_t slides_total) {
     t.batch = bt;
     if ((r = trial(t))) return r;
   }
-  if (h->cfg.router && best.engine == RTOD_ENGINE_WINDOW) {
+  if (h->cfg.router && best.engine == RTOD_ENGINE_WINDOW && !best.group) {
     for (float th : {0.3f, 0.7f}) {
       Tuning t = best;
       t.threshold = th;
@@ -1385,6 +1428,11 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
   // Engine of rtod_run: the span engine by default without the router.
   h->engine = cfg->engine != RTOD_ENGINE_AUTO ? cfg->engine
                                                : (!cfg->router ? RTOD_ENGINE_SPAN : RTOD_ENGINE_WINDOW);
+  // Window-engine count: group counts where no cell is ever all-inlier and
+  // a window holds enough points for long parts (auto_group), unless the
+  // router (which routes single points) is on.
+  h->group = cfg->count == RTOD_COUNT_GROUP ||
+             (cfg->count == RTOD_COUNT_AUTO && !cfg->router && auto_group(h->D, h->W, h->sm_count));
   // Windows per rtod_run launch: up to 32, within ~1 GiB of scratch.
   const int64_t per_job = (int64_t)NB * 24 + h->W * (4 + 8 + 4 + 4) + h->Wp * h->D * 4 + h->W / 8;
   h->batch_max = (int)std::max<int64_t>(1, std::min<int64_t>(32, (1ll << 30) / per_job));
@@ -1460,6 +1508,12 @@ RTOD_API int rtod_get_tuning(const rtod_handle* h, int32_t out[5]) {
   out[2] = h->D < 3 ? h->D : 3;
   out[3] = pick_batch(h, INT64_MAX);
   out[4] = use_span(h) ? RTOD_ENGINE_SPAN : RTOD_ENGINE_WINDOW;
+  return RTOD_OK;
+}
+
+RTOD_API int rtod_get_count_mode(const rtod_handle* h, int32_t* mode) {
+  if (!h || !mode) return fail(RTOD_ERR_ARG, "null argument");
+  *mode = h->group ? RTOD_COUNT_GROUP : RTOD_COUNT_POINT;
   return RTOD_OK;
 }
 
@@ -1928,16 +1982,29 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
     k_table<<<(TQ0 * TQ1 * TQ2 + 255) / 256, 256, 0, b->stream>>>(b->router);
     if (cudaGetLastError() != cudaSuccess) return bail(fail(RTOD_ERR_CUDA, "router table failed"));
   }
-  // Group the streams by (dimension, predicate).
+  // Streams counted with RTOD_COUNT_AUTO follow their (dimension, predicate)
+  // group's points: group counts when auto_group holds for all of them.
+  {
+    std::vector<int64_t> pts(n_streams, 0);
+    for (int i = 0; i < n_streams; ++i)
+      for (int k = 0; k < n_streams; ++k)
+        if (cfgs[k].count == RTOD_COUNT_AUTO && b->hs[k]->D == b->hs[i]->D && cfgs[k].pred == cfgs[i].pred)
+          pts[i] += b->hs[k]->W;
+    for (int i = 0; i < n_streams; ++i)
+      if (cfgs[i].count == RTOD_COUNT_AUTO)
+        b->hs[i]->group = !b->route && auto_group(b->hs[i]->D, pts[i], b->hs[i]->sm_count);
+  }
+  // Group the streams by (dimension, predicate, count mode).
   for (int i = 0; i < n_streams; ++i) {
     const rtod_handle* h = b->hs[i];
     rtod_batch::Group* g = nullptr;
     for (auto& x : b->groups)
-      if (x.geom.D == h->D && x.geom.pred == h->cfg.pred) g = &x;
+      if (x.geom.D == h->D && x.geom.pred == h->cfg.pred && x.geom.group == h->group) g = &x;
     if (!g) {
       b->groups.emplace_back();
       g = &b->groups.back();
-      g->geom = Geom{0, 0, h->D, h->cfg.pred, b->route, h->sm_count, h->block_warps, b->router};
+      g->geom = Geom{0, 0, h->D, h->cfg.pred, b->route && !h->group, h->sm_count, h->block_warps, b->router, 0,
+                     h->group};
     }
     g->streams.push_back(i);
     g->geom.Wmax = std::max(g->geom.Wmax, h->W);
@@ -1952,6 +2019,7 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
       g.out_cap += h->W;
       g.cmp_tiles += (h->W + CMP_TILE - 1) / CMP_TILE;
     }
+    for (auto& jb : tab) jb.gpts = group_part(g.out_cap, b->hs[g.streams[0]]->sm_count);
     if (dalloc(&g.jobs, ng, &dummy) || dalloc(&g.bs, 1, &dummy) || dalloc(&g.out, (size_t)g.out_cap, &dummy) ||
         dalloc(&g.active, ng, &dummy) || dalloc(&g.nout, ng, &dummy))
       return bail(RTOD_ERR_CUDA);
@@ -2201,6 +2269,7 @@ RTOD_API int rtod_detect_window_static(const float* pts, int64_t n, int32_t dim,
   jb.n = n_cells;
   jb.filter = 1;
   jb.ring = 0;
+  jb.gpts = 32;
   jb.pts = pts;
   jb.keys = (const uint64_t*)at(kStatic.keys);
   jb.stage = nullptr;

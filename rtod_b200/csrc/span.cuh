@@ -438,168 +438,37 @@ __device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* 
   return false;
 }
 
-// Stencil slot s of 2n+1 cells per hashed dimension: offsets d in [-n, n]^h
-// (1-d: 0, -1, +1, -2, +2, ..., nearest first; otherwise row-major) and the
-// bin offset of the cell k + d (bins are linear in the cell coordinates mod
-// NB: d, d1 + 256 d0, d2 + 64 d1 + 4096 d0).
-template <int H>
-__device__ __forceinline__ int slot_cell(int s, int n, int* d) {
-  if constexpr (H == 1) {
-    d[0] = (s & 1) ? -((s + 1) >> 1) : (s >> 1);
-    return d[0];
-  } else {
-    const int w = 2 * n + 1;
-#pragma unroll
-    for (int i = H - 1; i >= 0; --i) {
-      d[i] = s % w - n;
-      s /= w;
-    }
-    return H == 2 ? d[1] + 256 * d[0] : d[2] + 64 * d[1] + 4096 * d[0];
-  }
-}
-
-// Whether every point of cell k + d lies within R of every point of cell k:
-// sum of (|d_i| + 1)^2 < n^2 (cells of R(1+2^-12)/n; the margin is at least
-// 1/n^2 - 2^-11 of R^2, far above the predicates' rounding).
-template <int H>
-__device__ __forceinline__ bool slot_sure(const int* d, int n) {
-  int q = 0;
-#pragma unroll
-  for (int i = 0; i < H; ++i) {
-    const int a = (d[i] < 0 ? -d[i] : d[i]) + 1;
-    q += a * a;
-  }
-  return q < n * n;
-}
-
 // ---------------------------------------------------------------------------
 // Exact counts of the nq points of window j in bin `bin` (bin-ordered
-// positions [p, p + nq)) by one warp. Whatever cell k of the bin a point is
-// in, its stencil cells k + d lie in bins bin + delta(d) (mod NB), so the
-// stencil is the same for all of them: (2n+1)^h slots, taken 32 at a time
-// (lane s of a round takes slot r0 + s and that bin's window range; points
-// of other cells sharing those bins are rejected by the distance test). In
-// a pure span (D <= 3) the "sure" slots hold only cells whose points all lie
-// within R of the group's points: their window counts add up to `given`
-// without tests (given > K: all inliers; given plus every other candidate
-// <= K: all outliers). In each round a warp scan turns the other ranges'
-// lengths into offsets of one virtual candidate list, read 256 candidates
-// at a time (8 per lane, kept in registers); every undecided point of the
-// group (up to 32, one per lane) is tested against the chunk: per point, 8
-// tests per lane and one warp reduction; a point is decided as soon as its
-// count exceeds K, and the rounds stop when every point is decided.
+// positions [p, p + nq)) by one warp (count_group): the candidates of
+// stencil bin sb are its points in window j, positions [bin_start[sb] +
+// pre[j][sb], bin_start[sb] + pre[j + W/S][sb]); sure slots are used in a
+// pure span of up to 3 dimensions. Outliers set their bit in the slide's
+// bitset row.
 // ---------------------------------------------------------------------------
 template <int D, int PRED, typename T>
 __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp, int j, uint32_t p,
                                                  uint32_t nq, uint32_t bin, const uint32_t* p0,
                                                  const uint32_t* p1, bool pure) {
-  constexpr int H = Hashed<D>::value;
-  const int lane = threadIdx.x & 31;
   const Job& jb = b.jobs[j];
   const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
-  const T* sx = static_cast<const T*>(sp.s_x);
   uint32_t* row = sp.bits + ((jb.ctr->lo - sp.S) / sp.S % sp.chunk) * sp.words;
-  const int w = 2 * sp.n + 1;
-  const int slots = H == 1 ? w : (H == 2 ? w * w : w * w * w);
-  const bool can_sure = pure && D <= 3;
-  // window range of slot s; sure: counts without tests
-  auto slot = [&](int s, uint32_t& rs, uint32_t& len, bool& sure) {
-    rs = 0;
-    len = 0;
-    sure = false;
-    if (s >= slots) return;
-    int d[3] = {0, 0, 0};
-    const int delta = slot_cell<H>(s, sp.n, d);
-    sure = can_sure && slot_sure<H>(d, sp.n);
-    const uint32_t sb = (bin + (uint32_t)delta) & NB_MASK;
-    const uint32_t b0 = sp.bin_start[sb], b1 = sp.bin_start[sb + 1];
-    if (b1 > b0) {
-      const uint32_t a = p0[sb];
-      rs = b0 + a;
-      len = p1[sb] - a;
-    }
-  };
-  const bool one = slots <= 32;  // one round: its ranges stay in registers
-  uint32_t given = 0, total = 0, rs1 = 0, len1 = 0;
-  for (int r0 = 0; r0 < slots; r0 += 32) {
-    uint32_t rs, len;
-    bool sure;
-    slot(r0 + lane, rs, len, sure);
-    given += __reduce_add_sync(0xffffffffu, sure ? len : 0u);
-    total += __reduce_add_sync(0xffffffffu, len);
-    rs1 = rs;
-    len1 = sure ? 0u : len;
-  }
-  if (given > (uint32_t)sp.K) return;  // every point of the group is an inlier
-  int nout = 0;
-  for (uint32_t g = 0; g < nq; g += 32) {
-    const uint32_t q = g + lane;
-    const bool has = q < nq;
-    T qx[D];
-#pragma unroll
-    for (int d = 0; d < D; ++d) qx[d] = has ? sx[(int64_t)d * sp.Wp + p + q] : T(0);
-    int cnt = (int)given;
-    unsigned live = __ballot_sync(0xffffffffu, has);
-    for (int r0 = 0; r0 < slots && live && total > (uint32_t)sp.K; r0 += 32) {
-      uint32_t rs = rs1, len = len1;
-      if (!one) {
-        bool sure;
-        slot(r0 + lane, rs, len, sure);
-        if (sure) len = 0;
-      }
-      uint32_t inc = len;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += y;
-      }
-      const uint32_t off = inc - len;
-      const uint32_t ncand = __shfl_sync(0xffffffffu, inc, 31);
-      for (uint32_t c0 = 0; c0 < ncand && live; c0 += 256) {
-        T cx[8][D];
-        bool cv[8];
-#pragma unroll
-        for (int e = 0; e < 8; ++e) {
-          const uint32_t v = c0 + 32 * e + lane;
-          // lane holding v's range: the last lane whose offset is <= v
-          int s = 0;
-#pragma unroll
-          for (int step = 16; step > 0; step >>= 1) {
-            const int cand = s + step;
-            const uint32_t oc = __shfl_sync(0xffffffffu, off, cand & 31);
-            if (oc <= v) s = cand;
-          }
-          const uint32_t base = __shfl_sync(0xffffffffu, rs, s);
-          const uint32_t os = __shfl_sync(0xffffffffu, off, s);
-          cv[e] = v < ncand;
-          const uint32_t c = base + (v - os);
-#pragma unroll
-          for (int d = 0; d < D; ++d) cx[e][d] = cv[e] ? sx[(int64_t)d * sp.Wp + c] : T(0);
+  const GroupArgs ga{p, nq, bin, sp.n, sp.K, sp.R2f, sp.R, sp.R2, sp.Wp, pure && D <= 3};
+  const int nout = count_group<D, PRED, T>(
+      static_cast<const T*>(sp.s_x), ga,
+      [&](uint32_t sb, uint32_t& rs, uint32_t& len) {
+        const uint32_t b0 = sp.bin_start[sb], b1 = sp.bin_start[sb + 1];
+        if (b1 > b0) {
+          const uint32_t x = p0[sb];
+          rs = b0 + x;
+          len = p1[sb] - x;
         }
-        unsigned todo = live;
-        while (todo) {
-          const int qq = __ffs(todo) - 1;
-          todo &= todo - 1;
-          T y[D];
-#pragma unroll
-          for (int d = 0; d < D; ++d) y[d] = __shfl_sync(0xffffffffu, qx[d], qq);
-          unsigned m = 0;
-#pragma unroll
-          for (int e = 0; e < 8; ++e) m += (cv[e] && is_nbr<D, PRED, T>(y, cx[e], sp.R2f, sp.R, sp.R2)) ? 1u : 0u;
-          const unsigned tot = __reduce_add_sync(0xffffffffu, m);
-          if (lane == qq) cnt += (int)tot;
-        }
-        live &= __ballot_sync(0xffffffffu, cnt <= sp.K);
-      }
-    }
-    const bool out = has && cnt <= sp.K;
-    if (out) {
-      const int64_t w2 = (int64_t)sp.s_off[p + q] - shift;
-      atomicOr(&row[w2 >> 5], 1u << (w2 & 31));
-    }
-    nout += __popc(__ballot_sync(0xffffffffu, out));
-  }
-  if (lane == 0 && nout) atomicAdd(&jb.ctr->n_out, nout);
+      },
+      [&](uint32_t pos) {
+        const int64_t w2 = (int64_t)sp.s_off[pos] - shift;
+        atomicOr(&row[w2 >> 5], 1u << (w2 & 31));
+      });
+  if ((threadIdx.x & 31) == 0 && nout) atomicAdd(&jb.ctr->n_out, nout);
 }
 
 // Clears the per-bin state of the span's bins in use (all blocks of the

@@ -71,7 +71,8 @@ class Detector:
     def __init__(self, window: int, slide: int, R: float, K: int, dim: int = 1, opt: int = 2,
                  pred: str = "fp32_le", router: bool = False, tuner: bool = False,
                  cells_per_r: int = 0, block_warps: int = 0, use_graph: bool = True,
-                 batch: int = 0, device: int = 0, engine: str = "auto", coord: str = "f32"):
+                 batch: int = 0, device: int = 0, engine: str = "auto", coord: str = "f32",
+                 count: str = "auto"):
         cfg = Config()
         check(lib().rtod_config_init(ctypes.byref(cfg)))
         cfg.window, cfg.slide, cfg.R, cfg.K, cfg.dim, cfg.opt = window, slide, R, K, dim, opt
@@ -81,6 +82,7 @@ class Detector:
         cfg.use_graph, cfg.device, cfg.batch = int(use_graph), device, batch
         cfg.engine = _native.ENGINE[engine]
         cfg.coord = _native.COORD[coord]
+        cfg.count = _native.COUNT[count]
         self.f64 = coord == "f64"
         self.cfg = cfg
         self.window, self.slide, self.R, self.K, self.dim = window, slide, R, K, dim
@@ -206,6 +208,13 @@ class Detector:
         return {"cells_per_r": a[0], "block_warps": a[1], "hashed_dims": a[2], "batch": a[3],
                 "engine": _native.ENGINE_NAME.get(a[4], a[4])}
 
+    @property
+    def count_mode(self) -> str:
+        """Window-engine count: "point" (warp per point) or "group" (warp per bin)."""
+        m = ctypes.c_int32()
+        check(lib().rtod_get_count_mode(self._h, ctypes.byref(m)))
+        return _native.COUNT_NAME.get(m.value, m.value)
+
     def ring_slots(self, ids: np.ndarray) -> np.ndarray:
         """RTOD's outlier IDs (ring slots, optixScan.cpp:1097) for global indices."""
         return np.asarray(ids, np.int64) % self.window
@@ -217,7 +226,7 @@ class BatchDetector:
     captured CUDA graph (streams grouped by dimension and predicate).
 
     ``streams`` is a list of dicts with the Detector parameters (window,
-    slide, R, K, dim, opt, pred); ``router`` switches the shared learned
+    slide, R, K, dim, opt, pred, count); ``router`` switches the shared learned
     router on for all of them."""
 
     def __init__(self, streams, router: bool = False, device: int = 0):
@@ -229,6 +238,7 @@ class BatchDetector:
             c.window, c.slide, c.R, c.K = st["window"], st["slide"], st["R"], st["K"]
             c.dim, c.opt = st.get("dim", 1), st.get("opt", 2)
             c.pred = _native.PRED[st.get("pred", "fp32_le")]
+            c.count = _native.COUNT[st.get("count", "auto")]
             c.router, c.device = int(router), device
         self.streams = [dict(s) for s in streams]
         self._b = ctypes.c_void_p()

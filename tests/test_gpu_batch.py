@@ -36,15 +36,15 @@ def make_streams(n=9, seed=5):
     return out
 
 
-@pytest.mark.parametrize("router", [False, True])
-def test_batch_matches_oracle(rtod, oracle_mod, router):
+@pytest.mark.parametrize("router,count", [(False, "auto"), (True, "auto"), (False, "group"), (True, "point")])
+def test_batch_matches_oracle(rtod, oracle_mod, router, count):
     streams = make_streams()
     expect = []
     for st in streams:
         off, ids, _ = oracle_mod.detect(st["points"], st["window"], st["slide"], st["R"], st["K"],
                                         st["pred"], engine="grid", threads=4)
         expect.append((off, ids))
-    cfg = [{k: st[k] for k in ("window", "slide", "R", "K", "dim", "pred")} for st in streams]
+    cfg = [dict({k: st[k] for k in ("window", "slide", "R", "K", "dim", "pred")}, count=count) for st in streams]
     with rtod.BatchDetector(cfg, router=router) as bd:
         for i, st in enumerate(streams):
             bd.push(i, st["points"][:st["window"]])
