@@ -154,7 +154,9 @@ int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t* n_out, r
    detected, slide j covering points [(j+1)S, W+(j+1)S). The handle must be
    fresh (nothing pushed). out_offsets receives slides+1 CSR offsets into
    out_ids; *slides_out the number of slides. pts may be host or device
-   memory (n * dim floats). times may be NULL. */
+   memory (n * dim floats); so may out_ids (device memory and page-locked
+   host memory are written during the pass, other host memory by one copy
+   after it). times may be NULL. */
 int rtod_run(rtod_handle* h, const float* pts, int64_t n, int64_t max_slides,
              int64_t* out_offsets, int64_t* out_ids, int64_t ids_cap, int64_t* slides_out,
              rtod_times* times);

@@ -1409,6 +1409,40 @@ __device__ void finish_batch(const Batch& b) {
 }
 
 // ---------------------------------------------------------------------------
+// Head and tail of an rtod_run pass (kernels, so that a captured run has no
+// host copy at either end).
+// k_run_init: job j's counters start at window lo = first_lo + j*S and
+// advance by jobs*S per batch; the batch state is cleared.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_run_init(JobCtr* ctr, int32_t jobs, int64_t first_lo, int64_t S,
+                                                  BatchState* bs) {
+  pdl_trigger();
+  pdl_wait();
+  for (int j = threadIdx.x; j < jobs; j += blockDim.x) {
+    JobCtr c{};
+    c.lo = first_lo + (int64_t)j * S;
+    c.lo_step = (int64_t)jobs * S;
+    ctr[j] = c;
+  }
+  if (threadIdx.x == 0) *bs = BatchState{};
+}
+
+// k_run_out: the outlier IDs (at most cap) into a caller's page-locked host
+// buffer through its device mapping (consecutive 8-byte writes, one per
+// thread), then the batch state into the handle's mapped mirror.
+__global__ void __launch_bounds__(256) k_run_out(const int64_t* ids, int64_t* host_ids, int64_t cap,
+                                                 const BatchState* bs, BatchState* mirror) {
+  pdl_trigger();
+  pdl_wait();
+  if (host_ids) {
+    const int64_t n = min(bs->out_total, cap);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+      host_ids[i] = ids[i];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *mirror = *bs;
+}
+
+// ---------------------------------------------------------------------------
 // k_compact: outlier bits in window order -> sorted global indices, appended
 // to the batch output after the outliers of the earlier jobs. Grid
 // (max tiles per job, jobs); a tile covers CMP_TILE window offsets, one

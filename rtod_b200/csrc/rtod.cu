@@ -292,10 +292,18 @@ struct rtod_handle {
   long long* run_blk_lo = nullptr;  // per slide block: cell coordinate range [blocks][3]
   long long* run_blk_hi = nullptr;
   int64_t run_blk_cap = 0;
+  // Per-slide outlier and counted-point records of rtod_run, in mapped
+  // page-locked memory (written by the kernels, read by the host after the
+  // pass): device views rec_nout / rec_undet, host views *_h.
+  void* rec_host = nullptr;
   int32_t* rec_nout = nullptr;
   int32_t* rec_undet = nullptr;
-  int64_t* rec_base = nullptr;  // per-slide output offsets (span engine)
+  int32_t* rec_nout_h = nullptr;
+  int32_t* rec_undet_h = nullptr;
+  int64_t* rec_base = nullptr;  // per-slide output offsets (span engine), device
   int64_t rec_cap = 0;
+  BatchState* bs_mirror = nullptr;      // mapped page-locked copy of bs written by k_run_out
+  BatchState* bs_mirror_dev = nullptr;  // its device view
   int64_t* ids = nullptr;
   int64_t ids_cap = 0;
 
@@ -323,8 +331,6 @@ struct rtod_handle {
   cudaStream_t copy_stream = nullptr;     // host-stream pieces, overlapped with detection
   cudaEvent_t fork_ev = nullptr;          // the copy stream's start on the library stream
   std::vector<cudaEvent_t> piece_ev;      // one per piece
-  void* host_rb = nullptr;  // pinned read-back of the run's counters and per-slide records
-  size_t host_rb_bytes = 0;
   int64_t launches = 0;
   int64_t graph_replays = 0;
   int64_t undet_total = 0;
@@ -889,15 +895,28 @@ int ensure_ids(rtod_handle* h, int64_t cap) {
 }
 
 int ensure_records(rtod_handle* h, int64_t n) {
+  if (!h->bs_mirror) {
+    void* dp = nullptr;
+    CU(cudaHostAlloc((void**)&h->bs_mirror, sizeof(BatchState), cudaHostAllocMapped));
+    CU(cudaHostGetDevicePointer(&dp, h->bs_mirror, 0));
+    h->bs_mirror_dev = (BatchState*)dp;
+  }
   if (n <= h->rec_cap) return RTOD_OK;
-  if (h->rec_nout) h->device_bytes -= h->rec_cap * 16;
-  dfree(h->rec_nout);
-  dfree(h->rec_undet);
+  drop_graph(h);
+  if (h->rec_base) h->device_bytes -= h->rec_cap * 8;
   dfree(h->rec_base);
+  if (h->rec_host) cudaFreeHost(h->rec_host);
+  h->rec_host = nullptr;
+  h->rec_nout = h->rec_undet = h->rec_nout_h = h->rec_undet_h = nullptr;
   h->rec_cap = 0;
-  if (dalloc(&h->rec_nout, (size_t)n, &h->device_bytes) || dalloc(&h->rec_undet, (size_t)n, &h->device_bytes) ||
-      dalloc(&h->rec_base, (size_t)n, &h->device_bytes))
-    return RTOD_ERR_CUDA;
+  if (dalloc(&h->rec_base, (size_t)n, &h->device_bytes)) return RTOD_ERR_CUDA;
+  void* dp = nullptr;
+  CU(cudaHostAlloc(&h->rec_host, 2 * (size_t)n * sizeof(int32_t), cudaHostAllocMapped));
+  CU(cudaHostGetDevicePointer(&dp, h->rec_host, 0));
+  h->rec_nout_h = (int32_t*)h->rec_host;
+  h->rec_undet_h = h->rec_nout_h + n;
+  h->rec_nout = (int32_t*)dp;
+  h->rec_undet = h->rec_nout + n;
   h->rec_cap = n;
   return RTOD_OK;
 }
@@ -996,7 +1015,18 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
   // device; otherwise to the handle's buffer and out in one copy by the
   // caller (one bulk copy beats scattered device writes into host memory).
   const bool to_user = out_ids && ids_cap > 0 && is_device_ptr(out_ids) && device_addressable(out_ids, h->device);
-  if (direct) *direct = to_user;
+  // A page-locked host buffer gets the IDs from k_run_out at the end of the
+  // pass, through its device mapping.
+  int64_t* mapped_out = nullptr;
+  if (out_ids && ids_cap > 0 && !to_user) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, out_ids) == cudaSuccess) {
+      if (a.type == cudaMemoryTypeHost && a.devicePointer) mapped_out = static_cast<int64_t*>(a.devicePointer);
+    } else {
+      cudaGetLastError();
+    }
+  }
+  if (direct) *direct = to_user || mapped_out;
   if (!to_user && (r = ensure_ids(h, std::max<int64_t>(1, std::min(ids_cap, slides * W))))) return r;
   int64_t* const dst = to_user ? out_ids : h->ids;
   const bool span = use_span(h);
@@ -1004,7 +1034,6 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
   if ((r = ensure_pool(h, B, !span))) return r;
   const int64_t chunk = span ? span_chunk(h, B, slides) : 0;
   if (span && (r = ensure_span(h, W / S + B - 1, chunk))) return r;
-  if (e_begin) CU(cudaEventRecord(e_begin, h->stream));
   bool host = false, pinned = false;
   if ((r = stage_stream(h, pts, used, &src, &host, false, &pinned))) return r;
   // first detected window: [S, W + S)
@@ -1063,12 +1092,14 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
   const bool whole = span && (!host || pinned) && h->cfg.use_graph && !kev;
   // Everything from the scratch resets to the last compaction.
   auto enqueue = [&]() -> int {
+    // the pass starts here (a run graph: just before its launch)
+    if (e_begin && !whole) CU(cudaEventRecord(e_begin, h->stream));
     if (!span) {  // +inf / -inf patterns for the atomic min / max of k_keys
       CU(cudaMemsetAsync(h->run_blk_lo, 0x7f, (size_t)(blocks * 3) * sizeof(long long), h->stream));
       CU(cudaMemsetAsync(h->run_blk_hi, 0x80, (size_t)(blocks * 3) * sizeof(long long), h->stream));
     }
-    CU(cudaMemcpyAsync(h->ctr, h->ctr_init, sizeof(JobCtr) * B, cudaMemcpyHostToDevice, h->stream));
-    CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
+    CU(launch_k(k_run_init, dim3(1), 256, h->stream, h->ctr, (int32_t)B, S, S, h->bs));
+    h->launches++;
     int rr;
     if (host && (rr = copy_pieces())) return rr;
     if (!whole) CU(cudaEventRecord(h->ev[1], h->stream));  // start of the key kernel (profile)
@@ -1106,13 +1137,18 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
         if (kev) CU(cudaEventRecord(chunk_ev.back().second, h->stream));
       }
     }
+    // IDs to a page-locked caller buffer, the batch state to the mirror
+    const unsigned ox = mapped_out ? (unsigned)h->sm_count * 2 : 1u;
+    CU(launch_k(k_run_out, dim3(ox), 256, h->stream, (const int64_t*)dst, mapped_out, out_cap, h->bs,
+                h->bs_mirror_dev));
+    h->launches++;
     return RTOD_OK;
   };
   if (whole) {
     // key of the captured run: stream, sizes and the batch / span parameters
-    std::vector<unsigned char> key(sizeof(void*) + 4 * sizeof(int64_t) + sizeof(Batch) + sizeof(Span));
+    std::vector<unsigned char> key(sizeof(void*) + 5 * sizeof(int64_t) + sizeof(Batch) + sizeof(Span));
     unsigned char* k = key.data();
-    const int64_t ints[4] = {slides, out_cap, chunk, (int64_t)B};
+    const int64_t ints[5] = {slides, out_cap, chunk, (int64_t)B, (int64_t)(intptr_t)mapped_out};
     std::memcpy(k, &pts, sizeof(void*));  // the caller's stream (host pieces are copied from it)
     std::memcpy(k + sizeof(void*), ints, sizeof ints);
     std::memcpy(k + sizeof(void*) + sizeof ints, &bfull, sizeof(Batch));
@@ -1134,6 +1170,7 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
       h->run_graph_kernels = h->launches - l0;
       h->launches = l0;
     }
+    if (e_begin) CU(cudaEventRecord(e_begin, h->stream));
     CU(cudaGraphLaunch(h->run_graph, h->stream));
     h->launches += h->run_graph_kernels;
     h->graph_replays++;
@@ -1141,26 +1178,12 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
     if ((r = enqueue())) return r;
   }
   if (e_end) CU(cudaEventRecord(e_end, h->stream));
-  // Counters and per-slide records through one pinned buffer: async copies
-  // and a single wait.
-  const size_t rb = sizeof(BatchState) + 2 * (size_t)slides * sizeof(int32_t);
-  if (rb > h->host_rb_bytes) {
-    if (h->host_rb) cudaFreeHost(h->host_rb);
-    h->host_rb = nullptr;
-    h->host_rb_bytes = 0;
-    CU(cudaMallocHost(&h->host_rb, rb));
-    h->host_rb_bytes = rb;
-  }
-  char* hb = (char*)h->host_rb;
-  int32_t* hno = (int32_t*)(hb + sizeof(BatchState));
-  int32_t* hnu = hno + slides;
-  CU(cudaMemcpyAsync(hb, h->bs, sizeof(BatchState), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaMemcpyAsync(hno, h->rec_nout, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
-  CU(cudaMemcpyAsync(hnu, h->rec_undet, slides * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream));
+  // Counters and per-slide records: written by the kernels into mapped
+  // page-locked memory, read after a single wait.
   CU(cudaStreamSynchronize(h->stream));
-  std::memcpy(out_state, hb, sizeof(BatchState));
-  nout->assign(hno, hno + slides);
-  nund->assign(hnu, hnu + slides);
+  std::memcpy(out_state, h->bs_mirror, sizeof(BatchState));
+  nout->assign(h->rec_nout_h, h->rec_nout_h + slides);
+  nund->assign(h->rec_undet_h, h->rec_undet_h + slides);
   h->flush_ms = 0;
   for (const auto& pr : chunk_ev) h->flush_ms += elapsed(pr.first, pr.second);
   h->n_pushed = used;
@@ -1182,12 +1205,14 @@ void free_all(rtod_handle* h) {
   dfree(h->ctr); dfree(h->jobs_dev); dfree(h->bs); dfree(h->router); dfree(h->ring); dfree(h->ring_keys);
   dfree(h->ring_prev); dfree(h->staging); dfree(h->run_buf); dfree(h->run_keys); dfree(h->run_prev);
   dfree(h->run_blk_lo); dfree(h->run_blk_hi);
-  dfree(h->rec_nout); dfree(h->rec_undet); dfree(h->rec_base); dfree(h->ids);
+  dfree(h->rec_base); dfree(h->ids);
+  if (h->rec_host) cudaFreeHost(h->rec_host);
+  h->rec_host = nullptr;
+  h->rec_nout = h->rec_undet = h->rec_nout_h = h->rec_undet_h = nullptr;
+  if (h->bs_mirror) cudaFreeHost(h->bs_mirror);
+  h->bs_mirror = h->bs_mirror_dev = nullptr;
   if (h->ctr_init) cudaFreeHost(h->ctr_init);
   h->ctr_init = nullptr;
-  if (h->host_rb) cudaFreeHost(h->host_rb);
-  h->host_rb = nullptr;
-  h->host_rb_bytes = 0;
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
   for (auto e : h->piece_ev) cudaEventDestroy(e);
@@ -1664,16 +1689,20 @@ int run_impl(rtod_handle* h, const void* pts, int64_t n, int64_t max_slides, int
   if (r) return r;
   for (int64_t j = 0; j < slides; ++j) out_offsets[j + 1] = out_offsets[j] + nout[j];
   if (out_offsets[slides] != s.out_total) return fail(RTOD_ERR_CUDA, "inconsistent outlier totals");
-  CU(cudaEventRecord(d0, h->stream));
-  if (!direct && s.out_total > 0)  // the IDs are in the handle's buffer
+  // IDs still in the handle's buffer (a pageable host destination): one copy
+  const bool copy_out = !direct && s.out_total > 0;
+  if (copy_out) {
+    CU(cudaEventRecord(d0, h->stream));
     CU(cudaMemcpyAsync(out_ids, h->ids, (size_t)s.out_total * sizeof(int64_t), cudaMemcpyDefault, h->stream));
-  CU(cudaEventRecord(d1, h->stream));
-  CU(cudaStreamSynchronize(h->stream));
+    CU(cudaEventRecord(d1, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+  }
   if (times) {
     std::memset(times, 0, sizeof *times);
     const double inv = 1.0 / (double)slides;
+    const double d2h = copy_out ? elapsed(d0, d1) : 0.0;  // otherwise inside the pass (k_run_out)
     times->slides = slides;
-    times->copy_outlier_d2h = elapsed(d0, d1) * inv;
+    times->copy_outlier_d2h = d2h * inv;
     if (stage) {
       const int64_t nb = (int64_t)kev.size() / 8;
       double pc = elapsed(t0, t1), bb = 0, de = 0;  // input copy + cell keys count as preparing cells
@@ -1688,10 +1717,11 @@ int run_impl(rtod_handle* h, const void* pts, int64_t n, int64_t max_slides, int
       times->build_bvh = bb * inv;
       times->detect_outlier = de * inv;
     }
-    // Everything on the library stream from the input copy to the last
-    // kernel, plus the outlier copy-out (the per-slide counts read-back and
-    // its host wait are the only parts outside).
-    times->total = (elapsed(t0, t2) + elapsed(d0, d1)) * inv;
+    // Everything on the library stream from the start of the pass (input
+    // copy, counters) to its last kernel (which also delivers the IDs to a
+    // device or page-locked buffer), plus the copy to a pageable buffer; only
+    // the host's wait is outside.
+    times->total = (elapsed(t0, t2) + d2h) * inv;
     times->undetermined_per_slide = (double)s.undet_total * inv;
   }
   return RTOD_OK;

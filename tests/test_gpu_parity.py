@@ -126,6 +126,39 @@ def test_device_pointers(rtod):
         np.testing.assert_array_equal(r.ids.cpu().numpy(), ids)
 
 
+def test_output_buffers(rtod):
+    """IDs into pageable host memory (one copy after the pass), page-locked
+    host memory (written during the pass through its device mapping) and
+    device memory; replays with another page-locked buffer; a capacity error
+    writes nothing past the capacity."""
+    import torch
+    from rtod_b200 import datagen
+    w = datagen.stock_like()
+    pts = w.points[:w.window + 40 * w.slide]
+    with rtod.Detector(w.window, w.slide, w.R, w.K, engine="span") as det:
+        ref = det.run(pts)
+        n = len(ref.ids)
+        for _ in range(2):
+            for pinned in (True, False):
+                buf = torch.full((n + 64,), -7, dtype=torch.int64)
+                if pinned:
+                    buf = buf.pin_memory()
+                det.reset()
+                r = det.run(pts, out_ids=buf.numpy(), ids_cap=n + 64)
+                np.testing.assert_array_equal(r.offsets, ref.offsets)
+                np.testing.assert_array_equal(buf.numpy()[:n], ref.ids)
+                assert np.all(buf.numpy()[n:] == -7)
+        dev = torch.full((n,), -7, dtype=torch.int64, device="cuda")
+        det.reset()
+        r = det.run(torch.from_numpy(pts).cuda(), out_ids=dev, ids_cap=n)
+        np.testing.assert_array_equal(dev.cpu().numpy(), ref.ids)
+        small = torch.full((n,), -7, dtype=torch.int64).pin_memory()
+        det.reset()
+        with pytest.raises(rtod.RtodError):
+            det.run(pts, out_ids=small.numpy(), ids_cap=n // 2)
+        assert np.all(small.numpy()[n // 2:] == -7)
+
+
 def test_input_errors(rtod):
     pts = np.zeros(40, np.float32)
     pts[25] = np.nan
