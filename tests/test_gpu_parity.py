@@ -159,6 +159,28 @@ def test_output_buffers(rtod):
         assert np.all(small.numpy()[n // 2:] == -7)
 
 
+@pytest.mark.parametrize("kw", [dict(engine="span"), dict(engine="span", batch=16), dict(engine="span", batch=1),
+                                dict(engine="span", use_graph=False), dict(engine="window")])
+def test_page_locked_input(rtod, kw):
+    """A page-locked host stream: copied in pieces on a second stream, the
+    first piece in parts followed by the histogram part by part (run graph of
+    the span engine); the same results as from device memory, replay after
+    replay."""
+    import torch
+    from rtod_b200 import datagen
+    w = datagen.stock_like()
+    pts = torch.from_numpy(w.points).pin_memory()
+    with rtod.Detector(w.window, w.slide, w.R, w.K, **kw) as det:
+        ref = det.run(pts.cuda())
+        for _ in range(3):
+            det.reset()
+            assert_same(det.run(pts.numpy()), ref.offsets, ref.ids)
+        det.reset()
+        part = pts[:(w.window + 37 * w.slide)]  # a shorter stream: another graph
+        r = det.run(part.numpy())
+        assert_same(r, ref.offsets[:38], ref.ids[:ref.offsets[37]])
+
+
 def test_input_errors(rtod):
     pts = np.zeros(40, np.float32)
     pts[25] = np.nan
