@@ -206,6 +206,17 @@ def ncu_traffic(kernel: str):
     return None
 
 
+def pass_roofline(w, n_out_per_slide: float, us_per_slide: float, peak: float) -> dict:
+    """Bytes per slide that a detector reading every window point once per
+    slide moves (new slide in, ring write, one read of the window, IDs out),
+    against the measured device time per slide of the whole pass."""
+    d = w.dim
+    per_slide = 4 * d * w.slide + 4 * d * w.slide + 4 * d * w.window + 4 * n_out_per_slide
+    achieved = per_slide / (us_per_slide * 1e-6) / 1e9
+    return {"algorithmic_bytes_per_slide": per_slide, "us_per_slide": us_per_slide,
+            "achieved": achieved, "unit": "GB/s", "frac": achieved / peak}
+
+
 def used_bins(w, cells_per_r: int, batch: int) -> int:
     """Bins of the 65536-bin table holding points of the first span of
     `batch` windows (1-d cells of R(1+2^-12)/n, bin = cell mod 65536)."""
@@ -404,7 +415,11 @@ def emit_ours(args, world, w, res):
                      "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                      "algorithmic_bytes_per_launch": alg * per_launch, "windows_per_launch": per_launch,
                      "launch_ms": launch_ms, "used_bins": ub,
-                     "stage_ms_per_slide": prof},
+                     "stage_ms_per_slide": prof,
+                     # the whole pass against the per-slide bytes of a detector that
+                     # reads every window point once per slide: 4dS in + 4dS ring
+                     # write + 4dW window read + 4 n_out IDs
+                     "pass": pass_roofline(w, n_out, us_slide, peak)},
         "clocks": r["clocks"],
         "gpu_launches": r["launches"],
         "e2e": {"value": world * r["e2e_steps"] * slides * w.slide / r["e2e_s"], "unit": UNIT,
@@ -462,7 +477,7 @@ def run_reference(args, world, rank):
 
 def run_ncu_case(args, local):
     """Profiler pass of the headline workload with the settings the autotuner
-    picks on it in plain runs (span engine, 4 cells per R, 2-warp count
+    picks on it in plain runs (span engine, 3 cells per R, 2-warp count
     blocks, up to 256 windows per launch; under ncu the tuner's own timings
     would be distorted): one pass outside the profiler range, then two
     passes inside it (cudaProfilerStart/Stop: run ncu with
@@ -472,7 +487,7 @@ def run_ncu_case(args, local):
     w = workload()
     torch.cuda.set_device(local)
     pts = torch.from_numpy(w.points).to(f"cuda:{local}")
-    with Detector(w.window, w.slide, w.R, w.K, dim=w.dim, device=local, engine="span", cells_per_r=4,
+    with Detector(w.window, w.slide, w.R, w.K, dim=w.dim, device=local, engine="span", cells_per_r=3,
                   block_warps=2, batch=256) as det:
         r = det.run(pts)
         torch.cuda.synchronize()
