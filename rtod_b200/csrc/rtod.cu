@@ -183,8 +183,9 @@ struct SpanScratch {
   uint32_t* bin_start = nullptr;
   unsigned long long* kmin = nullptr;
   unsigned long long* kmax = nullptr;
-  uint32_t* cnt = nullptr;
-  uint32_t* pre = nullptr;
+  uint32_t* cnt = nullptr;  // [NB][ts]
+  uint32_t* pre = nullptr;  // [NB][ts]
+  int64_t ts = 0;           // nblk_cap + 1
   uint32_t* used = nullptr;
   uint32_t* s_off = nullptr;
   unsigned char* s_x = nullptr;  // coordinates, the handle's type
@@ -441,7 +442,7 @@ int scrub(rtod_handle* h) {
     CU(cudaMemsetAsync(sp.bin_count, 0, NB * sizeof(uint32_t), h->stream));
     CU(cudaMemsetAsync(sp.kmin, 0xff, NB * sizeof(unsigned long long), h->stream));
     CU(cudaMemsetAsync(sp.kmax, 0, NB * sizeof(unsigned long long), h->stream));
-    CU(cudaMemsetAsync(sp.cnt, 0, (size_t)(sp.nblk_cap * NB) * sizeof(uint32_t), h->stream));
+    CU(cudaMemsetAsync(sp.cnt, 0, (size_t)(sp.ts * NB) * sizeof(uint32_t), h->stream));
     CU(cudaMemsetAsync(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long), h->stream));
     SpanCtr c{};  // counters back to their starting values
     for (int d = 0; d < 3; ++d) {
@@ -480,7 +481,7 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
   int64_t bytes = 0;
   bool ok = !dalloc(&sp.bin_count, NB, &bytes) && !dalloc(&sp.bin_start, NB + 1, &bytes) &&
             !dalloc(&sp.kmin, NB, &bytes) && !dalloc(&sp.kmax, NB, &bytes) &&
-            !dalloc(&sp.cnt, (size_t)(nblk * NB), &bytes) && !dalloc(&sp.pre, (size_t)((nblk + 1) * NB), &bytes) &&
+            !dalloc(&sp.cnt, (size_t)((nblk + 1) * NB), &bytes) && !dalloc(&sp.pre, (size_t)((nblk + 1) * NB), &bytes) &&
             !dalloc(&sp.used, NB, &bytes) && !dalloc(&sp.s_off, (size_t)pts, &bytes) &&
             !dalloc(&sp.s_x, (size_t)(Wp * h->D * h->esz), &bytes) && !dalloc(&sp.scan_status, SCAN_TILES, &bytes) &&
             !dalloc(&sp.sc, 1, &bytes) && !dalloc(&sp.bits, (size_t)(chunk * words), &bytes) &&
@@ -492,6 +493,7 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
     return RTOD_ERR_CUDA;
   }
   sp.nblk_cap = nblk;
+  sp.ts = nblk + 1;
   sp.pts_cap = pts;
   sp.chunk_cap = chunk;
   sp.Wp = Wp;
@@ -499,7 +501,7 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
   CU(cudaMemset(sp.bin_count, 0, NB * sizeof(uint32_t)));
   CU(cudaMemset(sp.kmin, 0xff, NB * sizeof(unsigned long long)));
   CU(cudaMemset(sp.kmax, 0, NB * sizeof(unsigned long long)));
-  CU(cudaMemset(sp.cnt, 0, (size_t)(nblk * NB) * sizeof(uint32_t)));
+  CU(cudaMemset(sp.cnt, 0, (size_t)(sp.ts * NB) * sizeof(uint32_t)));
   CU(cudaMemset(sp.s_x, 0, (size_t)(Wp * h->D * h->esz)));
   CU(cudaMemset(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long)));
   SpanCtr c{};
@@ -554,6 +556,7 @@ Span make_span(const rtod_handle* h, int B, const void* stream_pts, int64_t chun
   sp.kmax = ss.kmax;
   sp.cnt = ss.cnt;
   sp.pre = ss.pre;
+  sp.ts = ss.ts;
   sp.used = ss.used;
   sp.s_off = ss.s_off;
   sp.s_x = ss.s_x;

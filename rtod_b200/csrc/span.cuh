@@ -7,12 +7,13 @@
 // bin, and inside each bin by block (points of one block in any order):
 //
 //   position of a point of block t in bin b
-//     = bin_start[b] + pre[t][b] + (its claim among the block's points in b),
-//   pre[t][b] = points of bin b in blocks before t.
+//     = bin_start[b] + pre[b][t] + (its claim among the block's points in b),
+//   pre[b][t] = points of bin b in blocks before t (a bin's row of blocks is
+//   contiguous, stride ts).
 //
 // So window j's points of bin b are the contiguous positions
-// [bin_start[b] + pre[j][b], bin_start[b] + pre[j + W/S][b]), and its count
-// of bin b is pre[j + W/S][b] - pre[j][b]: classification needs no per-point
+// [bin_start[b] + pre[b][j], bin_start[b] + pre[b][j + W/S]), and its count
+// of bin b is pre[b][j + W/S] - pre[b][j]: classification needs no per-point
 // work, and a queued point's candidates are (2n+1)^h such ranges (h = hashed
 // dimensions, min(D, 3)); all points of a bin share them.
 //
@@ -55,8 +56,9 @@ struct Span {
   uint32_t* bin_start;          // [NB + 1]
   unsigned long long* kmin;     // [NB] smallest / largest cell key of a bin over the span
   unsigned long long* kmax;
-  uint32_t* cnt;    // [nblk][NB] points of block t in bin b (claims count them back to zero)
-  uint32_t* pre;    // [nblk + 1][NB] points of bin b in the blocks before t (bins in use only)
+  uint32_t* cnt;    // [NB][ts] points of bin b in block t (claims count them back to zero)
+  uint32_t* pre;    // [NB][ts] points of bin b in the blocks before t, t <= nblk (bins in use only)
+  int64_t ts;       // row stride of cnt and pre (>= nblk + 1): a bin's blocks are contiguous
   uint32_t* used;   // [NB] bins holding span points, n_used of them, in no particular order
   uint32_t* s_off;  // [span] bin-ordered: offset from the span start
   void* s_x;        // [D][Wp] bin-ordered coordinates (the handle's coordinate type)
@@ -71,12 +73,24 @@ struct Span {
 // First global index of the span: the window of the batch's first job.
 __device__ __forceinline__ int64_t span_lo(const Batch& b) { return b.jobs[0].ctr->lo; }
 
+// Window j's per-bin counts from the prefix table: bin b's points in blocks
+// before block t are pre[b * ts + t], and window j covers blocks [j, j + wblk).
+struct WinPre {
+  const uint32_t* pre;
+  int64_t ts;
+  int32_t j, wblk;
+  __device__ __forceinline__ uint32_t count(uint32_t b) const {
+    const uint32_t* row = pre + (int64_t)b * ts + j;
+    return row[wblk] - row[0];
+  }
+};
+
 // ---------------------------------------------------------------------------
 // k_span_hist: the cell key of every span point (from its coordinates,
 // stored for k_span_scatter), the span's cell-coordinate range (its purity
 // is decided by k_span_scan), points per (block, bin) and per bin, and the
 // per-bin key range (a bin holds one cell iff min == max). Aggregated per
-// warp, then per block in a shared-memory table keyed by block * NB + bin,
+// warp, then per block in a shared-memory table keyed by bin * ts + block,
 // then one atomic per entry.
 // ---------------------------------------------------------------------------
 template <int D, typename T>
@@ -132,7 +146,7 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
       const int64_t i = w0 + u * 32 + lane;
       const bool valid = key[u] != EMPTY_KEY;
       const uint32_t bin = valid ? bin_of_key(key[u], H) : 0u;
-      const uint32_t comp = valid ? ((uint32_t)i / S32) * NB + bin : 0xffffffffu;
+      const uint32_t comp = valid ? bin * (uint32_t)sp.ts + (uint32_t)i / S32 : 0xffffffffu;
       const unsigned peers = __match_any_sync(0xffffffffu, comp);
       const int leader = __ffs(peers) - 1;
       const uint64_t lkey = __shfl_sync(0xffffffffu, key[u], leader);
@@ -197,7 +211,7 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
   for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
     const uint32_t comp = hkey[t];
     if (comp != 0xffffffffu) {
-      const uint32_t bin = comp & NB_MASK;
+      const uint32_t bin = comp / (uint32_t)sp.ts;
       atomicAdd(&sp.cnt[comp], hcnt[t]);
       atomicAdd(&sp.bin_count[bin], hcnt[t]);
       atomicMin(&sp.kmin[bin], hmin[t]);
@@ -208,50 +222,44 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
 
 // ---------------------------------------------------------------------------
 // k_span_prefix: one warp per bin in use (the list k_span_scan built),
-// striding over the list: lane l sums blocks [l*per, (l+1)*per), per =
-// ceil(nblk / 32), 8 loads in flight per step (kept in registers when per
-// <= 8, the usual case), a warp scan gives its offset, and it writes
-// pre[t][b] for its blocks (pre[nblk][b] by the last lane).
+// striding over the list. The bin's block counts are one contiguous row of
+// cnt: the warp reads it 32 blocks per load (8 loads in flight), scans each
+// 32-block step with a warp scan plus the running carry, and writes the
+// bin's row of pre (pre[b][nblk] = all its span points).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_span_prefix(Batch b, Span sp) {
   pdl_trigger();
   pdl_wait();
   const int lane = threadIdx.x & 31;
   const uint32_t nu = sp.sc->n_used;
-  const int64_t per = (sp.nblk + 31) / 32;
-  const int64_t t0 = min((int64_t)lane * per, sp.nblk), t1 = min(t0 + per, sp.nblk);
+  const int64_t nblk = sp.nblk;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   for (int64_t u = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); u < nu; u += warps) {
     const uint32_t bin = sp.used[u];
-    const uint32_t* __restrict__ cnt = sp.cnt + bin;
-    uint32_t* __restrict__ pre = sp.pre + bin;
-    uint32_t v[8];
-    uint32_t sum = 0;
-    for (int64_t t = t0; t < t1; t += 8) {
+    const uint32_t* __restrict__ cnt = sp.cnt + (int64_t)bin * sp.ts;
+    uint32_t* __restrict__ pre = sp.pre + (int64_t)bin * sp.ts;
+    uint32_t carry = 0;
+    for (int64_t r0 = 0; r0 < nblk; r0 += 256) {
+      uint32_t v[8];
 #pragma unroll
-      for (int e = 0; e < 8; ++e) v[e] = t + e < t1 ? cnt[(t + e) * NB] : 0u;
-#pragma unroll
-      for (int e = 0; e < 8; ++e) sum += v[e];
-    }
-    uint32_t inc = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += y;
-    }
-    uint32_t run = inc - sum;
-    for (int64_t t = t0; t < t1; t += 8) {
-      if (per > 8) {  // values of this step are no longer in registers
-#pragma unroll
-        for (int e = 0; e < 8; ++e) v[e] = t + e < t1 ? cnt[(t + e) * NB] : 0u;
+      for (int e = 0; e < 8; ++e) {
+        const int64_t t = r0 + 32 * e + lane;
+        v[e] = t < nblk ? cnt[t] : 0u;
       }
 #pragma unroll
       for (int e = 0; e < 8; ++e) {
-        if (t + e < t1) pre[(t + e) * NB] = run;
-        run += v[e];
+        uint32_t inc = v[e];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o) inc += y;
+        }
+        const int64_t t = r0 + 32 * e + lane;
+        if (t < nblk) pre[t] = carry + inc - v[e];
+        carry += __shfl_sync(0xffffffffu, inc, 31);
       }
     }
-    if (lane == 31) pre[sp.nblk * NB] = run;
+    if (lane == 0) pre[nblk] = carry;
   }
 }
 
@@ -335,7 +343,7 @@ __global__ void __launch_bounds__(256) k_span_scatter(Batch b, Span sp) {
     for (int u = 0; u < U; ++u) {
       const int64_t i = w0 + u * 32 + lane;
       const bool valid = key[u] != EMPTY_KEY;
-      comp[u] = valid ? ((uint32_t)i / S32) * NB + bin_of_key(key[u], H) : 0xffffffffu;
+      comp[u] = valid ? bin_of_key(key[u], H) * (uint32_t)sp.ts + (uint32_t)i / S32 : 0xffffffffu;
       const unsigned peers = __match_any_sync(0xffffffffu, comp[u]);
       const int leader = __ffs(peers) - 1;
       int sl_found = -1;
@@ -373,7 +381,7 @@ __global__ void __launch_bounds__(256) k_span_scatter(Batch b, Span sp) {
     for (int u = 0; u < U; ++u) {
       if (comp[u] != 0xffffffffu) {
         const int64_t i = w0 + u * 32 + lane;
-        const uint32_t bin = comp[u] & NB_MASK;
+        const uint32_t bin = comp[u] / (uint32_t)sp.ts;
         const uint32_t pos = sp.bin_start[bin] + sp.pre[comp[u]] + goff[u] + (slot[u] >= 0 ? tbase[slot[u]] : 0u);
         sp.s_off[pos] = (uint32_t)i;
 #pragma unroll
@@ -390,8 +398,7 @@ __global__ void __launch_bounds__(256) k_span_scatter(Batch b, Span sp) {
 // (all within R of each other), hold more than K window points, every bin
 // involved holding nothing in the window or only its expected cell over the
 // whole span.
-__device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* p0, const uint32_t* p1,
-                                                uint32_t bin, bool pure) {
+__device__ __forceinline__ bool span_group_safe(const Span& sp, const WinPre& wp, uint32_t bin, bool pure) {
   const int m = sp.n - 1;
   if (m < 2 || bin < (uint32_t)(m - 1) || bin + m > NB - 1) return false;
   constexpr int MMAX = 7;
@@ -405,7 +412,7 @@ __device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* 
     if (t < 2 * m - 1) {
       const uint32_t j = bin - m + 1 + t;
       const bool any = sp.bin_count[j] != 0;
-      wc[t] = any ? p1[j] - p0[j] : 0u;
+      wc[t] = any ? wp.count(j) : 0u;
       const unsigned long long want = key + (unsigned long long)(t - (m - 1));
       ok[t] = pure || wc[t] == 0 || (sp.kmin[j] == want && sp.kmax[j] == want);
     }
@@ -447,9 +454,9 @@ __device__ __forceinline__ bool span_group_safe(const Span& sp, const uint32_t* 
 // bitset row.
 // ---------------------------------------------------------------------------
 template <int D, int PRED, typename T>
-__device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp, int j, uint32_t p,
-                                                 uint32_t nq, uint32_t bin, const uint32_t* p0,
-                                                 const uint32_t* p1, bool pure) {
+__device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp, uint32_t p, uint32_t nq,
+                                                 uint32_t bin, const WinPre& wp, bool pure) {
+  const int j = wp.j;
   const Job& jb = b.jobs[j];
   const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
   uint32_t* row = sp.bits + ((jb.ctr->lo - sp.S) / sp.S % sp.chunk) * sp.words;
@@ -459,9 +466,9 @@ __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp,
       [&](uint32_t sb, uint32_t& rs, uint32_t& len) {
         const uint32_t b0 = sp.bin_start[sb], b1 = sp.bin_start[sb + 1];
         if (b1 > b0) {
-          const uint32_t x = p0[sb];
-          rs = b0 + x;
-          len = p1[sb] - x;
+          const uint32_t* row = wp.pre + (int64_t)sb * wp.ts + wp.j;
+          rs = b0 + row[0];
+          len = row[wp.wblk] - row[0];
         }
       },
       [&](uint32_t pos) {
@@ -510,22 +517,22 @@ __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
     if (e < pairs) {
       j = (int)(e / nu);
       bin = sp.used[e - (int64_t)j * nu];
-      const uint32_t* p0 = sp.pre + (int64_t)j * NB;
-      const uint32_t* p1 = p0 + (int64_t)sp.wblk * NB;
-      const uint32_t a = p0[bin];
-      wc = p1[bin] - a;
+      const WinPre wp{sp.pre, sp.ts, j, sp.wblk};
+      const uint32_t* row = sp.pre + (int64_t)bin * sp.ts + j;
+      const uint32_t a = row[0];
+      wc = row[sp.wblk] - a;
       if (wc) {
         bool safe = false;
         if (sp.filter) {
           const bool single = pure || sp.kmin[bin] == sp.kmax[bin];
           safe = single && wc > (uint32_t)sp.K;
-          if (!safe && single && sp.h == 1 && sp.n >= 3) safe = span_group_safe(sp, p0, p1, bin, pure);
+          if (!safe && single && sp.h == 1 && sp.n >= 3) safe = span_group_safe(sp, wp, bin, pure);
           if (!safe && pure && sp.h > 1 && sp.n_sure > 1) {
             // the sure neighbourhood: cells within R of every point of this one
             uint32_t sum = 0;
             for (int t = 0; t < sp.n_sure; ++t) {
               const uint32_t nb = (bin + (uint32_t)sp.sure_delta[t]) & NB_MASK;
-              if (sp.bin_count[nb]) sum += p1[nb] - p0[nb];
+              if (sp.bin_count[nb]) sum += wp.count(nb);
             }
             safe = sum > (uint32_t)sp.K;
           }
@@ -565,8 +572,7 @@ __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
   for (int64_t k = gtid >> 5; k < ng; k += gstride >> 5) {
     const uint4 g = sp.groups[k];
     const int j = (int)g.w;
-    const uint32_t* p0 = sp.pre + (int64_t)j * NB;
-    span_count_group<D, PRED, T>(b, sp, j, g.x, g.y, g.z, p0, p0 + (int64_t)sp.wblk * NB, pure);
+    span_count_group<D, PRED, T>(b, sp, g.x, g.y, g.z, WinPre{sp.pre, sp.ts, j, sp.wblk}, pure);
   }
   // The per-bin state is no longer read in this batch: clear it, then the
   // block that finishes last ends the batch.
