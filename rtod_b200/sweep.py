@@ -43,7 +43,7 @@ def settings(dataset: str, param: str):
     raise ValueError(param)
 
 
-def run(dataset: str, param: str, warmup: int = 2, router: bool = True, tuner: bool = False,
+def run(dataset: str, param: str, warmup: int = 2, router: bool = False, tuner: bool = False,
         max_slides: int = 10000):
     w, grid = settings(dataset, param)
     rows = []
@@ -65,10 +65,13 @@ def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--dataset", choices=sorted(GRIDS), default="stk")
     ap.add_argument("--param", choices=["window", "slide", "R", "K"], default="K")
-    ap.add_argument("--plain", action="store_true", help="router off")
-    ap.add_argument("--tuner", action="store_true")
+    ap.add_argument("--router", action="store_true", help="learned router on (window engine)")
+    ap.add_argument("--tuner", action="store_true", help="autotune each setting on its first slides")
+    ap.add_argument("--max-slides", type=int, default=10000, help="slides per pass (RTOD caps at 10000)")
+    ap.add_argument("--warmup", type=int, default=2)
     args = ap.parse_args(argv)
-    for row in run(args.dataset, args.param, router=not args.plain, tuner=args.tuner):
+    for row in run(args.dataset, args.param, warmup=args.warmup, router=args.router, tuner=args.tuner,
+                   max_slides=args.max_slides):
         print(json.dumps(row))
     return 0
 

@@ -49,3 +49,35 @@ def test_cli_report_and_outliers(tmp_path, capsys, oracle_mod):
     for j, line in enumerate(lines):
         got = [int(t) for t in line.split(":", 1)[1].split()]
         assert got == ids[off[j]:off[j + 1]].tolist()
+
+
+@pytest.mark.parametrize("dataset", ["stk", "gau", "tao"])
+@pytest.mark.parametrize("param", ["window", "slide", "R", "K"])
+def test_sweep_grids_follow_the_reference_driver(dataset, param):
+    """Five settings per parameter, as script/run.py:76-218 varies them; every
+    window a whole number of slides."""
+    from rtod_b200 import sweep
+    w, grid = sweep.settings(dataset, param)
+    assert len(grid) == 5
+    for st in grid:
+        assert st["window"] % st["slide"] == 0 and st["R"] > 0 and st["K"] > 0
+    assert len({tuple(sorted(st.items())) for st in grid}) == 5
+
+
+@pytest.mark.gpu
+def test_sweep_rows_match_oracle(oracle_mod):
+    """A K sweep on the sensor-like stream, 3 slides per setting: each row's
+    outliers per slide equal the oracle's for that setting."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from rtod_b200 import sweep
+    rows = sweep.run("tao", "K", warmup=0, max_slides=3)
+    w, grid = sweep.settings("tao", "K")
+    assert [r["K"] for r in rows] == [st["K"] for st in grid]
+    for r in rows:
+        assert r["slides"] == 3 and r["ms_per_slide"] > 0
+        pts = w.points[:r["window"] + 3 * r["slide"]]
+        off, ids, _ = oracle_mod.detect(pts, r["window"], r["slide"], r["R"], r["K"], "fp32_le",
+                                        engine="grid", threads=8)
+        assert r["outliers_per_slide"] == pytest.approx(len(ids) / 3)
