@@ -190,6 +190,15 @@ int rtod_get_tuning(const rtod_handle* h, int32_t out[5]);
 /* The resolved window-engine count (RTOD_COUNT_POINT or RTOD_COUNT_GROUP). */
 int rtod_get_count_mode(const rtod_handle* h, int32_t* mode);
 
+/* Self-check of the device-side failure detection: runs the look-back wait
+   of the library's scans (k_scan, k_compact, k_span_scan) for a tile whose
+   predecessor never publishes, on `device`. The wait gives up after its
+   bound (a few hundred milliseconds), records RTOD_ERR_TIMEOUT's device code
+   and returns; *timed_out = 1 when that was recorded, *ms = the kernel's
+   time. Nothing faults or hangs, and the device stays usable. No
+   counterpart in RTOD, which has no device-side waits. */
+int rtod_check_bounded_wait(int32_t device, int32_t* timed_out, double* ms);
+
 /* Counters since create: out[0] kernel launches issued by the library (a
    graph replay counts each of its kernels), out[1] graph replays, out[2]
    slides detected, out[3] points that needed an exact count, out[4] device

@@ -75,6 +75,7 @@ SIGNATURES = [
     ("rtod_slides_done", _i64, [_vp]),
     ("rtod_get_tuning", _i32, [_vp, _vp]),
     ("rtod_get_count_mode", _i32, [_vp, ctypes.POINTER(_i32)]),
+    ("rtod_check_bounded_wait", _i32, [_i32, ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_double)]),
     ("rtod_get_stats", _i32, [_vp, _vp]),
     ("rtod_profile_run", _i32, [_vp, _vp, _i64, _i64, _vp, _i32]),
     ("rtod_kernel_name", ctypes.c_char_p, [_i32]),

@@ -1556,6 +1556,52 @@ RTOD_API int rtod_get_count_mode(const rtod_handle* h, int32_t* mode) {
   return RTOD_OK;
 }
 
+namespace {
+// Tile 1 of a scan whose tile 0 never publishes: the look-back wait runs
+// out after its bound, records the timeout and returns a partial prefix.
+__global__ void k_wait_check(unsigned long long* status, BatchState* bs, uint32_t* out) {
+  const uint32_t ex = warp_lookback(status, 1, 7, bs);
+  if (threadIdx.x == 0) *out = ex;
+}
+}  // namespace
+
+RTOD_API int rtod_check_bounded_wait(int32_t device, int32_t* timed_out, double* ms) {
+  if (!timed_out || !ms) return fail(RTOD_ERR_ARG, "null argument");
+  *timed_out = 0;
+  *ms = 0;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return fail(RTOD_ERR_NODEV, "bad device ordinal %d", device);
+  }
+  CU(cudaSetDevice(device));
+  unsigned long long* status = nullptr;
+  BatchState* bs = nullptr;
+  uint32_t* out = nullptr;
+  int64_t bytes = 0;
+  struct Free {
+    unsigned long long*& a;
+    BatchState*& b;
+    uint32_t*& c;
+    ~Free() { dfree(a); dfree(b); dfree(c); }
+  } fr{status, bs, out};
+  if (dalloc(&status, 2, &bytes) || dalloc(&bs, 1, &bytes) || dalloc(&out, 1, &bytes)) return RTOD_ERR_CUDA;
+  CU(cudaMemset(status, 0, 2 * sizeof(unsigned long long)));  // tile 0 never publishes
+  CU(cudaMemset(bs, 0, sizeof(BatchState)));
+  EventSet es;
+  cudaEvent_t a = es.make(), b = es.make();
+  CU(cudaEventRecord(a, 0));
+  k_wait_check<<<1, 32>>>(status, bs, out);
+  CU(cudaGetLastError());
+  CU(cudaEventRecord(b, 0));
+  CU(cudaEventSynchronize(b));
+  BatchState hs{};
+  CU(cudaMemcpy(&hs, bs, sizeof hs, cudaMemcpyDeviceToHost));
+  *ms = elapsed(a, b);
+  *timed_out = hs.err == DERR_TIMEOUT ? 1 : 0;
+  return RTOD_OK;
+}
+
 RTOD_API int rtod_get_stats(const rtod_handle* h, int64_t out[5]) {
   if (!h || !out) return fail(RTOD_ERR_ARG, "null argument");
   out[0] = h->launches;
