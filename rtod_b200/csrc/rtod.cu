@@ -305,6 +305,12 @@ struct rtod_handle {
   int64_t rec_cap = 0;
   BatchState* bs_mirror = nullptr;      // mapped page-locked copy of bs written by k_run_out
   BatchState* bs_mirror_dev = nullptr;  // its device view
+  // Streaming (push/detect): a page-locked copy of the caller's slide, and
+  // the mapped landing buffer of one window's IDs written by k_run_out.
+  void* stage_host = nullptr;
+  int64_t* ids_host = nullptr;
+  int64_t* ids_host_dev = nullptr;
+  int64_t ids_host_cap = 0;
   int64_t* ids = nullptr;
   int64_t ids_cap = 0;
 
@@ -812,10 +818,21 @@ constexpr int kTrainEvery = 8;  // batches between two router training steps
 
 bool train_now(rtod_handle* h) { return h->cfg.router && (h->batches++ % kTrainEvery) == 0; }
 
+// End of a streaming detection (ring jobs): the window's IDs and the batch
+// state into the mapped landing buffers (ensure_detect_out).
+int launch_detect_tail(rtod_handle* h, int64_t* nk) {
+  const unsigned ox = (unsigned)std::max<int64_t>(1, std::min<int64_t>((h->W + 255) / 256, h->sm_count));
+  CU(launch_k(k_run_out, dim3(ox), 256, h->stream, (const int64_t*)h->ids, h->ids_host_dev,
+              std::min(h->ids_host_cap, h->ids_cap), h->bs, h->bs_mirror_dev));
+  ++*nk;
+  return RTOD_OK;
+}
+
 int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev, const Span* sp = nullptr) {
   int64_t nk = 0;
   int r = sp ? launch_span(geom_of(h), b, *sp, h->stream, kev, &nk)
              : launch_group(geom_of(h), b, ingest, train_now(h), h->stream, kev, &nk);
+  if (!r && ingest) r = launch_detect_tail(h, &nk);
   h->launches += nk;
   return r;
 }
@@ -836,6 +853,7 @@ int run_batch(rtod_handle* h, const Batch& b, bool ingest, const Span* sp = null
     int64_t nk = 0;
     int r = sp ? launch_span(geom_of(h), b, *sp, h->stream, nullptr, &nk)
                : launch_group(geom_of(h), b, ingest, train, h->stream, nullptr, &nk);
+    if (!r && ingest) r = launch_detect_tail(h, &nk);
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (r) return r;
     if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
@@ -921,6 +939,30 @@ int ensure_records(rtod_handle* h, int64_t n) {
   h->rec_nout = (int32_t*)dp;
   h->rec_undet = h->rec_nout + n;
   h->rec_cap = n;
+  return RTOD_OK;
+}
+
+// Landing buffers of streaming detection: the batch state mirror and one
+// window's IDs in mapped page-locked memory (k_run_out writes both at the
+// end of the detect graph, so the host waits once and copies nothing back).
+int ensure_detect_out(rtod_handle* h) {
+  if (!h->bs_mirror) {
+    void* dp = nullptr;
+    CU(cudaHostAlloc((void**)&h->bs_mirror, sizeof(BatchState), cudaHostAllocMapped));
+    CU(cudaHostGetDevicePointer(&dp, h->bs_mirror, 0));
+    h->bs_mirror_dev = (BatchState*)dp;
+  }
+  if (h->ids_host_cap < h->W) {
+    drop_graph(h);
+    if (h->ids_host) cudaFreeHost(h->ids_host);
+    h->ids_host = h->ids_host_dev = nullptr;
+    h->ids_host_cap = 0;
+    void* dp = nullptr;
+    CU(cudaHostAlloc((void**)&h->ids_host, (size_t)h->W * sizeof(int64_t), cudaHostAllocMapped));
+    CU(cudaHostGetDevicePointer(&dp, h->ids_host, 0));
+    h->ids_host_dev = (int64_t*)dp;
+    h->ids_host_cap = h->W;
+  }
   return RTOD_OK;
 }
 
@@ -1225,6 +1267,11 @@ void free_all(rtod_handle* h) {
   h->rec_nout = h->rec_undet = h->rec_nout_h = h->rec_undet_h = nullptr;
   if (h->bs_mirror) cudaFreeHost(h->bs_mirror);
   h->bs_mirror = h->bs_mirror_dev = nullptr;
+  if (h->stage_host) cudaFreeHost(h->stage_host);
+  h->stage_host = nullptr;
+  if (h->ids_host) cudaFreeHost(h->ids_host);
+  h->ids_host = h->ids_host_dev = nullptr;
+  h->ids_host_cap = 0;
   if (h->ctr_init) cudaFreeHost(h->ctr_init);
   h->ctr_init = nullptr;
   for (auto& e : h->ev)
@@ -1637,8 +1684,18 @@ int push_impl(rtod_handle* h, const void* pts, int64_t n, bool f64) {
     if (h->pending) return fail(RTOD_ERR_STATE, "rtod_detect must follow each slide push");
     if (n != S) return fail(RTOD_ERR_STATE, "a slide push must hold exactly S=%lld points", (long long)S);
   }
+  const size_t bytes = (size_t)(n * D * h->esz);
+  const void* src = pts;
+  if (h->n_pushed > 0 && !is_device_ptr(pts)) {
+    // A slide from host memory: copied on the host into a page-locked buffer
+    // (the caller may reuse its buffer at once), then one asynchronous DMA.
+    // The previous slide's DMA is done: every detection ends with a wait.
+    if (!h->stage_host) CU(cudaMallocHost(&h->stage_host, (size_t)(S * D * h->esz)));
+    std::memcpy(h->stage_host, pts, bytes);
+    src = h->stage_host;
+  }
   CU(cudaEventRecord(h->ev[4], h->stream));
-  CU(cudaMemcpyAsync(h->staging, pts, (size_t)(n * D * h->esz), cudaMemcpyDefault, h->stream));
+  CU(cudaMemcpyAsync(h->staging, src, bytes, cudaMemcpyDefault, h->stream));
   CU(cudaEventRecord(h->ev[5], h->stream));
   if (h->n_pushed == 0) {
     int r = configure(h, MODE_RING, 1, S, nullptr);  // first detected window: [S, W + S)
@@ -1671,6 +1728,7 @@ RTOD_API int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t*
   if (h->poisoned) return fail(RTOD_ERR_STATE, "handle is in an error state; call rtod_reset");
   if (!h->pending) return fail(RTOD_ERR_STATE, "no pushed slide to detect");
   CU(cudaSetDevice(h->device));
+  if (int r0 = ensure_detect_out(h)) return r0;
   // Per-call output: this slide's IDs start at the beginning of the buffer.
   CU(cudaMemsetAsync(&h->bs->out_total, 0, sizeof(int64_t), h->stream));
   const Batch b = make_batch(h, 1, h->ids_cap);
@@ -1682,9 +1740,12 @@ RTOD_API int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t*
   }
   int r = times ? launch_batch(h, b, true, kev) : run_batch(h, b, true);
   if (r) return r;
-  BatchState s;
-  CU(cudaMemcpyAsync(&s, h->bs, sizeof s, cudaMemcpyDeviceToHost, h->stream));
+  if (times) CU(cudaEventRecord(h->ev[7], h->stream));
+  // The IDs and the batch state arrive in the mapped landing buffers
+  // (k_run_out, the graph's last kernel): one wait.
   CU(cudaStreamSynchronize(h->stream));
+  BatchState s;
+  std::memcpy(&s, h->bs_mirror, sizeof s);
   h->pending = false;
   r = check_device_error(h, s);
   if (r) return r;
@@ -1693,19 +1754,23 @@ RTOD_API int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t*
   *n_out = s.out_total;
   if (s.out_total > cap)
     return fail(RTOD_ERR_CAPACITY, "%lld outliers but room for %lld", (long long)s.out_total, (long long)cap);
-  if (times) CU(cudaEventRecord(h->ev[6], h->stream));
-  if (s.out_total > 0)
-    CU(cudaMemcpyAsync(out_ids, h->ids, (size_t)s.out_total * sizeof(int64_t), cudaMemcpyDefault, h->stream));
-  if (times) CU(cudaEventRecord(h->ev[7], h->stream));
-  CU(cudaStreamSynchronize(h->stream));
+  if (s.out_total > 0) {
+    if (is_device_ptr(out_ids)) {
+      CU(cudaMemcpyAsync(out_ids, h->ids, (size_t)s.out_total * sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                         h->stream));
+      CU(cudaStreamSynchronize(h->stream));
+    } else {
+      std::memcpy(out_ids, h->ids_host, (size_t)s.out_total * sizeof(int64_t));
+    }
+  }
   if (times) {
     std::memset(times, 0, sizeof *times);
     times->copy_new_points_h2d = elapsed(h->ev[4], h->ev[5]);
     times->prepare_cell = elapsed(h->ev[0], kev[1]);   // ring update + occupancy
     times->build_bvh = elapsed(kev[1], kev[3]);       // scan + scatter
     times->detect_outlier = elapsed(kev[3], kev[5]);  // count + compact
-    times->copy_outlier_d2h = elapsed(h->ev[6], h->ev[7]);
-    times->total = times->copy_new_points_h2d + elapsed(h->ev[0], kev[5]) + times->copy_outlier_d2h;
+    times->copy_outlier_d2h = elapsed(kev[6], h->ev[7]);  // k_run_out
+    times->total = times->copy_new_points_h2d + elapsed(h->ev[0], h->ev[7]);
     times->undetermined_per_slide = (double)s.undet_total;
     times->slides = 1;
   }

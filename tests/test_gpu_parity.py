@@ -51,6 +51,28 @@ def test_push_detect_matches_golden(rtod, path):
         assert det.slides_done == len(off) - 1
 
 
+@pytest.mark.parametrize("source", ["host", "pinned", "device"])
+def test_push_buffer_reused_at_once(rtod, source):
+    """The caller may overwrite a pushed slide's buffer right after the push
+    returns: the detection still sees the pushed points (host slides are
+    copied into a page-locked buffer during the push)."""
+    import torch
+    meta, pts, off, ids = load_golden(golden_cases()[-1])
+    W, S = meta["W"], meta["S"]
+    buf = torch.empty((S, pts.shape[1]), dtype=torch.float32)
+    if source == "pinned":
+        buf = buf.pin_memory()
+    if source == "device":
+        buf = buf.cuda()
+    with rtod.Detector(W, S, meta["R"], meta["K"], dim=pts.shape[1], pred=meta["pred"]) as det:
+        det.push(pts[:W])
+        for j in range(len(off) - 1):
+            buf.copy_(torch.from_numpy(pts[W + j * S:W + (j + 1) * S]))
+            det.push(buf.numpy() if source != "device" else buf)
+            buf.fill_(1e30)  # garbage: must not reach the detection
+            np.testing.assert_array_equal(det.detect(), ids[off[j]:off[j + 1]])
+
+
 def oracle_check(rtod, oracle_mod, pts, W, S, R, K, slides, pred="fp32_le", **kw):
     pts = pts[:W + slides * S]
     off, ids, _ = oracle_mod.detect(pts, W, S, R, K, pred, engine="grid", threads=8)
