@@ -2210,7 +2210,17 @@ RTOD_API int rtod_batch_push(rtod_batch* b, int32_t s, const float* pts, int64_t
   if (b->pending[s]) return fail(RTOD_ERR_STATE, "stream %d already has a pending slide", s);
   if (n != h->S) return fail(RTOD_ERR_STATE, "stream %d: a slide push must hold exactly S=%lld points", s,
                              (long long)h->S);
-  CU(cudaMemcpyAsync(h->staging, pts, (size_t)(n * h->D) * sizeof(float), cudaMemcpyDefault, b->stream));
+  // Host slides go through the stream's page-locked buffer (copied here, so
+  // the caller may reuse its buffer at once); the step that follows waits
+  // for the DMA before the next push can touch that buffer.
+  const size_t bytes = (size_t)(n * h->D) * sizeof(float);
+  const void* src = pts;
+  if (!is_device_ptr(pts)) {
+    if (!h->stage_host) CU(cudaMallocHost(&h->stage_host, bytes));
+    std::memcpy(h->stage_host, pts, bytes);
+    src = h->stage_host;
+  }
+  CU(cudaMemcpyAsync(h->staging, src, bytes, cudaMemcpyDefault, b->stream));
   b->pending[s] = 1;
   return RTOD_OK;
 }

@@ -72,3 +72,27 @@ def test_batch_matches_oracle(rtod, oracle_mod, router, count):
         stats = bd.stats
         assert stats["groups"] == 4  # d=1, d=3, d=8 with fp32, and the f64 stream
         assert stats["detections"] == sum(st["slides"] for st in streams)
+
+
+def test_batch_push_buffer_reused_at_once(rtod, oracle_mod):
+    """Slides pushed from one page-locked buffer that the caller overwrites
+    right after each push: every step still detects the pushed points."""
+    import torch
+    streams = make_streams(n=3, seed=7)
+    expect = [oracle_mod.detect(st["points"], st["window"], st["slide"], st["R"], st["K"], st["pred"],
+                                engine="grid", threads=4)[:2] for st in streams]
+    cfg = [{k: st[k] for k in ("window", "slide", "R", "K", "dim", "pred")} for st in streams]
+    bufs = [torch.empty((st["slide"], st["dim"]), dtype=torch.float32).pin_memory() for st in streams]
+    with rtod.BatchDetector(cfg) as bd:
+        for i, st in enumerate(streams):
+            bd.push(i, st["points"][:st["window"]])
+        for j in range(min(st["slides"] for st in streams)):
+            for i, st in enumerate(streams):
+                W, S = st["window"], st["slide"]
+                bufs[i].copy_(torch.from_numpy(st["points"][W + j * S:W + (j + 1) * S]))
+                bd.push(i, bufs[i].numpy())
+                bufs[i].fill_(1e30)
+            res = bd.step()
+            for i in range(len(streams)):
+                off, ids = expect[i]
+                np.testing.assert_array_equal(res[i], ids[off[j]:off[j + 1]])
