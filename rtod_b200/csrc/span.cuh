@@ -500,6 +500,9 @@ __device__ __forceinline__ void span_clear_bins(const SpanCtr* c) {
 // of every point of its cell) is appended to the batch's list of groups to
 // count (first position, points, bin, window): one atomic per warp for the
 // list, one per window present in the warp for its count of listed points.
+// Pairs run bin-major (consecutive windows of a bin together), so the list
+// holds a bin's windows side by side and neighbouring count warps read
+// mostly the same candidates.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
   pdl_trigger();
@@ -515,8 +518,11 @@ __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
     uint32_t start = 0, wc = 0, bin = 0;
     bool need = false;
     if (e < pairs) {
-      j = (int)(e / nu);
-      bin = sp.used[e - (int64_t)j * nu];
+      // bin-major pairs: a warp takes consecutive windows of one bin (one
+      // contiguous row of pre), and consecutive groups share their stencil
+      const int64_t u = e / b.njobs;
+      j = (int)(e - u * b.njobs);
+      bin = sp.used[u];
       const WinPre wp{sp.pre, sp.ts, j, sp.wblk};
       const uint32_t* row = sp.pre + (int64_t)bin * sp.ts + j;
       const uint32_t a = row[0];
