@@ -30,11 +30,12 @@ def det(rtod, W, S, R, K, dim, **kw):
 
 
 @pytest.mark.parametrize("path", golden_cases_f64(), ids=lambda p: os.path.basename(p)[:-4])
-@pytest.mark.parametrize("engine,graph", [("window", True), ("window", False), ("span", True)])
+@pytest.mark.parametrize("engine,graph", [("window", True), ("window", False), ("span", True),
+                                          ("window-group", True)])
 def test_run_matches_double_golden(rtod, path, engine, graph):
     meta, pts, off, ids = load_golden(path)
-    with det(rtod, meta["W"], meta["S"], meta["R"], meta["K"], pts.shape[1], engine=engine,
-             use_graph=graph) as d:
+    kw = dict(engine="window", count="group") if engine == "window-group" else dict(engine=engine)
+    with det(rtod, meta["W"], meta["S"], meta["R"], meta["K"], pts.shape[1], use_graph=graph, **kw) as d:
         r = d.run(pts)
     np.testing.assert_array_equal(r.offsets, off)
     np.testing.assert_array_equal(r.ids, ids)

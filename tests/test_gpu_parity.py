@@ -257,3 +257,32 @@ def test_fine_cells_1d_match_golden(rtod, path, n):
     with rtod.Detector(meta["W"], meta["S"], meta["R"], meta["K"], pred=meta["pred"],
                        cells_per_r=n) as det:
         assert_same(det.run(pts), off, ids)
+
+
+def test_handles_on_several_host_threads(rtod):
+    """One handle per host thread, all running at once (each handle owns its
+    stream and graphs; the tuner's cache is shared): the same results as one
+    after another."""
+    import threading
+    from rtod_b200 import datagen
+    cases = [datagen.small_walk(), datagen.sensor_like(), datagen.gaussian_like(30), datagen.small_walk()]
+    def run(w, tuner):
+        with rtod.Detector(w.window, w.slide, w.R, w.K, dim=w.dim, tuner=tuner) as det:
+            return det.run(w.points, max_slides=40)
+    ref = [run(w, False) for w in cases]
+    got = [None] * len(cases)
+    errs = []
+    def worker(i):
+        try:
+            for _ in range(3):
+                got[i] = run(cases[i], i % 2 == 1)
+        except Exception as e:  # surfaced below
+            errs.append(e)
+    th = [threading.Thread(target=worker, args=(i,)) for i in range(len(cases))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs, errs
+    for r, g in zip(ref, got):
+        assert_same(g, r.offsets, r.ids)
