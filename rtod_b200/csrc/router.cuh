@@ -45,6 +45,7 @@ constexpr int MLP_P = OFF_B3 + MLP_B;             // 1316 parameters
 constexpr int TRAIN_CAP = 2048;                   // training samples buffered between steps
 constexpr int TRAIN_CHUNK = 128;                  // samples per chunk of k_train
 constexpr int TRAIN_MAX = 128;                    // samples used by one training step
+constexpr int TRAIN_STEPS = 2;                    // training steps per k_train launch at most
 constexpr uint32_t INLIER_THIN = 16;              // inlier samples kept: one in 16
 constexpr int TQ0 = 32, TQ1 = 32, TQ2 = 16;       // routing table grid
 constexpr float F0_MAX = 1.5f, F1_MAX = 2.5f, F2_MIN = -1.0f, F2_MAX = 2.0f;
@@ -274,20 +275,27 @@ __device__ void mlp_train_block(float* P, float* m, float* v, float* b1t, float*
   }
 }
 
-// Online training: one Adam step on up to TRAIN_MAX buffered samples once
-// enough have accumulated; the buffer is then emptied.
+// Online training: once enough samples are buffered, up to TRAIN_STEPS Adam
+// steps, each on the next TRAIN_MAX buffered samples; the buffer is then
+// emptied.
 __global__ void __launch_bounds__(256) k_train(RouterState* rs) {
   extern __shared__ float smem[];
   pdl_trigger();
   pdl_wait();
-  const uint32_t n = min(rs->n_samples, (uint32_t)TRAIN_MAX);
+  const uint32_t n = min(rs->n_samples, (uint32_t)TRAIN_CAP);
   if (n < rs->min_samples || n == 0) return;
   float loss = 0.0f;
-  mlp_train_block(rs->params, rs->m, rs->v, &rs->b1t, &rs->b2t, rs->lr, rs->beta1, rs->beta2, rs->eps,
-                  &rs->samples[0][0], 4, &rs->samples[0][3], 4, (int)n, nullptr, &loss, true, smem);
+  uint32_t steps = 0;
+  for (uint32_t off = 0; off < n && steps < (uint32_t)TRAIN_STEPS; off += TRAIN_MAX, ++steps) {
+    const int m = (int)min((uint32_t)TRAIN_MAX, n - off);
+    if (m < (int)rs->min_samples && steps > 0) break;  // a short tail waits for the next launch
+    mlp_train_block(rs->params, rs->m, rs->v, &rs->b1t, &rs->b2t, rs->lr, rs->beta1, rs->beta2, rs->eps,
+                    &rs->samples[off][0], 4, &rs->samples[off][3], 4, m, nullptr, &loss, true, smem);
+    __syncthreads();
+  }
   if (threadIdx.x == 0) {
     rs->last_loss = loss;
-    rs->steps += 1;
+    rs->steps += steps;
     rs->n_samples = 0;
   }
 }

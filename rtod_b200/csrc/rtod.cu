@@ -225,7 +225,7 @@ void init_router(RouterState* r) {
   for (int i = 0; i < MLP_B * MLP_H; ++i) r->params[OFF_W3 + i] = uni(a3);
   r->params[OFF_B3 + 3] = 2.0f;
   r->b1t = r->b2t = 1.0f;
-  r->lr = 1e-3f;
+  r->lr = 3e-3f;
   r->beta1 = 0.9f;
   r->beta2 = 0.999f;
   r->eps = 1e-8f;
@@ -814,9 +814,14 @@ Geom geom_of(const rtod_handle* h) {
               h->router, h->f64, h->group};
 }
 
-constexpr int kTrainEvery = 8;  // batches between two router training steps
+constexpr int kTrainEvery = 16;  // batches between two router training launches (after the first)
+constexpr int kTrainWarm = 32;   // the first batches train after every batch
 
-bool train_now(rtod_handle* h) { return h->cfg.router && (h->batches++ % kTrainEvery) == 0; }
+bool train_now(rtod_handle* h) {
+  if (!h->cfg.router) return false;
+  const int64_t n = h->batches++;
+  return n < kTrainWarm || n % kTrainEvery == 0;
+}
 
 // End of a streaming detection (ring jobs): the window's IDs and the batch
 // state into the mapped landing buffers (ensure_detect_out).
@@ -1430,12 +1435,12 @@ int autotune(rtod_handle* h, const void* pts, int64_t slides_total) {
     if ((r = trial(t))) return r;
   }
   if (h->cfg.router && best.engine == RTOD_ENGINE_WINDOW && !best.group) {
-    for (float th : {0.3f, 0.7f}) {
+    for (float th : {0.3f, 0.7f, 0.9f}) {
       Tuning t = best;
       t.threshold = th;
       if ((r = trial(t))) return r;
     }
-    for (uint32_t ms : {32u, 128u}) {
+    for (uint32_t ms : {32u, 128u, 512u}) {
       Tuning t = best;
       t.max_sweep = ms;
       if ((r = trial(t))) return r;
@@ -2235,7 +2240,7 @@ RTOD_API int rtod_batch_step(rtod_batch* b, int64_t* out_offsets, int64_t* out_i
       any |= g.active_h[k];
     }
   if (!any) return fail(RTOD_ERR_STATE, "no stream has a pushed slide");
-  const bool train = b->route && (b->steps % kTrainEvery) == 0;
+  const bool train = b->route && (b->steps < kTrainWarm || b->steps % kTrainEvery == 0);
   cudaGraphExec_t& gx = b->graphs[train ? 1 : 0];
   if (!gx) {
     cudaGraph_t gr;

@@ -146,6 +146,36 @@ def test_router_results_identical_to_plain(gpu, oracle_mod, case):
 
 
 @pytest.mark.gpu
+def test_router_learns_to_spot_outliers(gpu):
+    """On the Gaussian-mixture stream most counted points are outliers (noise
+    between the clusters): the untrained network (biased towards inliers)
+    sends them all to the early-exit queue, the trained one routes them to
+    the full-sweep queue and misroutes far fewer points. Results are the
+    same either way."""
+    rtod, _ = gpu
+    from rtod_b200 import datagen
+    w = datagen.gaussian_like(30)
+    with rtod.Detector(w.window, w.slide, w.R, w.K, engine="window") as plain:
+        ref = plain.run(w.points, max_slides=64)
+    with rtod.Detector(w.window, w.slide, w.R, w.K, engine="window", router=True) as det:
+        r = det.run(w.points, max_slides=64)
+        i0 = det.router_info()
+        first = i0["misrouted"] / max(1, i0["routed_early"] + i0["routed_sweep"])
+        for _ in range(8):
+            det.reset()
+            r = det.run(w.points, max_slides=64)
+        i1 = det.router_info()
+        n = i1["routed_early"] + i1["routed_sweep"] - i0["routed_early"] - i0["routed_sweep"]
+        later = (i1["misrouted"] - i0["misrouted"]) / max(1, n)
+        sweep = (i1["routed_sweep"] - i0["routed_sweep"]) / max(1, n)
+    np.testing.assert_array_equal(r.offsets, ref.offsets)
+    np.testing.assert_array_equal(r.ids, ref.ids)
+    assert first > 0.5            # untrained: the outliers go to the early-exit queue
+    assert later < 0.5 * first    # trained: far fewer misroutes
+    assert sweep > 0.3            # the outliers now take the full-sweep queue
+
+
+@pytest.mark.gpu
 def test_trained_router_beats_untrained(gpu):
     """What the trained network gains: after online training its routing makes
     fewer mistakes than the untrained network on the same stream."""
