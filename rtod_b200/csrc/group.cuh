@@ -69,7 +69,7 @@ __device__ __forceinline__ bool slot_sure(const int* d, int n) {
 // Candidates per lane and chunk: fewer for many dimensions (registers).
 template <int D>
 struct GroupCpl {
-  static constexpr int value = D == 1 ? 4 : (D <= 3 ? 8 : 4);
+  static constexpr int value = D == 1 ? 2 : (D <= 3 ? 8 : 4);
 };
 
 struct GroupArgs {
