@@ -835,6 +835,8 @@ int launch_detect_tail(rtod_handle* h, int64_t* nk) {
 
 int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev, const Span* sp = nullptr) {
   int64_t nk = 0;
+  // streaming detection: this window's IDs start at the beginning of the buffer
+  if (ingest) CU(cudaMemsetAsync(&h->bs->out_total, 0, sizeof(int64_t), h->stream));
   int r = sp ? launch_span(geom_of(h), b, *sp, h->stream, kev, &nk)
              : launch_group(geom_of(h), b, ingest, train_now(h), h->stream, kev, &nk);
   if (!r && ingest) r = launch_detect_tail(h, &nk);
@@ -856,6 +858,7 @@ int run_batch(rtod_handle* h, const Batch& b, bool ingest, const Span* sp = null
     cudaGraph_t g;
     CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int64_t nk = 0;
+    if (ingest) CU(cudaMemsetAsync(&h->bs->out_total, 0, sizeof(int64_t), h->stream));  // as in launch_batch
     int r = sp ? launch_span(geom_of(h), b, *sp, h->stream, nullptr, &nk)
                : launch_group(geom_of(h), b, ingest, train, h->stream, nullptr, &nk);
     if (!r && ingest) r = launch_detect_tail(h, &nk);
@@ -1734,8 +1737,6 @@ RTOD_API int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t*
   if (!h->pending) return fail(RTOD_ERR_STATE, "no pushed slide to detect");
   CU(cudaSetDevice(h->device));
   if (int r0 = ensure_detect_out(h)) return r0;
-  // Per-call output: this slide's IDs start at the beginning of the buffer.
-  CU(cudaMemsetAsync(&h->bs->out_total, 0, sizeof(int64_t), h->stream));
   const Batch b = make_batch(h, 1, h->ids_cap);
   cudaEvent_t kev[7];
   EventSet es;

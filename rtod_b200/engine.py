@@ -117,7 +117,9 @@ class Detector:
 
     def detect(self, times: bool = False):
         """Outliers (sorted global indices) of the window after the last push."""
-        out = np.empty(self.window, np.int64)
+        out = self.__dict__.get("_detect_out")
+        if out is None:  # one buffer per detector: a window has at most W outliers
+            out = self._detect_out = np.empty(self.window, np.int64)
         n_out = ctypes.c_int64()
         t = Times()
         check(lib().rtod_detect(self._h, out.ctypes.data_as(ctypes.c_void_p), out.size,
