@@ -30,7 +30,7 @@
 //    count.
 //  * Brute force: check_outlier, src/ods/optixScan.cpp:817-881.
 //
-// Deliberate differences, each documented in DESIGN.md:
+// Deliberate differences (none changes a result):
 //  * Predicate. PRED_FP32_LE (default): dx_i = fl32(p_i - q_i),
 //    d2 = fl32(...fl32(fl32(dx_0^2) + fl32(dx_1^2))... + fl32(dx_{d-1}^2))
 //    summed left to right without FMA, neighbour iff d2 <= fl32(Rf*Rf) with
