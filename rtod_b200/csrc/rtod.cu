@@ -449,7 +449,7 @@ int scrub(rtod_handle* h) {
     CU(cudaMemsetAsync(sp.kmin, 0xff, NB * sizeof(unsigned long long), h->stream));
     CU(cudaMemsetAsync(sp.kmax, 0, NB * sizeof(unsigned long long), h->stream));
     CU(cudaMemsetAsync(sp.cnt, 0, (size_t)(sp.ts * NB) * sizeof(uint32_t), h->stream));
-    CU(cudaMemsetAsync(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long), h->stream));
+    CU(cudaMemsetAsync(sp.scan_status, 0, SPAN_SCAN_TILES * sizeof(unsigned long long), h->stream));
     SpanCtr c{};  // counters back to their starting values
     for (int d = 0; d < 3; ++d) {
       c.cmin[d] = LLONG_MAX;
@@ -489,7 +489,7 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
             !dalloc(&sp.kmin, NB, &bytes) && !dalloc(&sp.kmax, NB, &bytes) &&
             !dalloc(&sp.cnt, (size_t)((nblk + 1) * NB), &bytes) && !dalloc(&sp.pre, (size_t)((nblk + 1) * NB), &bytes) &&
             !dalloc(&sp.used, NB, &bytes) && !dalloc(&sp.s_off, (size_t)pts, &bytes) &&
-            !dalloc(&sp.s_x, (size_t)(Wp * h->D * h->esz), &bytes) && !dalloc(&sp.scan_status, SCAN_TILES, &bytes) &&
+            !dalloc(&sp.s_x, (size_t)(Wp * h->D * h->esz), &bytes) && !dalloc(&sp.scan_status, SPAN_SCAN_TILES, &bytes) &&
             !dalloc(&sp.sc, 1, &bytes) && !dalloc(&sp.bits, (size_t)(chunk * words), &bytes) &&
             !dalloc(&sp.groups, (size_t)((nblk - h->W / h->S + 1) * std::min<int64_t>(h->W, NB)), &bytes);
   sp.bytes = bytes;
@@ -509,7 +509,7 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
   CU(cudaMemset(sp.kmax, 0, NB * sizeof(unsigned long long)));
   CU(cudaMemset(sp.cnt, 0, (size_t)(sp.ts * NB) * sizeof(uint32_t)));
   CU(cudaMemset(sp.s_x, 0, (size_t)(Wp * h->D * h->esz)));
-  CU(cudaMemset(sp.scan_status, 0, SCAN_TILES * sizeof(unsigned long long)));
+  CU(cudaMemset(sp.scan_status, 0, SPAN_SCAN_TILES * sizeof(unsigned long long)));
   SpanCtr c{};
   for (int d = 0; d < 3; ++d) {
     c.cmin[d] = LLONG_MAX;
@@ -776,7 +776,7 @@ int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, 
   if (kev) CU(cudaEventRecord(kev[0], st));
   DISPATCH_DT(g.f64, g.D, CU(launch_k(k_span_hist<D, T>, dim3((unsigned)hx), 256, st, b, sp)));
   if (kev) CU(cudaEventRecord(kev[1], st));
-  CU(launch_k(k_span_scan, dim3(SCAN_TILES), 256, st, b, sp));
+  CU(launch_k(k_span_scan, dim3(SPAN_SCAN_TILES), 256, st, b, sp));
   CU(launch_k(k_span_prefix, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
   if (kev) CU(cudaEventRecord(kev[2], st));
   DISPATCH_DT(g.f64, g.D, CU(launch_k(k_span_scatter<D, T>, dim3((unsigned)hx), 256, st, b, sp)));

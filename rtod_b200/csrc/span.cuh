@@ -62,7 +62,7 @@ struct Span {
   uint32_t* used;   // [NB] bins holding span points, n_used of them, in no particular order
   uint32_t* s_off;  // [span] bin-ordered: offset from the span start
   void* s_x;        // [D][Wp] bin-ordered coordinates (the handle's coordinate type)
-  unsigned long long* scan_status;  // [SCAN_TILES]
+  unsigned long long* scan_status;  // [SPAN_SCAN_TILES]
   SpanCtr* sc;
   uint4* groups;    // [B * min(W, NB)] listed groups: first position, points, bin, window
   uint32_t* bits;   // [chunk][words] outlier bits per window offset, row = slide % chunk
@@ -264,26 +264,27 @@ __global__ void __launch_bounds__(256) k_span_prefix(Batch b, Span sp) {
 }
 
 // k_span_scan: bin_start of the span (exclusive scan of bin_count), the list
-// of bins in use (each thread appends its non-empty bins of 16) and the
+// of bins in use (each thread appends its non-empty bins of 4) and the
 // span's purity.
 __global__ void __launch_bounds__(256) k_span_scan(Batch b, Span sp) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t s_base;
   pdl_trigger();
   pdl_wait();
-  scan_bins(sp.bin_count, sp.bin_start, sp.scan_status, &sp.sc->scan_ticket, b.bs);
-  // this block's 4096 bins (scan_bins took a tile by ticket; any split of the
-  // bins over the blocks will do here)
-  const uint32_t b0 = blockIdx.x * SCAN_TILE + threadIdx.x * 16;
-  uint32_t c[16];
+  scan_bins<SPAN_SCAN_TILE>(sp.bin_count, sp.bin_start, sp.scan_status, &sp.sc->scan_ticket, b.bs);
+  // this block's SPAN_SCAN_TILE bins (scan_bins took a tile by ticket; any
+  // split of the bins over the blocks will do here)
+  constexpr int Q = SPAN_SCAN_TILE / 1024;
+  const uint32_t b0 = blockIdx.x * SPAN_SCAN_TILE + threadIdx.x * 4 * Q;
+  uint32_t c[4 * Q];
   uint32_t nz = 0;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
+  for (int q = 0; q < Q; ++q) {
     const uint4 v = *reinterpret_cast<const uint4*>(sp.bin_count + b0 + 4 * q);
     c[4 * q] = v.x; c[4 * q + 1] = v.y; c[4 * q + 2] = v.z; c[4 * q + 3] = v.w;
   }
 #pragma unroll
-  for (int e = 0; e < 16; ++e) nz += c[e] != 0;
+  for (int e = 0; e < 4 * Q; ++e) nz += c[e] != 0;
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     // pure: the span's cells, widened by the sure / group-rule neighbours
     // (within n-2), map to distinct bins
@@ -299,7 +300,7 @@ __global__ void __launch_bounds__(256) k_span_scan(Batch b, Span sp) {
   __syncthreads();
   uint32_t o = s_base + ex;
 #pragma unroll
-  for (int e = 0; e < 16; ++e)
+  for (int e = 0; e < 4 * Q; ++e)
     if (c[e]) sp.used[o++] = b0 + e;
 }
 
@@ -319,7 +320,7 @@ __global__ void __launch_bounds__(256) k_span_scatter(Batch b, Span sp) {
   constexpr int U = 4;
   const int64_t lo0 = span_lo(b);
   const int64_t npts = sp.nblk * sp.S;
-  if (blockIdx.x == 0 && threadIdx.x < SCAN_TILES) sp.scan_status[threadIdx.x] = 0;
+  if (blockIdx.x == 0 && threadIdx.x < SPAN_SCAN_TILES) sp.scan_status[threadIdx.x] = 0;
   for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
     tkey[t] = 0xffffffffu;
     tcnt[t] = 0;
