@@ -772,7 +772,8 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
 // timed by run_stream).
 int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, cudaEvent_t* kev, int64_t* nk) {
   const int64_t npts = sp.nblk * sp.S;
-  const int64_t hx = std::max<int64_t>(1, std::min<int64_t>((npts + 1023) / 1024, (int64_t)g.sm_count * 8));
+  // histogram and scatter: 512 points per block and step, up to 16 blocks per SM
+  const int64_t hx = std::max<int64_t>(1, std::min<int64_t>((npts + 511) / 512, (int64_t)g.sm_count * 16));
   if (kev) CU(cudaEventRecord(kev[0], st));
   DISPATCH_DT(g.f64, g.D, CU(launch_k(k_span_hist<D, T>, dim3((unsigned)hx), 256, st, b, sp)));
   if (kev) CU(cudaEventRecord(kev[1], st));
