@@ -712,7 +712,7 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
     launched++;
   }
   if (kev) CU(cudaEventRecord(kev[0], st));
-  const int64_t per_block = 256 * (g.D <= 3 ? 4 : 2);  // points per block per loop iteration
+  const int64_t per_block = 256 * (g.D <= 3 ? 2 : 1);  // points per block per loop iteration (Unroll)
   const int64_t wx = std::max<int64_t>(
       1, std::min<int64_t>((W + per_block - 1) / per_block, std::max<int64_t>(2, (g.sm_count * 16 + nj - 1) / nj)));
   DISPATCH_D(g.D, CU(launch_k(k_hist<D>, dim3((unsigned)wx, gy), 256, st, b)));
