@@ -572,7 +572,8 @@ __device__ __forceinline__ bool window_pure(const Job& jb, int64_t lo) {
 
 
 
-constexpr int HIST_SLOTS = 256;  // block-local aggregation table of k_hist and k_scatter
+constexpr int HIST_BITS = 8;                  // slot index bits of the table below
+constexpr int HIST_SLOTS = 1 << HIST_BITS;  // block-local aggregation table of k_hist and k_scatter
 
 // k_hist: per-bin counts (and, unless the window is pure, the per-bin key
 // range), aggregated first per warp, then per block in a shared-memory hash
@@ -626,7 +627,7 @@ __global__ void __launch_bounds__(256) k_hist(Batch b) {
       int slot = -1;
       if (valid && lane == leader) {
         const uint32_t c = (uint32_t)__popc(peers);
-        uint32_t sl = (bin * 2654435761u) >> (32 - 8);
+        uint32_t sl = (bin * 2654435761u) >> (32 - HIST_BITS);
 #pragma unroll 1
         for (int probe = 0; probe < 8; ++probe) {
           const uint32_t old = atomicCAS(&hbin[sl], 0xffffffffu, bin);
@@ -853,7 +854,7 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
       uint32_t off = 0;
       if (src[u] >= 0 && lane == leader[u]) {
         const uint32_t c = (uint32_t)__popc(peers[u]);
-        uint32_t sl = (bin[u] * 2654435761u) >> (32 - 8);
+        uint32_t sl = (bin[u] * 2654435761u) >> (32 - HIST_BITS);
 #pragma unroll 1
         for (int probe = 0; probe < 8; ++probe) {
           const uint32_t old = atomicCAS(&tbin[sl], 0xffffffffu, bin[u]);

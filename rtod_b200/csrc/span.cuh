@@ -154,7 +154,7 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
       int slot = -1;
       if (valid && lane == leader) {
         const uint32_t c = (uint32_t)__popc(peers);
-        uint32_t sl = (comp * 2654435761u) >> (32 - 8);
+        uint32_t sl = (comp * 2654435761u) >> (32 - HIST_BITS);
 #pragma unroll 1
         for (int probe = 0; probe < 8; ++probe) {
           const uint32_t old = atomicCAS(&hkey[sl], 0xffffffffu, comp);
@@ -351,7 +351,7 @@ __global__ void __launch_bounds__(256) k_span_scatter(Batch b, Span sp) {
       uint32_t off = 0;
       if (valid && lane == leader) {
         const uint32_t c = (uint32_t)__popc(peers);
-        uint32_t sl = (comp[u] * 2654435761u) >> (32 - 8);
+        uint32_t sl = (comp[u] * 2654435761u) >> (32 - HIST_BITS);
 #pragma unroll 1
         for (int probe = 0; probe < 8; ++probe) {
           const uint32_t old = atomicCAS(&tkey[sl], 0xffffffffu, comp[u]);
