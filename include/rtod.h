@@ -179,12 +179,14 @@ int64_t rtod_slides_done(const rtod_handle* h);
    of rtod_run (RTOD_ENGINE_WINDOW or RTOD_ENGINE_SPAN). The window engine's
    count mode is read with rtod_get_count_mode.
    With rtod_config.tuner = 1 the first rtod_run times candidate settings
-   (in 1-d with engine = AUTO both engines, cells per R 1..3 or up to 6 in
-   1-d, 2/4/8 warps per block, 8..256 windows per launch (up to 32 with the
-   window engine) and, with the router on and the window engine, its routing
-   threshold and full-sweep size limit) on the first 256 slides of the
-   stream and keeps the fastest; the choice is cached per configuration for
-   the rest of the process. Results do not depend on it. */
+   (with engine = AUTO both engines, cells per R 1..3 or up to 6 in 1-d,
+   2/4/8 warps per block, 8..256 windows per launch (up to 32 with the
+   window engine), with the window engine and count = AUTO both count
+   modes, and with the router on and point counts its routing threshold and
+   full-sweep size limit) on the first 256 slides of the stream and keeps
+   the fastest; the choice is cached per configuration (including engine,
+   coordinate type and count mode) for the rest of the process. Results do
+   not depend on it. */
 int rtod_get_tuning(const rtod_handle* h, int32_t out[5]);
 
 /* The resolved window-engine count (RTOD_COUNT_POINT or RTOD_COUNT_GROUP). */
