@@ -71,8 +71,9 @@ extern "C" {
                               may choose either */
 #define RTOD_COUNT_POINT 1 /* one warp per point, early exit at K+1 (with the router: early-exit
                               and full-sweep queues) */
-#define RTOD_COUNT_GROUP 2 /* one warp per part of up to 32 points of a cell bin: they share the
-                              stencil's candidates, read once per part; the router is not used */
+#define RTOD_COUNT_GROUP 2 /* one warp per part of a cell bin (32 to 1024 points, longer for larger
+                              launches): they share the stencil's candidates, read once per part;
+                              the router is not used */
 
 typedef struct rtod_config {
   int64_t window;      /* W  (--window, src/ods/optixScan.cpp:166-171) */
