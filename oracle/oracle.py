@@ -2,7 +2,8 @@
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline and reference
 legs import this module. The product package (rtod_b200) never does.
-Parity unpinned: see the header of rtod_oracle.cpp.
+Pinned to RTOD's own code (tests/golden/ref_*.npz): see the header of
+rtod_oracle.cpp.
 """
 from __future__ import annotations
 

@@ -4,13 +4,17 @@
 // smoke check and bench.py's CPU-baseline / reference arm load it. The
 // product library (rtod_b200/librtod.so) never links, loads or calls it.
 //
-// Parity status: parity unpinned. RTOD ships no tests, golden vectors or
-// data files, and its detector cannot be built or run here (OptiX 7.5 +
-// RT cores + a cmake-generated header + the sutil library). The pins used
-// instead are (1) hand-derived known-answer cases in tests/golden/, (2) an
-// independent numpy brute force that generated the golden streams, and
-// (3) the agreement of this file's two engines (brute force and grid
-// filter) with each other.
+// Parity status: pinned to RTOD's own code. RTOD ships no tests, golden
+// vectors or data files, and its GPU path needs OptiX and RT cores; but its
+// host code (src/ods/optixScan.cpp: the slide loop, FixQueue grid filter,
+// outlier pick and the brute-force check_outlier) compiles unmodified here
+// (oracle/ref/Makefile, with the OptiX programs and AABB kernel restated on
+// the host in oracle/ref/ref_fakes.cpp). Its per-slide outliers on seeded
+// 1-d and 3-d streams are committed as tests/golden/ref_*.npz, and this
+// file's double mode (PRED_F64_LT on double storage) reproduces them on
+// every slide (tests/test_reference_pin.py). Further pins: hand-derived
+// known-answer cases and numpy brute-force fixtures in tests/golden/, and
+// the agreement of this file's two engines with each other.
 //
 // What is restated, and from where (paths relative to the RTOD project):
 //  * Slide schedule and ring order: src/ods/optixScan.cpp:1019-1126. The

@@ -14,6 +14,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "librtod.so")
+CLI = os.path.join(PKG, "rtod")  # native optixScan-compatible command line (rtod_cli.cpp)
 SOURCES = ["rtod.cu"]
 HEADERS = ["kernels.cuh", "router.cuh", "span.cuh", "group.cuh"]
 
@@ -43,6 +44,14 @@ def stale(out: str = LIB) -> bool:
     return any(os.path.exists(d) and os.path.getmtime(d) > t for d in deps)
 
 
+def cli_command() -> list[str]:
+    """The native command line: plain C++ against the C ABI, linked to
+    librtod.so beside it."""
+    cxx = os.environ.get("CXX") or shutil.which("g++") or "g++"
+    return [cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), "-o", CLI,
+            os.path.join(CSRC, "rtod_cli.cpp"), "-L", PKG, "-lrtod", "-Wl,-rpath,$ORIGIN"]
+
+
 def build(force: bool = False, verbose: bool = False) -> str:
     if force or stale():
         r = subprocess.run(command(ptxas_verbose=verbose), capture_output=True, text=True)
@@ -50,6 +59,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
             raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
         if verbose:
             sys.stdout.write(r.stdout + r.stderr)
+    cli_src = os.path.join(CSRC, "rtod_cli.cpp")
+    if force or not os.path.exists(CLI) or os.path.getmtime(CLI) < max(os.path.getmtime(LIB),
+                                                                          os.path.getmtime(cli_src)):
+        r = subprocess.run(cli_command(), capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("building the rtod command line failed:\n" + r.stdout + r.stderr)
     return LIB
 
 

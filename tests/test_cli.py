@@ -81,3 +81,83 @@ def test_sweep_rows_match_oracle(oracle_mod):
         off, ids, _ = oracle_mod.detect(pts, r["window"], r["slide"], r["R"], r["K"], "fp32_le",
                                         engine="grid", threads=8)
         assert r["outliers_per_slide"] == pytest.approx(len(ids) / 3)
+
+
+def write_stream(path, pts):
+    """RTOD's text format: one value per line in 1-d, x,y,z otherwise, with
+    enough digits that every double (and float32) reads back exactly."""
+    pts = np.asarray(pts, np.float64)
+    with open(path, "w") as f:
+        for row in pts:
+            f.write(",".join("%.17g" % v for v in row) + "\n")
+
+
+def parse_outliers(text):
+    rows = [l for l in text.splitlines() if l.startswith("slide ")]
+    return [[int(t) for t in l.split(":", 1)[1].split()] for l in rows]
+
+
+@pytest.mark.gpu
+def test_cli_double_input_bit_exact(tmp_path, capsys):
+    """--coord f64: RTOD's %lf input reaches the double detector without a
+    float32 cast; the double fixtures' outliers come out bit for bit."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from conftest import golden_cases_f64, load_golden
+    for path in golden_cases_f64():
+        meta, pts, off, ids = load_golden(path)
+        f = tmp_path / "s.txt"
+        write_stream(f, pts)
+        rc = cli.main(["--n", str(len(pts)), "--R", repr(meta["R"]), "--K", str(meta["K"]), "--window",
+                       str(meta["W"]), "--slide", str(meta["S"]), "-f", str(f), "--dim", str(pts.shape[1]),
+                       "--coord", "f64", "--warmup", "1", "--print-outliers"])
+        assert rc == 0
+        got = parse_outliers(capsys.readouterr().out)
+        assert got == [ids[off[j]:off[j + 1]].tolist() for j in range(len(off) - 1)], path
+
+
+def native_cli():
+    import os
+    from rtod_b200 import build
+    build.build()
+    return os.path.join(os.path.dirname(build.LIB), "rtod")
+
+
+def test_native_cli_usage():
+    """The native command line (C++ over the C ABI) is built beside the
+    library and rejects an incomplete command line before touching a GPU."""
+    import subprocess
+    r = subprocess.run([native_cli(), "--window", "10"], capture_output=True, text=True)
+    assert r.returncode == 1 and "need --file" in r.stderr
+    r = subprocess.run([native_cli(), "--bogus"], capture_output=True, text=True)
+    assert r.returncode == 1 and "Unknown option '--bogus'" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", ["f32", "f64"])
+def test_native_cli_matches_golden(tmp_path, kind):
+    """rtod (C++, include/rtod.h only) on RTOD-format text files: float
+    storage with the FP32 predicate against the float fixtures, double
+    storage with RTOD's double test against the double fixtures."""
+    import subprocess
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from conftest import golden_cases, golden_cases_f64, load_golden
+    cases = golden_cases_f64() if kind == "f64" else golden_cases()
+    for path in cases:
+        meta, pts, off, ids = load_golden(path)
+        if kind == "f32" and meta["pred"] != "fp32_le":
+            continue
+        f = tmp_path / "s.txt"
+        write_stream(f, pts)
+        for graph in ([], ["--no-graph"]):
+            cmd = [native_cli(), "--n", str(len(pts)), "--R", repr(meta["R"]), "--K", str(meta["K"]),
+                   "--window", str(meta["W"]), "--slide", str(meta["S"]), "-f", str(f), "--dim",
+                   str(pts.shape[1]), "--coord", kind, "--warmup", "1", "--print-outliers"] + graph
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            assert r.returncode == 0, r.stderr
+            assert "[Time] total time for a slide" in r.stdout and "BVH Node / slide" in r.stdout
+            got = parse_outliers(r.stdout)
+            assert got == [ids[off[j]:off[j + 1]].tolist() for j in range(len(off) - 1)], path

@@ -118,3 +118,30 @@ def test_coordinate_type_errors(rtod):
         pts = np.zeros(1000, np.float64)
         rc = _native.lib().rtod_push_slide_f64(d._h, pts.ctypes.data_as(ctypes.c_void_p), 1000)
         assert rc == -2 and b"float" in _native.lib().rtod_last_error()
+
+
+REF_CASES = sorted(__import__("glob").glob(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden",
+                                                        "ref_*.npz")))
+
+
+@pytest.mark.parametrize("path", REF_CASES, ids=lambda p: os.path.basename(p)[:-4])
+@pytest.mark.parametrize("engine", ["span", "window", "push"])
+def test_matches_rtod_reference_run(rtod, path, engine):
+    """Double storage against outliers produced by RTOD's own code
+    (tests/golden/ref_*.npz: detect_outlier and check_outlier of
+    src/ods/optixScan.cpp run on the same stream), every slide."""
+    from test_reference_pin import load_ref
+    meta, pts, off, ids = load_ref(path)
+    pts = pts.astype(np.float64)
+    W, S = meta["W"], meta["S"]
+    with det(rtod, W, S, meta["R"], meta["K"], pts.shape[1],
+             **({} if engine == "push" else dict(engine=engine))) as d:
+        if engine == "push":
+            d.push(pts[:W])
+            for j in range(meta["slides"]):
+                d.push(pts[W + j * S:W + (j + 1) * S])
+                np.testing.assert_array_equal(d.detect(), ids[off[j]:off[j + 1]])
+        else:
+            r = d.run(pts)
+            np.testing.assert_array_equal(r.offsets, off)
+            np.testing.assert_array_equal(r.ids, ids)

@@ -75,9 +75,12 @@ def test_push_buffer_reused_at_once(rtod, source):
 
 def oracle_check(rtod, oracle_mod, pts, W, S, R, K, slides, pred="fp32_le", **kw):
     pts = pts[:W + slides * S]
-    off, ids, _ = oracle_mod.detect(pts, W, S, R, K, pred, engine="grid", threads=8)
+    off, ids, _ = oracle_mod.detect(pts, W, S, R, K, pred, engine="grid", threads=os.cpu_count() or 4)
     with rtod.Detector(W, S, R, K, dim=pts.shape[1] if pts.ndim == 2 else 1, pred=pred, **kw) as det:
-        assert_same(det.run(pts), off, ids)
+        r = det.run(pts)
+        assert r.slides == slides
+        assert_same(r, off, ids)
+    return off, ids
 
 
 def test_small_walk_full_stream(rtod, oracle_mod):
@@ -86,24 +89,70 @@ def test_small_walk_full_stream(rtod, oracle_mod):
     oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, w.slides)
 
 
-def test_stock_like_prefix(rtod, oracle_mod):
+@pytest.mark.parametrize("kw", [dict(), dict(engine="window"), dict(tuner=True, router=True)])
+def test_stock_like_full_stream(rtod, oracle_mod, kw):
+    """Every slide (189) of the stock-like stream, W=100k, S=5k."""
     from rtod_b200 import datagen
     w = datagen.stock_like()
-    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, 12)
+    off, _ = oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, w.slides, **kw)
+    assert len(off) == 190
 
 
-def test_sensor_like_prefix(rtod, oracle_mod):
+@pytest.mark.parametrize("pred,kw", [("fp32_le", dict()), ("fp32_le", dict(engine="window", router=True)),
+                                     ("f64_lt", dict())])
+def test_sensor_like_full_stream(rtod, oracle_mod, pred, kw):
+    """Every slide (1130) of the 3-d sensor-like stream, W=10k, S=500,
+    under both predicates; the router on the window engine."""
     from rtod_b200 import datagen
     w = datagen.sensor_like()
-    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, 60)
-    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, 20, pred="f64_lt")
+    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, w.slides, pred=pred, **kw)
 
 
 @pytest.mark.parametrize("K", [30, 50, 70])
 def test_gaussian_like_K_sweep(rtod, oracle_mod, K):
+    """Every slide (180) of the Gaussian-mixture stream for each K."""
     from rtod_b200 import datagen
     w = datagen.gaussian_like(K)
-    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, 6)
+    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, w.slides)
+    oracle_check(rtod, oracle_mod, w.points, w.window, w.slide, w.R, w.K, w.slides, engine="window", router=True)
+
+
+@pytest.fixture(scope="module")
+def batched_expect(oracle_mod):
+    """The 64 uneven streams of the batched workload (W log-uniform in
+    [5k, 200k], S = W/20, d in {1, 3, 8}) and the oracle's outliers of their
+    first 3 slides."""
+    from rtod_b200 import datagen
+    streams = datagen.batched_streams(slides=3)
+    expect = [oracle_mod.detect(w.points, w.window, w.slide, w.R, w.K, engine="grid",
+                                threads=os.cpu_count() or 4)[:2] for w in streams]
+    return streams, expect
+
+
+@pytest.mark.parametrize("router", [False, True])
+def test_batched_streams_first_slides(rtod, batched_expect, router):
+    """All 64 streams of the batched workload through the multi-stream API
+    (one graph replay per step), first 3 slides of every stream."""
+    streams, expect = batched_expect
+    cfg = [dict(window=w.window, slide=w.slide, R=w.R, K=w.K, dim=w.dim) for w in streams]
+    with rtod.BatchDetector(cfg, router=router) as bd:
+        for i, w in enumerate(streams):
+            bd.push(i, w.points[:w.window])
+        for j in range(3):
+            for i, w in enumerate(streams):
+                bd.push(i, w.points[w.window + j * w.slide:w.window + (j + 1) * w.slide])
+            res = bd.step()
+            for i in range(len(streams)):
+                off, ids = expect[i]
+                np.testing.assert_array_equal(res[i], ids[off[j]:off[j + 1]], err_msg=streams[i].name)
+
+
+def test_batched_streams_span_engine(rtod, batched_expect):
+    """The same 64 streams, each through rtod_run (tuned engine), first 3 slides."""
+    streams, expect = batched_expect
+    for w, (off, ids) in zip(streams, expect):
+        with rtod.Detector(w.window, w.slide, w.R, w.K, dim=w.dim) as det:
+            assert_same(det.run(w.points), off, ids)
 
 
 @pytest.mark.parametrize("d", [2, 5, 8])
