@@ -2367,22 +2367,30 @@ static __device__ __align__(256) unsigned char g_static_scratch[RTOD_STATIC_SCRA
 constexpr int kMaxDevices = 64;
 std::mutex g_static_mu;
 unsigned char* g_static_addr[kMaxDevices] = {};
+int g_static_sms[kMaxDevices] = {};
 
-// Device address of the scratch array on the current device (looked up once
-// per device, with that device current).
-int static_scratch(unsigned char** out) {
+// Device address of the scratch array on the current device and its SM
+// count, looked up once per device with that device current (the device's
+// compute capability is checked at the same time).
+int static_scratch(unsigned char** out, int* sm_count) {
   int dev = 0;
   CU(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return fail(RTOD_ERR_NODEV, "device ordinal %d out of range", dev);
   std::lock_guard<std::mutex> lk(g_static_mu);
   if (!g_static_addr[dev]) {
+    int major = 0, sms = 0;
+    CU(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    CU(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (major != 10) return fail(RTOD_ERR_NODEV, "device %d is not sm_100", dev);
     void* p = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
     if (e != cudaSuccess || !p)
       return fail(RTOD_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+    g_static_sms[dev] = sms;
     g_static_addr[dev] = (unsigned char*)p;
   }
   *out = g_static_addr[dev];
+  *sm_count = g_static_sms[dev];
   return RTOD_OK;
 }
 
@@ -2401,13 +2409,9 @@ RTOD_API int rtod_detect_window_static(const float* pts, int64_t n, int32_t dim,
   if (pred != RTOD_PRED_FP32_LE && pred != RTOD_PRED_F64_LT) return fail(RTOD_ERR_CONFIG, "unknown predicate %d", pred);
   if (!is_device_ptr(pts) || !is_device_ptr(out_ids))
     return fail(RTOD_ERR_ARG, "pts and out_ids must be device memory");
-  int dev = 0;
-  CU(cudaGetDevice(&dev));
-  cudaDeviceProp prop;
-  CU(cudaGetDeviceProperties(&prop, dev));
-  if (prop.major != 10) return fail(RTOD_ERR_NODEV, "device %d is not sm_100", dev);
   unsigned char* base = nullptr;
-  int r = static_scratch(&base);
+  int sm = 0;
+  int r = static_scratch(&base, &sm);
   if (r) return r;
   cudaStream_t st = (cudaStream_t)stream;
   auto at = [&](size_t off) { return (void*)(base + off); };
@@ -2479,7 +2483,6 @@ RTOD_API int rtod_detect_window_static(const float* pts, int64_t n, int32_t dim,
   b.out_cap = n;
   b.cmp_tiles = (n + CMP_TILE - 1) / CMP_TILE;
 
-  int sm = prop.multiProcessorCount;
   const unsigned kx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sm * 8));
   DISPATCH_D(dim, CU(launch_k(k_keys<D, float>, dim3(kx), 256, st, pts, (int64_t)0, n, jb.inv_cell, (uint64_t*)at(kStatic.keys),
                                (uint8_t*)at(kStatic.prev), b.bs, n, (long long*)at(kStatic.blo),
