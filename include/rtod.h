@@ -103,7 +103,16 @@ typedef struct rtod_config {
   int32_t coord;       /* RTOD_COORD_F32 or RTOD_COORD_F64 */
   int32_t count;       /* RTOD_COUNT_*: window-engine count (push/detect, the multi-stream
                           API, rtod_run with the window engine) */
+  int32_t pipeline;    /* RTOD_PIPELINE_*: how push/detect and the multi-stream API launch
+                          the window engine. Results are identical. */
 } rtod_config;
+
+/* rtod_config.pipeline */
+#define RTOD_PIPELINE_FUSED 0  /* default: one cooperative launch per detection (per group of
+                                  streams in the multi-stream API) running every stage, the
+                                  stages separated by bounded grid barriers */
+#define RTOD_PIPELINE_STAGED 1 /* one launch per stage (ingest, hist, scan, scatter, count,
+                                  compact, output) */
 
 /* Per-slide stage times in ms, averaged over the slides of the last call,
    under the names of RTOD's Timer (src/ods/timer.h:16-24, :102-117). */
@@ -250,8 +259,10 @@ int rtod_batch_push(rtod_batch* b, int32_t s, const float* pts, int64_t n);
 int rtod_batch_step(rtod_batch* b, int64_t* out_offsets, int64_t* out_ids, int64_t cap, int64_t* n_total);
 
 /* out[0] steps, out[1] kernel launches (graph replays count their kernels),
-   out[2] window detections summed over streams, out[3] groups. */
-int rtod_batch_stats(const rtod_batch* b, int64_t out[4]);
+   out[2] window detections summed over streams, out[3] groups, out[4]
+   distance tests made by group counts (RTOD_COUNT_GROUP streams) since
+   create: the work of the compute-bound count, for its roofline. */
+int rtod_batch_stats(const rtod_batch* b, int64_t out[5]);
 
 void rtod_batch_destroy(rtod_batch* b);
 

@@ -30,6 +30,7 @@ ENGINE = {"auto": 0, "window": 1, "span": 2}
 COORD = {"f32": 0, "f64": 1}
 COUNT = {"auto": 0, "point": 1, "group": 2}
 COUNT_NAME = {1: "point", 2: "group"}
+PIPELINE = {"fused": 0, "staged": 1}
 ENGINE_NAME = {1: "window", 2: "span"}
 
 
@@ -41,6 +42,7 @@ class Config(ctypes.Structure):
         ("cells_per_r", ctypes.c_int32), ("block_warps", ctypes.c_int32),
         ("use_graph", ctypes.c_int32), ("device", ctypes.c_int32), ("batch", ctypes.c_int32),
         ("engine", ctypes.c_int32), ("coord", ctypes.c_int32), ("count", ctypes.c_int32),
+        ("pipeline", ctypes.c_int32),
     ]
 
 

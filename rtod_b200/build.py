@@ -15,8 +15,9 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "librtod.so")
 CLI = os.path.join(PKG, "rtod")  # native optixScan-compatible command line (rtod_cli.cpp)
-SOURCES = ["rtod.cu"]
-HEADERS = ["kernels.cuh", "router.cuh", "span.cuh", "group.cuh"]
+SOURCES = ["rtod.cu", "fused_f32.cu", "fused_f64.cu"]
+HEADERS = ["kernels.cuh", "router.cuh", "span.cuh", "group.cuh", "fused.cuh", "fused_impl.cuh"]
+OBJ_DIR = os.path.join(PKG, "_build")
 
 
 def nvcc() -> str:
@@ -26,13 +27,23 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def command(out: str = LIB, ptxas_verbose: bool = False) -> list[str]:
-    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-           "-Xcompiler", "-fPIC,-fvisibility=hidden", "-shared", "-I", os.path.join(ROOT, "include"),
-           "-o", out]
+FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+         "-Xcompiler", "-fPIC,-fvisibility=hidden"]
+
+
+def compile_command(src: str, ptxas_verbose: bool = False) -> list[str]:
+    """nvcc of one translation unit to an object in OBJ_DIR."""
+    cmd = [nvcc()] + FLAGS + ["-I", os.path.join(ROOT, "include"), "-c", os.path.join(CSRC, src),
+                              "-o", os.path.join(OBJ_DIR, src[:-3] + ".o")]
     if ptxas_verbose:
         cmd += ["-Xptxas", "-v"]
-    return cmd + [os.path.join(CSRC, s) for s in SOURCES]
+    return cmd
+
+
+def command(out: str = LIB) -> list[str]:
+    """Link of the objects into the shared library."""
+    return [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", out] + \
+        [os.path.join(OBJ_DIR, s[:-3] + ".o") for s in SOURCES]
 
 
 def stale(out: str = LIB) -> bool:
@@ -54,11 +65,20 @@ def cli_command() -> list[str]:
 
 def build(force: bool = False, verbose: bool = False) -> str:
     if force or stale():
-        r = subprocess.run(command(ptxas_verbose=verbose), capture_output=True, text=True)
-        if r.returncode != 0:
-            raise RuntimeError("nvcc failed:\n" + r.stdout + r.stderr)
+        # the translation units compile in parallel (the fused pipeline's
+        # instantiations are about as large as the rest of the library)
+        os.makedirs(OBJ_DIR, exist_ok=True)
+        procs = [subprocess.Popen(compile_command(src, verbose), stdout=subprocess.PIPE, stderr=subprocess.STDOUT,
+                                  text=True) for src in SOURCES]
+        outs = [p.communicate()[0] for p in procs]
+        for p, o in zip(procs, outs):
+            if p.returncode != 0:
+                raise RuntimeError("nvcc failed:\n" + o)
         if verbose:
-            sys.stdout.write(r.stdout + r.stderr)
+            sys.stdout.write("".join(outs))
+        r = subprocess.run(command(), capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("nvcc link failed:\n" + r.stdout + r.stderr)
     cli_src = os.path.join(CSRC, "rtod_cli.cpp")
     if force or not os.path.exists(CLI) or os.path.getmtime(CLI) < max(os.path.getmtime(LIB),
                                                                           os.path.getmtime(cli_src)):

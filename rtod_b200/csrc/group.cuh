@@ -84,6 +84,7 @@ struct GroupArgs {
   double R, R2;
   int64_t Wp;      // row stride of the coordinates
   bool can_sure;
+  unsigned long long* tests;  // distance tests made, added once per group (may be null)
 };
 
 // Counts the group; range(sb, rs, len) gives the candidate positions of
@@ -155,6 +156,7 @@ __device__ __forceinline__ int count_group(const T* sx, const GroupArgs& a, Rang
   uint32_t c0 = 0, next = 0, left = 0, mine = 0;
   bool has = false;
   int cnt = 0, nout = 0;
+  unsigned long long tests = 0;  // warp-uniform: live points x candidates of each chunk
   T qx[D];
 #pragma unroll
   for (int d = 0; d < D; ++d) qx[d] = T(0);
@@ -196,6 +198,7 @@ __device__ __forceinline__ int count_group(const T* sx, const GroupArgs& a, Rang
 #pragma unroll
       for (int d = 0; d < D; ++d) cx[e][d] = cv[e] ? sx[(int64_t)d * a.Wp + c] : T(0);
     }
+    tests += (unsigned long long)__popc(live) * min(CHUNK, ncand - c0);
     unsigned todo = live;
     while (todo) {
       const int qq = __ffs(todo) - 1;
@@ -234,6 +237,7 @@ __device__ __forceinline__ int count_group(const T* sx, const GroupArgs& a, Rang
       }
     }
   }
+  if (a.tests && lane == 0 && tests) atomicAdd(a.tests, tests);
   return nout;
 }
 

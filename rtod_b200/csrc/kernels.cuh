@@ -92,6 +92,7 @@ struct BatchState {
   int64_t undet_total;  // queued points summed over windows
   int32_t err;          // DERR_*
   uint32_t done;        // finished blocks of the running batch's last kernel
+  unsigned long long pair_tests;  // distance tests made by group counts so far
 };
 
 // Span engine counters (device), one per handle, and the per-bin arrays
@@ -101,6 +102,7 @@ struct SpanCtr {
   uint32_t n_used;       // bins holding span points
   int32_t pure;          // the span's cells and their sure neighbours map to distinct bins (k_span_scan)
   uint32_t n_groups;     // groups listed for exact counts in the running batch
+  uint32_t count_ticket; // next listed group for a count warp to take
   long long cmin[3];     // per hashed dimension, the span's cell coordinate range (k_span_hist)
   long long cmax[3];
   uint32_t* used;        // [NB] bins in use
@@ -166,7 +168,16 @@ struct Batch {
 
 __device__ __forceinline__ void set_err(BatchState* bs, int32_t code) { atomicCAS(&bs->err, 0, code); }
 
-__device__ __forceinline__ bool job_active(const Batch& b) { return !b.active || b.active[blockIdx.y]; }
+__device__ __forceinline__ bool job_active(const Batch& b, uint32_t job) { return !b.active || b.active[job]; }
+
+// Block coordinates of a pipeline stage: x index and extent of the block
+// within its job, and the job. A kernel of one stage passes its own
+// blockIdx / gridDim; the fused pipeline kernel (fused.cuh) runs each stage
+// over a virtual grid of such blocks.
+struct VB {
+  uint32_t x, y, gx;
+};
+__device__ __forceinline__ VB hw_block() { return VB{blockIdx.x, blockIdx.y, gridDim.x}; }
 
 // ---------------------------------------------------------------------------
 // Grid cells. Cell coordinate k_i = floor(x_i * inv_cell) in double
@@ -311,7 +322,7 @@ constexpr unsigned long long LB_PREFIX = 2ull << 62;  // inclusive prefix publis
 // publishes its own inclusive prefix. Tiles are claimed in ticket order, so
 // every predecessor is running or done and the chain always resolves; each
 // wait is still bounded (DERR_TIMEOUT, partial sum used).
-__device__ uint32_t warp_lookback(unsigned long long* status, uint32_t tile, uint32_t total,
+static __device__ uint32_t warp_lookback(unsigned long long* status, uint32_t tile, uint32_t total,
                                   BatchState* bs) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) {
@@ -480,18 +491,16 @@ __global__ void __launch_bounds__(256) k_keys(const T* pts, int64_t g0, int64_t 
 // [lo, lo + W), i.e. [lo + W - S, lo + W). Slot = global index % W.
 // ---------------------------------------------------------------------------
 template <int D, typename T>
-__global__ void __launch_bounds__(256) k_ingest(Batch b, int32_t fill) {
-  pdl_trigger();
-  pdl_wait();
-  if (!job_active(b)) return;
-  const Job& jb = b.jobs[blockIdx.y];
+__device__ __forceinline__ void ingest_body(const Batch& b, int32_t fill, VB v) {
+  if (!job_active(b, v.y)) return;
+  const Job& jb = b.jobs[v.y];
   T* ring = static_cast<T*>(const_cast<void*>(jb.pts));
   const T* stage = static_cast<const T*>(jb.stage);
   uint64_t* keys = const_cast<uint64_t*>(jb.keys);
   const int64_t n_new = fill ? jb.W : jb.S;
   const int64_t base = fill ? 0 : jb.ctr->lo + jb.W - jb.S;
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += stride) {
+  const int64_t stride = (int64_t)v.gx * blockDim.x;
+  for (int64_t i = (int64_t)v.x * blockDim.x + threadIdx.x; i < n_new; i += stride) {
     const int64_t slot = (base + i) % jb.W;
     T x[D];
 #pragma unroll
@@ -504,6 +513,13 @@ __global__ void __launch_bounds__(256) k_ingest(Batch b, int32_t fill) {
     keys[slot] = key;
     jb.prev[slot] = 254;
   }
+}
+
+template <int D, typename T>
+__global__ void __launch_bounds__(256) k_ingest(Batch b, int32_t fill) {
+  pdl_trigger();
+  pdl_wait();
+  ingest_body<D, T>(b, fill, hw_block());
 }
 
 // ---------------------------------------------------------------------------
@@ -578,25 +594,26 @@ constexpr int HIST_SLOTS = 1 << HIST_BITS;  // block-local aggregation table of 
 // k_hist: per-bin counts (and, unless the window is pure, the per-bin key
 // range), aggregated first per warp, then per block in a shared-memory hash
 // table, then flushed to global memory with one atomic per bin per block.
-template <int D>
-__global__ void __launch_bounds__(256) k_hist(Batch b) {
+// With INGEST (a ring job of the fused pipeline), the S newest points of the
+// window are taken from the staged slide instead: their keys are computed
+// here and they are written into the ring (k_ingest's work, folded in).
+template <int D, typename T = float, bool INGEST = false>
+__device__ __forceinline__ void hist_body(const Batch& b, VB v) {
   __shared__ uint32_t hbin[HIST_SLOTS];
   __shared__ uint32_t hcnt[HIST_SLOTS];
   __shared__ unsigned long long hmin[HIST_SLOTS], hmax[HIST_SLOTS];
   __shared__ int s_pure;
-  pdl_trigger();
-  pdl_wait();
-  if (!job_active(b)) return;
+  if (!job_active(b, v.y)) return;
   constexpr int H = Hashed<D>::value;
   constexpr int U = Unroll<D>::value;
-  const Job& jb = b.jobs[blockIdx.y];
+  const Job& jb = b.jobs[v.y];
   const int64_t lo = jb.ctr->lo;
   const int lane = threadIdx.x & 31;
   if (threadIdx.x < 32) {
     const bool pure = window_pure<H>(jb, lo);
     if (threadIdx.x == 0) {
       s_pure = pure;
-      if (blockIdx.x == 0) jb.ctr->pure = pure;
+      if (v.x == 0) jb.ctr->pure = pure;
     }
   }
   for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
@@ -608,13 +625,30 @@ __global__ void __launch_bounds__(256) k_hist(Batch b) {
   __syncthreads();
   const bool pure = s_pure;
   const int64_t chunk = (int64_t)blockDim.x * U;
-  for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < jb.W; c0 += (int64_t)gridDim.x * chunk) {
+  const int64_t first_new = jb.W - jb.S;  // window offset of the staged slide (INGEST)
+  for (int64_t c0 = (int64_t)v.x * chunk; c0 < jb.W; c0 += (int64_t)v.gx * chunk) {
     const int64_t w0 = c0 + (int64_t)(threadIdx.x >> 5) * 32 * U;
     uint64_t key[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int64_t i = w0 + u * 32 + lane;
-      key[u] = i < jb.W ? jb.keys[source_pos(jb, lo, i)] : EMPTY_KEY;
+      if (INGEST && i >= first_new && i < jb.W) {
+        const int64_t slot = source_pos(jb, lo, i);
+        const T* stage = static_cast<const T*>(jb.stage) + (i - first_new) * D;
+        T* ring = static_cast<T*>(const_cast<void*>(jb.pts));
+        T x[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) x[d] = stage[d];
+        int32_t code;
+        key[u] = cell_key<D, T>(x, jb.inv_cell, &code);
+        if (code) set_err(b.bs, code);
+#pragma unroll
+        for (int d = 0; d < D; ++d) ring[(int64_t)d * jb.W + slot] = x[d];
+        const_cast<uint64_t*>(jb.keys)[slot] = key[u];
+        jb.prev[slot] = 254;
+      } else {
+        key[u] = i < jb.W ? jb.keys[source_pos(jb, lo, i)] : EMPTY_KEY;
+      }
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -668,6 +702,13 @@ __global__ void __launch_bounds__(256) k_hist(Batch b) {
   }
 }
 
+template <int D>
+__global__ void __launch_bounds__(256) k_hist(Batch b) {
+  pdl_trigger();
+  pdl_wait();
+  hist_body<D>(b, hw_block());
+}
+
 // ---------------------------------------------------------------------------
 // k_scan: exclusive scan of each job's NB bin counts. Grid (NB / TILE, jobs),
 // 256 threads; each thread owns TILE / 256 consecutive bins (coalesced
@@ -717,12 +758,16 @@ __device__ __forceinline__ void scan_bins(const uint32_t* bin_count, uint32_t* b
   }
 }
 
-__global__ void __launch_bounds__(256) k_scan(Batch b) {
+__device__ __forceinline__ void scan_body(const Batch& b, VB v) {
+  if (!job_active(b, v.y)) return;
+  const Job& jb = b.jobs[v.y];
+  scan_bins<SCAN_TILE>(jb.bin_count, jb.bin_start, jb.scan_status, &jb.ctr->scan_ticket, b.bs);
+}
+
+static __global__ void __launch_bounds__(256) k_scan(Batch b) {
   pdl_trigger();
   pdl_wait();
-  if (!job_active(b)) return;
-  const Job& jb = b.jobs[blockIdx.y];
-  scan_bins<SCAN_TILE>(jb.bin_count, jb.bin_start, jb.scan_status, &jb.ctr->scan_ticket, b.bs);
+  scan_body(b, hw_block());
 }
 
 // ---------------------------------------------------------------------------
@@ -807,22 +852,20 @@ __device__ __forceinline__ bool group_safe_1d(const Job& jb, uint64_t key, uint3
 }
 
 template <int D, bool ROUTE, typename T, bool GROUP = false>
-__global__ void __launch_bounds__(256) k_scatter(Batch b) {
+__device__ __forceinline__ void scatter_body(const Batch& b, VB v) {
   // Block-local table: bin, points of the chunk in the bin, claimed base.
   __shared__ uint32_t tbin[HIST_SLOTS];
   __shared__ uint32_t tcnt[HIST_SLOTS];
   __shared__ uint32_t tbase[HIST_SLOTS];
   __shared__ unsigned long long s_routed[2];  // router statistics, flushed once per block
-  pdl_trigger();
-  pdl_wait();
-  if (!job_active(b)) return;
+  if (!job_active(b, v.y)) return;
   if (ROUTE && threadIdx.x < 2) s_routed[threadIdx.x] = 0;
   constexpr int H = Hashed<D>::value;
   constexpr int U = Unroll<D>::value;
-  const Job& jb = b.jobs[blockIdx.y];
+  const Job& jb = b.jobs[v.y];
   const int64_t lo = jb.ctr->lo;
   const bool pure = jb.ctr->pure;
-  if (blockIdx.x == 0 && threadIdx.x < SCAN_TILES) jb.scan_status[threadIdx.x] = 0;
+  if (v.x == 0 && threadIdx.x < SCAN_TILES) jb.scan_status[threadIdx.x] = 0;
   for (int t = threadIdx.x; t < HIST_SLOTS; t += blockDim.x) {
     tbin[t] = 0xffffffffu;
     tcnt[t] = 0;
@@ -831,7 +874,7 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = lanemask_lt();
   const int64_t chunk = (int64_t)blockDim.x * U;
-  for (int64_t c0 = (int64_t)blockIdx.x * chunk; c0 < jb.W; c0 += (int64_t)gridDim.x * chunk) {
+  for (int64_t c0 = (int64_t)v.x * chunk; c0 < jb.W; c0 += (int64_t)v.gx * chunk) {
     const int64_t w0 = c0 + (int64_t)(threadIdx.x >> 5) * 32 * U;
     int64_t src[U];
     uint64_t key[U];
@@ -991,6 +1034,13 @@ __global__ void __launch_bounds__(256) k_scatter(Batch b) {
   }
 }
 
+template <int D, bool ROUTE, typename T, bool GROUP = false>
+__global__ void __launch_bounds__(256) k_scatter(Batch b) {
+  pdl_trigger();
+  pdl_wait();
+  scatter_body<D, ROUTE, T, GROUP>(b, hw_block());
+}
+
 // Counts the neighbours of query qx among the candidates of one run
 // [rs, re), 128 per step: each lane loads 4 consecutive candidates per
 // dimension with one float4, the warp tallies them with ballot/popc.
@@ -1032,8 +1082,8 @@ __device__ __forceinline__ bool count_run(const Job& jb, const T* qx, uint32_t r
 // Returns false in *ok when a row wraps around the end of the bin table; the
 // caller then uses the row-by-row count.
 // ---------------------------------------------------------------------------
-__constant__ uint8_t c_rows2[3][7] = {{1, 0, 2}, {2, 1, 3, 0, 4}, {3, 2, 4, 1, 5, 0, 6}};
-__constant__ uint8_t c_rows3[3][49] = {
+static __constant__ uint8_t c_rows2[3][7] = {{1, 0, 2}, {2, 1, 3, 0, 4}, {3, 2, 4, 1, 5, 0, 6}};
+static __constant__ uint8_t c_rows3[3][49] = {
     {4, 3, 5, 1, 7, 0, 2, 6, 8},
     {12, 11, 13, 7, 17, 6, 8, 16, 18, 10, 14, 2, 22, 5, 9, 15, 19, 1, 3, 21, 23, 0, 4, 20, 24},
     {24, 23, 25, 17, 31, 16, 18, 30, 32, 22, 26, 10, 38, 15, 19, 29, 33, 9, 11, 37, 39, 8, 12, 36, 40,
@@ -1227,14 +1277,14 @@ __device__ __forceinline__ void flush_samples(SampleBuf& sb, RouterState* rs) {
 
 // Per-job cleanup done by k_count: per-bin key ranges and compaction
 // look-back words.
-__device__ __forceinline__ void reset_bins(const Job& jb) {
-  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < NB; t += stride) {
+__device__ __forceinline__ void reset_bins(const Job& jb, VB v) {
+  const int64_t stride = (int64_t)v.gx * blockDim.x;
+  for (int64_t t = (int64_t)v.x * blockDim.x + threadIdx.x; t < NB; t += stride) {
     jb.kmin[t] = EMPTY_KEY;
     jb.kmax[t] = 0;
   }
   const int64_t tiles = (jb.W + CMP_TILE - 1) / CMP_TILE;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < tiles; t += stride)
+  for (int64_t t = (int64_t)v.x * blockDim.x + threadIdx.x; t < tiles; t += stride)
     jb.cmp_status[t] = 0;
 }
 
@@ -1247,22 +1297,20 @@ __device__ __forceinline__ void reset_bins(const Job& jb) {
 //     every counted point becomes a training sample of the router.
 // ---------------------------------------------------------------------------
 template <int D, int PRED, bool ROUTE, typename T, bool GROUP = false>
-__global__ void __launch_bounds__(256) k_count(Batch b) {
+__device__ __forceinline__ void count_body(const Batch& b, VB v) {
   __shared__ SampleBuf sb;
-  pdl_trigger();
-  pdl_wait();
-  if (!job_active(b)) return;
-  const Job& jb = b.jobs[blockIdx.y];
+  if (!job_active(b, v.y)) return;
+  const Job& jb = b.jobs[v.y];
   if (ROUTE && threadIdx.x == 0) {
     sb.n = 0;
     sb.misrouted = 0;
   }
   if (ROUTE) __syncthreads();
-  reset_bins(jb);
+  reset_bins(jb, v);
   const int lane = threadIdx.x & 31;
   const int64_t lo = jb.ctr->lo;
-  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int64_t warp = ((int64_t)v.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)v.gx * blockDim.x) >> 5;
   if constexpr (GROUP) {
     // one warp per listed part of a bin: its points share the stencil (count_group)
     constexpr int H = Hashed<D>::value;
@@ -1273,7 +1321,7 @@ __global__ void __launch_bounds__(256) k_count(Batch b) {
       const uint32_t p = jb.queue[g];
       const uint32_t bin = bin_of_key(jb.s_ckey[p], H);
       const uint32_t nq = min((uint32_t)jb.gpts, jb.bin_start[bin + 1] - p);
-      const GroupArgs ga{p, nq, bin, jb.n, jb.K, jb.R2f, jb.R, jb.R2, jb.Wp, can_sure};
+      const GroupArgs ga{p, nq, bin, jb.n, jb.K, jb.R2f, jb.R, jb.R2, jb.Wp, can_sure, &b.bs->pair_tests};
       nout += count_group<D, PRED, T>(
           static_cast<const T*>(jb.s_x), ga,
           [&](uint32_t sb2, uint32_t& rs, uint32_t& len) {
@@ -1315,6 +1363,13 @@ __global__ void __launch_bounds__(256) k_count(Batch b) {
   }
 }
 
+template <int D, int PRED, bool ROUTE, typename T, bool GROUP = false>
+__global__ void __launch_bounds__(256) k_count(Batch b) {
+  pdl_trigger();
+  pdl_wait();
+  count_body<D, PRED, ROUTE, T, GROUP>(b, hw_block());
+}
+
 // ---------------------------------------------------------------------------
 // End of a batch, run by the block of the batch's last kernel that finishes
 // last (after a fence): per-slide records (outlier count, counted points and,
@@ -1322,7 +1377,7 @@ __global__ void __launch_bounds__(256) k_count(Batch b) {
 // per-job counter reset and the batch totals. Every thread of the block
 // calls it.
 // ---------------------------------------------------------------------------
-__device__ void finish_batch(const Batch& b) {
+static __device__ void finish_batch(const Batch& b) {
   __shared__ int64_t s_red[3][32];
   __shared__ int64_t s_scan[33];
   BatchState* bs = b.bs;
@@ -1408,6 +1463,7 @@ __device__ void finish_batch(const Batch& b) {
     if (b.span) {
       b.span->n_used = 0;
       b.span->n_groups = 0;
+      b.span->count_ticket = 0;
       for (int d = 0; d < 3; ++d) {
         b.span->cmin[d] = LLONG_MAX;
         b.span->cmax[d] = LLONG_MIN;
@@ -1422,7 +1478,7 @@ __device__ void finish_batch(const Batch& b) {
 // k_run_init: job j's counters start at window lo = first_lo + j*S and
 // advance by jobs*S per batch; the batch state is cleared.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_run_init(JobCtr* ctr, int32_t jobs, int64_t first_lo, int64_t S,
+static __global__ void __launch_bounds__(256) k_run_init(JobCtr* ctr, int32_t jobs, int64_t first_lo, int64_t S,
                                                   BatchState* bs) {
   pdl_trigger();
   pdl_wait();
@@ -1438,7 +1494,7 @@ __global__ void __launch_bounds__(256) k_run_init(JobCtr* ctr, int32_t jobs, int
 // k_run_out: the outlier IDs (at most cap) into a caller's page-locked host
 // buffer through its device mapping (consecutive 8-byte writes, one per
 // thread), then the batch state into the handle's mapped mirror.
-__global__ void __launch_bounds__(256) k_run_out(const int64_t* ids, int64_t* host_ids, int64_t cap,
+static __global__ void __launch_bounds__(256) k_run_out(const int64_t* ids, int64_t* host_ids, int64_t cap,
                                                  const BatchState* bs, BatchState* mirror) {
   pdl_trigger();
   pdl_wait();
@@ -1458,22 +1514,21 @@ __global__ void __launch_bounds__(256) k_run_out(const int64_t* ids, int64_t* ho
 // tile of the batch records per-slide counts, advances every job's window
 // and resets the per-job counters.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_compact(Batch b) {
+// Returns true in the block that ran finish_batch.
+__device__ __forceinline__ bool compact_body(const Batch& b, VB v) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t s_tile, s_prefix, s_last;
   __shared__ int64_t s_jobbase;
-  pdl_trigger();
-  pdl_wait();
-  const Job& jb = b.jobs[blockIdx.y];
+  const Job& jb = b.jobs[v.y];
   const int64_t ntiles = (jb.W + CMP_TILE - 1) / CMP_TILE;
-  if (blockIdx.x >= ntiles) return;  // smaller job in a mixed batch
+  if (v.x >= ntiles) return false;  // smaller job in a mixed batch
   BatchState* bs = b.bs;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const bool act = job_active(b);
+  const bool act = job_active(b, v.y);
   if (act && wid == 0) {
     // Output base of this job: IDs of all earlier jobs of the batch come first.
     int64_t part = 0;
-    for (int j = lane; j < (int)blockIdx.y; j += 32) part += b.jobs[j].ctr->n_out;
+    for (int j = lane; j < (int)v.y; j += 32) part += b.jobs[j].ctr->n_out;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
     if (lane == 0) {
@@ -1512,8 +1567,15 @@ __global__ void __launch_bounds__(256) k_compact(Batch b) {
   __syncthreads();
   if (threadIdx.x == 0) s_last = (atomicAdd(&bs->done, 1u) == (uint32_t)(b.cmp_tiles - 1));
   __syncthreads();
-  if (!s_last) return;
+  if (!s_last) return false;
   finish_batch(b);
+  return true;
+}
+
+static __global__ void __launch_bounds__(256) k_compact(Batch b) {
+  pdl_trigger();
+  pdl_wait();
+  compact_body(b, hw_block());
 }
 
 }  // namespace rtod

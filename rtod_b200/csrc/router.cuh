@@ -142,7 +142,7 @@ __device__ __forceinline__ float p_inlier(const float* z) {
 constexpr int TRAIN_ROW = MLP_IN + 4 * MLP_H + MLP_B;  // x, h1, h2, d1, d2, d3 = 135
 constexpr size_t TRAIN_SMEM = sizeof(float) * (TRAIN_CHUNK * TRAIN_ROW + MLP_P);
 
-__device__ void mlp_train_block(float* P, float* m, float* v, float* b1t, float* b2t, float lr, float beta1,
+static __device__ void mlp_train_block(float* P, float* m, float* v, float* b1t, float* b2t, float lr, float beta1,
                                 float beta2, float eps, const float* x, int xstride, const float* yf,
                                 int ystride, int n, float* grad, float* loss, bool adam, float* smem) {
   const int t = threadIdx.x;
@@ -278,7 +278,7 @@ __device__ void mlp_train_block(float* P, float* m, float* v, float* b1t, float*
 // Online training: once enough samples are buffered, up to TRAIN_STEPS Adam
 // steps, each on the next TRAIN_MAX buffered samples; the buffer is then
 // emptied.
-__global__ void __launch_bounds__(256) k_train(RouterState* rs) {
+static __global__ void __launch_bounds__(256) k_train(RouterState* rs) {
   extern __shared__ float smem[];
   pdl_trigger();
   pdl_wait();
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(256) k_train(RouterState* rs) {
 }
 
 // Routing table from the current parameters: one thread per grid cell.
-__global__ void __launch_bounds__(256) k_table(RouterState* rs) {
+static __global__ void __launch_bounds__(256) k_table(RouterState* rs) {
   __shared__ float P[MLP_P];
   pdl_trigger();
   pdl_wait();
@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(256) k_table(RouterState* rs) {
 
 // Test kernels behind the diagnostic C ABI: gradients of a given batch and
 // forward logits, on the parameters passed in.
-__global__ void __launch_bounds__(256) k_mlp_grad(float* params, const float* x, const int32_t* y, int n,
+static __global__ void __launch_bounds__(256) k_mlp_grad(float* params, const float* x, const int32_t* y, int n,
                                                   float* grad, float* loss, float* yf) {
   extern __shared__ float smem[];
   for (int i = threadIdx.x; i < n; i += blockDim.x) yf[i] = (float)y[i];
@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(256) k_mlp_grad(float* params, const float* x,
                   false, smem);
 }
 
-__global__ void __launch_bounds__(256) k_mlp_adam(float* params, float* m, float* v, float* bt, const float* x,
+static __global__ void __launch_bounds__(256) k_mlp_adam(float* params, float* m, float* v, float* bt, const float* x,
                                                   const int32_t* y, int n, float lr, float beta1, float beta2,
                                                   float eps, float* loss, float* yf) {
   extern __shared__ float smem[];
@@ -337,7 +337,7 @@ __global__ void __launch_bounds__(256) k_mlp_adam(float* params, float* m, float
   mlp_train_block(params, m, v, &bt[0], &bt[1], lr, beta1, beta2, eps, x, 3, yf, 1, n, nullptr, loss, true, smem);
 }
 
-__global__ void k_mlp_forward(const float* params, const float* x, int n, float* logits) {
+static __global__ void k_mlp_forward(const float* params, const float* x, int n, float* logits) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   float xs[MLP_IN], z[MLP_B];

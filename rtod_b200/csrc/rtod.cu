@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/rtod.h"
+#include "fused.cuh"
 #include "kernels.cuh"
 #include "span.cuh"
 
@@ -334,6 +335,8 @@ struct rtod_handle {
   int graph_ring = -1;
   int64_t batches = 0;
 
+  GridBar* bar = nullptr;  // grid barrier of the fused pipeline
+  int fused_grid = 0;      // its blocks (all resident), found on first use
   cudaEvent_t ev[16] = {};
   cudaStream_t copy_stream = nullptr;     // host-stream pieces, overlapped with detection
   cudaEvent_t fork_ev = nullptr;          // the copy stream's start on the library stream
@@ -379,6 +382,8 @@ int check_config(const rtod_config* c) {
     return fail(RTOD_ERR_CONFIG, "double coordinates need the double predicate (RTOD_PRED_F64_LT)");
   if (c->count < RTOD_COUNT_AUTO || c->count > RTOD_COUNT_GROUP)
     return fail(RTOD_ERR_CONFIG, "count must be 0 (auto), 1 (point) or 2 (group)");
+  if (c->pipeline != RTOD_PIPELINE_FUSED && c->pipeline != RTOD_PIPELINE_STAGED)
+    return fail(RTOD_ERR_CONFIG, "pipeline must be RTOD_PIPELINE_FUSED or RTOD_PIPELINE_STAGED");
   return RTOD_OK;
 }
 
@@ -461,6 +466,7 @@ int scrub(rtod_handle* h) {
   }
   CU(cudaMemsetAsync(h->ctr, 0, sizeof(JobCtr) * kMaxJobs, h->stream));
   CU(cudaMemsetAsync(h->bs, 0, sizeof(BatchState), h->stream));
+  if (h->bar) CU(cudaMemsetAsync(h->bar, 0, sizeof(GridBar), h->stream));
   return RTOD_OK;
 }
 
@@ -697,6 +703,24 @@ struct Geom {
   int group = 0;  // group counts (route is then 0)
 };
 
+// Online training of the router on the buffered counts (one block; it
+// returns at once until enough samples are buffered), then the routing table.
+int launch_train(const Geom& g, cudaStream_t st) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(1);
+  cfg.blockDim = dim3(256);
+  cfg.dynamicSmemBytes = TRAIN_SMEM;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  CU(cudaLaunchKernelEx(&cfg, k_train, g.router));
+  CU(launch_k(k_table, dim3((TQ0 * TQ1 * TQ2 + 255) / 256), 256, st, g.router));
+  return RTOD_OK;
+}
+
 // Launches one batch: [ingest] hist scan scatter count compact [train].
 // kev (may be null) receives an event after each kernel (kev[0] after ingest,
 // or at the start when there is none; kev[6] after training or compact).
@@ -744,23 +768,47 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
   if (kev) CU(cudaEventRecord(kev[5], st));
   launched += 5;
   if (g.route && train) {
-    // Online training on the buffered counts (one block; it returns at once
-    // until enough samples are buffered), then the routing table.
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(1);
-    cfg.blockDim = dim3(256);
-    cfg.dynamicSmemBytes = TRAIN_SMEM;
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    CU(cudaLaunchKernelEx(&cfg, k_train, g.router));
-    CU(launch_k(k_table, dim3((TQ0 * TQ1 * TQ2 + 255) / 256), 256, st, g.router));
+    if (int r = launch_train(g, st)) return r;
     launched += 2;
   }
   if (kev) CU(cudaEventRecord(kev[6], st));
+  if (nk) *nk = launched;
+  return RTOD_OK;
+}
+
+// One batch of ring jobs (push/detect, the multi-stream API) as a single
+// cooperative launch of the fused pipeline (fused.cuh), then the router's
+// training step when due. *grid caches the launch's block count: as many
+// blocks as can be resident (up to 2 per SM), found on first use.
+int launch_fused(const Geom& g, const Batch& b, GridBar* bar, bool reset_out, int64_t* ids_host,
+                 int64_t ids_host_cap, BatchState* mirror, bool train, cudaStream_t st, int* grid, int64_t* nk) {
+  const FusedKind kind{g.D, g.f64 ? RTOD_PRED_F64_LT : g.pred, g.route, g.group};
+  Fused f{};
+  f.bar = bar;
+  auto dispatch = [&](int gsize, int* per_sm) {
+    return g.f64 ? fused_dispatch<double>(kind, b, f, gsize, st, per_sm)
+                 : fused_dispatch<float>(kind, b, f, gsize, st, per_sm);
+  };
+  if (*grid <= 0) {
+    int per_sm = 0;
+    CU(dispatch(0, &per_sm));
+    if (per_sm < 1) return fail(RTOD_ERR_CUDA, "the fused pipeline kernel cannot be resident");
+    *grid = std::min(per_sm, 2) * g.sm_count;
+  }
+  const int64_t per_block = 256 * (g.D <= 3 ? 2 : 1);  // points per block and step (Unroll)
+  f.hx = (uint32_t)std::max<int64_t>(1, (g.Wmax + per_block - 1) / per_block);
+  f.cx = (uint32_t)*grid;  // every job's queue is shared by all warps of the grid
+  f.tx = (uint32_t)((g.Wmax + CMP_TILE - 1) / CMP_TILE);
+  f.reset_out = reset_out ? 1 : 0;
+  f.ids_host = ids_host;
+  f.ids_host_cap = ids_host_cap;
+  f.mirror = mirror;
+  CU(dispatch(*grid, nullptr));
+  int64_t launched = 1;
+  if (g.route && train) {
+    if (int r = launch_train(g, st)) return r;
+    launched += 2;
+  }
   if (nk) *nk = launched;
   return RTOD_OK;
 }
@@ -834,8 +882,20 @@ int launch_detect_tail(rtod_handle* h, int64_t* nk) {
   return RTOD_OK;
 }
 
+// Whether a streaming detection runs the fused pipeline (one launch): the
+// default, except when per-stage times are asked for.
+bool fused_ring(const rtod_handle* h, const cudaEvent_t* kev) {
+  return h->cfg.pipeline == RTOD_PIPELINE_FUSED && !kev;
+}
+
 int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev, const Span* sp = nullptr) {
   int64_t nk = 0;
+  if (ingest && !sp && fused_ring(h, kev)) {
+    int r = launch_fused(geom_of(h), b, h->bar, true, h->ids_host_dev, std::min(h->ids_host_cap, h->ids_cap),
+                         h->bs_mirror_dev, train_now(h), h->stream, &h->fused_grid, &nk);
+    h->launches += nk;
+    return r;
+  }
   // streaming detection: this window's IDs start at the beginning of the buffer
   if (ingest) CU(cudaMemsetAsync(&h->bs->out_total, 0, sizeof(int64_t), h->stream));
   int r = sp ? launch_span(geom_of(h), b, *sp, h->stream, kev, &nk)
@@ -859,10 +919,16 @@ int run_batch(rtod_handle* h, const Batch& b, bool ingest, const Span* sp = null
     cudaGraph_t g;
     CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int64_t nk = 0;
-    if (ingest) CU(cudaMemsetAsync(&h->bs->out_total, 0, sizeof(int64_t), h->stream));  // as in launch_batch
-    int r = sp ? launch_span(geom_of(h), b, *sp, h->stream, nullptr, &nk)
-               : launch_group(geom_of(h), b, ingest, train, h->stream, nullptr, &nk);
-    if (!r && ingest) r = launch_detect_tail(h, &nk);
+    int r;
+    if (ingest && !sp && fused_ring(h, nullptr)) {
+      r = launch_fused(geom_of(h), b, h->bar, true, h->ids_host_dev, std::min(h->ids_host_cap, h->ids_cap),
+                       h->bs_mirror_dev, train, h->stream, &h->fused_grid, &nk);
+    } else {
+      if (ingest) CU(cudaMemsetAsync(&h->bs->out_total, 0, sizeof(int64_t), h->stream));  // as in launch_batch
+      r = sp ? launch_span(geom_of(h), b, *sp, h->stream, nullptr, &nk)
+             : launch_group(geom_of(h), b, ingest, train, h->stream, nullptr, &nk);
+      if (!r && ingest) r = launch_detect_tail(h, &nk);
+    }
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (r) return r;
     if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
@@ -1267,7 +1333,7 @@ void free_all(rtod_handle* h) {
   }
   h->pool.clear();
   free_span(h);
-  dfree(h->ctr); dfree(h->jobs_dev); dfree(h->bs); dfree(h->router); dfree(h->ring); dfree(h->ring_keys);
+  dfree(h->ctr); dfree(h->jobs_dev); dfree(h->bs); dfree(h->router); dfree(h->bar); dfree(h->ring); dfree(h->ring_keys);
   dfree(h->ring_prev); dfree(h->staging); dfree(h->run_buf); dfree(h->run_keys); dfree(h->run_prev);
   dfree(h->run_blk_lo); dfree(h->run_blk_hi);
   dfree(h->rec_base); dfree(h->ids);
@@ -1548,7 +1614,8 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
        !dalloc(&h->ring_keys, (size_t)h->W, c) && !dalloc(&h->ring_prev, (size_t)h->W, c) &&
        !dalloc(&h->staging, (size_t)(h->W * h->D * h->esz), c);
   ok = ok && cudaMallocHost((void**)&h->ctr_init, sizeof(JobCtr) * kMaxJobs) == cudaSuccess;
-  ok = ok && !dalloc(&h->router, 1, c);
+  ok = ok && !dalloc(&h->router, 1, c) && !dalloc(&h->bar, 1, c) &&
+       cudaMemset(h->bar, 0, sizeof(GridBar)) == cudaSuccess;
   if (ok) {
     RouterState* init = new (std::nothrow) RouterState;
     ok = init != nullptr;
@@ -2022,6 +2089,7 @@ struct rtod_batch {
   int device = 0;
   int n = 0;
   int route = 0;
+  int fused = 1;  // RTOD_PIPELINE_FUSED: one cooperative launch per group and step
   cudaStream_t stream = nullptr;
   std::vector<rtod_handle*> hs;
   struct Group {
@@ -2037,6 +2105,8 @@ struct rtod_batch {
     int32_t* nout_h = nullptr;    // pinned host
     BatchState* bs_h = nullptr;   // pinned host
     int64_t cmp_tiles = 0;
+    GridBar* bar = nullptr;       // grid barrier of the group's fused launch
+    int fused_grid = 0;
   };
   std::vector<Group> groups;
   RouterState* router = nullptr;
@@ -2052,7 +2122,7 @@ void batch_free(rtod_batch* b) {
   for (auto g : b->graphs)
     if (g) cudaGraphExecDestroy(g);
   for (auto& g : b->groups) {
-    dfree(g.jobs); dfree(g.bs); dfree(g.out); dfree(g.active); dfree(g.nout);
+    dfree(g.jobs); dfree(g.bs); dfree(g.out); dfree(g.active); dfree(g.nout); dfree(g.bar);
     if (g.active_h) cudaFreeHost(g.active_h);
     if (g.nout_h) cudaFreeHost(g.nout_h);
     if (g.bs_h) cudaFreeHost(g.bs_h);
@@ -2083,9 +2153,15 @@ int batch_enqueue(rtod_batch* b, bool train, int64_t* nk_total) {
   for (auto& g : b->groups) {
     const int ng = (int)g.streams.size();
     CU(cudaMemcpyAsync(g.active, g.active_h, sizeof(int32_t) * ng, cudaMemcpyHostToDevice, b->stream));
-    CU(cudaMemsetAsync(&g.bs->out_total, 0, sizeof(int64_t), b->stream));
     int64_t nk = 0;
-    int r = launch_group(g.geom, group_batch(g, b->router), true, train, b->stream, nullptr, &nk);
+    int r;
+    if (b->fused) {
+      r = launch_fused(g.geom, group_batch(g, b->router), g.bar, true, nullptr, 0, nullptr, train, b->stream,
+                       &g.fused_grid, &nk);
+    } else {
+      CU(cudaMemsetAsync(&g.bs->out_total, 0, sizeof(int64_t), b->stream));
+      r = launch_group(g.geom, group_batch(g, b->router), true, train, b->stream, nullptr, &nk);
+    }
     if (r) return r;
     total += nk;
     CU(cudaMemcpyAsync(g.nout_h, g.nout, sizeof(int32_t) * ng, cudaMemcpyDeviceToHost, b->stream));
@@ -2111,6 +2187,7 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
   b->device = cfgs[0].device;
   b->n = n_streams;
   b->route = cfgs[0].router ? 1 : 0;
+  b->fused = cfgs[0].pipeline == RTOD_PIPELINE_FUSED;
   b->filled.assign(n_streams, 0);
   b->pending.assign(n_streams, 0);
   auto bail = [&](int code) {
@@ -2183,8 +2260,9 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
     }
     for (auto& jb : tab) jb.gpts = group_part(g.out_cap, b->hs[g.streams[0]]->sm_count);
     if (dalloc(&g.jobs, ng, &dummy) || dalloc(&g.bs, 1, &dummy) || dalloc(&g.out, (size_t)g.out_cap, &dummy) ||
-        dalloc(&g.active, ng, &dummy) || dalloc(&g.nout, ng, &dummy))
+        dalloc(&g.active, ng, &dummy) || dalloc(&g.nout, ng, &dummy) || dalloc(&g.bar, 1, &dummy))
       return bail(RTOD_ERR_CUDA);
+    if (cudaMemset(g.bar, 0, sizeof(GridBar))) return bail(fail(RTOD_ERR_CUDA, "group setup failed"));
     if (cudaMallocHost((void**)&g.active_h, sizeof(int32_t) * ng) || cudaMallocHost((void**)&g.nout_h, sizeof(int32_t) * ng) ||
         cudaMallocHost((void**)&g.bs_h, sizeof(BatchState)))
       return bail(fail(RTOD_ERR_CUDA, "pinned allocation failed"));
@@ -2303,12 +2381,15 @@ RTOD_API int rtod_batch_step(rtod_batch* b, int64_t* out_offsets, int64_t* out_i
   return RTOD_OK;
 }
 
-RTOD_API int rtod_batch_stats(const rtod_batch* b, int64_t out[4]) {
+RTOD_API int rtod_batch_stats(const rtod_batch* b, int64_t out[5]) {
   if (!b || !out) return fail(RTOD_ERR_ARG, "null argument");
   out[0] = b->steps;
   out[1] = b->launches;
   out[2] = b->detections;
   out[3] = (int64_t)b->groups.size();
+  int64_t tests = 0;
+  for (const auto& g : b->groups) tests += (int64_t)g.bs_h->pair_tests;
+  out[4] = tests;
   return RTOD_OK;
 }
 

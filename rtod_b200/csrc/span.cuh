@@ -227,7 +227,7 @@ __global__ void __launch_bounds__(256) k_span_hist(Batch b, Span sp) {
 // 32-block step with a warp scan plus the running carry, and writes the
 // bin's row of pre (pre[b][nblk] = all its span points).
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_span_prefix(Batch b, Span sp) {
+static __global__ void __launch_bounds__(256) k_span_prefix(Batch b, Span sp) {
   pdl_trigger();
   pdl_wait();
   const int lane = threadIdx.x & 31;
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(256) k_span_prefix(Batch b, Span sp) {
 // k_span_scan: bin_start of the span (exclusive scan of bin_count), the list
 // of bins in use (each thread appends its non-empty bins of 4) and the
 // span's purity.
-__global__ void __launch_bounds__(256) k_span_scan(Batch b, Span sp) {
+static __global__ void __launch_bounds__(256) k_span_scan(Batch b, Span sp) {
   __shared__ uint32_t sm[33];
   __shared__ uint32_t s_base;
   pdl_trigger();
@@ -461,7 +461,7 @@ __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp,
   const Job& jb = b.jobs[j];
   const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
   uint32_t* row = sp.bits + ((jb.ctr->lo - sp.S) / sp.S % sp.chunk) * sp.words;
-  const GroupArgs ga{p, nq, bin, sp.n, sp.K, sp.R2f, sp.R, sp.R2, sp.Wp, pure && D <= 3};
+  const GroupArgs ga{p, nq, bin, sp.n, sp.K, sp.R2f, sp.R, sp.R2, sp.Wp, pure && D <= 3, &b.bs->pair_tests};
   const int nout = count_group<D, PRED, T>(
       static_cast<const T*>(sp.s_x), ga,
       [&](uint32_t sb, uint32_t& rs, uint32_t& len) {
@@ -505,7 +505,7 @@ __device__ __forceinline__ void span_clear_bins(const SpanCtr* c) {
 // holds a bin's windows side by side and neighbouring count warps read
 // mostly the same candidates.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
+static __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
   pdl_trigger();
   pdl_wait();
   const int lane = threadIdx.x & 31;
@@ -562,21 +562,26 @@ __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
 }
 
 // ---------------------------------------------------------------------------
-// k_span_count: one warp per listed group of the batch (warps stride over the
-// list). Outliers set their bit in the slide's bitset row. Then the blocks
-// clear the per-bin state, and the block that finishes last ends the batch
-// (records, window advance, counters).
+// k_span_count: one warp per listed group of the batch, groups taken in list
+// order by ticket (one atomic per group), so that a warp that drew short
+// groups takes more of them and no warp idles while long groups remain.
+// Outliers set their bit in the slide's bitset row. Then the blocks clear the
+// per-bin state, and the block that finishes last ends the batch (records,
+// window advance, counters).
 // ---------------------------------------------------------------------------
 template <int D, int PRED, typename T>
 __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
   __shared__ int s_last;
   pdl_trigger();
   pdl_wait();
-  const int64_t gstride = (int64_t)gridDim.x * blockDim.x;
-  const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int64_t ng = sp.sc->n_groups;
+  const int lane = threadIdx.x & 31;
+  const uint32_t ng = sp.sc->n_groups;
   const bool pure = sp.sc->pure;
-  for (int64_t k = gtid >> 5; k < ng; k += gstride >> 5) {
+  while (true) {
+    uint32_t k = 0;
+    if (lane == 0) k = atomicAdd(&sp.sc->count_ticket, 1u);
+    k = __shfl_sync(0xffffffffu, k, 0);
+    if (k >= ng) break;
     const uint4 g = sp.groups[k];
     const int j = (int)g.w;
     span_count_group<D, PRED, T>(b, sp, g.x, g.y, g.z, WinPre{sp.pre, sp.ts, j, sp.wblk}, pure);
@@ -606,7 +611,7 @@ struct SpanOut {
   BatchState* bs;
 };
 
-__global__ void __launch_bounds__(1024) k_span_compact(SpanOut o, int64_t s0) {
+static __global__ void __launch_bounds__(1024) k_span_compact(SpanOut o, int64_t s0) {
   __shared__ uint32_t sm[33];
   pdl_trigger();
   pdl_wait();

@@ -72,7 +72,7 @@ class Detector:
                  pred: str = "fp32_le", router: bool = False, tuner: bool = False,
                  cells_per_r: int = 0, block_warps: int = 0, use_graph: bool = True,
                  batch: int = 0, device: int = 0, engine: str = "auto", coord: str = "f32",
-                 count: str = "auto"):
+                 count: str = "auto", pipeline: str = "fused"):
         cfg = Config()
         check(lib().rtod_config_init(ctypes.byref(cfg)))
         cfg.window, cfg.slide, cfg.R, cfg.K, cfg.dim, cfg.opt = window, slide, R, K, dim, opt
@@ -83,6 +83,7 @@ class Detector:
         cfg.engine = _native.ENGINE[engine]
         cfg.coord = _native.COORD[coord]
         cfg.count = _native.COUNT[count]
+        cfg.pipeline = _native.PIPELINE[pipeline]
         self.f64 = coord == "f64"
         self.cfg = cfg
         self.window, self.slide, self.R, self.K, self.dim = window, slide, R, K, dim
@@ -241,6 +242,7 @@ class BatchDetector:
             c.dim, c.opt = st.get("dim", 1), st.get("opt", 2)
             c.pred = _native.PRED[st.get("pred", "fp32_le")]
             c.count = _native.COUNT[st.get("count", "auto")]
+            c.pipeline = _native.PIPELINE[st.get("pipeline", "fused")]
             c.router, c.device = int(router), device
         self.streams = [dict(s) for s in streams]
         self._b = ctypes.c_void_p()
@@ -282,6 +284,6 @@ class BatchDetector:
 
     @property
     def stats(self) -> dict:
-        a = (ctypes.c_int64 * 4)()
+        a = (ctypes.c_int64 * 5)()
         check(lib().rtod_batch_stats(self._b, a))
-        return {"steps": a[0], "launches": a[1], "detections": a[2], "groups": a[3]}
+        return {"steps": a[0], "launches": a[1], "detections": a[2], "groups": a[3], "pair_tests": a[4]}

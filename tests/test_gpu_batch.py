@@ -36,15 +36,18 @@ def make_streams(n=9, seed=5):
     return out
 
 
-@pytest.mark.parametrize("router,count", [(False, "auto"), (True, "auto"), (False, "group"), (True, "point")])
-def test_batch_matches_oracle(rtod, oracle_mod, router, count):
+@pytest.mark.parametrize("router,count,pipeline", [(False, "auto", "fused"), (True, "auto", "fused"),
+                                                   (False, "group", "fused"), (True, "point", "fused"),
+                                                   (False, "auto", "staged"), (True, "auto", "staged")])
+def test_batch_matches_oracle(rtod, oracle_mod, router, count, pipeline):
     streams = make_streams()
     expect = []
     for st in streams:
         off, ids, _ = oracle_mod.detect(st["points"], st["window"], st["slide"], st["R"], st["K"],
                                         st["pred"], engine="grid", threads=4)
         expect.append((off, ids))
-    cfg = [dict({k: st[k] for k in ("window", "slide", "R", "K", "dim", "pred")}, count=count) for st in streams]
+    cfg = [dict({k: st[k] for k in ("window", "slide", "R", "K", "dim", "pred")}, count=count, pipeline=pipeline)
+           for st in streams]
     with rtod.BatchDetector(cfg, router=router) as bd:
         for i, st in enumerate(streams):
             bd.push(i, st["points"][:st["window"]])
@@ -71,6 +74,7 @@ def test_batch_matches_oracle(rtod, oracle_mod, router, count):
         assert all(done[i] == st["slides"] for i, st in enumerate(streams))
         stats = bd.stats
         assert stats["groups"] == 4  # d=1, d=3, d=8 with fp32, and the f64 stream
+        assert stats["pair_tests"] >= 0
         assert stats["detections"] == sum(st["slides"] for st in streams)
 
 

@@ -39,16 +39,43 @@ def test_run_matches_golden(rtod, path, opt, graph, n, engine):
 
 
 @pytest.mark.parametrize("path", golden_cases(), ids=lambda p: os.path.basename(p)[:-4])
-def test_push_detect_matches_golden(rtod, path):
+@pytest.mark.parametrize("pipeline,graph", [("fused", True), ("fused", False), ("staged", True)])
+def test_push_detect_matches_golden(rtod, path, pipeline, graph):
+    """RTOD's per-slide loop: push S points, detect; the fused pipeline (one
+    cooperative launch per detection) and the staged one."""
     meta, pts, off, ids = load_golden(path)
     W, S = meta["W"], meta["S"]
-    with rtod.Detector(W, S, meta["R"], meta["K"], dim=pts.shape[1], pred=meta["pred"]) as det:
+    with rtod.Detector(W, S, meta["R"], meta["K"], dim=pts.shape[1], pred=meta["pred"], pipeline=pipeline,
+                       use_graph=graph) as det:
         det.push(pts[:W])
         for j in range(len(off) - 1):
             det.push(pts[W + j * S:W + (j + 1) * S])
             got = det.detect()
             np.testing.assert_array_equal(got, ids[off[j]:off[j + 1]])
         assert det.slides_done == len(off) - 1
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(router=True), dict(count="group"), dict(cells_per_r=4),
+                                dict(pred="f64_lt"), dict(router=True, use_graph=False),
+                                dict(pipeline="staged")])
+def test_push_detect_stock_like_stream(rtod, oracle_mod, kw):
+    """The stock-like stream (W=100k, S=5k) slide by slide, 40 slides, against
+    the oracle; every seventh detection asks for stage times (the staged
+    pipeline then runs, with per-stage events) and must agree too."""
+    from rtod_b200 import datagen
+    w = datagen.stock_like()
+    n = 40
+    pred = kw.get("pred", "fp32_le")
+    off, ids, _ = oracle_mod.detect(w.points[:w.window + n * w.slide], w.window, w.slide, w.R, w.K, pred,
+                                    engine="grid", threads=os.cpu_count() or 4)
+    with rtod.Detector(w.window, w.slide, w.R, w.K, **kw) as det:
+        det.push(w.points[:w.window])
+        for j in range(n):
+            det.push(w.points[w.window + j * w.slide:w.window + (j + 1) * w.slide])
+            got = det.detect(times=(j % 7 == 3))
+            if isinstance(got, tuple):
+                got = got[0]
+            np.testing.assert_array_equal(got, ids[off[j]:off[j + 1]])
 
 
 @pytest.mark.parametrize("source", ["host", "pinned", "device"])
@@ -129,12 +156,12 @@ def batched_expect(oracle_mod):
     return streams, expect
 
 
-@pytest.mark.parametrize("router", [False, True])
-def test_batched_streams_first_slides(rtod, batched_expect, router):
+@pytest.mark.parametrize("router,pipeline", [(False, "fused"), (True, "fused"), (False, "staged")])
+def test_batched_streams_first_slides(rtod, batched_expect, router, pipeline):
     """All 64 streams of the batched workload through the multi-stream API
     (one graph replay per step), first 3 slides of every stream."""
     streams, expect = batched_expect
-    cfg = [dict(window=w.window, slide=w.slide, R=w.R, K=w.K, dim=w.dim) for w in streams]
+    cfg = [dict(window=w.window, slide=w.slide, R=w.R, K=w.K, dim=w.dim, pipeline=pipeline) for w in streams]
     with rtod.BatchDetector(cfg, router=router) as bd:
         for i, w in enumerate(streams):
             bd.push(i, w.points[:w.window])
