@@ -355,6 +355,7 @@ def run_ours(args, world, rank, local):
         assert np.array_equal(r["ids"], base["ids"]), name
     base["streaming"] = measure_streaming(w, local, base)
     base["batched"] = None if args.no_batched else measure_batched(local)
+    base["router_ab"] = measure_router_ab(local)
     ranks.close()
     if rank != 0:
         return None
@@ -390,7 +391,8 @@ OPS_PER_TEST = {d: 3 * d for d in range(1, 9)}
 def measure_batched(local, steps: int = 20, warmup: int = 3):
     """The batched workload: 64 independent streams (W log-uniform in [5k,
     200k], S = W/20, d in {1, 3, 8}) through the multi-stream API, one graph
-    replay of the fused pipeline per step. The step time is the wall time of
+    replay per step (staged launches; the persistent fused launch is timed
+    beside it). The step time is the wall time of
     rtod_batch_step (it ends with one stream wait); e2e adds the step's 64
     host pushes. The 8-d streams also run alone, to set their group count's
     distance tests against the FP32 issue rate (compute bound: every point
@@ -400,7 +402,7 @@ def measure_batched(local, steps: int = 20, warmup: int = 3):
     streams = datagen.batched_streams(slides=warmup + steps)
     pts_per_step = sum(s.slide for s in streams)
 
-    def run(subset, pipeline="fused"):
+    def run(subset, pipeline="staged"):
         cfg = [dict(window=s.window, slide=s.slide, R=s.R, K=s.K, dim=s.dim, pipeline=pipeline) for s in subset]
         with BatchDetector(cfg, device=local) as bd:
             for i, s in enumerate(subset):
@@ -425,7 +427,7 @@ def measure_batched(local, steps: int = 20, warmup: int = 3):
     torch.cuda.synchronize()
     with ClockSampler(physical_gpu_index(local)) as clk:
         t_step, t_e2e, st, _ = run(streams)
-    t_staged, _, _, _ = run(streams, "staged")
+    t_fused, _, _, _ = run(streams, "fused")
     d8 = [s for s in streams if s.dim == 8]
     t8, _, _, tests8 = run(d8)
     sm = torch.cuda.get_device_properties(local).multi_processor_count
@@ -439,7 +441,7 @@ def measure_batched(local, steps: int = 20, warmup: int = 3):
         "window_points_per_s": sum(s.window for s in streams) * steps / t_step,
         "e2e": {"ms_per_step": t_e2e / steps * 1e3, "points_per_s": pts_per_step * steps / t_e2e,
                 "h2d_bytes_per_step": sum(4 * s.dim * s.slide for s in streams)},
-        "staged_pipeline_ms_per_step": t_staged / steps * 1e3,
+        "fused_pipeline_ms_per_step": t_fused / steps * 1e3,
         "launches_per_step": st["launches"] / max(1, st["steps"]), "groups": st["groups"],
         "clocks": clk.summary(),
         "roofline_8d": {"bound": "fp32 issue", "streams": len(d8), "ms_per_step": t8 / steps * 1e3,
@@ -448,6 +450,41 @@ def measure_batched(local, steps: int = 20, warmup: int = 3):
                         "frac": achieved_ops / peak_ops,
                         "peak_source": f"{sm} SMs x 128 FP32 lanes x {mhz:.0f} MHz (median SM clock sampled)"},
     }
+
+
+def measure_router_ab(local, steps: int = 11):
+    """The learned router on and off, both autotuned, on the configurations
+    that name it (sensor-like 3-d: router on; Gaussian mixture K=30: router
+    vs plain) and the headline stream: device time per slide (median over
+    steps passes, device-resident stream and outputs), outliers identical."""
+    import torch
+    from rtod_b200 import Detector, datagen
+    out = {}
+    for w in (datagen.stock_like(), datagen.sensor_like(), datagen.gaussian_like(30)):
+        pts = torch.from_numpy(w.points).to(f"cuda:{local}")
+        cap = w.slides * w.window // 4 + 1024
+        ids = torch.empty(cap, dtype=torch.int64, device=f"cuda:{local}")
+        row, ref = {}, None
+        for router in (False, True):
+            with Detector(w.window, w.slide, w.R, w.K, dim=w.dim, device=local, tuner=True, router=router) as det:
+                ts = []
+                for _ in range(3 + steps):
+                    det.reset()
+                    r = det.run(pts, out_ids=ids, ids_cap=cap, times=True)
+                    ts.append(r.times["total"] * 1e3)
+                got = (r.offsets.copy(), ids[:int(r.offsets[-1])].cpu().numpy())
+                if ref is None:
+                    ref = got
+                assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+                key = "router_on" if router else "router_off"
+                row[key] = {"us_per_slide": float(np.median(ts[3:])), "tuning": det.tuning}
+                if router:
+                    info = det.router_info()
+                    row[key]["router"] = {k: info[k] for k in ("steps", "routed_early", "routed_sweep", "misrouted")}
+        row["speedup"] = row["router_off"]["us_per_slide"] / row["router_on"]["us_per_slide"]
+        row["bit_exact"] = True
+        out[w.name] = row
+    return out
 
 
 def cpu_baseline(w):
@@ -537,6 +574,7 @@ def emit_ours(args, world, w, res):
         "bit_exact_across_engines": True,
         "streaming": r.get("streaming"),
         "batched": r.get("batched"),
+        "router_ab": r.get("router_ab"),
     }
     if not args.no_cpu_baseline and world == 1:
         cb, (coff, cids) = cpu_baseline(w)

@@ -84,8 +84,12 @@ typedef struct rtod_config {
   int32_t opt;         /* OPTIMIZATION macro (optixScan.h:22-24): 0 = no grid filter,
                           1 and 2 = grid filter (identical results) */
   int32_t pred;        /* RTOD_PRED_*; default RTOD_PRED_FP32_LE */
-  int32_t router;      /* 1 = learned router on (routes counted points into an early-exit
-                          and a full-sweep queue); results are identical either way */
+  int32_t router;      /* 1 = learned router on: in the span engine it routes each bin's
+                          counts to independent early-exit counts or to delta segments
+                          (windows counted from the previous window's counts and the two
+                          changed slide blocks); in the window engine it routes counted
+                          points into an early-exit and a full-sweep queue. Results are
+                          identical either way */
   int32_t tuner;       /* 1 = autotune cell width and block shape on the first slides */
   int32_t cells_per_r; /* grid cells per R along each hashed dimension (1..3, 1..8 in 1-d;
                           0 = auto) */
@@ -94,8 +98,8 @@ typedef struct rtod_config {
   int32_t device;      /* CUDA device ordinal */
   int32_t batch;       /* rtod_run: windows detected per launch (0 = auto); each window is
                           processed on its own, so results do not depend on it */
-  int32_t engine;      /* rtod_run engine: RTOD_ENGINE_AUTO (span engine without the
-                          router, else window engine; the tuner may choose either),
+  int32_t engine;      /* rtod_run engine: RTOD_ENGINE_AUTO (span engine; the tuner may
+                          choose either),
                           RTOD_ENGINE_WINDOW (one counting sort per window) or
                           RTOD_ENGINE_SPAN (one counting sort per batch of windows;
                           falls back to the window engine when W/S > 2047).
@@ -108,11 +112,15 @@ typedef struct rtod_config {
 } rtod_config;
 
 /* rtod_config.pipeline */
-#define RTOD_PIPELINE_FUSED 0  /* default: one cooperative launch per detection (per group of
+#define RTOD_PIPELINE_STAGED 0 /* default: one launch per stage (ingest, hist, scan, scatter,
+                                  count, compact, output), PDL-chained, replayed as a graph */
+#define RTOD_PIPELINE_FUSED 1  /* one persistent cooperative launch per detection (per group of
                                   streams in the multi-stream API) running every stage, the
-                                  stages separated by bounded grid barriers */
-#define RTOD_PIPELINE_STAGED 1 /* one launch per stage (ingest, hist, scan, scatter, count,
-                                  compact, output) */
+                                  stages separated by bounded grid barriers. Measured on B200:
+                                  no faster per window than the staged launches (the stages'
+                                  own dependent memory round trips dominate, not the launches),
+                                  and slower on 8-d multi-stream steps (one register budget for
+                                  every stage lowers the count stage's occupancy) */
 
 /* Per-slide stage times in ms, averaged over the slides of the last call,
    under the names of RTOD's Timer (src/ods/timer.h:16-24, :102-117). */
@@ -306,6 +314,14 @@ int rtod_detect_window_static(const float* pts, int64_t n, int32_t dim, double R
    inlier but outlier, or the reverse), [5] routing threshold. No counterpart
    in RTOD (it has no learned component). */
 int rtod_router_info(rtod_handle* h, float* params, double info[6]);
+
+/* Sets the router's threshold: a count (span engine: a bin's run of windows;
+   window engine: a point) goes to the early-exit path when the network's
+   probability of "mostly inliers" is at least the threshold, else to the
+   delta segments / full-sweep queue. 0 sends everything to early exit, any
+   value above 1 sends everything eligible to the other path. The tuner sets
+   it when on. Results do not depend on it. No counterpart in RTOD. */
+int rtod_router_set_threshold(rtod_handle* h, float threshold);
 
 /* Router network test entry points (no counterpart in RTOD), run on the
    given device with host buffers: parameter count; forward logits

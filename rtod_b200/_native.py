@@ -30,7 +30,7 @@ ENGINE = {"auto": 0, "window": 1, "span": 2}
 COORD = {"f32": 0, "f64": 1}
 COUNT = {"auto": 0, "point": 1, "group": 2}
 COUNT_NAME = {1: "point", 2: "group"}
-PIPELINE = {"fused": 0, "staged": 1}
+PIPELINE = {"staged": 0, "fused": 1}
 ENGINE_NAME = {1: "window", 2: "span"}
 
 
@@ -82,6 +82,7 @@ SIGNATURES = [
     ("rtod_profile_run", _i32, [_vp, _vp, _i64, _i64, _vp, _i32]),
     ("rtod_kernel_name", ctypes.c_char_p, [_i32]),
     ("rtod_router_info", _i32, [_vp, _vp, _vp]),
+    ("rtod_router_set_threshold", _i32, [_vp, ctypes.c_float]),
     ("rtod_detect_window_static", _i32, [_vp, _i64, _i32, ctypes.c_double, _i32, _i32, _vp,
                                          ctypes.POINTER(_i64), _vp]),
     ("rtod_batch_create", _i32, [_vp, _i32, ctypes.POINTER(_vp)]),

@@ -87,11 +87,20 @@ struct GroupArgs {
   unsigned long long* tests;  // distance tests made, added once per group (may be null)
 };
 
+// Bounds of a count: [lo, hi], hi = CNT_INF when only a lower bound is known.
+constexpr int32_t CNT_INF = 1 << 29;
+
 // Counts the group; range(sb, rs, len) gives the candidate positions of
 // stencil bin sb, mark(pos) records an outlier (called by one lane per
-// outlier). Returns the number of outliers (the same on every lane).
-template <int D, int PRED, typename T, class Range, class Mark>
-__device__ __forceinline__ int count_group(const T* sx, const GroupArgs& a, Range range, Mark mark) {
+// outlier). pick(i) is the position of the group's i-th point (i < a.nq) and
+// rec(pos, lo, hi) receives bounds of each point's count (exact when equal:
+// the outliers; inliers get lo > K and hi = CNT_INF); *made (may be null)
+// receives the distance tests made. Returns the number of outliers (the
+// same on every lane).
+template <int D, int PRED, typename T, class Range, class Mark, class Pick, class Rec>
+__device__ __forceinline__ int count_group_ex(const T* sx, const GroupArgs& a, Range range, Mark mark, Pick pick,
+                                              Rec rec, unsigned long long* made = nullptr) {
+  if (made) *made = 0;
   constexpr int H = Hashed<D>::value;
   constexpr int CPL = GroupCpl<D>::value;
   constexpr uint32_t CHUNK = 32 * CPL;
@@ -123,9 +132,15 @@ __device__ __forceinline__ int count_group(const T* sx, const GroupArgs& a, Rang
     rs1 = rs;
     len1 = sure ? 0u : len;
   }
-  if (given > (uint32_t)a.K) return 0;  // every point of the group is an inlier
-  if (total <= (uint32_t)a.K) {          // every point of the group is an outlier
-    for (uint32_t q = lane; q < a.nq; q += 32) mark(a.p + q);
+  if (given > (uint32_t)a.K) {  // every point of the group is an inlier
+    for (uint32_t q = lane; q < a.nq; q += 32) rec(pick(q), (int)given, CNT_INF);
+    return 0;
+  }
+  if (total <= (uint32_t)a.K) {  // every point of the group is an outlier
+    for (uint32_t q = lane; q < a.nq; q += 32) {
+      mark(pick(q));
+      rec(pick(q), 1, (int)total);
+    }
     return (int)a.nq;
   }
   // Current round: per-lane range, exclusive offset of the lane's range in
@@ -166,7 +181,7 @@ __device__ __forceinline__ int count_group(const T* sx, const GroupArgs& a, Rang
     if (empty && next < a.nq) {
       const uint32_t rank = (uint32_t)__popc(empty & lanemask_lt());
       if (!has && next + rank < a.nq) {
-        mine = a.p + next + rank;
+        mine = pick(next + rank);
 #pragma unroll
         for (int d = 0; d < D; ++d) qx[d] = sx[(int64_t)d * a.Wp + mine];
         cnt = (int)given;
@@ -216,8 +231,10 @@ __device__ __forceinline__ int count_group(const T* sx, const GroupArgs& a, Rang
     if (has) {
       --left;
       if (cnt > a.K) {
+        rec(mine, cnt, CNT_INF);
         has = false;
       } else if (left == 0) {
+        rec(mine, cnt, cnt);
         out = true;
         has = false;
       }
@@ -238,7 +255,15 @@ __device__ __forceinline__ int count_group(const T* sx, const GroupArgs& a, Rang
     }
   }
   if (a.tests && lane == 0 && tests) atomicAdd(a.tests, tests);
+  if (made) *made = tests;
   return nout;
+}
+
+// count_group_ex over the contiguous positions [a.p, a.p + a.nq), no bounds kept.
+template <int D, int PRED, typename T, class Range, class Mark>
+__device__ __forceinline__ int count_group(const T* sx, const GroupArgs& a, Range range, Mark mark) {
+  return count_group_ex<D, PRED, T>(
+      sx, a, range, mark, [&](uint32_t i) { return a.p + i; }, [](uint32_t, int, int) {});
 }
 
 }  // namespace rtod

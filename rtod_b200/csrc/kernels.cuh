@@ -102,7 +102,8 @@ struct SpanCtr {
   uint32_t n_used;       // bins holding span points
   int32_t pure;          // the span's cells and their sure neighbours map to distinct bins (k_span_scan)
   uint32_t n_groups;     // groups listed for exact counts in the running batch
-  uint32_t count_ticket; // next listed group for a count warp to take
+  uint32_t n_segs;       // delta segments listed (learned router on), from the back of the list
+  uint32_t seg_ticket;   // next delta segment for a count warp to take
   long long cmin[3];     // per hashed dimension, the span's cell coordinate range (k_span_hist)
   long long cmax[3];
   uint32_t* used;        // [NB] bins in use
@@ -707,6 +708,17 @@ __global__ void __launch_bounds__(256) k_hist(Batch b) {
   pdl_trigger();
   pdl_wait();
   hist_body<D>(b, hw_block());
+}
+
+// k_hist of ring jobs with the slide's ingest folded in (the S newest points
+// keyed from the staged slide and written into the ring); with reset_out it
+// also starts the batch output at zero (read by the compaction).
+template <int D, typename T>
+__global__ void __launch_bounds__(256) k_hist_ingest(Batch b, int32_t reset_out) {
+  pdl_trigger();
+  pdl_wait();
+  if (reset_out && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) b.bs->out_total = 0;
+  hist_body<D, T, true>(b, hw_block());
 }
 
 // ---------------------------------------------------------------------------
@@ -1463,7 +1475,8 @@ static __device__ void finish_batch(const Batch& b) {
     if (b.span) {
       b.span->n_used = 0;
       b.span->n_groups = 0;
-      b.span->count_ticket = 0;
+      b.span->n_segs = 0;
+      b.span->seg_ticket = 0;
       for (int d = 0; d < 3; ++d) {
         b.span->cmin[d] = LLONG_MAX;
         b.span->cmax[d] = LLONG_MIN;
@@ -1576,6 +1589,87 @@ static __global__ void __launch_bounds__(256) k_compact(Batch b) {
   pdl_trigger();
   pdl_wait();
   compact_body(b, hw_block());
+}
+
+// ---------------------------------------------------------------------------
+// k_compact_one: the compaction of windows of at most COMPACT1_MAX offsets,
+// one block of 1024 threads per job (grid = jobs): the job's whole bitset in
+// one block scan (CMP1_WPT words per thread), no look-back chain between
+// tiles. The block that finishes last ends the batch (finish_batch) and, for
+// a streaming detection, writes the IDs and the batch state into the mapped
+// page-locked landing buffers (k_run_out's work, folded in).
+// ---------------------------------------------------------------------------
+constexpr int CMP1_WPT = 8;
+constexpr int64_t COMPACT1_MAX = 1024 * 32 * CMP1_WPT;  // 262144 window offsets
+
+static __global__ void __launch_bounds__(1024) k_compact_one(Batch b, int64_t* ids_host, int64_t ids_host_cap,
+                                                             BatchState* mirror) {
+  __shared__ uint32_t sm[33];
+  __shared__ int64_t s_jobbase;
+  __shared__ uint32_t s_last;
+  pdl_trigger();
+  pdl_wait();
+  const uint32_t job = blockIdx.x;
+  const Job& jb = b.jobs[job];
+  BatchState* bs = b.bs;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const bool act = job_active(b, job);
+  if (act && wid == 0) {
+    // Output base of this job: IDs of all earlier jobs of the batch come first.
+    int64_t part = 0;
+    for (int j = lane; j < (int)job; j += 32)
+      if (job_active(b, j)) part += b.jobs[j].ctr->n_out;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if (lane == 0) s_jobbase = bs->out_total + part;
+  }
+  __syncthreads();
+  if (act) {
+    const int64_t lo = jb.ctr->lo;
+    const int64_t nwords = (jb.W + 31) >> 5;
+    const int64_t w0 = (int64_t)threadIdx.x * CMP1_WPT;
+    uint32_t bits[CMP1_WPT];
+    uint32_t cnt = 0;
+#pragma unroll
+    for (int e = 0; e < CMP1_WPT; ++e) {
+      bits[e] = w0 + e < nwords ? jb.flags[w0 + e] : 0u;
+      if (bits[e]) jb.flags[w0 + e] = 0;
+      cnt += __popc(bits[e]);
+    }
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan(cnt, &total, sm);
+    int64_t o = s_jobbase + ex;
+#pragma unroll
+    for (int e = 0; e < CMP1_WPT; ++e) {
+      uint32_t v = bits[e];
+      while (v) {
+        const int f = __ffs(v) - 1;
+        v &= v - 1;
+        if (o < b.out_cap) b.out_ids[o] = lo + (w0 + e) * 32 + f;
+        else set_err(bs, DERR_CAPACITY);
+        ++o;
+      }
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_last = atomicAdd(&bs->done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  finish_batch(b);
+  if (ids_host || mirror) {
+    __syncthreads();
+    __threadfence();
+    if (ids_host) {
+      const int64_t n = min(bs->out_total, ids_host_cap);
+      for (int64_t i = threadIdx.x; i < n; i += blockDim.x) ids_host[i] = b.out_ids[i];
+    }
+    __syncthreads();
+    if (mirror && threadIdx.x == 0) {
+      __threadfence_system();
+      *mirror = *bs;
+    }
+  }
 }
 
 }  // namespace rtod

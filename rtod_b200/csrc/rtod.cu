@@ -198,6 +198,7 @@ struct SpanScratch {
   int64_t pts_cap = 0;
   int64_t chunk_cap = 0;
   int64_t Wp = 0;
+  int64_t gcap = 0;  // entries of groups
   int64_t bytes = 0;
 };
 
@@ -329,9 +330,9 @@ struct rtod_handle {
   // A whole rtod_run of a device-resident stream with the span engine, as one
   // graph (memsets, counter upload, keys, batches, compaction), replayed while
   // its key (stream, slides, batch and span parameters) stays the same.
-  cudaGraphExec_t run_graph = nullptr;
-  std::vector<unsigned char> run_graph_key;
-  int64_t run_graph_kernels = 0;
+  cudaGraphExec_t run_graph[2] = {nullptr, nullptr};  // without / with the router's training step
+  std::vector<unsigned char> run_graph_key[2];
+  int64_t run_graph_kernels[2] = {0, 0};
   int graph_ring = -1;
   int64_t batches = 0;
 
@@ -348,6 +349,7 @@ struct rtod_handle {
   double flush_ms = 0;  // device ms of the span engine's deferred compaction in the last profiled run
   float threshold = 0.5f;
   uint32_t max_sweep = 64;
+  int span_route = 1;  // with the router on: the span engine routes its counts (the tuner may turn it off)
 };
 
 namespace {
@@ -401,8 +403,10 @@ void drop_graph(rtod_handle* h) {
     g = nullptr;
   }
   h->graph_ring = -1;
-  if (h->run_graph) cudaGraphExecDestroy(h->run_graph);
-  h->run_graph = nullptr;
+  for (auto& rg : h->run_graph) {
+    if (rg) cudaGraphExecDestroy(rg);
+    rg = nullptr;
+  }
 }
 
 // Pool entries for `jobs` jobs; with `full`, their window-engine scratch.
@@ -509,6 +513,7 @@ int ensure_span(rtod_handle* h, int64_t nblk, int64_t chunk) {
   sp.pts_cap = pts;
   sp.chunk_cap = chunk;
   sp.Wp = Wp;
+  sp.gcap = (nblk - h->W / h->S + 1) * std::min<int64_t>(h->W, NB);
   CU(cudaMemset(sp.bits, 0, (size_t)(chunk * words) * sizeof(uint32_t)));
   CU(cudaMemset(sp.bin_count, 0, NB * sizeof(uint32_t)));
   CU(cudaMemset(sp.kmin, 0xff, NB * sizeof(unsigned long long)));
@@ -578,6 +583,14 @@ Span make_span(const rtod_handle* h, int B, const void* stream_pts, int64_t chun
   sp.bits = ss.bits;
   sp.words = (h->W + 31) / 32;
   sp.chunk = chunk;
+  sp.gcap = (uint32_t)ss.gcap;
+  // delta segments (learned router): stencils of at most 32 slots, a cell
+  // filter, and up to 3 dimensions
+  {
+    const int w = 2 * h->n + 1;
+    const int slots = sp.h == 1 ? w : (sp.h == 2 ? w * w : w * w * w);
+    sp.route = (h->cfg.router && h->span_route && h->D <= 3 && slots <= 32) ? 1 : 0;
+  }
   return sp;
 }
 
@@ -721,25 +734,26 @@ int launch_train(const Geom& g, cudaStream_t st) {
   return RTOD_OK;
 }
 
-// Launches one batch: [ingest] hist scan scatter count compact [train].
-// kev (may be null) receives an event after each kernel (kev[0] after ingest,
-// or at the start when there is none; kev[6] after training or compact).
+// Launches one batch: hist (with the ring jobs' ingest folded in) scan
+// scatter count compact [train]. kev (may be null) receives an event at the
+// start (kev[0]) and after each kernel (kev[6] after training or compact).
+// ids_host / mirror (streaming): the mapped landing buffers that the
+// compaction's last block fills with the IDs and the batch state.
 // Returns the number of kernels launched in *nk.
 int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStream_t st, cudaEvent_t* kev,
-                 int64_t* nk) {
+                 int64_t* nk, int64_t* ids_host = nullptr, int64_t ids_host_cap = 0, BatchState* mirror = nullptr) {
   const int64_t W = g.Wmax, nj = b.njobs;
   const unsigned gy = (unsigned)nj;
   int64_t launched = 0;
-  if (ingest) {
-    const int64_t gx = std::max<int64_t>(1, std::min<int64_t>((g.Smax + 255) / 256, g.sm_count * 4));
-    DISPATCH_DT(g.f64, g.D, CU(launch_k(k_ingest<D, T>, dim3((unsigned)gx, gy), 256, st, b, 0)));
-    launched++;
-  }
   if (kev) CU(cudaEventRecord(kev[0], st));
   const int64_t per_block = 256 * (g.D <= 3 ? 2 : 1);  // points per block per loop iteration (Unroll)
   const int64_t wx = std::max<int64_t>(
       1, std::min<int64_t>((W + per_block - 1) / per_block, std::max<int64_t>(2, (g.sm_count * 16 + nj - 1) / nj)));
-  DISPATCH_D(g.D, CU(launch_k(k_hist<D>, dim3((unsigned)wx, gy), 256, st, b)));
+  if (ingest) {  // ring jobs: the slide's ingest folded into the histogram, the output restarted
+    DISPATCH_DT(g.f64, g.D, CU(launch_k(k_hist_ingest<D, T>, dim3((unsigned)wx, gy), 256, st, b, 1)));
+  } else {
+    DISPATCH_D(g.D, CU(launch_k(k_hist<D>, dim3((unsigned)wx, gy), 256, st, b)));
+  }
   if (kev) CU(cudaEventRecord(kev[1], st));
   CU(launch_k(k_scan, dim3(SCAN_TILES, gy), 256, st, b));
   if (kev) CU(cudaEventRecord(kev[2], st));
@@ -764,7 +778,16 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
                  CU(launch_k(k_count<D, PRED, false, T>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
   }
   if (kev) CU(cudaEventRecord(kev[4], st));
-  CU(launch_k(k_compact, dim3((unsigned)((W + CMP_TILE - 1) / CMP_TILE), gy), 256, st, b));
+  if (W <= COMPACT1_MAX) {  // one block per window (delivers a streaming detection's IDs itself)
+    CU(launch_k(k_compact_one, dim3(gy), 1024, st, b, ids_host, ids_host_cap, mirror));
+  } else {
+    CU(launch_k(k_compact, dim3((unsigned)((W + CMP_TILE - 1) / CMP_TILE), gy), 256, st, b));
+    if (ids_host || mirror) {
+      const unsigned ox = (unsigned)std::max<int64_t>(1, std::min<int64_t>((W + 255) / 256, g.sm_count));
+      CU(launch_k(k_run_out, dim3(ox), 256, st, (const int64_t*)b.out_ids, ids_host, ids_host_cap, b.bs, mirror));
+      launched++;
+    }
+  }
   if (kev) CU(cudaEventRecord(kev[5], st));
   launched += 5;
   if (g.route && train) {
@@ -830,11 +853,25 @@ int launch_span(const Geom& g, const Batch& b, const Span& sp, cudaStream_t st, 
   if (kev) CU(cudaEventRecord(kev[2], st));
   DISPATCH_DT(g.f64, g.D, CU(launch_k(k_span_scatter<D, T>, dim3((unsigned)hx), 256, st, b, sp)));
   if (kev) CU(cudaEventRecord(kev[3], st));
-  CU(launch_k(k_span_classify, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
+  if (sp.route) {
+    CU(launch_k(k_span_classify<true>, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
+  } else {
+    CU(launch_k(k_span_classify<false>, dim3((unsigned)(g.sm_count * 4)), 256, st, b, sp));
+  }
   if (kev) CU(cudaEventRecord(kev[4], st));
   const int wpb = g.block_warps;
   const int64_t cx = (int64_t)g.sm_count * (64 / wpb);
-  DISPATCH_DPT(g.f64, g.D, g.pred, CU(launch_k(k_span_count<D, PRED, T>, dim3((unsigned)cx), wpb * 32, st, b, sp)));
+  DISPATCH_DPT(g.f64, g.D, g.pred, {
+    if constexpr (D <= 3) {
+      if (sp.route) {
+        CU(launch_k(k_span_count<D, PRED, T, true>, dim3((unsigned)cx), wpb * 32, st, b, sp));
+      } else {
+        CU(launch_k(k_span_count<D, PRED, T>, dim3((unsigned)cx), wpb * 32, st, b, sp));
+      }
+    } else {
+      CU(launch_k(k_span_count<D, PRED, T>, dim3((unsigned)cx), wpb * 32, st, b, sp));
+    }
+  });
   if (kev) CU(cudaEventRecord(kev[5], st));
   if (kev) CU(cudaEventRecord(kev[6], st));  // no per-batch compaction: see span_flush
   if (nk) *nk = 6;
@@ -874,16 +911,15 @@ bool train_now(rtod_handle* h) {
 
 // End of a streaming detection (ring jobs): the window's IDs and the batch
 // state into the mapped landing buffers (ensure_detect_out).
-int launch_detect_tail(rtod_handle* h, int64_t* nk) {
-  const unsigned ox = (unsigned)std::max<int64_t>(1, std::min<int64_t>((h->W + 255) / 256, h->sm_count));
-  CU(launch_k(k_run_out, dim3(ox), 256, h->stream, (const int64_t*)h->ids, h->ids_host_dev,
-              std::min(h->ids_host_cap, h->ids_cap), h->bs, h->bs_mirror_dev));
-  ++*nk;
-  return RTOD_OK;
+// A streaming detection of the staged pipeline: its launch sequence, ending
+// with the window's IDs and the batch state in the mapped landing buffers.
+int launch_ring(rtod_handle* h, const Batch& b, bool train, cudaEvent_t* kev, int64_t* nk) {
+  return launch_group(geom_of(h), b, true, train, h->stream, kev, nk, h->ids_host_dev,
+                      std::min(h->ids_host_cap, h->ids_cap), h->bs_mirror_dev);
 }
 
-// Whether a streaming detection runs the fused pipeline (one launch): the
-// default, except when per-stage times are asked for.
+// Whether a streaming detection runs the fused pipeline (one launch): when
+// configured, except when per-stage times are asked for.
 bool fused_ring(const rtod_handle* h, const cudaEvent_t* kev) {
   return h->cfg.pipeline == RTOD_PIPELINE_FUSED && !kev;
 }
@@ -896,11 +932,9 @@ int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev, 
     h->launches += nk;
     return r;
   }
-  // streaming detection: this window's IDs start at the beginning of the buffer
-  if (ingest) CU(cudaMemsetAsync(&h->bs->out_total, 0, sizeof(int64_t), h->stream));
   int r = sp ? launch_span(geom_of(h), b, *sp, h->stream, kev, &nk)
-             : launch_group(geom_of(h), b, ingest, train_now(h), h->stream, kev, &nk);
-  if (!r && ingest) r = launch_detect_tail(h, &nk);
+             : (ingest ? launch_ring(h, b, train_now(h), kev, &nk)
+                       : launch_group(geom_of(h), b, false, train_now(h), h->stream, kev, &nk));
   h->launches += nk;
   return r;
 }
@@ -924,10 +958,9 @@ int run_batch(rtod_handle* h, const Batch& b, bool ingest, const Span* sp = null
       r = launch_fused(geom_of(h), b, h->bar, true, h->ids_host_dev, std::min(h->ids_host_cap, h->ids_cap),
                        h->bs_mirror_dev, train, h->stream, &h->fused_grid, &nk);
     } else {
-      if (ingest) CU(cudaMemsetAsync(&h->bs->out_total, 0, sizeof(int64_t), h->stream));  // as in launch_batch
       r = sp ? launch_span(geom_of(h), b, *sp, h->stream, nullptr, &nk)
-             : launch_group(geom_of(h), b, ingest, train, h->stream, nullptr, &nk);
-      if (!r && ingest) r = launch_detect_tail(h, &nk);
+             : (ingest ? launch_ring(h, b, train, nullptr, &nk)
+                       : launch_group(geom_of(h), b, false, train, h->stream, nullptr, &nk));
     }
     cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (r) return r;
@@ -1221,6 +1254,8 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
   // a whole run as one graph: span engine, a device-resident or pinned host
   // stream (a graph's copy may not read pageable memory), no stage events
   const bool whole = span && (!host || pinned) && h->cfg.use_graph && !kev;
+  // the span engine's learned router trains once per pass when due
+  const bool train_pass = span && sfull.route && train_now(h);
   // Everything from the scratch resets to the last compaction.
   auto enqueue = [&]() -> int {
     // the pass starts here (a run graph: just before its launch)
@@ -1268,6 +1303,10 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
         if (kev) CU(cudaEventRecord(chunk_ev.back().second, h->stream));
       }
     }
+    if (train_pass) {
+      if ((rr = launch_train(geom_of(h), h->stream))) return rr;
+      h->launches += 2;
+    }
     // IDs to a page-locked caller buffer, the batch state to the mirror
     const unsigned ox = mapped_out ? (unsigned)h->sm_count * 2 : 1u;
     CU(launch_k(k_run_out, dim3(ox), 256, h->stream, (const int64_t*)dst, mapped_out, out_cap, h->bs,
@@ -1284,9 +1323,10 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
     std::memcpy(k + sizeof(void*), ints, sizeof ints);
     std::memcpy(k + sizeof(void*) + sizeof ints, &bfull, sizeof(Batch));
     std::memcpy(k + sizeof(void*) + sizeof ints + sizeof(Batch), &sfull, sizeof(Span));
-    if (!h->run_graph || key != h->run_graph_key) {
-      if (h->run_graph) cudaGraphExecDestroy(h->run_graph);
-      h->run_graph = nullptr;
+    cudaGraphExec_t& rg = h->run_graph[train_pass ? 1 : 0];
+    if (!rg || key != h->run_graph_key[train_pass ? 1 : 0]) {
+      if (rg) cudaGraphExecDestroy(rg);
+      rg = nullptr;
       const int64_t l0 = h->launches;
       cudaGraph_t g;
       CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -1294,16 +1334,16 @@ int run_stream(rtod_handle* h, const void* pts, int64_t slides, int64_t ids_cap,
       cudaError_t e = cudaStreamEndCapture(h->stream, &g);
       if (r) return r;
       if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-      e = cudaGraphInstantiate(&h->run_graph, g, 0);
+      e = cudaGraphInstantiate(&rg, g, 0);
       cudaGraphDestroy(g);
       if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
-      h->run_graph_key = key;
-      h->run_graph_kernels = h->launches - l0;
+      h->run_graph_key[train_pass ? 1 : 0] = key;
+      h->run_graph_kernels[train_pass ? 1 : 0] = h->launches - l0;
       h->launches = l0;
     }
     if (e_begin) CU(cudaEventRecord(e_begin, h->stream));
-    CU(cudaGraphLaunch(h->run_graph, h->stream));
-    h->launches += h->run_graph_kernels;
+    CU(cudaGraphLaunch(rg, h->stream));
+    h->launches += h->run_graph_kernels[train_pass ? 1 : 0];
     h->graph_replays++;
   } else {
     if ((r = enqueue())) return r;
@@ -1378,6 +1418,7 @@ struct Tuning {
   uint32_t max_sweep = 64;
   int engine = RTOD_ENGINE_WINDOW;
   int group = 0;
+  int route = 1;  // span engine with the router on: route its counts (0: plain counts)
 };
 
 struct TuneEntry {
@@ -1402,6 +1443,7 @@ int apply_tuning(rtod_handle* h, const Tuning& t) {
   h->max_sweep = t.max_sweep;
   h->engine = t.engine;
   h->group = t.group;
+  h->span_route = t.route;
   if (h->router) {
     CU(cudaMemcpy((char*)h->router + offsetof(RouterState, threshold), &t.threshold, sizeof(float),
                   cudaMemcpyHostToDevice));
@@ -1504,6 +1546,23 @@ int autotune(rtod_handle* h, const void* pts, int64_t slides_total) {
     t.batch = bt;
     if ((r = trial(t))) return r;
   }
+  if (h->cfg.router && best.engine == RTOD_ENGINE_SPAN) {
+    // the span engine's routing: off (plain counts), every eligible run in
+    // delta segments (threshold above 1), or the network's routing at a few
+    // thresholds (it has trained on the trial passes so far)
+    const Tuning start = best;
+    {
+      Tuning t = start;
+      t.route = 0;
+      if ((r = trial(t))) return r;
+    }
+    for (float th : {2.0f, 0.35f, 0.65f}) {
+      Tuning t = start;
+      t.route = 1;
+      t.threshold = th;
+      if ((r = trial(t))) return r;
+    }
+  }
   if (h->cfg.router && best.engine == RTOD_ENGINE_WINDOW && !best.group) {
     for (float th : {0.3f, 0.7f, 0.9f}) {
       Tuning t = best;
@@ -1586,9 +1645,9 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
     h->R2f = r2f;
   }
   set_grid(h, cfg->cells_per_r ? cfg->cells_per_r : 2);
-  // Engine of rtod_run: the span engine by default without the router.
-  h->engine = cfg->engine != RTOD_ENGINE_AUTO ? cfg->engine
-                                               : (!cfg->router ? RTOD_ENGINE_SPAN : RTOD_ENGINE_WINDOW);
+  // Engine of rtod_run: the span engine by default (with the router on, it
+  // routes the span engine's counts; the tuner may pick the window engine).
+  h->engine = cfg->engine != RTOD_ENGINE_AUTO ? cfg->engine : RTOD_ENGINE_SPAN;
   // Window-engine count: group counts where no cell is ever all-inlier and
   // a window holds enough points for long parts (auto_group), unless the
   // router (which routes single points) is on.
@@ -1843,7 +1902,7 @@ RTOD_API int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t*
     times->prepare_cell = elapsed(h->ev[0], kev[1]);   // ring update + occupancy
     times->build_bvh = elapsed(kev[1], kev[3]);       // scan + scatter
     times->detect_outlier = elapsed(kev[3], kev[5]);  // count + compact
-    times->copy_outlier_d2h = elapsed(kev[6], h->ev[7]);  // k_run_out
+    times->copy_outlier_d2h = elapsed(kev[6], h->ev[7]);  // after the compaction's delivery
     times->total = times->copy_new_points_h2d + elapsed(h->ev[0], h->ev[7]);
     times->undetermined_per_slide = (double)s.undet_total;
     times->slides = 1;
@@ -1995,6 +2054,17 @@ RTOD_API int rtod_router_info(rtod_handle* h, float* params, double info[6]) {
   return RTOD_OK;
 }
 
+RTOD_API int rtod_router_set_threshold(rtod_handle* h, float threshold) {
+  if (!h) return fail(RTOD_ERR_ARG, "handle is null");
+  if (!(threshold >= 0.0f) || !(threshold <= 2.0f)) return fail(RTOD_ERR_ARG, "threshold must be in [0, 2]");
+  CU(cudaSetDevice(h->device));
+  CU(cudaStreamSynchronize(h->stream));
+  CU(cudaMemcpy((char*)h->router + offsetof(RouterState, threshold), &threshold, sizeof(float),
+                cudaMemcpyHostToDevice));
+  h->threshold = threshold;
+  return RTOD_OK;
+}
+
 namespace {
 struct DevBuf {
   void* p = nullptr;
@@ -2089,7 +2159,7 @@ struct rtod_batch {
   int device = 0;
   int n = 0;
   int route = 0;
-  int fused = 1;  // RTOD_PIPELINE_FUSED: one cooperative launch per group and step
+  int fused = 0;  // RTOD_PIPELINE_FUSED: one cooperative launch per group and step
   cudaStream_t stream = nullptr;
   std::vector<rtod_handle*> hs;
   struct Group {
@@ -2159,7 +2229,6 @@ int batch_enqueue(rtod_batch* b, bool train, int64_t* nk_total) {
       r = launch_fused(g.geom, group_batch(g, b->router), g.bar, true, nullptr, 0, nullptr, train, b->stream,
                        &g.fused_grid, &nk);
     } else {
-      CU(cudaMemsetAsync(&g.bs->out_total, 0, sizeof(int64_t), b->stream));
       r = launch_group(g.geom, group_batch(g, b->router), true, train, b->stream, nullptr, &nk);
     }
     if (r) return r;

@@ -68,6 +68,8 @@ struct Span {
   uint32_t* bits;   // [chunk][words] outlier bits per window offset, row = slide % chunk
   int64_t words;    // ceil(W / 32)
   int64_t chunk;    // slides per bitset chunk (a multiple of the batch)
+  int32_t route;    // learned router on: groups routed to delta segments or independent counts
+  uint32_t gcap;    // entries of `groups`: groups from the front, delta segments from the back
 };
 
 // First global index of the span: the window of the batch's first job.
@@ -455,14 +457,15 @@ __device__ __forceinline__ bool span_group_safe(const Span& sp, const WinPre& wp
 // bitset row.
 // ---------------------------------------------------------------------------
 template <int D, int PRED, typename T>
-__device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp, uint32_t p, uint32_t nq,
-                                                 uint32_t bin, const WinPre& wp, bool pure) {
+__device__ __forceinline__ int span_count_group(const Batch& b, const Span& sp, uint32_t p, uint32_t nq,
+                                                uint32_t bin, const WinPre& wp, bool pure,
+                                                unsigned long long* made = nullptr) {
   const int j = wp.j;
   const Job& jb = b.jobs[j];
   const int64_t shift = (int64_t)j * sp.S;  // window offset = span offset - shift
   uint32_t* row = sp.bits + ((jb.ctr->lo - sp.S) / sp.S % sp.chunk) * sp.words;
   const GroupArgs ga{p, nq, bin, sp.n, sp.K, sp.R2f, sp.R, sp.R2, sp.Wp, pure && D <= 3, &b.bs->pair_tests};
-  const int nout = count_group<D, PRED, T>(
+  const int nout = count_group_ex<D, PRED, T>(
       static_cast<const T*>(sp.s_x), ga,
       [&](uint32_t sb, uint32_t& rs, uint32_t& len) {
         const uint32_t b0 = sp.bin_start[sb], b1 = sp.bin_start[sb + 1];
@@ -475,8 +478,278 @@ __device__ __forceinline__ void span_count_group(const Batch& b, const Span& sp,
       [&](uint32_t pos) {
         const int64_t w2 = (int64_t)sp.s_off[pos] - shift;
         atomicOr(&row[w2 >> 5], 1u << (w2 & 31));
-      });
+      },
+      [&](uint32_t i) { return p + i; }, [](uint32_t, int, int) {}, made);
   if ((threadIdx.x & 31) == 0 && nout) atomicAdd(&jb.ctr->n_out, nout);
+  return nout;
+}
+
+// ---------------------------------------------------------------------------
+// Learned routing of the span engine's exact counts (rtod_config.router).
+//
+// Consecutive windows of a batch share all but two slide blocks, so a
+// point's neighbour count in window j equals its count in window j-1 plus
+// its neighbours in the block that window j adds, minus those in the block
+// it drops. A "delta segment" is a run of up to SEG_LEN consecutive windows
+// of one bin that all need counting, taken by one warp in window order: the
+// first window is counted in full (count_group), and every later window
+// only tests the points both windows share against the two changed blocks
+// of the stencil (about 2/(W/S) of the candidates), keeping for each point
+// bounds [lo, hi] of its count (exact after a full sweep; lo > K only after
+// an early exit). A point whose bounds leave K inside after the update, and
+// the window's new points, are counted in full again. The result is exact
+// either way. A delta segment pays off when the bin's points would test many
+// candidates (large stencils, outliers); an independent early-exit count
+// when they test few, since it runs in parallel instead of window after
+// window. The router's network predicts, from the cell occupancy of the
+// run's first window (cheap to read at classification), whether an
+// independent count is the cheaper (bucket 3), a label the count kernel
+// derives from what it has just counted (the stencil's candidates and the
+// outliers found, route_label); k_span_classify routes predicted bucket-3
+// runs to independent counts and the rest to delta segments. The network is
+// trained on the GPU on samples of those counts (k_train); the autotuner
+// also times routing off and the threshold's extremes.
+// ---------------------------------------------------------------------------
+constexpr int SEG_LEN = 8;                // windows per delta segment at most
+constexpr int SEG_CAP = 64;               // points of the bin in any window of a delta segment at most
+constexpr int SEG_RING = 2 * SEG_CAP;     // per-warp bounds, indexed by position mod SEG_RING
+constexpr uint32_t SAMPLE_THIN = 8;       // groups and segment windows sampled for training: one in 8
+
+// Router features of (window j, bin): f0 = log2(1 + points of the bin) / 8,
+// f1 = log2(1 + points of the bins b-1, b, b+1: the neighbouring cells along
+// the last hashed dimension) / 8, f2 = points of the bin / (K + 1), at most 2.
+__device__ __forceinline__ void span_features(const Span& sp, const WinPre& wp, uint32_t bin, uint32_t wc, float* f) {
+  uint32_t row = 0;
+#pragma unroll
+  for (int d = -1; d <= 1; ++d) {
+    const uint32_t nb = (bin + (uint32_t)d) & NB_MASK;
+    if (sp.bin_start[nb + 1] > sp.bin_start[nb]) row += wp.count(nb);
+  }
+  f[0] = log2f(1.0f + (float)wc) * 0.125f;
+  f[1] = log2f(1.0f + (float)row) * 0.125f;
+  f[2] = fminf(2.0f, (float)wc / (float)(sp.K + 1));
+}
+
+// Candidates of (window j, bin) over its whole stencil (one warp; slots <= 32).
+template <int H>
+__device__ __forceinline__ uint32_t span_stencil_total(const Span& sp, uint32_t bin, uint32_t j) {
+  const int lane = threadIdx.x & 31;
+  const int w = 2 * sp.n + 1;
+  const int slots = H == 1 ? w : (H == 2 ? w * w : w * w * w);
+  uint32_t c = 0;
+  if (lane < slots) {
+    int d[3] = {0, 0, 0};
+    const uint32_t sb = (bin + (uint32_t)slot_cell<H>(lane, sp.n, d)) & NB_MASK;
+    if (sp.bin_start[sb + 1] > sp.bin_start[sb]) {
+      const uint32_t* r = sp.pre + (int64_t)sb * sp.ts + j;
+      c = r[sp.wblk] - r[0];
+    }
+  }
+  return __reduce_add_sync(0xffffffffu, c);
+}
+
+// Label of a counted (window, bin) of wc points, nout of them outliers, C
+// stencil candidates: 3 when an independent early-exit count costs less
+// than a delta step, else 0. Costs in distance tests plus a fixed cost per
+// count for running it: independent, `made` tests when it ran that way
+// (else: outliers sweep all C candidates, inliers about half of them) plus
+// 512; a delta step, `made` tests when it ran that way (else: the shared
+// points against the two changed blocks, 2C/(W/S) each, and the new points,
+// wc/(W/S), in full) plus 2048, as it runs window after window in one warp
+// instead of in parallel. The fixed costs place the crossover where the
+// measurements put it: the 1-d streams' small bins cheaper independently,
+// the 3-d sensor-like stream's large stencils cheaper in delta segments.
+__device__ __forceinline__ int route_label(const Span& sp, uint32_t wc, int nout, uint32_t C, bool ran_indep,
+                                           unsigned long long made) {
+  const float f = (float)C, blk = (float)sp.wblk, n = (float)wc, o = (float)nout;
+  const float ind = (ran_indep ? (float)made : o * f + (n - o) * 0.5f * f) + 512.0f;
+  const float del = (ran_indep ? n * 2.0f * f / blk + n / blk * f : (float)made) + 2048.0f;
+  return ind <= del ? 3 : 0;
+}
+
+// One training sample (lane 0 of the warp) into the block's buffer.
+__device__ __forceinline__ void span_sample(SampleBuf& sb, const float* f, int label, bool routed_early) {
+  if ((label == 3) != routed_early) atomicAdd(&sb.misrouted, 1u);
+  const uint32_t k = atomicAdd(&sb.n, 1u);
+  if (k >= BLOCK_SAMPLES) return;
+  sb.s[k][0] = f[0];
+  sb.s[k][1] = f[1];
+  sb.s[k][2] = f[2];
+  sb.s[k][3] = (float)label;
+}
+
+__device__ __forceinline__ bool span_sampled(uint32_t bin, uint32_t j) {
+  return ((bin * 2654435761u + j * 40503u) >> 16) % SAMPLE_THIN == 0;
+}
+
+struct SegWarp {
+  int32_t lo[SEG_RING];
+  int32_t hi[SEG_RING];
+  uint32_t redo[SEG_CAP];
+};
+
+// Counts a delta segment: windows j0 .. j0 + len - 1 of bin `bin`, every one
+// holding 1..SEG_CAP points of the bin. One warp; sw is its shared state.
+template <int D, int PRED, typename T>
+__device__ void span_count_segment(const Batch& b, const Span& sp, uint32_t bin, uint32_t j0, uint32_t len,
+                                   bool pure, SegWarp& sw, SampleBuf& sbuf) {
+  constexpr int H = Hashed<D>::value;
+  const int lane = threadIdx.x & 31;
+  const T* sx = static_cast<const T*>(sp.s_x);
+  const uint32_t B0 = sp.bin_start[bin];
+  const uint32_t* prow = sp.pre + (int64_t)bin * sp.ts;
+  // this lane's stencil slot (at most 32 slots: checked by the host)
+  const int w = 2 * sp.n + 1;
+  const int slots = H == 1 ? w : (H == 2 ? w * w : w * w * w);
+  uint32_t sbase = 0;
+  const uint32_t* srow = nullptr;
+  if (lane < slots) {
+    int d[3] = {0, 0, 0};
+    const uint32_t sb = (bin + (uint32_t)slot_cell<H>(lane, sp.n, d)) & NB_MASK;
+    if (sp.bin_start[sb + 1] > sp.bin_start[sb]) {
+      sbase = sp.bin_start[sb];
+      srow = sp.pre + (int64_t)sb * sp.ts;
+    }
+  }
+  unsigned long long tests = 0;
+  uint32_t e_prev = 0;
+  for (uint32_t t = 0; t < len; ++t) {
+    const uint32_t j = j0 + t;
+    const uint32_t s = B0 + prow[j], e = B0 + prow[j + sp.wblk];
+    const Job& jb = b.jobs[j];
+    uint32_t* row = sp.bits + ((jb.ctr->lo - sp.S) / sp.S % sp.chunk) * sp.words;
+    const int64_t shift = (int64_t)j * sp.S;
+    const WinPre wp{sp.pre, sp.ts, (int)j, sp.wblk};
+    auto mark = [&](uint32_t pos) {
+      const int64_t w2 = (int64_t)sp.s_off[pos] - shift;
+      atomicOr(&row[w2 >> 5], 1u << (w2 & 31));
+    };
+    auto rec = [&](uint32_t pos, int lo, int hi) {
+      sw.lo[pos & (SEG_RING - 1)] = lo;
+      sw.hi[pos & (SEG_RING - 1)] = hi;
+    };
+    auto range = [&](uint32_t sb, uint32_t& rs, uint32_t& l) {
+      const uint32_t b0 = sp.bin_start[sb], b1 = sp.bin_start[sb + 1];
+      if (b1 > b0) {
+        const uint32_t* r = wp.pre + (int64_t)sb * wp.ts + wp.j;
+        rs = b0 + r[0];
+        l = r[wp.wblk] - r[0];
+      }
+    };
+    int nout = 0;
+    uint32_t nredo = 0, first_new = s;
+    unsigned long long made = 0;  // distance tests of this window
+    if (t > 0) {
+      // Points of both windows, positions [s, e_prev): their counts change by
+      // their neighbours in block j - 1 + W/S (added) minus those in block
+      // j - 1 (dropped). The lane's slot contributes its points of both blocks
+      // to one virtual list of signed candidates.
+      const uint32_t told = j - 1, tnew = j - 1 + (uint32_t)sp.wblk;
+      uint32_t ds = 0, dn = 0, as = 0, an = 0;
+      if (srow) {
+        ds = sbase + srow[told];
+        dn = srow[told + 1] - srow[told];
+        as = sbase + srow[tnew];
+        an = srow[tnew + 1] - srow[tnew];
+      }
+      const uint32_t mine = dn + an;
+      uint32_t inc = mine;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
+      }
+      const uint32_t off = inc - mine, nd = __shfl_sync(0xffffffffu, inc, 31);
+      const uint32_t nc = e_prev - s;
+      T x0[D], x1[D];
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        x0[d] = lane < (int)nc ? sx[(int64_t)d * sp.Wp + s + lane] : T(0);
+        x1[d] = lane + 32 < (int)nc ? sx[(int64_t)d * sp.Wp + s + 32 + lane] : T(0);
+      }
+      int acc0 = 0, acc1 = 0;
+      for (uint32_t c0 = 0; c0 < nd; c0 += 32) {
+        const uint32_t v = c0 + lane;
+        int src = 0;  // lane holding v: the last lane whose offset is <= v
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const int cand = src + step;
+          if (__shfl_sync(0xffffffffu, off, cand & 31) <= v) src = cand;
+        }
+        const uint32_t o_off = __shfl_sync(0xffffffffu, off, src), o_ds = __shfl_sync(0xffffffffu, ds, src),
+                       o_dn = __shfl_sync(0xffffffffu, dn, src), o_as = __shfl_sync(0xffffffffu, as, src);
+        const uint32_t k = v - o_off;
+        const bool valid = v < nd;
+        const uint32_t pos = k < o_dn ? o_ds + k : o_as + (k - o_dn);
+        const int sg = k < o_dn ? -1 : 1;
+        T cx[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) cx[d] = valid ? sx[(int64_t)d * sp.Wp + pos] : T(0);
+        const uint32_t m = min(32u, nd - c0);
+        for (uint32_t c = 0; c < m; ++c) {
+          T y[D];
+#pragma unroll
+          for (int d = 0; d < D; ++d) y[d] = __shfl_sync(0xffffffffu, cx[d], c);
+          const int g = __shfl_sync(0xffffffffu, sg, c);
+          if (lane < (int)nc && is_nbr<D, PRED, T>(x0, y, sp.R2f, sp.R, sp.R2)) acc0 += g;
+          if (lane + 32 < (int)nc && is_nbr<D, PRED, T>(x1, y, sp.R2f, sp.R, sp.R2)) acc1 += g;
+        }
+      }
+      tests += (unsigned long long)nc * nd;
+      made += (unsigned long long)nc * nd;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const uint32_t idx = (uint32_t)lane + 32u * h;
+        const uint32_t pos = s + idx;
+        bool out = false, redo = false;
+        if (idx < nc) {
+          const int sl = pos & (SEG_RING - 1);
+          const int acc = h ? acc1 : acc0;
+          const int lo = sw.lo[sl] + acc;
+          const int hi = sw.hi[sl] >= CNT_INF ? CNT_INF : sw.hi[sl] + acc;
+          sw.lo[sl] = lo;
+          sw.hi[sl] = hi;
+          if (lo <= sp.K) {
+            if (hi <= sp.K) {
+              out = true;
+              mark(pos);
+            } else {
+              redo = true;
+            }
+          }
+        }
+        nout += __popc(__ballot_sync(0xffffffffu, out));
+        const unsigned rm = __ballot_sync(0xffffffffu, redo);
+        if (redo) sw.redo[nredo + __popc(rm & lanemask_lt())] = pos;
+        nredo += __popc(rm);
+      }
+      __syncwarp();
+      first_new = e_prev;
+    }
+    // Full counts: the window's new points [first_new, e) and the points
+    // whose bounds still hold K.
+    const uint32_t nnew = e - first_new;
+    if (nnew + nredo) {
+      const GroupArgs ga{first_new, nnew + nredo, bin, sp.n, sp.K, sp.R2f, sp.R, sp.R2, sp.Wp, pure && D <= 3,
+                         &b.bs->pair_tests};
+      unsigned long long m2 = 0;
+      nout += count_group_ex<D, PRED, T>(
+          sx, ga, range, mark, [&](uint32_t i) { return i < nnew ? first_new + i : sw.redo[i - nnew]; }, rec, &m2);
+      made += m2;
+    }
+    __syncwarp();
+    if (lane == 0 && nout) atomicAdd(&jb.ctr->n_out, nout);
+    if (span_sampled(bin, j)) {
+      const uint32_t C = span_stencil_total<H>(sp, bin, j);
+      if (lane == 0) {
+        float f[MLP_IN];
+        span_features(sp, wp, bin, e - s, f);
+        span_sample(sbuf, f, route_label(sp, e - s, nout, C, false, made), false);
+      }
+    }
+    e_prev = e;
+  }
+  if (lane == 0 && tests) atomicAdd(&b.bs->pair_tests, tests);
 }
 
 // Clears the per-bin state of the span's bins in use (all blocks of the
@@ -503,9 +776,15 @@ __device__ __forceinline__ void span_clear_bins(const SpanCtr* c) {
 // list, one per window present in the warp for its count of listed points.
 // Pairs run bin-major (consecutive windows of a bin together), so the list
 // holds a bin's windows side by side and neighbouring count warps read
-// mostly the same candidates.
+// mostly the same candidates. With ROUTE (the learned router), runs of up to
+// SEG_LEN consecutive windows of one bin, each with at most SEG_CAP points of
+// the bin, are routed by the network (features of the run's first window):
+// predicted mostly-inlier runs are listed window by window as above, the
+// others as one delta segment each (from the back of the list: first
+// position, windows, bin, first window).
 // ---------------------------------------------------------------------------
-static __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
+template <bool ROUTE>
+__global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) {
   pdl_trigger();
   pdl_wait();
   const int lane = threadIdx.x & 31;
@@ -548,44 +827,116 @@ static __global__ void __launch_bounds__(256) k_span_classify(Batch b, Span sp) 
         start = sp.bin_start[bin] + a;
       }
     }
-    const unsigned nmask = __ballot_sync(0xffffffffu, need);
-    uint32_t gbase = 0;
-    if (lane == 0 && nmask) gbase = atomicAdd(&sp.sc->n_groups, (uint32_t)__popc(nmask));
-    gbase = __shfl_sync(0xffffffffu, gbase, 0);
     const unsigned peers = __match_any_sync(0xffffffffu, need ? j : -1);
     if (need) {
-      sp.groups[gbase + __popc(nmask & lanemask_lt())] = make_uint4(start, wc, bin, (uint32_t)j);
       const uint32_t pts = __reduce_add_sync(peers, wc);
       if (lane == __ffs(peers) - 1) atomicAdd(&b.jobs[j].ctr->n_undet, (int)pts);
     }
+    bool indep = need;  // listed as an independent group
+    if constexpr (ROUTE) {
+      // Runs of eligible windows of one bin inside the warp's 32 pairs, cut
+      // into segments of SEG_LEN windows; each segment's first lane routes it.
+      const bool el = need && wc <= (uint32_t)SEG_CAP;
+      const uint32_t pbin = __shfl_up_sync(0xffffffffu, bin, 1);
+      const bool pel = __shfl_up_sync(0xffffffffu, el ? 1 : 0, 1) != 0;
+      const unsigned cont = __ballot_sync(0xffffffffu, lane > 0 && el && pel && pbin == bin);
+      const unsigned elm = __ballot_sync(0xffffffffu, el);
+      const unsigned le = lane == 31 ? 0xffffffffu : ((2u << lane) - 1u);  // lanes <= this one
+      const unsigned heads = elm & ~cont;
+      const int rhead = el ? 31 - __clz(heads & le) : lane;
+      const bool shead = el && ((lane - rhead) % SEG_LEN) == 0;
+      const unsigned sheads = __ballot_sync(0xffffffffu, shead);
+      const int myhead = el ? 31 - __clz(sheads & le) : lane;
+      bool delta = false;
+      uint32_t slen = 0;
+      if (shead) {
+        float f[MLP_IN];
+        span_features(sp, WinPre{sp.pre, sp.ts, j, sp.wblk}, bin, wc, f);
+        delta = !route_early(b.router, f);
+        const unsigned stop = (~cont | sheads) & ~le;  // lanes after this one that start a run or segment
+        slen = (uint32_t)((stop ? __ffs(stop) - 1 : 32) - lane);
+      }
+      const bool my_delta = __shfl_sync(0xffffffffu, delta ? 1 : 0, myhead & 31) != 0;
+      if (el && my_delta) indep = false;
+      const unsigned dheads = __ballot_sync(0xffffffffu, shead && delta);
+      uint32_t sbase = 0;
+      if (lane == 0 && dheads) sbase = atomicAdd(&sp.sc->n_segs, (uint32_t)__popc(dheads));
+      sbase = __shfl_sync(0xffffffffu, sbase, 0);
+      if (shead && delta)
+        sp.groups[sp.gcap - 1 - (sbase + __popc(dheads & lanemask_lt()))] = make_uint4(start, slen, bin, (uint32_t)j);
+      const unsigned em = __ballot_sync(0xffffffffu, el);
+      const unsigned dm = __ballot_sync(0xffffffffu, el && my_delta);
+      if (lane == 0 && (em || dm)) {
+        atomicAdd(&b.router->routed_early, (unsigned long long)__popc(em & ~dm));
+        atomicAdd(&b.router->routed_sweep, (unsigned long long)__popc(dm));
+      }
+    }
+    const unsigned nmask = __ballot_sync(0xffffffffu, indep);
+    uint32_t gbase = 0;
+    if (lane == 0 && nmask) gbase = atomicAdd(&sp.sc->n_groups, (uint32_t)__popc(nmask));
+    gbase = __shfl_sync(0xffffffffu, gbase, 0);
+    if (indep) sp.groups[gbase + __popc(nmask & lanemask_lt())] = make_uint4(start, wc, bin, (uint32_t)j);
   }
 }
 
 // ---------------------------------------------------------------------------
-// k_span_count: one warp per listed group of the batch, groups taken in list
-// order by ticket (one atomic per group), so that a warp that drew short
-// groups takes more of them and no warp idles while long groups remain.
-// Outliers set their bit in the slide's bitset row. Then the blocks clear the
-// per-bin state, and the block that finishes last ends the batch (records,
-// window advance, counters).
+// k_span_count: one warp per listed group of the batch, warps striding over
+// the list (measured against groups taken by ticket, one atomic per group or
+// only for the last round: the static stride was as fast on the 3-d
+// sensor-like stream and 20-40% faster on the 1-d streams, whose groups are
+// too short to pay for the atomics). Outliers set their bit in the slide's
+// bitset row. Then the blocks clear the per-bin state, and the block that
+// finishes last ends the batch (records, window advance, counters).
 // ---------------------------------------------------------------------------
-template <int D, int PRED, typename T>
+// With ROUTE, the warps first take the delta segments by ticket (from the
+// back of the list), and every sampled group or segment window leaves a
+// training sample for the router.
+template <int D, int PRED, typename T, bool ROUTE = false>
 __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
   __shared__ int s_last;
+  __shared__ SegWarp s_seg[ROUTE ? 8 : 1];
+  __shared__ SampleBuf s_samples;
   pdl_trigger();
   pdl_wait();
   const int lane = threadIdx.x & 31;
   const uint32_t ng = sp.sc->n_groups;
   const bool pure = sp.sc->pure;
-  while (true) {
-    uint32_t k = 0;
-    if (lane == 0) k = atomicAdd(&sp.sc->count_ticket, 1u);
-    k = __shfl_sync(0xffffffffu, k, 0);
-    if (k >= ng) break;
-    const uint4 g = sp.groups[k];
-    const int j = (int)g.w;
-    span_count_group<D, PRED, T>(b, sp, g.x, g.y, g.z, WinPre{sp.pre, sp.ts, j, sp.wblk}, pure);
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if constexpr (ROUTE) {
+    if (threadIdx.x == 0) {
+      s_samples.n = 0;
+      s_samples.misrouted = 0;
+    }
+    __syncthreads();
+    const uint32_t ns = sp.sc->n_segs;
+    while (true) {
+      uint32_t k = 0;
+      if (lane == 0) k = atomicAdd(&sp.sc->seg_ticket, 1u);
+      k = __shfl_sync(0xffffffffu, k, 0);
+      if (k >= ns) break;
+      const uint4 g = sp.groups[sp.gcap - 1 - k];
+      span_count_segment<D, PRED, T>(b, sp, g.z, g.w, g.y, pure, s_seg[(threadIdx.x >> 5) & 7], s_samples);
+    }
   }
+  auto one = [&](uint32_t k) {
+    const uint4 g = sp.groups[k];
+    unsigned long long made = 0;
+    const int nout = span_count_group<D, PRED, T>(b, sp, g.x, g.y, g.z, WinPre{sp.pre, sp.ts, (int)g.w, sp.wblk},
+                                                  pure, ROUTE ? &made : nullptr);
+    if constexpr (ROUTE) {
+      if (span_sampled(g.z, g.w)) {
+        const uint32_t C = span_stencil_total<Hashed<D>::value>(sp, g.z, g.w);
+        if (lane == 0) {
+          float f[MLP_IN];
+          span_features(sp, WinPre{sp.pre, sp.ts, (int)g.w, sp.wblk}, g.z, g.y, f);
+          span_sample(s_samples, f, route_label(sp, g.y, nout, C, true, made), true);
+        }
+      }
+    }
+  };
+  for (uint32_t k = warp; k < ng; k += nw) one(k);
+  if constexpr (ROUTE) flush_samples(s_samples, b.router);
   // The per-bin state is no longer read in this batch: clear it, then the
   // block that finishes last ends the batch.
   span_clear_bins(sp.sc);

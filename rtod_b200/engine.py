@@ -72,7 +72,7 @@ class Detector:
                  pred: str = "fp32_le", router: bool = False, tuner: bool = False,
                  cells_per_r: int = 0, block_warps: int = 0, use_graph: bool = True,
                  batch: int = 0, device: int = 0, engine: str = "auto", coord: str = "f32",
-                 count: str = "auto", pipeline: str = "fused"):
+                 count: str = "auto", pipeline: str = "staged"):
         cfg = Config()
         check(lib().rtod_config_init(ctypes.byref(cfg)))
         cfg.window, cfg.slide, cfg.R, cfg.K, cfg.dim, cfg.opt = window, slide, R, K, dim, opt
@@ -200,6 +200,10 @@ class Detector:
                 "routed_early": int(info[2]), "routed_sweep": int(info[3]),
                 "misrouted": int(info[4]), "threshold": float(info[5])}
 
+    def set_router_threshold(self, threshold: float) -> None:
+        """Routing threshold of the learned router (see rtod_router_set_threshold)."""
+        check(lib().rtod_router_set_threshold(self._h, float(threshold)))
+
     @property
     def slides_done(self) -> int:
         return int(lib().rtod_slides_done(self._h))
@@ -242,7 +246,7 @@ class BatchDetector:
             c.dim, c.opt = st.get("dim", 1), st.get("opt", 2)
             c.pred = _native.PRED[st.get("pred", "fp32_le")]
             c.count = _native.COUNT[st.get("count", "auto")]
-            c.pipeline = _native.PIPELINE[st.get("pipeline", "fused")]
+            c.pipeline = _native.PIPELINE[st.get("pipeline", "staged")]
             c.router, c.device = int(router), device
         self.streams = [dict(s) for s in streams]
         self._b = ctypes.c_void_p()

@@ -57,7 +57,7 @@ def test_push_detect_matches_golden(rtod, path, pipeline, graph):
 
 @pytest.mark.parametrize("kw", [dict(), dict(router=True), dict(count="group"), dict(cells_per_r=4),
                                 dict(pred="f64_lt"), dict(router=True, use_graph=False),
-                                dict(pipeline="staged")])
+                                dict(pipeline="fused"), dict(pipeline="fused", router=True)])
 def test_push_detect_stock_like_stream(rtod, oracle_mod, kw):
     """The stock-like stream (W=100k, S=5k) slide by slide, 40 slides, against
     the oracle; every seventh detection asks for stage times (the staged
