@@ -350,6 +350,7 @@ struct rtod_handle {
   float threshold = 0.5f;
   uint32_t max_sweep = 64;
   int span_route = 1;  // with the router on: the span engine routes its counts (the tuner may turn it off)
+  bool tuning_pass = false;  // the tuner's timed passes train nothing (it trains between them)
 };
 
 namespace {
@@ -778,7 +779,7 @@ int launch_group(const Geom& g, const Batch& b, bool ingest, bool train, cudaStr
                  CU(launch_k(k_count<D, PRED, false, T>, dim3((unsigned)cx, gy), wpb * 32, st, b)));
   }
   if (kev) CU(cudaEventRecord(kev[4], st));
-  if (W <= COMPACT1_MAX) {  // one block per window (delivers a streaming detection's IDs itself)
+  if (ingest && W <= COMPACT1_MAX) {  // ring jobs: one block per window, delivering a detection's IDs itself
     CU(launch_k(k_compact_one, dim3(gy), 1024, st, b, ids_host, ids_host_cap, mirror));
   } else {
     CU(launch_k(k_compact, dim3((unsigned)((W + CMP_TILE - 1) / CMP_TILE), gy), 256, st, b));
@@ -904,7 +905,7 @@ constexpr int kTrainEvery = 16;  // batches between two router training launches
 constexpr int kTrainWarm = 32;   // the first batches train after every batch
 
 bool train_now(rtod_handle* h) {
-  if (!h->cfg.router) return false;
+  if (!h->cfg.router || h->tuning_pass) return false;
   const int64_t n = h->batches++;
   return n < kTrainWarm || n % kTrainEvery == 0;
 }
@@ -1464,12 +1465,18 @@ int time_pass(rtod_handle* h, const void* dev_pts, int64_t slides, float* ms) {
     if (r) return r;
     BatchState s{};
     std::vector<int32_t> nout, nund;
+    h->tuning_pass = true;  // the router trains between timed passes, not inside them
     CU(cudaEventRecord(a, h->stream));
     r = run_stream(h, dev_pts, slides, slides * h->W, nullptr, nullptr, nullptr, nullptr, &s, &nout, &nund);
+    h->tuning_pass = false;
     if (r) return r;
     CU(cudaEventRecord(b, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     best = std::min(best, elapsed(a, b));
+  }
+  if (h->cfg.router) {  // on the samples the passes left
+    if (int r = launch_train(geom_of(h), h->stream)) return r;
+    CU(cudaStreamSynchronize(h->stream));
   }
   *ms = best;
   return RTOD_OK;

@@ -512,6 +512,9 @@ __device__ __forceinline__ int span_count_group(const Batch& b, const Span& sp, 
 // ---------------------------------------------------------------------------
 constexpr int SEG_LEN = 8;                // windows per delta segment at most
 constexpr int SEG_CAP = 64;               // points of the bin in any window of a delta segment at most
+                                          // (measured: 128 lets dense bins in, whose inliers exit
+                                          // early, and the 3-d sensor-like gain fell from 27% to 5%)
+constexpr int SEG_PPL = SEG_CAP / 32;     // shared points per lane in a delta step
 constexpr int SEG_RING = 2 * SEG_CAP;     // per-warp bounds, indexed by position mod SEG_RING
 constexpr uint32_t SAMPLE_THIN = 8;       // groups and segment windows sampled for training: one in 8
 
@@ -550,20 +553,20 @@ __device__ __forceinline__ uint32_t span_stencil_total(const Span& sp, uint32_t 
 
 // Label of a counted (window, bin) of wc points, nout of them outliers, C
 // stencil candidates: 3 when an independent early-exit count costs less
-// than a delta step, else 0. Costs in distance tests plus a fixed cost per
-// count for running it: independent, `made` tests when it ran that way
-// (else: outliers sweep all C candidates, inliers about half of them) plus
-// 512; a delta step, `made` tests when it ran that way (else: the shared
-// points against the two changed blocks, 2C/(W/S) each, and the new points,
-// wc/(W/S), in full) plus 2048, as it runs window after window in one warp
-// instead of in parallel. The fixed costs place the crossover where the
-// measurements put it: the 1-d streams' small bins cheaper independently,
-// the 3-d sensor-like stream's large stencils cheaper in delta segments.
+// than a delta step, else 0: the work of each in distance tests plus a
+// fixed cost per count. Independent: `made` tests when it ran that way (else
+// outliers sweep all C candidates, inliers about half of them); a delta
+// step: `made` tests when it ran that way (else the shared points against
+// the two changed blocks, 2C/(W/S) each, and the new points, wc/(W/S), in
+// full). The label measures work only; where the count stage is bound by
+// latency rather than work (short 1-d candidate lists, whose delta segments
+// lengthen the chain of dependent steps), the autotuner, which times routing
+// off as well, turns routing off.
 __device__ __forceinline__ int route_label(const Span& sp, uint32_t wc, int nout, uint32_t C, bool ran_indep,
                                            unsigned long long made) {
   const float f = (float)C, blk = (float)sp.wblk, n = (float)wc, o = (float)nout;
-  const float ind = (ran_indep ? (float)made : o * f + (n - o) * 0.5f * f) + 512.0f;
-  const float del = (ran_indep ? n * 2.0f * f / blk + n / blk * f : (float)made) + 2048.0f;
+  const float ind = (ran_indep ? (float)made : o * f + (n - o) * 0.5f * f) + 256.0f;
+  const float del = (ran_indep ? n * 2.0f * f / blk + n / blk * f : (float)made) + 256.0f;
   return ind <= del ? 3 : 0;
 }
 
@@ -661,13 +664,15 @@ __device__ void span_count_segment(const Batch& b, const Span& sp, uint32_t bin,
       }
       const uint32_t off = inc - mine, nd = __shfl_sync(0xffffffffu, inc, 31);
       const uint32_t nc = e_prev - s;
-      T x0[D], x1[D];
+      T xq[SEG_PPL][D];
 #pragma unroll
-      for (int d = 0; d < D; ++d) {
-        x0[d] = lane < (int)nc ? sx[(int64_t)d * sp.Wp + s + lane] : T(0);
-        x1[d] = lane + 32 < (int)nc ? sx[(int64_t)d * sp.Wp + s + 32 + lane] : T(0);
-      }
-      int acc0 = 0, acc1 = 0;
+      for (int h = 0; h < SEG_PPL; ++h)
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+          xq[h][d] = lane + 32 * h < (int)nc ? sx[(int64_t)d * sp.Wp + s + 32 * h + lane] : T(0);
+      int acc[SEG_PPL];
+#pragma unroll
+      for (int h = 0; h < SEG_PPL; ++h) acc[h] = 0;
       for (uint32_t c0 = 0; c0 < nd; c0 += 32) {
         const uint32_t v = c0 + lane;
         int src = 0;  // lane holding v: the last lane whose offset is <= v
@@ -691,22 +696,22 @@ __device__ void span_count_segment(const Batch& b, const Span& sp, uint32_t bin,
 #pragma unroll
           for (int d = 0; d < D; ++d) y[d] = __shfl_sync(0xffffffffu, cx[d], c);
           const int g = __shfl_sync(0xffffffffu, sg, c);
-          if (lane < (int)nc && is_nbr<D, PRED, T>(x0, y, sp.R2f, sp.R, sp.R2)) acc0 += g;
-          if (lane + 32 < (int)nc && is_nbr<D, PRED, T>(x1, y, sp.R2f, sp.R, sp.R2)) acc1 += g;
+#pragma unroll
+          for (int h = 0; h < SEG_PPL; ++h)
+            if (lane + 32 * h < (int)nc && is_nbr<D, PRED, T>(xq[h], y, sp.R2f, sp.R, sp.R2)) acc[h] += g;
         }
       }
       tests += (unsigned long long)nc * nd;
       made += (unsigned long long)nc * nd;
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      for (int h = 0; h < SEG_PPL; ++h) {
         const uint32_t idx = (uint32_t)lane + 32u * h;
         const uint32_t pos = s + idx;
         bool out = false, redo = false;
         if (idx < nc) {
           const int sl = pos & (SEG_RING - 1);
-          const int acc = h ? acc1 : acc0;
-          const int lo = sw.lo[sl] + acc;
-          const int hi = sw.hi[sl] >= CNT_INF ? CNT_INF : sw.hi[sl] + acc;
+          const int lo = sw.lo[sl] + acc[h];
+          const int hi = sw.hi[sl] >= CNT_INF ? CNT_INF : sw.hi[sl] + acc[h];
           sw.lo[sl] = lo;
           sw.hi[sl] = hi;
           if (lo <= sp.K) {

@@ -94,20 +94,24 @@ def test_delta_segments_double_storage(rtod):
             np.testing.assert_array_equal(r.ids, ids, err_msg=path)
 
 
-def test_router_trains_on_span_counts(rtod):
+def test_router_trains_on_span_counts(rtod, oracle_mod):
     """The span engine's counts train the network: after some passes it has
-    taken Adam steps, its loss is finite, and on the Gaussian-mixture stream
-    (K = 30, most counted bins hold mostly outliers) it routes runs to delta
-    segments."""
+    taken Adam steps with a finite loss, and on the 3-d sensor-like stream
+    (every point counted against large stencils, where delta segments cost
+    less) it routes runs to delta segments; results stay exact throughout."""
     from rtod_b200 import datagen
-    w = datagen.gaussian_like(30)
-    with rtod.Detector(w.window, w.slide, w.R, w.K, engine="span", router=True, cells_per_r=2) as det:
-        for _ in range(12):
+    w = datagen.sensor_like()
+    off, ids = expect(oracle_mod, w, slides=300)
+    pts = w.points[:w.window + 300 * w.slide]
+    with rtod.Detector(w.window, w.slide, w.R, w.K, dim=3, engine="span", router=True, cells_per_r=1) as det:
+        for _ in range(30):
             det.reset()
-            det.run(w.points)
+            r = det.run(pts)
+            np.testing.assert_array_equal(r.offsets, off)
+            np.testing.assert_array_equal(r.ids, ids)
         info = det.router_info()
         assert info["steps"] > 0 and np.isfinite(info["last_loss"])
         before = info["routed_sweep"]
         det.reset()
-        det.run(w.points)
+        det.run(pts)
         assert det.router_info()["routed_sweep"] > before
