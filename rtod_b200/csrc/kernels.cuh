@@ -104,6 +104,7 @@ struct SpanCtr {
   uint32_t n_groups;     // groups listed for exact counts in the running batch
   uint32_t n_segs;       // delta segments listed (learned router on), from the back of the list
   uint32_t seg_ticket;   // next delta segment for a count warp to take
+  uint32_t group_ticket; // next independent group for a count warp to take (router on)
   long long cmin[3];     // per hashed dimension, the span's cell coordinate range (k_span_hist)
   long long cmax[3];
   uint32_t* used;        // [NB] bins in use
@@ -1477,6 +1478,7 @@ static __device__ void finish_batch(const Batch& b) {
       b.span->n_groups = 0;
       b.span->n_segs = 0;
       b.span->seg_ticket = 0;
+      b.span->group_ticket = 0;
       for (int d = 0; d < 3; ++d) {
         b.span->cmin[d] = LLONG_MAX;
         b.span->cmax[d] = LLONG_MIN;

@@ -128,8 +128,12 @@ def test_router_results_identical_to_plain(gpu, oracle_mod, case):
         pts = datagen.random_walk(40_000, 0.1, seed=9, dim=8)
         W, S, R, K, sl = 8000, 400, 0.6, 20, 40
     dim = pts.shape[1]
-    with rtod.Detector(W, S, R, K, dim=dim, router=False) as plain, \
-            rtod.Detector(W, S, R, K, dim=dim, router=True) as routed:
+    # the span engine routes where its stencils have at most 32 cells (3-d:
+    # one cell per R) and up to 3 dimensions; the 8-d stream is routed by the
+    # window engine's point queues
+    kw = dict(cells_per_r=1) if case == "tao" else (dict(engine="window", count="point") if case == "walk8" else {})
+    with rtod.Detector(W, S, R, K, dim=dim, router=False, **kw) as plain, \
+            rtod.Detector(W, S, R, K, dim=dim, router=True, **kw) as routed:
         a = plain.run(pts, max_slides=sl)
         for _ in range(3):  # the router keeps training across runs
             routed.reset()
@@ -177,21 +181,44 @@ def test_router_learns_to_spot_outliers(gpu):
 
 @pytest.mark.gpu
 def test_trained_router_beats_untrained(gpu):
-    """What the trained network gains: after online training its routing makes
-    fewer mistakes than the untrained network on the same stream."""
+    """What the trained network gains, on the sensor-like 3-d stream (span
+    engine, one cell per R, where most runs cost less in delta segments):
+    untrained (biased towards independent counts) it sends almost nothing
+    to delta segments, trained most runs; and the trained routing runs the
+    pass faster than the same engine with the router off (median device
+    time of 9 passes), with identical outliers."""
     rtod, _ = gpu
+    import torch
     from rtod_b200 import datagen
     w = datagen.sensor_like()
-    pts = w.points[:w.window + 300 * w.slide]
-    with rtod.Detector(w.window, w.slide, w.R, w.K, dim=3, router=True) as det:
-        det.run(pts)
-        i0 = det.router_info()
-        first = i0["misrouted"] / max(1, i0["routed_early"] + i0["routed_sweep"])
-        for _ in range(4):
+    pts = torch.from_numpy(w.points).cuda()
+    out = torch.empty(w.slides * w.window // 4, dtype=torch.int64, device="cuda")
+
+    def timed(det):
+        ts = []
+        for _ in range(9):
             det.reset()
-            det.run(pts)
+            r = det.run(pts, out_ids=out, ids_cap=out.numel(), times=True)
+            ts.append(r.times["total"])
+        return float(np.median(ts)), r.offsets.copy(), out[:int(r.offsets[-1])].cpu().numpy()
+
+    with rtod.Detector(w.window, w.slide, w.R, w.K, dim=3, engine="span", cells_per_r=1, batch=256) as plain:
+        t_plain, off, ids = timed(plain)
+    with rtod.Detector(w.window, w.slide, w.R, w.K, dim=3, engine="span", cells_per_r=1, batch=256,
+                       router=True) as det:
+        det.run(pts, out_ids=out, ids_cap=out.numel())
+        i0 = det.router_info()
+        first = i0["routed_sweep"] / max(1, i0["routed_early"] + i0["routed_sweep"])
+        for _ in range(30):
+            det.reset()
+            det.run(pts, out_ids=out, ids_cap=out.numel())
         i1 = det.router_info()
-        later = (i1["misrouted"] - i0["misrouted"]) / max(
-            1, i1["routed_early"] + i1["routed_sweep"] - i0["routed_early"] - i0["routed_sweep"])
-        assert i1["steps"] > i0["steps"]
-        assert later <= first + 1e-9
+        t_routed, off2, ids2 = timed(det)
+        i2 = det.router_info()
+        later = (i2["routed_sweep"] - i1["routed_sweep"]) / max(
+            1, i2["routed_early"] + i2["routed_sweep"] - i1["routed_early"] - i1["routed_sweep"])
+    np.testing.assert_array_equal(off2, off)
+    np.testing.assert_array_equal(ids2, ids)
+    assert i1["steps"] > i0["steps"]
+    assert first < 0.2 and later > 0.5
+    assert t_routed < 0.96 * t_plain, (t_routed, t_plain)
