@@ -620,7 +620,7 @@ def run_reference(args, world, rank):
 
 def run_ncu_case(args, local):
     """Profiler pass of the headline workload with the settings the autotuner
-    picks on it in plain runs (span engine, 3 cells per R, 2-warp count
+    picks on it in plain runs (span engine, 3 cells per R, 4-warp count
     blocks, up to 256 windows per launch; under ncu the tuner's own timings
     would be distorted): one pass outside the profiler range, then two
     passes inside it (cudaProfilerStart/Stop: run ncu with
@@ -631,7 +631,7 @@ def run_ncu_case(args, local):
     torch.cuda.set_device(local)
     pts = torch.from_numpy(w.points).to(f"cuda:{local}")
     with Detector(w.window, w.slide, w.R, w.K, dim=w.dim, device=local, engine="span", cells_per_r=3,
-                  block_warps=2, batch=256) as det:
+                  block_warps=4, batch=256) as det:
         r = det.run(pts)
         torch.cuda.synchronize()
         torch.cuda.profiler.start()
