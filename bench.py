@@ -365,21 +365,77 @@ def run_ours(args, world, rank, local):
 def measure_streaming(w, local, base, slides: int = 60):
     """RTOD's own per-slide loop through the public API: push S points from
     host memory, detect, read the IDs back (host wall clock per slide, after
-    10 untimed slides); the IDs must match the whole-stream run."""
+    10 untimed slides), with the streaming grid engine (the default of
+    push/detect) and with the window engine; the IDs must match the
+    whole-stream run. The device time of a slide comes from a second pass
+    with per-detection stage times (CUDA events around the detection's
+    launches). The native command line (C++ over the C ABI, no Python in the
+    loop) runs the same loop on the whole stream."""
     from rtod_b200 import Detector
     W, S = w.window, w.slide
     n = min(slides, w.slides)
-    ts = []
-    with Detector(W, S, w.R, w.K, dim=w.dim, device=local) as det:
-        det.push(w.points[:W])
-        for j in range(n):
-            t0 = time.perf_counter()
-            det.push(w.points[W + j * S:W + (j + 1) * S])
-            ids = det.detect()
-            ts.append(time.perf_counter() - t0)
-            assert np.array_equal(ids, base["ids"][base["offsets"][j]:base["offsets"][j + 1]])
-    return {"us_per_slide_wall": float(np.median(ts[10:])) * 1e6, "slides": n,
-            "api": "rtod_push_slide + rtod_detect, window engine, host arrays"}
+    out = {"slides": n, "api": "rtod_push_slide + rtod_detect, host arrays"}
+    for engine in ("grid", "window"):
+        ts, dev = [], []
+        with Detector(W, S, w.R, w.K, dim=w.dim, device=local, engine=engine) as det:
+            for timed in (False, True):
+                det.reset()
+                det.push(w.points[:W])
+                for j in range(n):
+                    t0 = time.perf_counter()
+                    det.push(w.points[W + j * S:W + (j + 1) * S])
+                    got = det.detect(times=timed)
+                    t1 = time.perf_counter()
+                    ids = got[0] if timed else got
+                    if timed:
+                        dev.append(got[1]["total"] * 1e3)
+                    else:
+                        ts.append(t1 - t0)
+                    assert np.array_equal(ids, base["ids"][base["offsets"][j]:base["offsets"][j + 1]])
+            info = det.stream_engine
+        out[engine] = {"us_per_slide_wall": float(np.median(ts[10:])) * 1e6,
+                       "us_per_slide_device": float(np.median(dev[10:])),
+                       "engine": info["engine"], "grid_builds": info["builds"]}
+    out["us_per_slide_wall"] = out["grid"]["us_per_slide_wall"]
+    out["native"] = native_streaming(w, local, base)
+    return out
+
+
+def native_streaming(w, local, base):
+    """The native rtod command line in its --streaming mode (RTOD's per-slide
+    loop in C++ through rtod_push_slide + rtod_detect) on the same stream,
+    written in RTOD's text format: median wall time per slide, its outliers
+    checked against the whole-stream run."""
+    import subprocess
+    import tempfile
+    from rtod_b200 import build
+    exe = os.path.join(os.path.dirname(build.LIB), "rtod")
+    if not os.path.exists(exe):
+        return None
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "stream.txt")
+        np.savetxt(path, w.points.reshape(len(w.points), -1).astype(np.float64), fmt="%.9g",
+                   delimiter=",")
+        res = {}
+        for engine in ("grid", "window"):
+            cmd = [exe, "-f", path, "--n", str(len(w.points)), "--window", str(w.window), "--slide", str(w.slide),
+                   "--R", repr(float(w.R)), "--K", str(w.K), "--dim", str(w.dim), "--streaming", "--engine",
+                   engine, "--warmup", "10", "--device", str(local), "--print-outliers"]
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=600)
+            if r.returncode != 0:
+                return {"error": r.stderr.strip()[-300:]}
+            wall = [ln for ln in r.stdout.splitlines() if ln.startswith("[Wall]")]
+            total = [ln for ln in r.stdout.splitlines() if ln.startswith("[Time] total time for a slide")]
+            rows = [ln for ln in r.stdout.splitlines() if ln.startswith("slide ")]
+            same = len(rows) == w.slides and all(
+                np.array_equal(np.array(ln.split(":", 1)[1].split(), dtype=np.int64),
+                               base["ids"][base["offsets"][j]:base["offsets"][j + 1]])
+                for j, ln in enumerate(rows))
+            res[engine] = {"us_per_slide_wall_median": float(wall[0].split("median:")[1].split("us")[0]),
+                           "us_per_slide_device": float(total[0].split(":")[1].split("ms")[0]) * 1e3,
+                           "slides": len(rows), "same_outliers": bool(same)}
+    res["api"] = "rtod --streaming (C++), rtod_push_slide + rtod_detect from host arrays"
+    return res
 
 
 # FP32 operations of one distance test under the FP32 predicate in d
@@ -388,48 +444,64 @@ def measure_streaming(w, local, base, slides: int = 60):
 OPS_PER_TEST = {d: 3 * d for d in range(1, 9)}
 
 
-def measure_batched(local, steps: int = 20, warmup: int = 3):
+def measure_batched(local, steps: int = 20, warmup: int = 3, tune_max: int = 24):
     """The batched workload: 64 independent streams (W log-uniform in [5k,
     200k], S = W/20, d in {1, 3, 8}) through the multi-stream API, one graph
-    replay per step (staged launches; the persistent fused launch is timed
-    beside it). The step time is the wall time of
+    replay per step: with the autotuner (each group's cell width, count block
+    shape and count mode tried over the first steps, untimed, then fixed),
+    with the learned router on as well, with the default settings, and with
+    the persistent fused launch. The step time is the wall time of
     rtod_batch_step (it ends with one stream wait); e2e adds the step's 64
     host pushes. The 8-d streams also run alone, to set their group count's
     distance tests against the FP32 issue rate (compute bound: every point
     is counted against thousands of candidates)."""
     import torch
     from rtod_b200 import BatchDetector, datagen
-    streams = datagen.batched_streams(slides=warmup + steps)
+    streams = datagen.batched_streams(slides=tune_max + warmup + steps)
     pts_per_step = sum(s.slide for s in streams)
 
-    def run(subset, pipeline="staged"):
+    def run(subset, pipeline="staged", tuner=False, router=False):
         cfg = [dict(window=s.window, slide=s.slide, R=s.R, K=s.K, dim=s.dim, pipeline=pipeline) for s in subset]
-        with BatchDetector(cfg, device=local) as bd:
+        with BatchDetector(cfg, device=local, tuner=tuner, router=router) as bd:
             for i, s in enumerate(subset):
                 bd.push(i, s.points[:s.window])
             t_step, t_e2e = [], []
             tests0 = 0
-            for j in range(warmup + steps):
-                if j == warmup:
-                    tests0 = bd.stats["pair_tests"]
+            j = 0
+
+            def one(timed):
+                nonlocal j
                 t0 = time.perf_counter()
                 for i, s in enumerate(subset):
                     bd.push(i, s.points[s.window + j * s.slide:s.window + (j + 1) * s.slide])
                 t1 = time.perf_counter()
                 bd.step()
                 t2 = time.perf_counter()
-                if j >= warmup:
+                j += 1
+                if timed:
                     t_step.append(t2 - t1)
                     t_e2e.append(t2 - t0)
+
+            while tuner and j < tune_max and not all(g["settled"] for g in bd.tuning):
+                one(False)
+            tune_steps = j
+            for _ in range(warmup):
+                one(False)
+            tests0 = bd.stats["pair_tests"]
+            for _ in range(steps):
+                one(True)
             st = bd.stats
-            return float(np.sum(t_step)), float(np.sum(t_e2e)), st, st["pair_tests"] - tests0
+            return (float(np.sum(t_step)), float(np.sum(t_e2e)), st, st["pair_tests"] - tests0,
+                    {"tuning_steps": tune_steps, "groups": bd.tuning})
 
     torch.cuda.synchronize()
     with ClockSampler(physical_gpu_index(local)) as clk:
-        t_step, t_e2e, st, _ = run(streams)
-    t_fused, _, _, _ = run(streams, "fused")
+        t_step, t_e2e, st, _, tinfo = run(streams, tuner=True)
+    t_plain, _, _, _, _ = run(streams)
+    t_router, _, _, _, rinfo = run(streams, tuner=True, router=True)
+    t_fused, _, _, _, _ = run(streams, "fused")
     d8 = [s for s in streams if s.dim == 8]
-    t8, _, _, tests8 = run(d8)
+    t8, _, _, tests8, _ = run(d8, tuner=True)
     sm = torch.cuda.get_device_properties(local).multi_processor_count
     mhz = clk.summary()["sm_mhz"] or 1965.0
     peak_ops = sm * 128 * mhz * 1e6  # FP32 lanes x clock: one FP32 operation per lane and cycle
@@ -441,6 +513,8 @@ def measure_batched(local, steps: int = 20, warmup: int = 3):
         "window_points_per_s": sum(s.window for s in streams) * steps / t_step,
         "e2e": {"ms_per_step": t_e2e / steps * 1e3, "points_per_s": pts_per_step * steps / t_e2e,
                 "h2d_bytes_per_step": sum(4 * s.dim * s.slide for s in streams)},
+        "autotuner": dict(tinfo, untuned_ms_per_step=t_plain / steps * 1e3),
+        "router_on": {"ms_per_step": t_router / steps * 1e3, "tuning_steps": rinfo["tuning_steps"]},
         "fused_pipeline_ms_per_step": t_fused / steps * 1e3,
         "launches_per_step": st["launches"] / max(1, st["steps"]), "groups": st["groups"],
         "clocks": clk.summary(),

@@ -60,6 +60,8 @@ extern "C" {
 #define RTOD_ENGINE_AUTO 0
 #define RTOD_ENGINE_WINDOW 1
 #define RTOD_ENGINE_SPAN 2
+#define RTOD_ENGINE_GRID 3 /* push/detect: the streaming grid engine (a persistent cell grid of the
+                              window, updated by each slide's points); rtod_run: the span engine */
 
 /* rtod_config.count: how the window engine counts the points of a cell
    that are not provably inliers (the range count of RTOD's intersection
@@ -103,7 +105,13 @@ typedef struct rtod_config {
                           RTOD_ENGINE_WINDOW (one counting sort per window) or
                           RTOD_ENGINE_SPAN (one counting sort per batch of windows;
                           falls back to the window engine when W/S > 2047).
-                          push/detect always use the window engine. Results are identical. */
+                          push/detect: RTOD_ENGINE_GRID runs the streaming grid engine
+                          (each bin of the cell grid keeps its window points as a FIFO
+                          that a slide's expiry and insertion update in place, three
+                          launches per slide) for dim <= 3, W <= 262144 and W/S <= 4096;
+                          RTOD_ENGINE_AUTO does the same unless the router is on, the
+                          pipeline is fused or a count mode is named; every other case
+                          runs the window engine. Results are identical. */
   int32_t coord;       /* RTOD_COORD_F32 or RTOD_COORD_F64 */
   int32_t count;       /* RTOD_COUNT_*: window-engine count (push/detect, the multi-stream
                           API, rtod_run with the window engine) */
@@ -226,6 +234,21 @@ int rtod_check_bounded_wait(int32_t device, int32_t* timed_out, double* ms);
    for data", src/ods/optixScan.cpp:1172-1174). */
 int rtod_get_stats(const rtod_handle* h, int64_t out[5]);
 
+/* Engine of push/detect: out[0] RTOD_ENGINE_GRID or RTOD_ENGINE_WINDOW,
+   out[1] builds of the streaming grid from the ring (its first window, and
+   rebuilds after its pool ran out), out[2] pool slots of the grid, out[3]
+   the largest bin occupancy of the last counted window. The grid engine has
+   no counterpart in RTOD, which rebuilds or refits its BVH every slide
+   (src/ods/optixScan.cpp:335-426). */
+int rtod_get_stream_engine(const rtod_handle* h, int64_t out[4]);
+
+/* Pool size of the streaming grid (slots of D coordinates and a 32-bit ring
+   slot each; default 16 W + 2^22, at most 2^31): the grid's first build
+   starts from it and doubles it while the bins' regions do not fit. For
+   callers that bound the library's device memory, and for tests of the
+   rebuild path. Call before the first push (or after rtod_reset). */
+int rtod_set_grid_pool(rtod_handle* h, int64_t slots);
+
 /* Diagnostic run: like rtod_run on a fresh handle but launches every kernel
    individually with a CUDA event after each, and writes the average device
    time per slide of each pipeline stage, in order (keys, hist, scan,
@@ -271,6 +294,21 @@ int rtod_batch_step(rtod_batch* b, int64_t* out_offsets, int64_t* out_ids, int64
    distance tests made by group counts (RTOD_COUNT_GROUP streams) since
    create: the work of the compute-bound count, for its roofline. */
 int rtod_batch_stats(const rtod_batch* b, int64_t out[5]);
+
+/* Settings of each group of streams (one per dimension, predicate and
+   count mode): out[6 * i + 0..5] = dimension, predicate, cells per R, count
+   block warps, count mode (RTOD_COUNT_POINT or RTOD_COUNT_GROUP), and 1 once
+   the autotuner has settled that group (always 1 without the tuner).
+   Returns the number of groups (fills at most cap of them).
+   Autotuner: when any stream's rtod_config.tuner is 1, every group tries
+   its candidate settings over the first steps, one setting per step, each
+   timed on the device around the group's launches (two rounds), then keeps
+   the fastest: cells per R (2..4 in 1-d, 1..3 up to 3-d, 1..2 beyond,
+   unless the stream's config fixes it; the streams' ring keys are recomputed
+   when it changes) x count block warps (2, 4, 8; 4, 8 beyond 3-d) x, beyond
+   3 dimensions and with the router off, both count modes. Steps run without
+   the captured graph while tuning. Results do not depend on any setting. */
+int rtod_batch_get_tuning(const rtod_batch* b, int32_t* out, int32_t cap);
 
 void rtod_batch_destroy(rtod_batch* b);
 

@@ -26,12 +26,12 @@ class RtodError(RuntimeError):
         self.code = code
 
 
-ENGINE = {"auto": 0, "window": 1, "span": 2}
+ENGINE = {"auto": 0, "window": 1, "span": 2, "grid": 3}
 COORD = {"f32": 0, "f64": 1}
 COUNT = {"auto": 0, "point": 1, "group": 2}
 COUNT_NAME = {1: "point", 2: "group"}
 PIPELINE = {"staged": 0, "fused": 1}
-ENGINE_NAME = {1: "window", 2: "span"}
+ENGINE_NAME = {1: "window", 2: "span", 3: "grid"}
 
 
 class Config(ctypes.Structure):
@@ -79,6 +79,8 @@ SIGNATURES = [
     ("rtod_get_count_mode", _i32, [_vp, ctypes.POINTER(_i32)]),
     ("rtod_check_bounded_wait", _i32, [_i32, ctypes.POINTER(_i32), ctypes.POINTER(ctypes.c_double)]),
     ("rtod_get_stats", _i32, [_vp, _vp]),
+    ("rtod_get_stream_engine", _i32, [_vp, _vp]),
+    ("rtod_set_grid_pool", _i32, [_vp, _i64]),
     ("rtod_profile_run", _i32, [_vp, _vp, _i64, _i64, _vp, _i32]),
     ("rtod_kernel_name", ctypes.c_char_p, [_i32]),
     ("rtod_router_info", _i32, [_vp, _vp, _vp]),
@@ -89,6 +91,7 @@ SIGNATURES = [
     ("rtod_batch_push", _i32, [_vp, _i32, _vp, _i64]),
     ("rtod_batch_step", _i32, [_vp, _vp, _vp, _i64, ctypes.POINTER(_i64)]),
     ("rtod_batch_stats", _i32, [_vp, _vp]),
+    ("rtod_batch_get_tuning", _i32, [_vp, _vp, _i32]),
     ("rtod_batch_destroy", None, [_vp]),
     ("rtod_mlp_param_count", _i32, []),
     ("rtod_mlp_forward", _i32, [_i32, _vp, _vp, _i64, _vp]),

@@ -15,8 +15,8 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "librtod.so")
 CLI = os.path.join(PKG, "rtod")  # native optixScan-compatible command line (rtod_cli.cpp)
-SOURCES = ["rtod.cu", "fused_f32.cu", "fused_f64.cu"]
-HEADERS = ["kernels.cuh", "router.cuh", "span.cuh", "group.cuh", "fused.cuh", "fused_impl.cuh"]
+SOURCES = ["rtod.cu", "fused_f32.cu", "fused_f64.cu", "grid.cu"]
+HEADERS = ["kernels.cuh", "router.cuh", "span.cuh", "group.cuh", "fused.cuh", "fused_impl.cuh", "grid.cuh"]
 OBJ_DIR = os.path.join(PKG, "_build")
 
 

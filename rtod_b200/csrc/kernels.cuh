@@ -67,7 +67,8 @@ constexpr int SPIN_LIMIT = 1 << 22;         // bounded waits (then DERR_TIMEOUT)
 
 // Device error codes (first one wins).
 enum : int32_t {
-  DERR_NONE = 0, DERR_NONFINITE = 1, DERR_RANGE = 2, DERR_CAPACITY = 3, DERR_TIMEOUT = 4
+  DERR_NONE = 0, DERR_NONFINITE = 1, DERR_RANGE = 2, DERR_CAPACITY = 3, DERR_TIMEOUT = 4,
+  DERR_GRID = 5  // the streaming grid (grid.cuh) must be rebuilt from the ring: not the caller's error
 };
 
 // Per-job counters (device). lo is the first global index of the job's
@@ -522,6 +523,27 @@ __global__ void __launch_bounds__(256) k_ingest(Batch b, int32_t fill) {
   pdl_trigger();
   pdl_wait();
   ingest_body<D, T>(b, fill, hw_block());
+}
+
+// k_rekey: the cell key of every ring slot of every job, recomputed from the
+// ring's coordinates with the job's current cell (after the multi-stream
+// autotuner changed a group's cell width). Grid (x, jobs).
+template <int D, typename T>
+__global__ void __launch_bounds__(256) k_rekey(Batch b) {
+  pdl_trigger();
+  pdl_wait();
+  if (!job_active(b, blockIdx.y)) return;
+  const Job& jb = b.jobs[blockIdx.y];
+  const T* ring = static_cast<const T*>(jb.pts);
+  uint64_t* keys = const_cast<uint64_t*>(jb.keys);
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < jb.W; s += (int64_t)gridDim.x * blockDim.x) {
+    T x[D];
+#pragma unroll
+    for (int d = 0; d < D; ++d) x[d] = ring[(int64_t)d * jb.W + s];
+    int32_t code;
+    keys[s] = cell_key<D, T>(x, jb.inv_cell, &code);
+    if (code) set_err(b.bs, code);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1614,6 +1636,15 @@ static __global__ void __launch_bounds__(1024) k_compact_one(Batch b, int64_t* i
   const uint32_t job = blockIdx.x;
   const Job& jb = b.jobs[job];
   BatchState* bs = b.bs;
+  if (*(volatile int32_t*)&bs->err == DERR_GRID) {
+    // the streaming grid could not take the slide and nothing was counted:
+    // no batch end; the host rebuilds the grid and counts the window again
+    if (blockIdx.x == 0 && threadIdx.x == 0 && mirror) {
+      __threadfence_system();
+      *mirror = *bs;
+    }
+    return;
+  }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const bool act = job_active(b, job);
   if (act && wid == 0) {

@@ -22,6 +22,7 @@
 
 #include "../../include/rtod.h"
 #include "fused.cuh"
+#include "grid.cuh"
 #include "kernels.cuh"
 #include "span.cuh"
 
@@ -238,6 +239,17 @@ void init_router(RouterState* r) {
 
 enum Mode { MODE_NONE = 0, MODE_RING = 1, MODE_RUN = 2 };
 
+// Streaming grid engine of push/detect (grid.cuh): its device arrays and
+// the kernel argument that points at them.
+struct GridHost {
+  bool on = false;     // push/detect run the grid engine
+  bool built = false;  // the grid holds the ring's window
+  Grid g{};
+  int64_t bytes = 0;
+  int64_t builds = 0;  // builds from the ring (first window and rebuilds)
+  uint64_t pool_first = 0;  // pool slots of the first build (0: 16 W + 2^21)
+};
+
 struct EventSet {
   std::vector<cudaEvent_t> ev;
   cudaEvent_t make() {
@@ -336,6 +348,7 @@ struct rtod_handle {
   int graph_ring = -1;
   int64_t batches = 0;
 
+  GridHost grid;           // streaming grid engine (push/detect)
   GridBar* bar = nullptr;  // grid barrier of the fused pipeline
   int fused_grid = 0;      // its blocks (all resident), found on first use
   cudaEvent_t ev[16] = {};
@@ -377,8 +390,8 @@ int check_config(const rtod_config* c) {
       c->block_warps != 8)
     return fail(RTOD_ERR_CONFIG, "block_warps must be 0 (auto), 1, 2, 4 or 8");
   if (c->batch < 0 || c->batch > 256) return fail(RTOD_ERR_CONFIG, "batch must be 0..256");
-  if (c->engine < RTOD_ENGINE_AUTO || c->engine > RTOD_ENGINE_SPAN)
-    return fail(RTOD_ERR_CONFIG, "engine must be 0 (auto), 1 (window) or 2 (span)");
+  if (c->engine < RTOD_ENGINE_AUTO || c->engine > RTOD_ENGINE_GRID)
+    return fail(RTOD_ERR_CONFIG, "engine must be 0 (auto), 1 (window), 2 (span) or 3 (grid)");
   if (c->coord != RTOD_COORD_F32 && c->coord != RTOD_COORD_F64)
     return fail(RTOD_ERR_CONFIG, "coord must be RTOD_COORD_F32 or RTOD_COORD_F64");
   if (c->coord == RTOD_COORD_F64 && c->pred != RTOD_PRED_F64_LT)
@@ -925,8 +938,176 @@ bool fused_ring(const rtod_handle* h, const cudaEvent_t* kev) {
   return h->cfg.pipeline == RTOD_PIPELINE_FUSED && !kev;
 }
 
+// ---------------------------------------------------------------------------
+// Streaming grid engine (push/detect; grid.cuh)
+// ---------------------------------------------------------------------------
+constexpr int64_t kGridMaxW = COMPACT1_MAX;  // one compaction block per detection
+constexpr int64_t kGridMaxBlocks = 4096;    // slide blocks per window (per-block cell ranges)
+constexpr uint64_t kGridMaxPool = 1ull << 31;  // pool slots (slot numbers are 32-bit)
+
+int check_device_error(rtod_handle* h, const BatchState& s);
+
+bool grid_wanted(const rtod_handle* h) {
+  const rtod_config& c = h->cfg;
+  if (c.engine != RTOD_ENGINE_GRID &&
+      (c.engine != RTOD_ENGINE_AUTO || c.router || c.pipeline == RTOD_PIPELINE_FUSED || c.count != RTOD_COUNT_AUTO))
+    return false;
+  return h->D <= 3 && h->W <= kGridMaxW && h->W / h->S <= kGridMaxBlocks;
+}
+
+int64_t grid_pool_bytes(const rtod_handle* h, uint64_t pool) { return (int64_t)pool * (h->D * h->esz + 4); }
+
+void free_grid_pool(rtod_handle* h) {
+  Grid& g = h->grid.g;
+  if (g.px) {
+    h->grid.bytes -= grid_pool_bytes(h, g.pool);
+    h->device_bytes -= grid_pool_bytes(h, g.pool);
+  }
+  dfree(g.px);
+  dfree(g.pslot);
+  g.pool = 0;
+  h->grid.built = false;
+}
+
+void free_grid(rtod_handle* h) {
+  Grid& g = h->grid.g;
+  free_grid_pool(h);
+  dfree(g.ctl); dfree(g.head); dfree(g.tail); dfree(g.base); dfree(g.cap); dfree(g.ref); dfree(g.mixed);
+  dfree(g.growflag); dfree(g.grow); dfree(g.ovf_bin); dfree(g.ovf_pos); dfree(g.ovf_slot); dfree(g.ovf_x);
+  dfree(g.brange); dfree(g.qpos); dfree(g.qbin);
+  h->device_bytes -= h->grid.bytes;
+  h->grid.bytes = 0;
+}
+
+// Device arrays of the grid; a pool of at least `pool` slots (replaced when
+// it is smaller).
+int ensure_grid(rtod_handle* h, uint64_t pool) {
+  GridHost& G = h->grid;
+  Grid& g = G.g;
+  if (!g.ctl) {
+    int64_t n = 0;
+    const size_t S = (size_t)h->S;
+    g.ovf_cap = (uint32_t)S;
+    g.nslots = (int32_t)(h->W / h->S + 1);
+    bool ok = !dalloc(&g.ctl, 1, &n) && !dalloc(&g.head, NB, &n) && !dalloc(&g.tail, NB, &n) &&
+              !dalloc(&g.base, NB, &n) && !dalloc(&g.cap, NB, &n) && !dalloc(&g.ref, NB, &n) &&
+              !dalloc(&g.mixed, NB, &n) && !dalloc(&g.growflag, NB, &n) && !dalloc(&g.grow, S, &n) &&
+              !dalloc(&g.ovf_bin, S, &n) && !dalloc(&g.ovf_pos, S, &n) && !dalloc(&g.ovf_slot, S, &n) &&
+              !dalloc((unsigned char**)&g.ovf_x, S * (size_t)(h->D * h->esz), &n) &&
+              !dalloc(&g.brange, (size_t)g.nslots * 6, &n) && !dalloc(&g.qpos, (size_t)h->W, &n) &&
+              !dalloc(&g.qbin, (size_t)h->W, &n);
+    G.bytes += n;
+    h->device_bytes += n;
+    if (!ok) return RTOD_ERR_CUDA;
+  }
+  if (g.pool < pool) {
+    drop_graph(h);
+    free_grid_pool(h);
+    int64_t n = 0;
+    if (dalloc((unsigned char**)&g.px, (size_t)pool * (size_t)(h->D * h->esz), &n) ||
+        dalloc(&g.pslot, (size_t)pool, &n)) {
+      dfree(g.px);
+      dfree(g.pslot);
+      return RTOD_ERR_CUDA;
+    }
+    g.pool = (uint32_t)pool;
+    G.bytes += grid_pool_bytes(h, pool);
+    h->device_bytes += grid_pool_bytes(h, pool);
+  }
+  return RTOD_OK;
+}
+
+GridKind grid_kind(const rtod_handle* h) { return GridKind{h->D, h->cfg.pred, h->f64}; }
+
+// Builds the grid of the ring's window [lo, lo + W), doubling the pool
+// while the regions do not fit. Returns RTOD_OK with h->grid.on cleared when
+// no pool within kGridMaxPool holds them (push/detect then run the window
+// engine).
+int grid_build(rtod_handle* h, int64_t lo) {
+  GridHost& G = h->grid;
+  // default: the bins' starting regions (2 * GRID_FRESH_CAP slots each) and
+  // eight times the window for grown regions and their garbage
+  const uint64_t first = G.pool_first ? G.pool_first : 16ull * (uint64_t)h->W + 4ull * GRID_FRESH_CAP * NB;
+  uint64_t pool = std::max<uint64_t>(G.g.pool, std::min<uint64_t>(kGridMaxPool, first));
+  const Batch b = make_batch(h, 1, h->ids_cap);
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    if (int r = ensure_grid(h, pool)) return r;
+    CU(cudaMemsetAsync(&h->bs->err, 0, sizeof(int32_t), h->stream));
+    CU(grid_launch_build(grid_kind(h), b, G.g, lo, h->W, h->S, h->sm_count, h->stream));
+    h->launches += h->W / h->S + 4;
+    int32_t err = 0;
+    CU(cudaMemcpyAsync(&err, &h->bs->err, sizeof err, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaStreamSynchronize(h->stream));
+    G.builds++;
+    if (err == DERR_NONE) {
+      G.built = true;
+      return RTOD_OK;
+    }
+    if (err != DERR_GRID) {
+      BatchState s{};
+      s.err = err;
+      return check_device_error(h, s);
+    }
+    if (pool >= kGridMaxPool) break;
+    pool = std::min<uint64_t>(kGridMaxPool, 2 * pool);
+  }
+  // no pool holds the window's regions: the window engine takes over
+  CU(cudaMemsetAsync(&h->bs->err, 0, sizeof(int32_t), h->stream));
+  CU(cudaStreamSynchronize(h->stream));
+  free_grid(h);
+  G.on = false;
+  drop_graph(h);
+  return RTOD_OK;
+}
+
+// After a detection that reported DERR_GRID (nothing counted, the window
+// not advanced): rebuilds the grid from the ring, which holds the window
+// with the new slide, and counts it again; or, when no pool holds the
+// grid, lets the window engine take the slide (its histogram re-ingests
+// the staged slide) and the rest of the stream.
+int launch_ring(rtod_handle* h, const Batch& b, bool train, cudaEvent_t* kev, int64_t* nk);
+int launch_grid(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev, int64_t* nk);
+
+int grid_recount(rtod_handle* h, const Batch& b) {
+  if (int r = grid_build(h, h->S * (h->slides_done + 1))) return r;
+  int64_t nk = 0;
+  int r = h->grid.on ? launch_grid(h, b, false, nullptr, &nk) : launch_ring(h, b, false, nullptr, &nk);
+  if (r) return r;
+  h->launches += nk;
+  CU(cudaStreamSynchronize(h->stream));
+  return RTOD_OK;
+}
+
+// One streaming detection of the grid engine: ingest, classify, count, compaction
+// (into the mapped landing buffers). kev as for launch_group.
+int launch_grid(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev, int64_t* nk) {
+  const GridKind k = grid_kind(h);
+  if (kev) CU(cudaEventRecord(kev[0], h->stream));
+  if (ingest) CU(grid_launch_ingest(k, b, h->grid.g, h->S, h->sm_count, h->stream));
+  if (kev) {
+    CU(cudaEventRecord(kev[1], h->stream));
+    CU(cudaEventRecord(kev[2], h->stream));
+    CU(cudaEventRecord(kev[3], h->stream));
+  }
+  CU(grid_launch_count(k, b, h->grid.g, h->sm_count, h->stream));
+  if (kev) CU(cudaEventRecord(kev[4], h->stream));
+  CU(launch_k(k_compact_one, dim3(1), 1024, h->stream, b, h->ids_host_dev, std::min(h->ids_host_cap, h->ids_cap),
+              h->bs_mirror_dev));
+  if (kev) {
+    CU(cudaEventRecord(kev[5], h->stream));
+    CU(cudaEventRecord(kev[6], h->stream));
+  }
+  if (nk) *nk = ingest ? 4 : 3;
+  return RTOD_OK;
+}
+
 int launch_batch(rtod_handle* h, const Batch& b, bool ingest, cudaEvent_t* kev, const Span* sp = nullptr) {
   int64_t nk = 0;
+  if (ingest && !sp && h->grid.on) {
+    int r = launch_grid(h, b, true, kev, &nk);
+    h->launches += nk;
+    return r;
+  }
   if (ingest && !sp && fused_ring(h, kev)) {
     int r = launch_fused(geom_of(h), b, h->bar, true, h->ids_host_dev, std::min(h->ids_host_cap, h->ids_cap),
                          h->bs_mirror_dev, train_now(h), h->stream, &h->fused_grid, &nk);
@@ -955,7 +1136,9 @@ int run_batch(rtod_handle* h, const Batch& b, bool ingest, const Span* sp = null
     CU(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
     int64_t nk = 0;
     int r;
-    if (ingest && !sp && fused_ring(h, nullptr)) {
+    if (ingest && !sp && h->grid.on) {
+      r = launch_grid(h, b, true, nullptr, &nk);
+    } else if (ingest && !sp && fused_ring(h, nullptr)) {
       r = launch_fused(geom_of(h), b, h->bar, true, h->ids_host_dev, std::min(h->ids_host_cap, h->ids_cap),
                        h->bs_mirror_dev, train, h->stream, &h->fused_grid, &nk);
     } else {
@@ -1010,6 +1193,11 @@ int reset_state(rtod_handle* h) {
   h->pending = false;
   h->poisoned = false;
   h->mode = MODE_NONE;
+  // the next first push builds the grid again (or retries it, when no pool held it)
+  const bool want = grid_wanted(h);
+  if (want != h->grid.on) drop_graph(h);
+  h->grid.on = want;
+  h->grid.built = false;
   return RTOD_OK;
 }
 
@@ -1374,6 +1562,7 @@ void free_all(rtod_handle* h) {
   }
   h->pool.clear();
   free_span(h);
+  free_grid(h);
   dfree(h->ctr); dfree(h->jobs_dev); dfree(h->bs); dfree(h->router); dfree(h->bar); dfree(h->ring); dfree(h->ring_keys);
   dfree(h->ring_prev); dfree(h->staging); dfree(h->run_buf); dfree(h->run_keys); dfree(h->run_prev);
   dfree(h->run_blk_lo); dfree(h->run_blk_hi);
@@ -1654,7 +1843,9 @@ RTOD_API int rtod_create(const rtod_config* cfg, rtod_handle** out) {
   set_grid(h, cfg->cells_per_r ? cfg->cells_per_r : 2);
   // Engine of rtod_run: the span engine by default (with the router on, it
   // routes the span engine's counts; the tuner may pick the window engine).
-  h->engine = cfg->engine != RTOD_ENGINE_AUTO ? cfg->engine : RTOD_ENGINE_SPAN;
+  h->engine = cfg->engine == RTOD_ENGINE_WINDOW ? RTOD_ENGINE_WINDOW : RTOD_ENGINE_SPAN;
+  // Engine of push/detect: the streaming grid engine where it applies.
+  h->grid.on = grid_wanted(h);
   // Window-engine count: group counts where no cell is ever all-inlier and
   // a window holds enough points for long parts (auto_group), unless the
   // router (which routes single points) is on.
@@ -1801,6 +1992,35 @@ RTOD_API int rtod_get_stats(const rtod_handle* h, int64_t out[5]) {
   return RTOD_OK;
 }
 
+RTOD_API int rtod_get_stream_engine(const rtod_handle* h, int64_t out[4]) {
+  if (!h || !out) return fail(RTOD_ERR_ARG, "null argument");
+  out[0] = h->grid.on ? RTOD_ENGINE_GRID : RTOD_ENGINE_WINDOW;
+  out[1] = h->grid.builds;
+  out[2] = h->grid.g.pool;
+  out[3] = 0;
+  if (h->grid.on && h->grid.g.ctl) {
+    GridCtl c{};
+    CU(cudaSetDevice(h->device));
+    CU(cudaStreamSynchronize(h->stream));
+    CU(cudaMemcpy(&c, h->grid.g.ctl, sizeof c, cudaMemcpyDeviceToHost));
+    out[3] = c.max_occ;
+  }
+  return RTOD_OK;
+}
+
+RTOD_API int rtod_set_grid_pool(rtod_handle* h, int64_t slots) {
+  if (!h) return fail(RTOD_ERR_ARG, "handle is null");
+  if (slots < 1024 || (uint64_t)slots > kGridMaxPool)
+    return fail(RTOD_ERR_ARG, "pool slots must be in [1024, 2^31]");
+  if (h->n_pushed != 0) return fail(RTOD_ERR_STATE, "set the pool before the first push (or after rtod_reset)");
+  CU(cudaSetDevice(h->device));
+  CU(cudaStreamSynchronize(h->stream));
+  free_grid_pool(h);
+  drop_graph(h);
+  h->grid.pool_first = (uint64_t)slots;
+  return RTOD_OK;
+}
+
 RTOD_API const char* rtod_kernel_name(int32_t i) { return (i >= 0 && i < kPipeKernels) ? kKernelNames[i] : nullptr; }
 
 namespace {
@@ -1851,6 +2071,7 @@ int push_impl(rtod_handle* h, const void* pts, int64_t n, bool f64) {
     CU(cudaStreamSynchronize(h->stream));
     r = check_device_error(h, s);
     if (r) return r;
+    if (h->grid.on && (r = grid_build(h, 0))) return r;
   } else {
     h->pending = true;
   }
@@ -1886,6 +2107,10 @@ RTOD_API int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t*
   CU(cudaStreamSynchronize(h->stream));
   BatchState s;
   std::memcpy(&s, h->bs_mirror, sizeof s);
+  if (s.err == DERR_GRID && h->grid.on) {
+    if ((r = grid_recount(h, b))) return r;
+    std::memcpy(&s, h->bs_mirror, sizeof s);
+  }
   h->pending = false;
   r = check_device_error(h, s);
   if (r) return r;
@@ -2184,10 +2409,24 @@ struct rtod_batch {
     int64_t cmp_tiles = 0;
     GridBar* bar = nullptr;       // grid barrier of the group's fused launch
     int fused_grid = 0;
+    // Autotuner (rtod_config.tuner): settings tried one per step, each timed
+    // on the device around the group's launches, `rounds` times over.
+    struct Setting {
+      int n, bw, group;
+    };
+    Setting cur{2, 8, 0};
+    std::vector<Setting> cand;
+    std::vector<float> ms;
+    int idx = 0, round = 0;
+    bool tuned = true;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
   };
   std::vector<Group> groups;
   RouterState* router = nullptr;
   std::vector<char> filled, pending;
+  bool tuning = false;   // the autotuner is still trying settings (no graph replay meanwhile)
+  int tune_rounds = 2;
+  int64_t tune_steps = 0;
   cudaGraphExec_t graphs[2] = {nullptr, nullptr};  // without / with the router's training step
   int64_t graph_kernels[2] = {0, 0};
   int64_t steps = 0, launches = 0, detections = 0;
@@ -2199,6 +2438,8 @@ void batch_free(rtod_batch* b) {
   for (auto g : b->graphs)
     if (g) cudaGraphExecDestroy(g);
   for (auto& g : b->groups) {
+    if (g.e0) cudaEventDestroy(g.e0);
+    if (g.e1) cudaEventDestroy(g.e1);
     dfree(g.jobs); dfree(g.bs); dfree(g.out); dfree(g.active); dfree(g.nout); dfree(g.bar);
     if (g.active_h) cudaFreeHost(g.active_h);
     if (g.nout_h) cudaFreeHost(g.nout_h);
@@ -2225,11 +2466,12 @@ Batch group_batch(const rtod_batch::Group& g, RouterState* router) {
 }
 
 // One step for all groups: active flags in, counters reset, pipeline, counts out.
-int batch_enqueue(rtod_batch* b, bool train, int64_t* nk_total) {
+int batch_enqueue(rtod_batch* b, bool train, int64_t* nk_total, bool timed = false) {
   int64_t total = 0;
   for (auto& g : b->groups) {
     const int ng = (int)g.streams.size();
     CU(cudaMemcpyAsync(g.active, g.active_h, sizeof(int32_t) * ng, cudaMemcpyHostToDevice, b->stream));
+    if (timed) CU(cudaEventRecord(g.e0, b->stream));
     int64_t nk = 0;
     int r;
     if (b->fused) {
@@ -2240,10 +2482,106 @@ int batch_enqueue(rtod_batch* b, bool train, int64_t* nk_total) {
     }
     if (r) return r;
     total += nk;
+    if (timed) CU(cudaEventRecord(g.e1, b->stream));
     CU(cudaMemcpyAsync(g.nout_h, g.nout, sizeof(int32_t) * ng, cudaMemcpyDeviceToHost, b->stream));
     CU(cudaMemcpyAsync(g.bs_h, g.bs, sizeof(BatchState), cudaMemcpyDeviceToHost, b->stream));
   }
   *nk_total = total;
+  return RTOD_OK;
+}
+
+// Job table of a group from its streams' current settings.
+int upload_group_jobs(rtod_batch* b, rtod_batch::Group& g) {
+  const int ng = (int)g.streams.size();
+  std::vector<Job> tab(ng);
+  for (int k = 0; k < ng; ++k) tab[k] = make_job(b->hs[g.streams[k]], 0, true, nullptr);
+  for (auto& jb : tab) jb.gpts = group_part(g.out_cap, b->hs[g.streams[0]]->sm_count);
+  CU(cudaMemcpy(g.jobs, tab.data(), sizeof(Job) * ng, cudaMemcpyHostToDevice));
+  return RTOD_OK;
+}
+
+// Applies a setting to a group: cell width (its streams' ring keys are
+// recomputed), count block shape and count mode. Results do not depend on
+// any of them.
+int apply_group_setting(rtod_batch* b, rtod_batch::Group& g, const rtod_batch::Group::Setting& st,
+                        bool rings_filled = true) {
+  const bool rekey = st.n != g.cur.n;
+  for (int s : g.streams) {
+    rtod_handle* h = b->hs[s];
+    if (rekey) set_grid(h, st.n);
+    h->group = st.group;
+    h->block_warps = st.bw;
+  }
+  if (st.group != g.cur.group) g.fused_grid = 0;  // another kernel instantiation: residency found again
+  g.geom.block_warps = st.bw;
+  g.geom.group = st.group;
+  g.geom.route = b->route && !st.group;
+  if (int r = upload_group_jobs(b, g)) return r;
+  if (rekey && rings_filled) {
+    // the rings of the streams that hold a window
+    std::vector<int32_t> filled(g.streams.size());
+    for (size_t k = 0; k < g.streams.size(); ++k) filled[k] = b->filled[g.streams[k]] ? 1 : 0;
+    CU(cudaMemcpy(g.active, filled.data(), sizeof(int32_t) * filled.size(), cudaMemcpyHostToDevice));
+    Batch bt = group_batch(g, b->router);
+    const unsigned gx = (unsigned)std::max<int64_t>(1, std::min<int64_t>((g.geom.Wmax + 255) / 256, 1024));
+    DISPATCH_D(g.geom.D, CU(launch_k(k_rekey<D, float>, dim3(gx, (unsigned)g.streams.size()), 256, b->stream, bt)));
+  }
+  g.cur = st;
+  return RTOD_OK;
+}
+
+// Candidate settings of a group: cell widths x block shapes (and, beyond 3
+// dimensions, both count modes), except what the streams' configs fix.
+void init_group_tuning(rtod_batch* b, rtod_batch::Group& g, const rtod_config& c) {
+  std::vector<int> ns, bws, gs;
+  if (c.cells_per_r) ns = {c.cells_per_r};
+  else if (g.geom.D == 1) ns = {2, 3, 4};
+  else if (g.geom.D <= 3) ns = {1, 2, 3};
+  else ns = {1, 2};
+  if (c.block_warps) bws = {c.block_warps};
+  else if (g.geom.D <= 3) bws = {2, 4, 8};
+  else bws = {4, 8};
+  if (c.count != RTOD_COUNT_AUTO || b->route || g.geom.D <= 3) gs = {g.cur.group};
+  else gs = {1, 0};
+  g.cand.clear();
+  for (int n : ns)
+    for (int gm : gs)
+      for (int bw : bws) g.cand.push_back({n, bw, gm});
+  g.ms.assign(g.cand.size(), INFINITY);
+  g.idx = 0;
+  g.round = 0;
+  g.tuned = g.cand.size() <= 1;
+}
+
+// Records the device time of each group's setting of this step and moves
+// the tuners on; the best setting of a finished group is applied.
+int advance_tuning(rtod_batch* b) {
+  bool all = true;
+  for (auto& g : b->groups) {
+    if (g.tuned) continue;
+    float ms = 0;
+    CU(cudaEventElapsedTime(&ms, g.e0, g.e1));
+    g.ms[g.idx] = std::min(g.ms[g.idx], ms);
+    if (++g.idx == (int)g.cand.size()) {
+      g.idx = 0;
+      if (++g.round == b->tune_rounds) {
+        const size_t best = (size_t)(std::min_element(g.ms.begin(), g.ms.end()) - g.ms.begin());
+        g.tuned = true;
+        if (int r = apply_group_setting(b, g, g.cand[best])) return r;
+        continue;
+      }
+    }
+    if (int r = apply_group_setting(b, g, g.cand[g.idx])) return r;
+    all = false;
+  }
+  if (all) {
+    b->tuning = false;
+    for (auto& gx : b->graphs)
+      if (gx) {
+        cudaGraphExecDestroy(gx);
+        gx = nullptr;
+      }
+  }
   return RTOD_OK;
 }
 
@@ -2278,6 +2616,7 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
     c.batch = 1;
     c.router = b->route;
     c.use_graph = 0;
+    c.engine = RTOD_ENGINE_WINDOW;  // the step runs every stream's window as a window-engine job
     rtod_handle* h = nullptr;
     int r = rtod_create(&c, &h);
     if (r) return bail(r);
@@ -2346,6 +2685,23 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
         cudaMemset(g.bs, 0, sizeof(BatchState)))
       return bail(fail(RTOD_ERR_CUDA, "group setup failed"));
   }
+  // Autotuner: when any stream asks for it, every group tries its candidate
+  // settings over the first steps (one per step, tune_rounds times), then
+  // keeps the fastest.
+  for (int i = 0; i < n_streams; ++i) b->tuning = b->tuning || cfgs[i].tuner;
+  bool any = false;
+  for (auto& g : b->groups) {
+    const rtod_handle* h0 = b->hs[g.streams[0]];
+    g.cur = {h0->n, h0->block_warps, h0->group};
+    if (cudaEventCreate(&g.e0) || cudaEventCreate(&g.e1)) return bail(fail(RTOD_ERR_CUDA, "event creation failed"));
+    if (!b->tuning) continue;
+    init_group_tuning(b, g, cfgs[g.streams[0]]);
+    if (!g.tuned) {
+      any = true;
+      if (int r = apply_group_setting(b, g, g.cand[0], false)) return bail(r);
+    }
+  }
+  b->tuning = any;
   *out = b;
   return RTOD_OK;
 }
@@ -2397,8 +2753,13 @@ RTOD_API int rtod_batch_step(rtod_batch* b, int64_t* out_offsets, int64_t* out_i
     }
   if (!any) return fail(RTOD_ERR_STATE, "no stream has a pushed slide");
   const bool train = b->route && (b->steps < kTrainWarm || b->steps % kTrainEvery == 0);
+  const bool tuning = b->tuning;
   cudaGraphExec_t& gx = b->graphs[train ? 1 : 0];
-  if (!gx) {
+  int64_t nk = 0;
+  if (tuning) {  // direct launches, each group timed on the device
+    if (int r = batch_enqueue(b, train, &nk, true)) return r;
+    b->tune_steps++;
+  } else if (!gx) {
     cudaGraph_t gr;
     CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     int64_t nk0 = 0;
@@ -2411,8 +2772,10 @@ RTOD_API int rtod_batch_step(rtod_batch* b, int64_t* out_offsets, int64_t* out_i
     if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph instantiate failed: %s", cudaGetErrorString(e));
     b->graph_kernels[train ? 1 : 0] = nk0;
   }
-  const int64_t nk = b->graph_kernels[train ? 1 : 0];
-  CU(cudaGraphLaunch(gx, b->stream));
+  if (!tuning) {
+    nk = b->graph_kernels[train ? 1 : 0];
+    CU(cudaGraphLaunch(gx, b->stream));
+  }
   CU(cudaStreamSynchronize(b->stream));
   b->launches += nk;
   b->steps++;
@@ -2454,7 +2817,27 @@ RTOD_API int rtod_batch_step(rtod_batch* b, int64_t* out_offsets, int64_t* out_i
       b->hs[s]->slides_done++;
       b->detections++;
     }
+  if (tuning) {
+    if (int r = advance_tuning(b)) return r;
+    CU(cudaStreamSynchronize(b->stream));
+  }
   return RTOD_OK;
+}
+
+RTOD_API int rtod_batch_get_tuning(const rtod_batch* b, int32_t* out, int32_t cap) {
+  if (!b || (cap > 0 && !out)) return fail(RTOD_ERR_ARG, "null argument");
+  const int32_t ng = (int32_t)b->groups.size();
+  for (int32_t i = 0; i < ng && i < cap; ++i) {
+    const auto& g = b->groups[(size_t)i];
+    int32_t* o = out + 6 * i;
+    o[0] = g.geom.D;
+    o[1] = g.geom.pred;
+    o[2] = g.cur.n;
+    o[3] = g.cur.bw;
+    o[4] = g.cur.group ? RTOD_COUNT_GROUP : RTOD_COUNT_POINT;
+    o[5] = g.tuned ? 1 : 0;
+  }
+  return ng;
 }
 
 RTOD_API int rtod_batch_stats(const rtod_batch* b, int64_t out[5]) {

@@ -10,7 +10,12 @@
 // --opt (OPTIMIZATION, optixScan.h:22-24). Further flags: --coord f32|f64
 // (f64 keeps RTOD's doubles and its double predicate end to end), --pred
 // fp32_le|f64_lt, --router, --tuner, --no-graph, --warmup N (RTOD: 10),
-// --max-slides N, --device N, --print-outliers.
+// --max-slides N, --device N, --print-outliers, --engine auto|window|grid,
+// and --streaming: RTOD's own per-slide loop (detect_outlier,
+// optixScan.cpp:1045-1121) through rtod_push_slide + rtod_detect, one
+// window per call, timed on the host clock per slide (the last warm-up
+// slides excluded); the report then gives the median and mean wall time of a
+// slide and the device stage split of the timed slides.
 //
 // Input is read like read_data (optixScan.cpp:95-147): %lf per line in 1-d,
 // comma-separated values otherwise, parsed as doubles. Timing follows main()
@@ -25,6 +30,8 @@
 // fails (its message from rtod_last_error on stderr).
 #include <sys/resource.h>
 
+#include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -46,8 +53,9 @@ struct Args {
   int64_t start_copy_pos = 0;
   int dim = 1, opt = 2, warmup = 10, device = 0;
   int64_t max_slides = 10000;
-  bool f64 = false, router = false, tuner = false, graph = true, print = false;
+  bool f64 = false, router = false, tuner = false, graph = true, print = false, streaming = false;
   int pred = -1;
+  int engine = RTOD_ENGINE_AUTO;
 };
 
 void usage(const char* argv0) {
@@ -59,7 +67,7 @@ void usage(const char* argv0) {
                "         --start_copy_pos <int> --launch_ray_num <int>\n"
                "         --dim <1..8> --opt <0|1|2> --coord <f32|f64> --pred <fp32_le|f64_lt>\n"
                "         --router --tuner --no-graph --warmup <int> --max-slides <int> --device <int>\n"
-               "         --print-outliers\n",
+               "         --print-outliers --streaming --engine <auto|window|grid>\n",
                argv0);
   std::exit(1);
 }
@@ -98,6 +106,14 @@ bool parse(int argc, char** argv, Args* a) {
     else if (s == "--max-slides") a->max_slides = std::atoll(next());
     else if (s == "--device") a->device = std::atoi(next());
     else if (s == "--print-outliers") a->print = true;
+    else if (s == "--streaming") a->streaming = true;
+    else if (s == "--engine") {
+      const std::string v = next();
+      if (v == "auto") a->engine = RTOD_ENGINE_AUTO;
+      else if (v == "window") a->engine = RTOD_ENGINE_WINDOW;
+      else if (v == "grid") a->engine = RTOD_ENGINE_GRID;
+      else usage(argv[0]);
+    }
     else {
       std::fprintf(stderr, "Unknown option '%s'\n", s.c_str());
       usage(argv[0]);
@@ -191,6 +207,7 @@ int main(int argc, char** argv) {
   cfg.tuner = a.tuner;
   cfg.use_graph = a.graph;
   cfg.device = a.device;
+  cfg.engine = a.engine;
   const long rss0 = rss_kb();
   rtod_handle* h = nullptr;
   if (rtod_create(&cfg, &h) != RTOD_OK) return lib_fail("rtod_create");
@@ -216,14 +233,76 @@ int main(int argc, char** argv) {
                                     (int64_t)ids.size(), &slides, tp);
     return rc == RTOD_OK ? 0 : lib_fail("rtod_run");
   };
-  for (int w = 0; w < a.warmup; ++w)
-    if (int rc = pass(nullptr)) return rc;
-  if (int rc = pass(&t)) return rc;
+  // RTOD's per-slide loop: W points, then one push and one detection per
+  // slide; wall time per slide after `warmup` slides.
+  std::vector<double> wall_us;
+  auto stream_pass = [&]() -> int {
+    if (rtod_reset(h) != RTOD_OK) return lib_fail("rtod_reset");
+    auto push = [&](int64_t first, int64_t cnt) {
+      return a.f64 ? rtod_push_slide_f64(h, p64 + first * D, cnt) : rtod_push_slide(h, rows32.data() + first * D, cnt);
+    };
+    if (push(0, a.window) != RTOD_OK) return lib_fail("rtod_push_slide");
+    for (int64_t j = 0; j < slides_max; ++j) {
+      const bool timing = j >= a.warmup;
+      const auto t0 = std::chrono::steady_clock::now();
+      if (push(a.window + j * a.slide, a.slide) != RTOD_OK) return lib_fail("rtod_push_slide");
+      int64_t nout = 0;
+      if (rtod_detect(h, ids.data() + offsets[(size_t)j], (int64_t)ids.size() - offsets[(size_t)j], &nout, nullptr) !=
+          RTOD_OK)
+        return lib_fail("rtod_detect");
+      const auto t1 = std::chrono::steady_clock::now();
+      offsets[(size_t)j + 1] = offsets[(size_t)j] + nout;
+      if (timing) wall_us.push_back(std::chrono::duration<double, std::micro>(t1 - t0).count());
+    }
+    slides = slides_max;
+    return 0;
+  };
+  if (a.streaming) {
+    if (int rc = stream_pass()) return rc;
+    // stage split: a second pass with per-detection stage times
+    if (rtod_reset(h) != RTOD_OK) return lib_fail("rtod_reset");
+    auto push = [&](int64_t first, int64_t cnt) {
+      return a.f64 ? rtod_push_slide_f64(h, p64 + first * D, cnt) : rtod_push_slide(h, rows32.data() + first * D, cnt);
+    };
+    if (push(0, a.window) != RTOD_OK) return lib_fail("rtod_push_slide");
+    std::vector<int64_t> tmp((size_t)a.window);
+    int64_t timed = 0;
+    for (int64_t j = 0; j < slides_max; ++j) {
+      rtod_times st{};
+      int64_t nout = 0;
+      if (push(a.window + j * a.slide, a.slide) != RTOD_OK) return lib_fail("rtod_push_slide");
+      if (rtod_detect(h, tmp.data(), (int64_t)tmp.size(), &nout, j >= a.warmup ? &st : nullptr) != RTOD_OK)
+        return lib_fail("rtod_detect");
+      if (j < a.warmup) continue;
+      t.copy_new_points_h2d += st.copy_new_points_h2d;
+      t.copy_outlier_d2h += st.copy_outlier_d2h;
+      t.prepare_cell += st.prepare_cell;
+      t.build_bvh += st.build_bvh;
+      t.detect_outlier += st.detect_outlier;
+      t.total += st.total;
+      t.undetermined_per_slide += st.undetermined_per_slide;
+      ++timed;
+    }
+    if (timed) {
+      const double k = 1.0 / (double)timed;
+      t.copy_new_points_h2d *= k;
+      t.copy_outlier_d2h *= k;
+      t.prepare_cell *= k;
+      t.build_bvh *= k;
+      t.detect_outlier *= k;
+      t.total *= k;
+      t.undetermined_per_slide *= k;
+    }
+  } else {
+    for (int w = 0; w < a.warmup; ++w)
+      if (int rc = pass(nullptr)) return rc;
+    if (int rc = pass(&t)) return rc;
+  }
 
   // A graph-replayed pass gives the total only: the stage split comes from
   // one diagnostic pass on the same handle (kernels launched one by one).
   bool split_from_profile = false;
-  if (a.graph && !a.f64) {
+  if (a.graph && !a.f64 && !a.streaming) {
     double ms[8] = {0};
     if (rtod_reset(h) == RTOD_OK && rtod_profile_run(h, rows32.data(), n, a.max_slides, ms, 8) == RTOD_OK) {
       // stage slots: keys, hist, scan, scatter, count, compact, train
@@ -242,6 +321,20 @@ int main(int argc, char** argv) {
   std::printf("[Time] detect outlier: %g ms\n", t.detect_outlier);
   std::printf("[Time] total time for a slide: %g ms\n", t.total);
   std::printf("##############################\n");
+  if (a.streaming && !wall_us.empty()) {
+    std::vector<double> w = wall_us;
+    std::sort(w.begin(), w.end());
+    double mean = 0;
+    for (double v : w) mean += v;
+    mean /= (double)w.size();
+    int64_t eng[4] = {0};
+    rtod_get_stream_engine(h, eng);
+    std::printf("(per-slide loop: rtod_push_slide + rtod_detect, %s engine; [Time] figures are the device\n"
+                " stage times of a second pass, averaged over its slides after the warm-up)\n",
+                eng[0] == RTOD_ENGINE_GRID ? "grid" : "window");
+    std::printf("[Wall] slide (push + detect), median: %.3f us, mean: %.3f us, over %zu slides\n",
+                w[w.size() / 2], mean, w.size());
+  }
   if (split_from_profile)
     std::printf("(stage split: device time per slide of a diagnostic pass on the same handle, kernels launched "
                 "one by one; total: the graph-replayed pass)\n");

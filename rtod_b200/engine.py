@@ -190,6 +190,19 @@ class Detector:
     def reset(self) -> None:
         check(lib().rtod_reset(self._h))
 
+    @property
+    def stream_engine(self) -> dict:
+        """Engine of push/detect ("grid": the streaming grid engine, or
+        "window"), builds of the grid from the ring, its pool slots and the
+        largest bin occupancy of the last counted window."""
+        a = (ctypes.c_int64 * 4)()
+        check(lib().rtod_get_stream_engine(self._h, a))
+        return {"engine": _native.ENGINE_NAME.get(a[0], a[0]), "builds": a[1], "pool": a[2], "max_occ": a[3]}
+
+    def set_grid_pool(self, slots: int) -> None:
+        """Pool slots of the streaming grid's first build (before the first push)."""
+        check(lib().rtod_set_grid_pool(self._h, int(slots)))
+
     def router_info(self) -> dict:
         """Learned-router state: parameters, training steps and routing counters."""
         params = np.zeros(int(lib().rtod_mlp_param_count()), np.float32)
@@ -233,10 +246,12 @@ class BatchDetector:
     captured CUDA graph (streams grouped by dimension and predicate).
 
     ``streams`` is a list of dicts with the Detector parameters (window,
-    slide, R, K, dim, opt, pred, count); ``router`` switches the shared learned
-    router on for all of them."""
+    slide, R, K, dim, opt, pred, count, cells_per_r, block_warps); ``router``
+    switches the shared learned router on for all of them; ``tuner`` lets the
+    autotuner pick each group's cell width, count block shape and (beyond 3
+    dimensions) count mode over the first steps."""
 
-    def __init__(self, streams, router: bool = False, device: int = 0):
+    def __init__(self, streams, router: bool = False, device: int = 0, tuner: bool = False):
         n = len(streams)
         cfgs = (Config * n)()
         for i, st in enumerate(streams):
@@ -247,7 +262,8 @@ class BatchDetector:
             c.pred = _native.PRED[st.get("pred", "fp32_le")]
             c.count = _native.COUNT[st.get("count", "auto")]
             c.pipeline = _native.PIPELINE[st.get("pipeline", "staged")]
-            c.router, c.device = int(router), device
+            c.cells_per_r, c.block_warps = st.get("cells_per_r", 0), st.get("block_warps", 0)
+            c.router, c.device, c.tuner = int(router), device, int(tuner)
         self.streams = [dict(s) for s in streams]
         self._b = ctypes.c_void_p()
         check(lib().rtod_batch_create(cfgs, n, ctypes.byref(self._b)))
@@ -275,6 +291,18 @@ class BatchDetector:
         ptr, n, keep = _as_points(points, int(self.streams[s].get("dim", 1)))
         check(lib().rtod_batch_push(self._b, s, ptr, n))
         del keep
+
+    @property
+    def tuning(self) -> list:
+        """Per group of streams: its dimension, predicate, cells per R, count
+        block warps, count mode and whether the autotuner has settled it."""
+        a = (ctypes.c_int32 * (6 * 64))()
+        ng = lib().rtod_batch_get_tuning(self._b, a, 64)
+        if ng < 0:
+            check(ng)
+        return [{"dim": a[6 * i], "pred": a[6 * i + 1], "cells_per_r": a[6 * i + 2], "block_warps": a[6 * i + 3],
+                 "count": _native.COUNT_NAME.get(a[6 * i + 4], a[6 * i + 4]), "settled": bool(a[6 * i + 5])}
+                for i in range(min(ng, 64))]
 
     def step(self):
         """Per-stream sorted outlier IDs of this step (empty for streams that

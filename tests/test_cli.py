@@ -152,12 +152,16 @@ def test_native_cli_matches_golden(tmp_path, kind):
             continue
         f = tmp_path / "s.txt"
         write_stream(f, pts)
-        for graph in ([], ["--no-graph"]):
+        # whole-stream passes (graph and not), and RTOD's per-slide loop through
+        # push/detect with the grid engine and the window engine
+        for extra in ([], ["--no-graph"], ["--streaming"], ["--streaming", "--engine", "window"]):
             cmd = [native_cli(), "--n", str(len(pts)), "--R", repr(meta["R"]), "--K", str(meta["K"]),
                    "--window", str(meta["W"]), "--slide", str(meta["S"]), "-f", str(f), "--dim",
-                   str(pts.shape[1]), "--coord", kind, "--warmup", "1", "--print-outliers"] + graph
+                   str(pts.shape[1]), "--coord", kind, "--warmup", "1", "--print-outliers"] + extra
             r = subprocess.run(cmd, capture_output=True, text=True)
             assert r.returncode == 0, r.stderr
             assert "[Time] total time for a slide" in r.stdout and "BVH Node / slide" in r.stdout
+            if "--streaming" in extra and len(off) > 2:
+                assert "[Wall] slide (push + detect)" in r.stdout
             got = parse_outliers(r.stdout)
-            assert got == [ids[off[j]:off[j + 1]].tolist() for j in range(len(off) - 1)], path
+            assert got == [ids[off[j]:off[j + 1]].tolist() for j in range(len(off) - 1)], (path, extra)

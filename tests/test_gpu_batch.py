@@ -17,7 +17,7 @@ def rtod():
     return rtod_b200
 
 
-def make_streams(n=9, seed=5):
+def make_streams(n=9, seed=5, slides=12):
     from rtod_b200 import datagen
     rng = np.random.default_rng(seed)
     out = []
@@ -25,7 +25,6 @@ def make_streams(n=9, seed=5):
         d = [1, 3, 8][i % 3]
         W = int(rng.choice([2000, 3000, 5000, 8000]))
         S = W // int(rng.choice([4, 10, 20]))
-        slides = 12
         if rng.random() < 0.5:
             pts = datagen.random_walk(W + slides * S, 0.1, seed=100 + i, dim=d)
         else:
@@ -100,3 +99,34 @@ def test_batch_push_buffer_reused_at_once(rtod, oracle_mod):
             for i in range(len(streams)):
                 off, ids = expect[i]
                 np.testing.assert_array_equal(res[i], ids[off[j]:off[j + 1]])
+
+
+@pytest.mark.parametrize("router", [False, True])
+def test_batch_autotuner_keeps_results(rtod, oracle_mod, router):
+    """With the autotuner on, the first steps try every group's candidate
+    settings (cell width with the rings re-keyed, count block shape, count
+    mode beyond 3-d), one per step; every step's outliers still match the
+    oracle, and every group settles on one setting."""
+    streams = make_streams(n=6, seed=9, slides=30)
+    expect = [oracle_mod.detect(st["points"], st["window"], st["slide"], st["R"], st["K"], st["pred"],
+                                engine="grid", threads=4)[:2] for st in streams]
+    cfg = [{k: st[k] for k in ("window", "slide", "R", "K", "dim", "pred")} for st in streams]
+    with rtod.BatchDetector(cfg, router=router, tuner=True) as bd:
+        before = bd.tuning
+        assert not all(g["settled"] for g in before)
+        for i, st in enumerate(streams):
+            bd.push(i, st["points"][:st["window"]])
+        seen = {}
+        for j in range(30):
+            for i, st in enumerate(streams):
+                W, S = st["window"], st["slide"]
+                bd.push(i, st["points"][W + j * S:W + (j + 1) * S])
+            res = bd.step()
+            for g in bd.tuning:
+                seen.setdefault((g["dim"], g["pred"]), set()).add((g["cells_per_r"], g["block_warps"], g["count"]))
+            for i in range(len(streams)):
+                off, ids = expect[i]
+                np.testing.assert_array_equal(res[i], ids[off[j]:off[j + 1]], err_msg=f"stream {i} slide {j}")
+        after = bd.tuning
+        assert all(g["settled"] for g in after)
+        assert all(len(v) > 1 for v in seen.values())  # each group tried several settings
