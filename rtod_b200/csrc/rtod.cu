@@ -1036,7 +1036,9 @@ int grid_build(rtod_handle* h, int64_t lo) {
     CU(grid_launch_build(grid_kind(h), b, G.g, lo, h->W, h->S, h->sm_count, h->stream));
     h->launches += h->W / h->S + 4;
     int32_t err = 0;
+    unsigned long long wanted = 0;  // slots the regions asked for (k_grid_alloc counts every bin)
     CU(cudaMemcpyAsync(&err, &h->bs->err, sizeof err, cudaMemcpyDeviceToHost, h->stream));
+    CU(cudaMemcpyAsync(&wanted, &G.g.ctl->pool_top, sizeof wanted, cudaMemcpyDeviceToHost, h->stream));
     CU(cudaStreamSynchronize(h->stream));
     G.builds++;
     if (err == DERR_NONE) {
@@ -1049,7 +1051,8 @@ int grid_build(rtod_handle* h, int64_t lo) {
       return check_device_error(h, s);
     }
     if (pool >= kGridMaxPool) break;
-    pool = std::min<uint64_t>(kGridMaxPool, 2 * pool);
+    // room for the regions and as much again for their growth
+    pool = std::min<uint64_t>(kGridMaxPool, std::max<uint64_t>(2 * pool, 2 * (uint64_t)wanted));
   }
   // no pool holds the window's regions: the window engine takes over
   CU(cudaMemsetAsync(&h->bs->err, 0, sizeof(int32_t), h->stream));
