@@ -54,8 +54,10 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-stream multi-stream measurement")
-    ap.add_argument("--mode", choices=["bench", "ncu", "replica-check"], default="bench",
+    ap.add_argument("--mode", choices=["bench", "ncu", "ncu-stream", "ncu-stream-grid", "replica-check"],
+                    default="bench",
                     help="ncu: passes of the headline workload inside a cudaProfilerStart/Stop range; "
+                         "ncu-stream(-grid): 30 push/detect slides of it (window or grid engine) inside one; "
                          "replica-check: the multi-rank plumbing on host ranks (gloo), no GPU")
     return ap.parse_args()
 
@@ -365,9 +367,9 @@ def run_ours(args, world, rank, local):
 def measure_streaming(w, local, base, slides: int = 60):
     """RTOD's own per-slide loop through the public API: push S points from
     host memory, detect, read the IDs back (host wall clock per slide, after
-    10 untimed slides), with the streaming grid engine (the default of
-    push/detect) and with the window engine; the IDs must match the
-    whole-stream run. The device time of a slide comes from a second pass
+    10 untimed slides), with the window engine (the default of push/detect)
+    and with the streaming grid engine; the IDs must match the whole-stream
+    run. The device time of a slide comes from a second pass
     with per-detection stage times (CUDA events around the detection's
     launches). The native command line (C++ over the C ABI, no Python in the
     loop) runs the same loop on the whole stream."""
@@ -396,7 +398,7 @@ def measure_streaming(w, local, base, slides: int = 60):
         out[engine] = {"us_per_slide_wall": float(np.median(ts[10:])) * 1e6,
                        "us_per_slide_device": float(np.median(dev[10:])),
                        "engine": info["engine"], "grid_builds": info["builds"]}
-    out["us_per_slide_wall"] = out["grid"]["us_per_slide_wall"]
+    out["us_per_slide_wall"] = out["window"]["us_per_slide_wall"]
     out["native"] = native_streaming(w, local, base)
     return out
 
@@ -718,6 +720,31 @@ def run_ncu_case(args, local):
     print(json.dumps({"mode": "ncu", "slides": r.slides, "outliers": int(r.offsets[-1]), "tuning": tuning}))
 
 
+def run_ncu_stream(args, local, slides: int = 30, engine: str = "window"):
+    """Profiler pass of RTOD's per-slide loop on the headline workload
+    (push S points from host memory, detect): 10 slides outside the profiler
+    range, then `slides` slides inside it (cudaProfilerStart/Stop: run ncu
+    with --profile-from-start off)."""
+    import torch
+    from rtod_b200 import Detector
+    w = workload()
+    torch.cuda.set_device(local)
+    W, S = w.window, w.slide
+    with Detector(W, S, w.R, w.K, dim=w.dim, device=local, engine=engine) as det:
+        det.push(w.points[:W])
+        n_out = 0
+        for j in range(10 + slides):
+            if j == 10:
+                torch.cuda.synchronize()
+                torch.cuda.profiler.start()
+            det.push(w.points[W + j * S:W + (j + 1) * S])
+            n_out += len(det.detect())
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        info = det.stream_engine
+    print(json.dumps({"mode": "ncu-stream", "slides": slides, "outliers": n_out, "engine": info["engine"]}))
+
+
 def run_replica_check(world, rank):
     """The replica path of this file on host ranks (gloo): every rank detects
     the same slides of the small random walk with the oracle (the CPU
@@ -749,6 +776,9 @@ def main():
     world, rank, local = dist_env()
     if args.mode == "ncu":
         run_ncu_case(args, local)
+        return
+    if args.mode in ("ncu-stream", "ncu-stream-grid"):
+        run_ncu_stream(args, local, engine="grid" if args.mode == "ncu-stream-grid" else "window")
         return
     if args.mode == "replica-check":
         run_replica_check(world, rank)

@@ -109,9 +109,9 @@ typedef struct rtod_config {
                           (each bin of the cell grid keeps its window points as a FIFO
                           that a slide's expiry and insertion update in place, three
                           launches per slide) for dim <= 3, W <= 262144 and W/S <= 4096;
-                          RTOD_ENGINE_AUTO does the same unless the router is on, the
-                          pipeline is fused or a count mode is named; every other case
-                          runs the window engine. Results are identical. */
+                          every other case runs the window engine (measured as fast or
+                          faster per slide on the stock-like, sensor-like and Gaussian-
+                          mixture streams). Results are identical. */
   int32_t coord;       /* RTOD_COORD_F32 or RTOD_COORD_F64 */
   int32_t count;       /* RTOD_COUNT_*: window-engine count (push/detect, the multi-stream
                           API, rtod_run with the window engine) */
@@ -159,7 +159,10 @@ int rtod_create(const rtod_config* cfg, rtod_handle** out);
 /* Appends n points to the stream. The first push must be exactly W points
    (the initial window, src/ods/optixScan.cpp:1020-1034); every later push
    must be exactly S points (one slide, :1051-1064) and must be followed by
-   rtod_detect before the next push. */
+   rtod_detect before the next push. The caller may reuse pts at once. When
+   the last rtod_detect was called with times = NULL, a slide push also
+   launches the slide's detection on the handle's stream right behind the
+   copy, and the next rtod_detect only waits for it and delivers the IDs. */
 int rtod_push_slide(rtod_handle* h, const float* pts, int64_t n);
 
 /* rtod_push_slide for a handle created with coord = RTOD_COORD_F64: n * dim
@@ -171,7 +174,10 @@ int rtod_push_slide_f64(rtod_handle* h, const double* pts, int64_t n);
 /* Detects the outliers of the window produced by the last push and copies
    their sorted global indices to out_ids (host or device memory, room for
    cap entries); *n_out receives the count even when it exceeds cap (then
-   RTOD_ERR_CAPACITY is returned). times may be NULL. */
+   RTOD_ERR_CAPACITY is returned). times may be NULL; with times, the
+   detection launched by the push before it (see rtod_push_slide) reports its
+   copy and total times without the stage split, and the next push leaves the
+   launch to rtod_detect, so that per-stage times are measured again. */
 int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t* n_out, rtod_times* times);
 
 /* Runs a whole stream the way RTOD's detect_outlier does

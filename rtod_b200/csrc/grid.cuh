@@ -33,9 +33,11 @@
 //                  K points of one cell (cells of side R(1+2^-12)/n, n >= 2,
 //                  D <= 3: a cell's diagonal is below R) or when its sure
 //                  stencil cells do; all-outlier when its whole stencil holds
-//                  at most K points; otherwise its points are queued.
-//   k_grid_count   one warp per queued point: exact count over the runs of its
-//                  stencil bins, early exit past K; outliers set their
+//                  at most K points; otherwise its points are listed as count
+//                  parts of up to GRID_PART consecutive entries.
+//   k_grid_count   one warp per part: the group count of group.cuh over the
+//                  runs of the bin's stencil bins (candidates shared by the
+//                  part's points), early exit past K; outliers set their
 //                  window-offset bit.
 //   k_compact_one  bitset -> sorted global IDs in the mapped landing buffers,
 //                  end of the detection (kernels.cuh).
@@ -58,6 +60,9 @@ constexpr uint32_t GRID_MIN_CAP = 64;     // smallest capacity of a grown region
 constexpr uint32_t GRID_FRESH_CAP = 16;   // capacity of an empty bin's region at a build
 constexpr int GRID_INGEST_THREADS = 256;
 constexpr int GRID_COUNT_THREADS = 256;   // 8 warps, one tile of 32 bins each
+constexpr uint32_t GRID_PART = 64;        // points of a bin per listed count part (one warp each)
+constexpr int GRID_SLOT_BATCH = 8;        // stencil bins whose occupancy loads are in flight together
+constexpr int GRID_COPY_UNROLL = 4;       // entries per lane in flight when a region moves
 
 // Grid control block (device).
 struct GridCtl {
@@ -68,7 +73,7 @@ struct GridCtl {
   unsigned long long pool_top;  // pool slots handed out
   int32_t fail;        // the pool ran out: the grid must be rebuilt
   uint32_t max_occ;    // largest bin occupancy of the last counted window
-  uint32_t n_queue;    // points queued for an exact count (k_grid_classify)
+  uint32_t n_queue;    // count parts listed by k_grid_classify (up to GRID_PART points of a bin each)
   long long cmin[3];   // the window's cell-coordinate box (grid_purity)
   long long cmax[3];
 };
@@ -88,12 +93,13 @@ struct Grid {
   uint32_t pool;             // slots of the pool (row stride of px)
   uint32_t ovf_cap;          // room of the overflow and grow lists (S)
   uint32_t* grow;            // [ovf_cap] bins to grow
+  uint32_t* grow_to;         // [2 ovf_cap] their new regions: first pool slot, capacity
   uint32_t* ovf_bin;         // [ovf_cap]
   uint32_t* ovf_pos;         // [ovf_cap] entry number
   uint32_t* ovf_slot;        // [ovf_cap] ring slot
   void* ovf_x;               // [D][ovf_cap] coordinates
-  uint32_t* qpos;            // [W] queued points: pool slot of the point
-  uint32_t* qbin;            // [W] and its bin
+  uint32_t* qpos;            // [W] count parts: pool slot of the part's first point
+  uint32_t* qbin;            // [W] and its bin | points << 16
   long long* brange;         // [nslots][6] per slide block (block t at t % nslots):
                              // smallest then largest cell coordinate per hashed dimension
   int32_t nslots;            // W / S + 1
@@ -202,7 +208,11 @@ __device__ __forceinline__ void grid_expire(const Grid& g, bool valid, uint64_t 
 
 // Run by the last block of an ingest or insert launch (all threads), after
 // every other block's appends: grows the listed bins and places the overflow
-// entries. On pool exhaustion the grid is marked failed (DERR_GRID).
+// entries. Phases separated by block barriers, each a few dependent memory
+// round trips: new regions (a thread per bin), live entries moved (a warp
+// per bin, GRID_COPY_UNROLL entries per lane in flight), the bins' region
+// fields updated, overflow entries placed (4 per thread in flight). On pool
+// exhaustion nothing moves and the grid is marked failed (DERR_GRID).
 template <int D, typename T>
 __device__ void grid_fixup(const Grid& g, BatchState* bs) {
   GridCtl* ctl = g.ctl;
@@ -213,46 +223,14 @@ __device__ void grid_fixup(const Grid& g, BatchState* bs) {
   __shared__ int s_fail;
   if (threadIdx.x == 0) s_fail = 0;
   __syncthreads();
-  for (uint32_t gi = (uint32_t)wid; gi < n_grow; gi += (uint32_t)nw) {
+  for (uint32_t gi = threadIdx.x; gi < n_grow; gi += blockDim.x) {
     const uint32_t bin = g.grow[gi];
-    const uint32_t h = g.head[bin], t = g.tail[bin];
-    const uint32_t occ = t - h;
+    const uint32_t occ = g.tail[bin] - g.head[bin];
     const uint32_t nc = pow2_at_least(max(2u * occ, GRID_MIN_CAP));
-    unsigned long long nb64 = 0;
-    int ok = 1;
-    if (lane == 0) {
-      nb64 = atomicAdd(&ctl->pool_top, 2ull * nc);
-      ok = nb64 + 2ull * nc <= (unsigned long long)g.pool;
-      if (!ok) s_fail = 1;
-    }
-    const uint32_t nb = (uint32_t)__shfl_sync(0xffffffffu, nb64, 0);
-    ok = __shfl_sync(0xffffffffu, ok, 0);
-    if (!ok) continue;
-    const uint32_t oc = g.cap[bin], ob = g.base[bin];
-    // live entries from the old region (an overflowed entry reads a stale
-    // slot here and is rewritten from the overflow list below)
-    for (uint32_t e = h + (uint32_t)lane; e - h < occ; e += 32u) {
-      const uint32_t dst = nb + (e & (nc - 1u));
-      if (oc) {
-        const uint32_t src = ob + (e & (oc - 1u));
-#pragma unroll
-        for (int d = 0; d < D; ++d) {
-          T* row = grid_row<T>(g, d);
-          const T v = row[src];
-          row[dst] = v;
-          row[dst + nc] = v;
-        }
-        const uint32_t sl = g.pslot[src];
-        g.pslot[dst] = sl;
-        g.pslot[dst + nc] = sl;
-      }
-    }
-    __syncwarp();
-    if (lane == 0) {
-      g.base[bin] = nb;
-      g.cap[bin] = nc;
-      g.growflag[bin] = 0;
-    }
+    const unsigned long long nb = atomicAdd(&ctl->pool_top, 2ull * nc);
+    if (nb + 2ull * nc > (unsigned long long)g.pool) s_fail = 1;
+    g.grow_to[2 * gi] = (uint32_t)nb;
+    g.grow_to[2 * gi + 1] = nc;
   }
   __syncthreads();
   if (s_fail) {
@@ -262,19 +240,81 @@ __device__ void grid_fixup(const Grid& g, BatchState* bs) {
     }
     return;
   }
-  for (uint32_t o = threadIdx.x; o < n_ovf; o += blockDim.x) {
-    const uint32_t bin = g.ovf_bin[o], pos = g.ovf_pos[o];
-    const uint32_t c = g.cap[bin];
-    const uint32_t s0 = g.base[bin] + (pos & (c - 1u));
+  // live entries from the old regions (an overflowed entry reads a stale
+  // slot here and is rewritten from the overflow list below)
+  for (uint32_t gi = (uint32_t)wid; gi < n_grow; gi += (uint32_t)nw) {
+    const uint32_t bin = g.grow[gi];
+    const uint32_t oc = g.cap[bin];
+    if (!oc) continue;
+    const uint32_t nb = g.grow_to[2 * gi], nc = g.grow_to[2 * gi + 1];
+    const uint32_t ob = g.base[bin], h = g.head[bin], occ = g.tail[bin] - h;
+    for (uint32_t e0 = 0; e0 < occ; e0 += 32u * GRID_COPY_UNROLL) {
+      T v[GRID_COPY_UNROLL][D];
+      uint32_t sl[GRID_COPY_UNROLL];
 #pragma unroll
-    for (int d = 0; d < D; ++d) {
-      T* row = grid_row<T>(g, d);
-      const T v = static_cast<const T*>(g.ovf_x)[(size_t)d * g.ovf_cap + o];
-      row[s0] = v;
-      row[s0 + c] = v;
+      for (int u = 0; u < GRID_COPY_UNROLL; ++u) {
+        const uint32_t k = e0 + 32u * u + (uint32_t)lane;
+        const uint32_t src = ob + ((h + k) & (oc - 1u));
+#pragma unroll
+        for (int d = 0; d < D; ++d) v[u][d] = k < occ ? grid_row<T>(g, d)[src] : T(0);
+        sl[u] = k < occ ? g.pslot[src] : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < GRID_COPY_UNROLL; ++u) {
+        const uint32_t k = e0 + 32u * u + (uint32_t)lane;
+        if (k >= occ) continue;
+        const uint32_t dst = nb + ((h + k) & (nc - 1u));
+#pragma unroll
+        for (int d = 0; d < D; ++d) {
+          T* row = grid_row<T>(g, d);
+          row[dst] = v[u][d];
+          row[dst + nc] = v[u][d];
+        }
+        g.pslot[dst] = sl[u];
+        g.pslot[dst + nc] = sl[u];
+      }
     }
-    g.pslot[s0] = g.ovf_slot[o];
-    g.pslot[s0 + c] = g.ovf_slot[o];
+  }
+  __syncthreads();
+  for (uint32_t gi = threadIdx.x; gi < n_grow; gi += blockDim.x) {
+    const uint32_t bin = g.grow[gi];
+    g.base[bin] = g.grow_to[2 * gi];
+    g.cap[bin] = g.grow_to[2 * gi + 1];
+    g.growflag[bin] = 0;
+  }
+  __syncthreads();
+  for (uint32_t o0 = 0; o0 < n_ovf; o0 += 4u * blockDim.x) {
+    uint32_t bin[4], pos[4], sl[4], c[4], base[4];
+    T v[4][D];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t o = o0 + (uint32_t)u * blockDim.x + threadIdx.x;
+      const bool ok = o < n_ovf;
+      bin[u] = ok ? g.ovf_bin[o] : 0u;
+      pos[u] = ok ? g.ovf_pos[o] : 0u;
+      sl[u] = ok ? g.ovf_slot[o] : 0u;
+#pragma unroll
+      for (int d = 0; d < D; ++d) v[u][d] = ok ? static_cast<const T*>(g.ovf_x)[(size_t)d * g.ovf_cap + o] : T(0);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool ok = o0 + (uint32_t)u * blockDim.x + threadIdx.x < n_ovf;
+      c[u] = ok ? g.cap[bin[u]] : 0u;
+      base[u] = ok ? g.base[bin[u]] : 0u;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (o0 + (uint32_t)u * blockDim.x + threadIdx.x >= n_ovf) continue;
+      const uint32_t s0 = base[u] + (pos[u] & (c[u] - 1u));
+#pragma unroll
+      for (int d = 0; d < D; ++d) {
+        T* row = grid_row<T>(g, d);
+        row[s0] = v[u][d];
+        row[s0 + c[u]] = v[u][d];
+      }
+      g.pslot[s0] = sl[u];
+      g.pslot[s0 + c[u]] = sl[u];
+    }
   }
   if (threadIdx.x == 0) {
     ctl->n_grow = 0;
@@ -480,33 +520,12 @@ static __global__ void __launch_bounds__(256) k_grid_reset(Grid g) {
 }
 
 // ---------------------------------------------------------------------------
-// Stencil slot s of a bin: run of its live entries (start slot, length) and
-// whether its cell lies within R of every point of the centre cell (counted
-// without tests when the window is alias-free). Slots as in group.cuh:
-// offsets d in [-n, n]^h, bin + delta(d) mod NB.
-// ---------------------------------------------------------------------------
-template <int H>
-__device__ __forceinline__ void grid_slot(const Grid& g, uint32_t bin, int s, int slots, int n, bool can_sure,
-                                          uint32_t& rs, uint32_t& len, bool& sure) {
-  rs = 0;
-  len = 0;
-  sure = false;
-  if (s >= slots) return;
-  int d[3] = {0, 0, 0};
-  const uint32_t sb = (bin + (uint32_t)slot_cell<H>(s, n, d)) & NB_MASK;
-  sure = can_sure && slot_sure<H>(d, n);
-  const uint32_t sh = g.head[sb];
-  len = g.tail[sb] - sh;
-  rs = len ? g.base[sb] + (sh & (g.cap[sb] - 1u)) : 0u;
-}
-
-// ---------------------------------------------------------------------------
 // k_grid_classify: one lane per bin (tiles of 32 bins per warp). A bin is
 // decided without tests when it holds more than K points of one cell
-// (all-inlier), when its sure stencil cells hold more than K points
-// (all-inlier), or when its whole stencil holds at most K points
-// (all-outlier: marked here); the points of every other bin are queued for
-// an exact count. Empty bins drop their reference key.
+// (all-inlier), or, for short stencils, when its sure stencil cells hold more
+// than K points (all-inlier) or its whole stencil holds at most K points
+// (all-outlier: marked here); the points of every other bin are listed for an
+// exact count. Empty bins drop their reference key.
 // ---------------------------------------------------------------------------
 template <int D>
 __global__ void __launch_bounds__(GRID_COUNT_THREADS) k_grid_classify(Batch b, Grid g) {
@@ -523,6 +542,10 @@ __global__ void __launch_bounds__(GRID_COUNT_THREADS) k_grid_classify(Batch b, G
   const bool can_sure = jb.filter && pure && D <= 3;
   const int w = 2 * jb.n + 1;
   const int slots = H == 1 ? w : (H == 2 ? w * w : w * w * w);
+  // Short stencils (1-d, 2-d with one cell per R) are summed here, a lane per
+  // bin, to decide whole bins without a count; longer ones are left to the
+  // count's warp-wide pass over the stencil, which decides the same bins.
+  const bool sums = slots <= 2 * GRID_SLOT_BATCH;
   // An alias-free window's points all lie in its cell box: only the box's
   // bins are visited (in rows along the last hashed dimension, whose bins are
   // consecutive); otherwise every bin.
@@ -570,19 +593,38 @@ __global__ void __launch_bounds__(GRID_COUNT_THREADS) k_grid_classify(Batch b, G
         g.ref[bin] = EMPTY_KEY;
         g.mixed[bin] = 0;
       }
+    } else if (!(jb.filter && c > (uint32_t)jb.K && (pure || g.mixed[bin] == 0)) && !sums) {
+      queue = true;  // the group count takes the stencil sums, 32 bins per round
     } else if (!(jb.filter && c > (uint32_t)jb.K && (pure || g.mixed[bin] == 0))) {
+      // stencil occupancy, GRID_SLOT_BATCH bins' loads in flight at a time
       uint32_t given = 0, total = 0;
-      for (int s = 0; s < slots; ++s) {
-        int d[3] = {0, 0, 0};
-        const uint32_t sb = (bin + (uint32_t)slot_cell<H>(s, jb.n, d)) & NB_MASK;
-        const uint32_t len = g.tail[sb] - g.head[sb];
-        given += (can_sure && slot_sure<H>(d, jb.n)) ? len : 0u;
-        total += len;
+      for (int s0 = 0; s0 < slots; s0 += GRID_SLOT_BATCH) {
+        uint32_t hh[GRID_SLOT_BATCH], tt[GRID_SLOT_BATCH];
+        bool su[GRID_SLOT_BATCH];
+#pragma unroll
+        for (int e = 0; e < GRID_SLOT_BATCH; ++e) {
+          hh[e] = 0;
+          tt[e] = 0;
+          su[e] = false;
+          if (s0 + e < slots) {
+            int d[3] = {0, 0, 0};
+            const uint32_t sb = (bin + (uint32_t)slot_cell<H>(s0 + e, jb.n, d)) & NB_MASK;
+            su[e] = can_sure && slot_sure<H>(d, jb.n);
+            hh[e] = g.head[sb];
+            tt[e] = g.tail[sb];
+          }
+        }
+#pragma unroll
+        for (int e = 0; e < GRID_SLOT_BATCH; ++e) {
+          const uint32_t len = tt[e] - hh[e];
+          given += su[e] ? len : 0u;
+          total += len;
+        }
       }
-      const uint32_t own = g.base[bin] + (h & (g.cap[bin] - 1u));
       if (given > (uint32_t)jb.K) {
         // all inliers
       } else if (total <= (uint32_t)jb.K) {  // all outliers
+        const uint32_t own = g.base[bin] + (h & (g.cap[bin] - 1u));
         for (uint32_t i = 0; i < c; ++i) {
           const uint32_t sl = g.pslot[own + i];
           const uint32_t off = sl >= lo_mod ? sl - lo_mod : sl + Wu - lo_mod;
@@ -593,9 +635,10 @@ __global__ void __launch_bounds__(GRID_COUNT_THREADS) k_grid_classify(Batch b, G
         queue = true;
       }
     }
-    // one queue reservation per warp for the lanes' queued points
-    const uint32_t nq = queue ? c : 0u;
-    uint32_t inc = nq;
+    // the bin's points as count parts of up to GRID_PART points; one queue
+    // reservation per warp
+    const uint32_t np = queue ? (c + GRID_PART - 1u) / GRID_PART : 0u;
+    uint32_t inc = np;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
@@ -605,27 +648,22 @@ __global__ void __launch_bounds__(GRID_COUNT_THREADS) k_grid_classify(Batch b, G
     if (wtot) {
       uint32_t q0 = 0;
       if (lane == 31) q0 = atomicAdd(&g.ctl->n_queue, wtot);
-      q0 = __shfl_sync(0xffffffffu, q0, 31) + inc - nq;
-      const uint32_t own = queue ? g.base[bin] + (h & (g.cap[bin] - 1u)) : 0u;
-      // the warp writes each queued bin's entries together
-      unsigned todo = __ballot_sync(0xffffffffu, queue);
-      while (todo) {
-        const int ql = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const uint32_t qq0 = __shfl_sync(0xffffffffu, q0, ql), qown = __shfl_sync(0xffffffffu, own, ql);
-        const uint32_t qc = __shfl_sync(0xffffffffu, c, ql), qb = __shfl_sync(0xffffffffu, bin, ql);
-        for (uint32_t i = (uint32_t)lane; i < qc; i += 32u) {
-          g.qpos[qq0 + i] = qown + i;
-          g.qbin[qq0 + i] = qb;
+      q0 = __shfl_sync(0xffffffffu, q0, 31) + inc - np;
+      if (queue) {
+        const uint32_t own = g.base[bin] + (h & (g.cap[bin] - 1u));
+        for (uint32_t k = 0; k < np; ++k) {
+          g.qpos[q0 + k] = own + k * GRID_PART;
+          g.qbin[q0 + k] = bin | (min(GRID_PART, c - k * GRID_PART) << 16);
         }
+        queued += c;
       }
-      queued += wtot;
     }
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     occmax = max(occmax, __shfl_xor_sync(0xffffffffu, occmax, o));
     nout += __shfl_xor_sync(0xffffffffu, nout, o);
+    queued += __shfl_xor_sync(0xffffffffu, queued, o);
   }
   if (lane == 0) {
     if (nout) atomicAdd(&jb.ctr->n_out, nout);
@@ -635,25 +673,18 @@ __global__ void __launch_bounds__(GRID_COUNT_THREADS) k_grid_classify(Batch b, G
 }
 
 // ---------------------------------------------------------------------------
-// k_grid_count: exact count of each queued point, one warp per point (warps
-// striding over the queue), early exit once the count exceeds K. The
-// stencil's runs form one virtual candidate list (32 slots per round, sure
-// slots counted without tests first); each step tests 32 x CPL candidates
-// with one ballot per candidate row. The last block to finish rearms the
-// queue for the next slide.
+// k_grid_count: exact counts of the listed parts, one warp per part (warps
+// striding over the list). A part's points are consecutive entries of one
+// bin, so they share the bin's stencil: count_group (group.cuh) reads its
+// candidates (the live runs of the stencil bins, one virtual list) 32 x CPL
+// at a time into registers and tests every undecided point of the part
+// against them, early exit past K. The last block to finish rearms the list
+// for the next slide.
 // ---------------------------------------------------------------------------
-template <int D>
-struct GridCpl {
-  static constexpr int value = D == 1 ? 2 : 4;
-};
-
 template <int D, int PRED, typename T>
 __global__ void __launch_bounds__(GRID_COUNT_THREADS) k_grid_count(Batch b, Grid g) {
   pdl_trigger();
   pdl_wait();
-  constexpr int H = Hashed<D>::value;
-  constexpr int CPL = GridCpl<D>::value;
-  constexpr uint32_t STEP = 32 * CPL;
   if (*(volatile int32_t*)&g.ctl->fail) return;
   const Job& jb = b.jobs[0];
   const int lane = threadIdx.x & 31;
@@ -661,70 +692,24 @@ __global__ void __launch_bounds__(GRID_COUNT_THREADS) k_grid_count(Batch b, Grid
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   const uint32_t lo_mod = (uint32_t)(jb.ctr->lo % jb.W), Wu = (uint32_t)jb.W;
   const bool can_sure = jb.filter && g.ctl->pure != 0 && D <= 3;
-  const int w = 2 * jb.n + 1;
-  const int slots = H == 1 ? w : (H == 2 ? w * w : w * w * w);
-  const int rounds = (slots + 31) >> 5;
   const uint32_t nq = *(volatile uint32_t*)&g.ctl->n_queue;
   const T* px = static_cast<const T*>(g.px);
   int nout = 0;
   for (uint32_t q = warp; q < nq; q += nwarps) {
-    const uint32_t pos = g.qpos[q], bin = g.qbin[q];
-    T qx[D];
-#pragma unroll
-    for (int d = 0; d < D; ++d) qx[d] = px[(size_t)d * g.pool + pos];
-    // sure slots first
-    int cnt = 0;
-    for (int r = 0; r < rounds; ++r) {
-      uint32_t rs, len;
-      bool sure;
-      grid_slot<H>(g, bin, 32 * r + lane, slots, jb.n, can_sure, rs, len, sure);
-      cnt += (int)__reduce_add_sync(0xffffffffu, sure ? len : 0u);
-    }
-    for (int r = 0; r < rounds && cnt <= jb.K; ++r) {
-      uint32_t rs, len;
-      bool sure;
-      grid_slot<H>(g, bin, 32 * r + lane, slots, jb.n, can_sure, rs, len, sure);
-      if (sure) len = 0;
-      uint32_t inc = len;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += y;
-      }
-      const uint32_t off = inc - len;
-      const uint32_t ncand = __shfl_sync(0xffffffffu, inc, 31);
-      for (uint32_t c0 = 0; c0 < ncand && cnt <= jb.K; c0 += STEP) {
-        unsigned m = 0;
-#pragma unroll
-        for (int e = 0; e < CPL; ++e) {
-          const uint32_t v = c0 + 32 * e + (uint32_t)lane;
-          // lane holding v's run: the last lane whose offset is <= v
-          int sl = 0;
-#pragma unroll
-          for (int step = 16; step > 0; step >>= 1) {
-            const int cand = sl + step;
-            const uint32_t oc = __shfl_sync(0xffffffffu, off, cand & 31);
-            if (oc <= v) sl = cand;
-          }
-          const uint32_t base = __shfl_sync(0xffffffffu, rs, sl);
-          const uint32_t os = __shfl_sync(0xffffffffu, off, sl);
-          if (v < ncand) {
-            T cx[D];
-            const uint32_t cpos = base + (v - os);
-#pragma unroll
-            for (int d = 0; d < D; ++d) cx[d] = px[(size_t)d * g.pool + cpos];
-            m += is_nbr<D, PRED, T>(qx, cx, jb.R2f, jb.R, jb.R2) ? 1u : 0u;
-          }
-        }
-        cnt += (int)__reduce_add_sync(0xffffffffu, m);
-      }
-    }
-    if (cnt <= jb.K && lane == 0) {
-      const uint32_t sl = g.pslot[pos];
-      const uint32_t o = sl >= lo_mod ? sl - lo_mod : sl + Wu - lo_mod;
-      atomicOr(&jb.flags[o >> 5], 1u << (o & 31));
-      ++nout;
-    }
+    const uint32_t p = g.qpos[q], pb = g.qbin[q];
+    const GroupArgs ga{p, pb >> 16, pb & 0xffffu, jb.n, jb.K, jb.R2f, jb.R, jb.R2, (int64_t)g.pool, can_sure, nullptr};
+    nout += count_group<D, PRED, T>(
+        px, ga,
+        [&](uint32_t sb, uint32_t& rs, uint32_t& len) {
+          const uint32_t sh = g.head[sb];
+          len = g.tail[sb] - sh;
+          rs = len ? g.base[sb] + (sh & (g.cap[sb] - 1u)) : 0u;
+        },
+        [&](uint32_t pos) {
+          const uint32_t sl = g.pslot[pos];
+          const uint32_t o = sl >= lo_mod ? sl - lo_mod : sl + Wu - lo_mod;
+          atomicOr(&jb.flags[o >> 5], 1u << (o & 31));
+        });
   }
   if (lane == 0 && nout) atomicAdd(&jb.ctr->n_out, nout);
   if (grid_last_block(g.ctl)) {

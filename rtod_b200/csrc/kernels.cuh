@@ -1621,16 +1621,22 @@ static __global__ void __launch_bounds__(256) k_compact(Batch b) {
 // one block scan (CMP1_WPT words per thread), no look-back chain between
 // tiles. The block that finishes last ends the batch (finish_batch) and, for
 // a streaming detection, writes the IDs and the batch state into the mapped
-// page-locked landing buffers (k_run_out's work, folded in).
+// page-locked landing buffers (k_run_out's work, folded in). A thread's 8
+// bitset words are one 32-byte sector, read and cleared as two 16-byte
+// vectors; the job's IDs are gathered in shared memory (up to CMP1_SMEM_IDS)
+// and written out by consecutive threads: one thread's run of single 8-byte
+// stores held the block about 9 us on B200, the coalesced copy 2-3 us.
 // ---------------------------------------------------------------------------
 constexpr int CMP1_WPT = 8;
 constexpr int64_t COMPACT1_MAX = 1024 * 32 * CMP1_WPT;  // 262144 window offsets
+constexpr uint32_t CMP1_SMEM_IDS = 4096;
 
 static __global__ void __launch_bounds__(1024) k_compact_one(Batch b, int64_t* ids_host, int64_t ids_host_cap,
                                                              BatchState* mirror) {
   __shared__ uint32_t sm[33];
   __shared__ int64_t s_jobbase;
   __shared__ uint32_t s_last;
+  __shared__ int64_t s_ids[CMP1_SMEM_IDS];
   pdl_trigger();
   pdl_wait();
   const uint32_t job = blockIdx.x;
@@ -1639,10 +1645,7 @@ static __global__ void __launch_bounds__(1024) k_compact_one(Batch b, int64_t* i
   if (*(volatile int32_t*)&bs->err == DERR_GRID) {
     // the streaming grid could not take the slide and nothing was counted:
     // no batch end; the host rebuilds the grid and counts the window again
-    if (blockIdx.x == 0 && threadIdx.x == 0 && mirror) {
-      __threadfence_system();
-      *mirror = *bs;
-    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && mirror) *mirror = *bs;
     return;
   }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -1663,24 +1666,51 @@ static __global__ void __launch_bounds__(1024) k_compact_one(Batch b, int64_t* i
     const int64_t w0 = (int64_t)threadIdx.x * CMP1_WPT;
     uint32_t bits[CMP1_WPT];
     uint32_t cnt = 0;
+    if (w0 + CMP1_WPT <= nwords) {  // bitsets start 256-byte aligned
+      uint4* f4 = reinterpret_cast<uint4*>(jb.flags + w0);
+      const uint4 a = f4[0], c = f4[1];
+      bits[0] = a.x; bits[1] = a.y; bits[2] = a.z; bits[3] = a.w;
+      bits[4] = c.x; bits[5] = c.y; bits[6] = c.z; bits[7] = c.w;
+      if ((a.x | a.y | a.z | a.w | c.x | c.y | c.z | c.w) != 0u) {
+        f4[0] = make_uint4(0u, 0u, 0u, 0u);
+        f4[1] = make_uint4(0u, 0u, 0u, 0u);
+      }
+    } else {
 #pragma unroll
-    for (int e = 0; e < CMP1_WPT; ++e) {
-      bits[e] = w0 + e < nwords ? jb.flags[w0 + e] : 0u;
-      if (bits[e]) jb.flags[w0 + e] = 0;
-      cnt += __popc(bits[e]);
+      for (int e = 0; e < CMP1_WPT; ++e) {
+        bits[e] = w0 + e < nwords ? jb.flags[w0 + e] : 0u;
+        if (bits[e]) jb.flags[w0 + e] = 0;
+      }
     }
+#pragma unroll
+    for (int e = 0; e < CMP1_WPT; ++e) cnt += __popc(bits[e]);
     uint32_t total;
     const uint32_t ex = block_exclusive_scan(cnt, &total, sm);
-    int64_t o = s_jobbase + ex;
+    if (total <= CMP1_SMEM_IDS && s_jobbase + total <= b.out_cap) {
+      uint32_t k = ex;
 #pragma unroll
-    for (int e = 0; e < CMP1_WPT; ++e) {
-      uint32_t v = bits[e];
-      while (v) {
-        const int f = __ffs(v) - 1;
-        v &= v - 1;
-        if (o < b.out_cap) b.out_ids[o] = lo + (w0 + e) * 32 + f;
-        else set_err(bs, DERR_CAPACITY);
-        ++o;
+      for (int e = 0; e < CMP1_WPT; ++e) {
+        uint32_t v = bits[e];
+        while (v) {
+          const int f = __ffs(v) - 1;
+          v &= v - 1;
+          s_ids[k++] = lo + (w0 + e) * 32 + f;
+        }
+      }
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) b.out_ids[s_jobbase + i] = s_ids[i];
+    } else {
+      int64_t o = s_jobbase + ex;
+#pragma unroll
+      for (int e = 0; e < CMP1_WPT; ++e) {
+        uint32_t v = bits[e];
+        while (v) {
+          const int f = __ffs(v) - 1;
+          v &= v - 1;
+          if (o < b.out_cap) b.out_ids[o] = lo + (w0 + e) * 32 + f;
+          else set_err(bs, DERR_CAPACITY);
+          ++o;
+        }
       }
     }
   }
@@ -1698,10 +1728,10 @@ static __global__ void __launch_bounds__(1024) k_compact_one(Batch b, int64_t* i
       for (int64_t i = threadIdx.x; i < n; i += blockDim.x) ids_host[i] = b.out_ids[i];
     }
     __syncthreads();
-    if (mirror && threadIdx.x == 0) {
-      __threadfence_system();
-      *mirror = *bs;
-    }
+    // No system-scope fence: the host reads the landing buffers only after
+    // its stream wait, by which time the kernel's writes are visible (a
+    // fence here held the block for about 20 us on B200).
+    if (mirror && threadIdx.x == 0) *mirror = *bs;
   }
 }
 

@@ -322,6 +322,8 @@ struct rtod_handle {
   // Streaming (push/detect): a page-locked copy of the caller's slide, and
   // the mapped landing buffer of one window's IDs written by k_run_out.
   void* stage_host = nullptr;
+  void* slide_host = nullptr;      // mapped page-locked slide of a streaming push from host memory
+  void* slide_host_dev = nullptr;  // its device address, which the ingest kernels read in place
   int64_t* ids_host = nullptr;
   int64_t* ids_host_dev = nullptr;
   int64_t ids_host_cap = 0;
@@ -333,6 +335,8 @@ struct rtod_handle {
   int64_t slides_done = 0;
   bool pending = false;
   bool poisoned = false;
+  bool launched = false;   // the pending slide's detection is already on the stream (eager push)
+  bool eager = false;      // slide pushes launch their detection (the last rtod_detect asked for no times)
 
   cudaGraphExec_t graphs[2] = {nullptr, nullptr};  // without / with the router's training step
   int64_t graph_kernels[2] = {0, 0};
@@ -949,9 +953,9 @@ int check_device_error(rtod_handle* h, const BatchState& s);
 
 bool grid_wanted(const rtod_handle* h) {
   const rtod_config& c = h->cfg;
-  if (c.engine != RTOD_ENGINE_GRID &&
-      (c.engine != RTOD_ENGINE_AUTO || c.router || c.pipeline == RTOD_PIPELINE_FUSED || c.count != RTOD_COUNT_AUTO))
-    return false;
+  // only on request: the window engine's per-slide sort was measured as fast
+  // or faster on every benchmark stream
+  if (c.engine != RTOD_ENGINE_GRID) return false;
   return h->D <= 3 && h->W <= kGridMaxW && h->W / h->S <= kGridMaxBlocks;
 }
 
@@ -973,7 +977,7 @@ void free_grid(rtod_handle* h) {
   Grid& g = h->grid.g;
   free_grid_pool(h);
   dfree(g.ctl); dfree(g.head); dfree(g.tail); dfree(g.base); dfree(g.cap); dfree(g.ref); dfree(g.mixed);
-  dfree(g.growflag); dfree(g.grow); dfree(g.ovf_bin); dfree(g.ovf_pos); dfree(g.ovf_slot); dfree(g.ovf_x);
+  dfree(g.growflag); dfree(g.grow); dfree(g.grow_to); dfree(g.ovf_bin); dfree(g.ovf_pos); dfree(g.ovf_slot); dfree(g.ovf_x);
   dfree(g.brange); dfree(g.qpos); dfree(g.qbin);
   h->device_bytes -= h->grid.bytes;
   h->grid.bytes = 0;
@@ -991,7 +995,7 @@ int ensure_grid(rtod_handle* h, uint64_t pool) {
     g.nslots = (int32_t)(h->W / h->S + 1);
     bool ok = !dalloc(&g.ctl, 1, &n) && !dalloc(&g.head, NB, &n) && !dalloc(&g.tail, NB, &n) &&
               !dalloc(&g.base, NB, &n) && !dalloc(&g.cap, NB, &n) && !dalloc(&g.ref, NB, &n) &&
-              !dalloc(&g.mixed, NB, &n) && !dalloc(&g.growflag, NB, &n) && !dalloc(&g.grow, S, &n) &&
+              !dalloc(&g.mixed, NB, &n) && !dalloc(&g.growflag, NB, &n) && !dalloc(&g.grow, S, &n) && !dalloc(&g.grow_to, 2 * S, &n) &&
               !dalloc(&g.ovf_bin, S, &n) && !dalloc(&g.ovf_pos, S, &n) && !dalloc(&g.ovf_slot, S, &n) &&
               !dalloc((unsigned char**)&g.ovf_x, S * (size_t)(h->D * h->esz), &n) &&
               !dalloc(&g.brange, (size_t)g.nslots * 6, &n) && !dalloc(&g.qpos, (size_t)h->W, &n) &&
@@ -1194,6 +1198,7 @@ int reset_state(rtod_handle* h) {
   h->n_pushed = 0;
   h->slides_done = 0;
   h->pending = false;
+  h->launched = false;
   h->poisoned = false;
   h->mode = MODE_NONE;
   // the next first push builds the grid again (or retries it, when no pool held it)
@@ -1577,6 +1582,8 @@ void free_all(rtod_handle* h) {
   h->bs_mirror = h->bs_mirror_dev = nullptr;
   if (h->stage_host) cudaFreeHost(h->stage_host);
   h->stage_host = nullptr;
+  if (h->slide_host) cudaFreeHost(h->slide_host);
+  h->slide_host = h->slide_host_dev = nullptr;
   if (h->ids_host) cudaFreeHost(h->ids_host);
   h->ids_host = h->ids_host_dev = nullptr;
   h->ids_host_cap = 0;
@@ -2036,6 +2043,19 @@ int check_coord(const rtod_handle* h, bool f64) {
   return RTOD_OK;
 }
 
+// Points the streaming job's slide source (Job::stage, read by the ingest
+// kernels) at `stage`: the mapped page-locked slide of a host push, or the
+// device staging buffer. The job table is read by the kernels at run time,
+// so captured graphs stay valid.
+int set_ring_stage(rtod_handle* h, const void* stage) {
+  if (h->tab_host.empty() || h->tab_host[0].stage == stage) return RTOD_OK;
+  h->tab_host[0].stage = stage;
+  CU(cudaMemcpyAsync(reinterpret_cast<unsigned char*>(h->jobs_dev) + offsetof(Job, stage), &h->tab_host[0].stage,
+                     sizeof(void*), cudaMemcpyHostToDevice, h->stream));
+  CU(cudaStreamSynchronize(h->stream));  // the source lives in tab_host, which configure may replace
+  return RTOD_OK;
+}
+
 int push_impl(rtod_handle* h, const void* pts, int64_t n, bool f64) {
   if (!h || !pts) return fail(RTOD_ERR_ARG, "null argument");
   if (int r = check_coord(h, f64)) return r;
@@ -2050,18 +2070,29 @@ int push_impl(rtod_handle* h, const void* pts, int64_t n, bool f64) {
     if (n != S) return fail(RTOD_ERR_STATE, "a slide push must hold exactly S=%lld points", (long long)S);
   }
   const size_t bytes = (size_t)(n * D * h->esz);
-  const void* src = pts;
   if (h->n_pushed > 0 && !is_device_ptr(pts)) {
-    // A slide from host memory: copied on the host into a page-locked buffer
-    // (the caller may reuse its buffer at once), then one asynchronous DMA.
-    // The previous slide's DMA is done: every detection ends with a wait.
-    if (!h->stage_host) CU(cudaMallocHost(&h->stage_host, (size_t)(S * D * h->esz)));
-    std::memcpy(h->stage_host, pts, bytes);
-    src = h->stage_host;
+    // A slide from host memory: copied on the host into a mapped page-locked
+    // buffer (the caller may reuse its buffer at once) that the detection's
+    // ingest kernel reads in place over the bus: no copy operation, whose
+    // completion the first kernel would wait for. The previous detection has
+    // finished with the buffer: every detection ends with a wait.
+    if (!h->slide_host) {
+      CU(cudaHostAlloc(&h->slide_host, (size_t)(S * D * h->esz), cudaHostAllocMapped));
+      CU(cudaHostGetDevicePointer(&h->slide_host_dev, h->slide_host, 0));
+    }
+    std::memcpy(h->slide_host, pts, bytes);
+    if (int r = set_ring_stage(h, h->slide_host_dev)) return r;
+    CU(cudaEventRecord(h->ev[4], h->stream));
+    CU(cudaEventRecord(h->ev[5], h->stream));
+  } else {
+    if (h->n_pushed > 0)
+      if (int r = set_ring_stage(h, h->staging)) return r;
+    CU(cudaEventRecord(h->ev[4], h->stream));
+    CU(cudaMemcpyAsync(h->staging, pts, bytes, cudaMemcpyDefault, h->stream));
+    CU(cudaEventRecord(h->ev[5], h->stream));
+    // a slide in device memory may be overwritten once the push returns
+    if (h->n_pushed > 0) CU(cudaEventSynchronize(h->ev[5]));
   }
-  CU(cudaEventRecord(h->ev[4], h->stream));
-  CU(cudaMemcpyAsync(h->staging, src, bytes, cudaMemcpyDefault, h->stream));
-  CU(cudaEventRecord(h->ev[5], h->stream));
   if (h->n_pushed == 0) {
     int r = configure(h, MODE_RING, 1, S, nullptr);  // first detected window: [S, W + S)
     if (r) return r;
@@ -2077,6 +2108,14 @@ int push_impl(rtod_handle* h, const void* pts, int64_t n, bool f64) {
     if (h->grid.on && (r = grid_build(h, 0))) return r;
   } else {
     h->pending = true;
+    if (h->eager) {
+      // the detection follows the copy on the stream at once; rtod_detect waits for it
+      if (int r = ensure_detect_out(h)) return r;
+      CU(cudaEventRecord(h->ev[0], h->stream));
+      if (int r = run_batch(h, make_batch(h, 1, h->ids_cap), true)) return r;
+      CU(cudaEventRecord(h->ev[7], h->stream));
+      h->launched = true;
+    }
   }
   h->n_pushed += n;
   return RTOD_OK;
@@ -2098,13 +2137,20 @@ RTOD_API int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t*
   const Batch b = make_batch(h, 1, h->ids_cap);
   cudaEvent_t kev[7];
   EventSet es;
-  if (times) {
-    for (auto& e : kev) e = es.make();
-    CU(cudaEventRecord(h->ev[0], h->stream));
+  const bool split = times && !h->launched;  // stage events need the detection launched here
+  int r = RTOD_OK;
+  if (!h->launched) {
+    if (split) {
+      for (auto& e : kev) e = es.make();
+      CU(cudaEventRecord(h->ev[0], h->stream));
+    }
+    r = split ? launch_batch(h, b, true, kev) : run_batch(h, b, true);
+    if (r) return r;
+    if (split) CU(cudaEventRecord(h->ev[7], h->stream));
   }
-  int r = times ? launch_batch(h, b, true, kev) : run_batch(h, b, true);
-  if (r) return r;
-  if (times) CU(cudaEventRecord(h->ev[7], h->stream));
+  const bool was_launched = h->launched;
+  h->launched = false;
+  h->eager = times == nullptr;
   // The IDs and the batch state arrive in the mapped landing buffers
   // (k_run_out, the graph's last kernel): one wait.
   CU(cudaStreamSynchronize(h->stream));
@@ -2134,10 +2180,12 @@ RTOD_API int rtod_detect(rtod_handle* h, int64_t* out_ids, int64_t cap, int64_t*
   if (times) {
     std::memset(times, 0, sizeof *times);
     times->copy_new_points_h2d = elapsed(h->ev[4], h->ev[5]);
-    times->prepare_cell = elapsed(h->ev[0], kev[1]);   // ring update + occupancy
-    times->build_bvh = elapsed(kev[1], kev[3]);       // scan + scatter
-    times->detect_outlier = elapsed(kev[3], kev[5]);  // count + compact
-    times->copy_outlier_d2h = elapsed(kev[6], h->ev[7]);  // after the compaction's delivery
+    if (!was_launched) {
+      times->prepare_cell = elapsed(h->ev[0], kev[1]);   // ring update + occupancy
+      times->build_bvh = elapsed(kev[1], kev[3]);       // scan + scatter
+      times->detect_outlier = elapsed(kev[3], kev[5]);  // count + compact
+      times->copy_outlier_d2h = elapsed(kev[6], h->ev[7]);  // after the compaction's delivery
+    }
     times->total = times->copy_new_points_h2d + elapsed(h->ev[0], h->ev[7]);
     times->undetermined_per_slide = (double)s.undet_total;
     times->slides = 1;

@@ -71,10 +71,10 @@ def test_grid_double_storage_matches_golden(rtod, path):
     assert_slides(got, [ids[off[j]:off[j + 1]] for j in range(len(off) - 1)])
 
 
-def test_grid_is_the_default_where_it_applies(rtod):
-    cases = [(dict(), 1, "grid"), (dict(), 3, "grid"), (dict(router=True), 1, "window"),
-             (dict(pipeline="fused"), 1, "window"), (dict(count="point"), 1, "window"),
-             (dict(engine="window"), 1, "window"), (dict(engine="span"), 1, "window"), (dict(), 8, "window"),
+def test_grid_runs_where_requested_and_applicable(rtod):
+    cases = [(dict(), 1, "window"), (dict(), 3, "window"), (dict(engine="grid"), 1, "grid"),
+             (dict(engine="grid"), 3, "grid"), (dict(engine="grid"), 8, "window"),
+             (dict(engine="window"), 1, "window"), (dict(engine="span"), 1, "window"),
              (dict(engine="grid", router=True), 1, "grid")]
     for kw, dim, want in cases:
         with rtod.Detector(2000, 100, 0.5, 10, dim=dim, **kw) as det:
@@ -87,7 +87,7 @@ def test_grid_stock_like_full_stream(rtod, oracle_mod):
     from rtod_b200 import datagen
     w = datagen.stock_like()
     want = expect(oracle_mod, w.points, w.window, w.slide, w.R, w.K, w.slides)
-    with rtod.Detector(w.window, w.slide, w.R, w.K) as det:
+    with rtod.Detector(w.window, w.slide, w.R, w.K, engine="grid") as det:
         got = stream(det, w.points, w.window, w.slide, w.slides)
         info = det.stream_engine
         assert info["engine"] == "grid" and info["builds"] == 1 and info["max_occ"] > 0
@@ -101,7 +101,7 @@ def test_grid_sensor_like(rtod, oracle_mod, pred):
     from rtod_b200 import datagen
     w = datagen.sensor_like()
     want = expect(oracle_mod, w.points, w.window, w.slide, w.R, w.K, 300, pred)
-    with rtod.Detector(w.window, w.slide, w.R, w.K, dim=3, pred=pred) as det:
+    with rtod.Detector(w.window, w.slide, w.R, w.K, dim=3, pred=pred, engine="grid") as det:
         got = stream(det, w.points, w.window, w.slide, 300)
         assert det.stream_engine["engine"] == "grid"
     assert_slides(got, want)
@@ -114,7 +114,7 @@ def test_grid_dense_bins(rtod, oracle_mod, K):
     from rtod_b200 import datagen
     w = datagen.gaussian_like(K)
     want = expect(oracle_mod, w.points, w.window, w.slide, w.R, w.K, 40)
-    with rtod.Detector(w.window, w.slide, w.R, w.K) as det:
+    with rtod.Detector(w.window, w.slide, w.R, w.K, engine="grid") as det:
         got = stream(det, w.points, w.window, w.slide, 40)
         assert det.stream_engine["max_occ"] > 1000
     assert_slides(got, want)
@@ -129,7 +129,7 @@ def test_grid_rebuilds_when_its_pool_runs_out(rtod, oracle_mod, pool):
     pts = datagen.random_walk(40_000, 0.3, seed=11, jump_frac=0.01)
     W, S, R, K, slides = 4000, 200, 0.4, 12, 180
     want = expect(oracle_mod, pts, W, S, R, K, slides)
-    with rtod.Detector(W, S, R, K, cells_per_r=3) as det:
+    with rtod.Detector(W, S, R, K, cells_per_r=3, engine="grid") as det:
         det.set_grid_pool(pool)
         got = stream(det, pts, W, S, slides)
         info = det.stream_engine
@@ -147,7 +147,7 @@ def test_grid_aliased_bins_1d(rtod, oracle_mod):
     pts = (base[rng.integers(0, 300, size=30_000)] + rng.normal(0, 2e-3, size=30_000)).astype(np.float32)
     W, S, R, K, slides = 6000, 300, 2e-3, 8, 60
     want = expect(oracle_mod, pts, W, S, R, K, slides)
-    with rtod.Detector(W, S, R, K) as det:
+    with rtod.Detector(W, S, R, K, engine="grid") as det:
         got = stream(det, pts, W, S, slides)
     assert_slides(got, want)
 
@@ -159,7 +159,7 @@ def test_grid_matches_window_engine_and_run(rtod):
     pts = datagen.random_walk(60_000, 0.1, seed=12, jump_frac=0.005, dim=2)
     W, S, R, K = 10_000, 500, 0.3, 25
     slides = (len(pts) - W) // S
-    with rtod.Detector(W, S, R, K, dim=2) as det:
+    with rtod.Detector(W, S, R, K, dim=2, engine="grid") as det:
         grid = stream(det, pts, W, S, slides)
     with rtod.Detector(W, S, R, K, dim=2, engine="window") as det:
         win = stream(det, pts, W, S, slides)
@@ -175,7 +175,7 @@ def test_grid_k_edges(rtod, oracle_mod, K):
     pts = datagen.random_walk(12_000, 0.1, seed=13, jump_frac=0.01)
     W, S, R, slides = 4000, 400, 0.2, 20
     want = expect(oracle_mod, pts, W, S, R, K, slides)
-    with rtod.Detector(W, S, R, K) as det:
+    with rtod.Detector(W, S, R, K, engine="grid") as det:
         got = stream(det, pts, W, S, slides)
     assert_slides(got, want)
 
@@ -187,7 +187,7 @@ def test_grid_input_error_then_reset(rtod, oracle_mod):
     pts = datagen.random_walk(8_000, 0.1, seed=14, jump_frac=0.01)
     W, S, R, K, slides = 2000, 200, 0.3, 10, 30
     want = expect(oracle_mod, pts, W, S, R, K, slides)
-    with rtod.Detector(W, S, R, K) as det:
+    with rtod.Detector(W, S, R, K, engine="grid") as det:
         det.push(pts[:W])
         bad = pts[W:W + S].copy()
         bad[7] = np.nan
