@@ -54,10 +54,13 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-stream multi-stream measurement")
-    ap.add_argument("--mode", choices=["bench", "ncu", "ncu-stream", "ncu-stream-grid", "replica-check"],
+    ap.add_argument("--mode", choices=["bench", "ncu", "ncu-stream", "ncu-stream-grid", "ncu-batched",
+                                       "replica-check"],
                     default="bench",
                     help="ncu: passes of the headline workload inside a cudaProfilerStart/Stop range; "
                          "ncu-stream(-grid): 30 push/detect slides of it (window or grid engine) inside one; "
+                         "ncu-batched: 2 multi-stream steps of the 8-d streams of the 64-stream workload "
+                         "inside one; "
                          "replica-check: the multi-rank plumbing on host ranks (gloo), no GPU")
     return ap.parse_args()
 
@@ -745,6 +748,33 @@ def run_ncu_stream(args, local, slides: int = 30, engine: str = "window"):
     print(json.dumps({"mode": "ncu-stream", "slides": slides, "outliers": n_out, "engine": info["engine"]}))
 
 
+def run_ncu_batched(args, local, steps: int = 2):
+    """Profiler pass of the 8-d streams of the 64-stream workload (26
+    streams, W from 5k to 169k, default settings: group counts): two
+    multi-stream steps outside the profiler range, then `steps` steps inside
+    it (cudaProfilerStart/Stop: run ncu with --profile-from-start off)."""
+    import torch
+    from rtod_b200 import BatchDetector, datagen
+    d8 = [s for s in datagen.batched_streams(slides=2 + steps) if s.dim == 8]
+    cfg = [dict(window=s.window, slide=s.slide, R=s.R, K=s.K, dim=s.dim) for s in d8]
+    n_out = 0
+    with BatchDetector(cfg, device=local) as bd:
+        for i, s in enumerate(d8):
+            bd.push(i, s.points[:s.window])
+        for j in range(2 + steps):
+            if j == 2:
+                torch.cuda.synchronize()
+                torch.cuda.profiler.start()
+            for i, s in enumerate(d8):
+                bd.push(i, s.points[s.window + j * s.slide:s.window + (j + 1) * s.slide])
+            n_out += sum(len(o) for o in bd.step())
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        tuning = bd.tuning
+    print(json.dumps({"mode": "ncu-batched", "streams": len(d8), "steps": steps, "outliers": n_out,
+                      "tuning": tuning}))
+
+
 def run_replica_check(world, rank):
     """The replica path of this file on host ranks (gloo): every rank detects
     the same slides of the small random walk with the oracle (the CPU
@@ -779,6 +809,9 @@ def main():
         return
     if args.mode in ("ncu-stream", "ncu-stream-grid"):
         run_ncu_stream(args, local, engine="grid" if args.mode == "ncu-stream-grid" else "window")
+        return
+    if args.mode == "ncu-batched":
+        run_ncu_batched(args, local)
         return
     if args.mode == "replica-check":
         run_replica_check(world, rank)

@@ -214,6 +214,17 @@ __device__ __forceinline__ int count_group_ex(const T* sx, const GroupArgs& a, R
       for (int d = 0; d < D; ++d) cx[e][d] = cv[e] ? sx[(int64_t)d * a.Wp + c] : T(0);
     }
     tests += (unsigned long long)__popc(live) * min(CHUNK, ncand - c0);
+    // Above 3 dimensions the FP32 test dominates: candidates in pairs for
+    // the paired FP32 instructions (half the arithmetic instructions, the
+    // same sums bit for bit).
+    constexpr bool PAIRED = PRED == 0 && D > 3 && CPL % 2 == 0 && sizeof(T) == sizeof(float);
+    unsigned long long cp[PAIRED ? CPL / 2 : 1][PAIRED ? D : 1];
+    if constexpr (PAIRED) {
+#pragma unroll
+      for (int e = 0; e < CPL / 2; ++e)
+#pragma unroll
+        for (int d = 0; d < D; ++d) cp[e][d] = f2_pack((float)cx[2 * e][d], (float)cx[2 * e + 1][d]);
+    }
     unsigned todo = live;
     while (todo) {
       const int qq = __ffs(todo) - 1;
@@ -222,8 +233,20 @@ __device__ __forceinline__ int count_group_ex(const T* sx, const GroupArgs& a, R
 #pragma unroll
       for (int d = 0; d < D; ++d) y[d] = __shfl_sync(0xffffffffu, qx[d], qq);
       unsigned m = 0;
+      if constexpr (PAIRED) {
+        unsigned long long y2[D];
 #pragma unroll
-      for (int e = 0; e < CPL; ++e) m += (cv[e] && is_nbr<D, PRED, T>(y, cx[e], a.R2f, a.R, a.R2)) ? 1u : 0u;
+        for (int d = 0; d < D; ++d) y2[d] = f2_pack((float)y[d], (float)y[d]);
+#pragma unroll
+        for (int e = 0; e < CPL / 2; ++e) {
+          bool n0, n1;
+          is_nbr_f32x2<D>(y2, cp[e], a.R2f, n0, n1);
+          m += (cv[2 * e] && n0 ? 1u : 0u) + (cv[2 * e + 1] && n1 ? 1u : 0u);
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < CPL; ++e) m += (cv[e] && is_nbr<D, PRED, T>(y, cx[e], a.R2f, a.R, a.R2)) ? 1u : 0u;
+      }
       const unsigned tot = __reduce_add_sync(0xffffffffu, m);
       if (lane == qq) cnt += (int)tot;
     }

@@ -94,6 +94,7 @@ struct BatchState {
   int32_t err;          // DERR_*
   uint32_t done;        // finished blocks of the running batch's last kernel
   unsigned long long pair_tests;  // distance tests made by group counts so far
+  uint32_t count_ticket;  // next entry of the batch-wide count list (k_count), reset by the batch end
 };
 
 // Span engine counters (device), one per handle, and the per-bin arrays
@@ -293,6 +294,36 @@ __device__ __forceinline__ bool is_nbr(const T* q, const T* c, float R2f, double
       return s < R2;
     }
   }
+}
+
+// The FP32 predicate (PRED 0) for two candidates at once, with sm_100's
+// paired single-precision instructions: each half of sub/mul/add.rn.f32x2 is
+// the IEEE single-precision operation rounded to nearest on its own (no
+// contraction: the instructions are explicit), so each half's sum is
+// bit-identical to is_nbr<D, 0> on that candidate. q2[i] holds the query's
+// coordinate i twice; c2[i] holds coordinate i of the two candidates.
+__device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+
+template <int D>
+__device__ __forceinline__ void is_nbr_f32x2(const unsigned long long* q2, const unsigned long long* c2, float R2f,
+                                             bool& n0, bool& n1) {
+  unsigned long long s = 0;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    unsigned long long dx, t;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(dx) : "l"(q2[i]), "l"(c2[i]));
+    asm("mul.rn.f32x2 %0, %1, %1;" : "=l"(t) : "l"(dx));
+    if (i == 0) s = t;
+    else asm("add.rn.f32x2 %0, %1, %2;" : "=l"(s) : "l"(s), "l"(t));
+  }
+  float s0, s1;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(s0), "=f"(s1) : "l"(s));
+  n0 = s0 <= R2f;
+  n1 = s1 <= R2f;
 }
 
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -1324,9 +1355,63 @@ __device__ __forceinline__ void reset_bins(const Job& jb, VB v) {
 }
 
 // ---------------------------------------------------------------------------
+// Batch-wide count list. The count work of every job of a launch (parts of
+// bins in group mode, runs of queued points otherwise) forms one list,
+// job after job, that warps take entry by entry from BatchState::count_ticket.
+// Every warp of the launch keeps working while any job has work left: a
+// job with many entries (a long or dense window among short ones) is not
+// left to the blocks that the grid assigns to it alone.
+// ---------------------------------------------------------------------------
+constexpr int BATCH_JOBS_MAX = 256;  // jobs per launch (the host's limit is checked against it)
+constexpr uint32_t COUNT_RUN = 16;   // queued points per entry of a point-count list
+
+// s_pre[j] = entries of jobs 0..j-1 (inactive jobs hold none); returns the
+// total. Every thread of the block calls it.
+template <class Entries>
+__device__ __forceinline__ uint32_t count_list_prefix(const Batch& b, uint32_t* s_pre, uint32_t* s_scan,
+                                                      Entries entries) {
+  const int nj = b.njobs;
+  const int per = (nj + (int)blockDim.x - 1) / (int)blockDim.x;
+  const int j0 = min(nj, (int)threadIdx.x * per), j1 = min(nj, j0 + per);
+  uint32_t mine = 0;
+  for (int j = j0; j < j1; ++j)
+    if (job_active(b, j)) mine += entries(b.jobs[j]);
+  uint32_t total;
+  uint32_t ex = block_exclusive_scan(mine, &total, s_scan);
+  for (int j = j0; j < j1; ++j) {
+    s_pre[j] = ex;
+    if (job_active(b, j)) ex += entries(b.jobs[j]);
+  }
+  __syncthreads();
+  return total;
+}
+
+// The job of list entry t < total: the last j with s_pre[j] <= t (jobs
+// without entries repeat their successor's offset and are skipped).
+__device__ __forceinline__ int count_list_job(const uint32_t* s_pre, int nj, uint32_t t) {
+  int lo = 0, hi = nj;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (s_pre[mid] <= t) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Next list entry for the calling warp (the same on every lane).
+__device__ __forceinline__ uint32_t count_list_take(BatchState* bs) {
+  uint32_t t = 0;
+  if ((threadIdx.x & 31) == 0) t = atomicAdd(&bs->count_ticket, 1u);
+  return __shfl_sync(0xffffffffu, t, 0);
+}
+
+// ---------------------------------------------------------------------------
 // k_count: the exact count always decides: outlier iff count <= K.
-//   plain (ROUTE = false): one warp per queued point, warps striding over
-//     the queue, stencil rows in order.
+//   plain (ROUTE = false): one warp per queued point, stencil rows in order;
+//     a single job's warps stride over its queue, the jobs of a multi-job
+//     launch share the batch-wide list in runs of COUNT_RUN points.
+//   group mode: one warp per listed part of a bin, parts taken from the
+//     batch-wide list.
 //   routed: early-exit queue as above; full-sweep queue one lane per point,
 //     32 points per warp, each lane sweeping its own (short) candidate list;
 //     every counted point becomes a training sample of the router.
@@ -1334,7 +1419,66 @@ __device__ __forceinline__ void reset_bins(const Job& jb, VB v) {
 template <int D, int PRED, bool ROUTE, typename T, bool GROUP = false>
 __device__ __forceinline__ void count_body(const Batch& b, VB v) {
   __shared__ SampleBuf sb;
-  if (!job_active(b, v.y)) return;
+  const bool home = job_active(b, v.y);
+  if constexpr (GROUP || !ROUTE) {
+    if (GROUP || b.njobs > 1) {
+      // the batch-wide list: this block's share of its own job's resets,
+      // then entries of any job until the list runs out
+      __shared__ uint32_t s_pre[BATCH_JOBS_MAX];
+      __shared__ uint32_t s_scan[33];
+      if (home) reset_bins(b.jobs[v.y], v);
+      const int lane = threadIdx.x & 31;
+      if constexpr (GROUP) {
+        // one warp per listed part of a bin: its points share the stencil (count_group)
+        constexpr int H = Hashed<D>::value;
+        const uint32_t total =
+            count_list_prefix(b, s_pre, s_scan, [](const Job& j) { return (uint32_t)j.ctr->n_groups; });
+        for (;;) {
+          const uint32_t t = count_list_take(b.bs);
+          if (t >= total) break;
+          const int j = count_list_job(s_pre, b.njobs, t);
+          const Job& J = b.jobs[j];
+          const uint32_t p = J.queue[t - s_pre[j]];
+          const uint32_t bin = bin_of_key(J.s_ckey[p], H);
+          const uint32_t nq = min((uint32_t)J.gpts, J.bin_start[bin + 1] - p);
+          const GroupArgs ga{p,   nq,   bin,  J.n,  J.K, J.R2f, J.R, J.R2, J.Wp, J.ctr->pure && D <= 3,
+                             &b.bs->pair_tests};
+          const int nout = count_group<D, PRED, T>(
+              static_cast<const T*>(J.s_x), ga,
+              [&](uint32_t sb2, uint32_t& rs, uint32_t& len) {
+                rs = J.bin_start[sb2];
+                len = J.bin_start[sb2 + 1] - rs;
+              },
+              [&](uint32_t pos) {
+                const uint32_t i = J.s_off[pos];
+                atomicOr(&J.flags[i >> 5], 1u << (i & 31));
+              });
+          if (lane == 0 && nout) atomicAdd(&J.ctr->n_out, nout);
+        }
+      } else {
+        const uint32_t total = count_list_prefix(b, s_pre, s_scan, [](const Job& j) {
+          return ((uint32_t)j.ctr->n_undet + COUNT_RUN - 1) / COUNT_RUN;
+        });
+        for (;;) {
+          const uint32_t t = count_list_take(b.bs);
+          if (t >= total) break;
+          const int j = count_list_job(s_pre, b.njobs, t);
+          const Job& J = b.jobs[j];
+          const int64_t lo = J.ctr->lo;
+          const uint32_t q0 = (t - s_pre[j]) * COUNT_RUN;
+          const uint32_t q1 = min((uint32_t)J.ctr->n_undet, q0 + COUNT_RUN);
+          for (uint32_t q = q0; q < q1; ++q) {
+            const uint32_t pos = J.queue[q];
+            int cnt;
+            const bool inlier = count_query<D, PRED, T>(J, pos, cnt);
+            if (lane == 0) record_count(J, lo, pos, inlier, cnt);
+          }
+        }
+      }
+      return;
+    }
+  }
+  if (!home) return;
   const Job& jb = b.jobs[v.y];
   if (ROUTE && threadIdx.x == 0) {
     sb.n = 0;
@@ -1346,31 +1490,6 @@ __device__ __forceinline__ void count_body(const Batch& b, VB v) {
   const int64_t lo = jb.ctr->lo;
   const int64_t warp = ((int64_t)v.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)v.gx * blockDim.x) >> 5;
-  if constexpr (GROUP) {
-    // one warp per listed part of a bin: its points share the stencil (count_group)
-    constexpr int H = Hashed<D>::value;
-    const int64_t ng = jb.ctr->n_groups;
-    const bool can_sure = jb.ctr->pure && D <= 3;
-    int nout = 0;
-    for (int64_t g = warp; g < ng; g += nwarps) {
-      const uint32_t p = jb.queue[g];
-      const uint32_t bin = bin_of_key(jb.s_ckey[p], H);
-      const uint32_t nq = min((uint32_t)jb.gpts, jb.bin_start[bin + 1] - p);
-      const GroupArgs ga{p, nq, bin, jb.n, jb.K, jb.R2f, jb.R, jb.R2, jb.Wp, can_sure, &b.bs->pair_tests};
-      nout += count_group<D, PRED, T>(
-          static_cast<const T*>(jb.s_x), ga,
-          [&](uint32_t sb2, uint32_t& rs, uint32_t& len) {
-            rs = jb.bin_start[sb2];
-            len = jb.bin_start[sb2 + 1] - rs;
-          },
-          [&](uint32_t pos) {
-            const uint32_t i = jb.s_off[pos];
-            atomicOr(&jb.flags[i >> 5], 1u << (i & 31));
-          });
-    }
-    if (lane == 0 && nout) atomicAdd(&jb.ctr->n_out, nout);
-    return;
-  }
   const int64_t nq = jb.ctr->n_undet;
   for (int64_t q = warp; q < nq; q += nwarps) {
     const uint32_t pos = jb.queue[q];
@@ -1495,6 +1614,7 @@ static __device__ void finish_batch(const Batch& b) {
     bs->undet_total += tu;
     bs->slides += tn;
     bs->done = 0;
+    bs->count_ticket = 0;
     if (b.span) {
       b.span->n_used = 0;
       b.span->n_groups = 0;

@@ -204,6 +204,7 @@ struct SpanScratch {
 };
 
 constexpr int kMaxJobs = 256;  // windows per launch, either engine
+static_assert(kMaxJobs <= BATCH_JOBS_MAX, "the batch-wide count list holds one prefix entry per job");
 
 constexpr int kPipeKernels = 7;
 const char* kKernelNames[kPipeKernels] = {"k_keys",  "k_hist",    "k_scan", "k_scatter",
@@ -2699,12 +2700,15 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
       if (cfgs[i].count == RTOD_COUNT_AUTO)
         b->hs[i]->group = !b->route && auto_group(b->hs[i]->D, pts[i], b->hs[i]->sm_count);
   }
-  // Group the streams by (dimension, predicate, count mode).
+  // Group the streams by (dimension, predicate, count mode), at most
+  // BATCH_JOBS_MAX streams per group (one launch's count list).
   for (int i = 0; i < n_streams; ++i) {
     const rtod_handle* h = b->hs[i];
     rtod_batch::Group* g = nullptr;
     for (auto& x : b->groups)
-      if (x.geom.D == h->D && x.geom.pred == h->cfg.pred && x.geom.group == h->group) g = &x;
+      if (x.geom.D == h->D && x.geom.pred == h->cfg.pred && x.geom.group == h->group &&
+          (int)x.streams.size() < BATCH_JOBS_MAX)
+        g = &x;
     if (!g) {
       b->groups.emplace_back();
       g = &b->groups.back();
