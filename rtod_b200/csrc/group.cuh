@@ -226,29 +226,51 @@ __device__ __forceinline__ int count_group_ex(const T* sx, const GroupArgs& a, R
         for (int d = 0; d < D; ++d) cp[e][d] = f2_pack((float)cx[2 * e][d], (float)cx[2 * e + 1][d]);
     }
     unsigned todo = live;
-    while (todo) {
-      const int qq = __ffs(todo) - 1;
-      todo &= todo - 1;
-      T y[D];
+    if constexpr (PAIRED) {
+      // two queries per step: four independent chains of paired
+      // instructions per lane (a lone last query is tested twice, the second
+      // result dropped)
+      while (todo) {
+        const int qa = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const int qb = todo ? __ffs(todo) - 1 : -1;
+        todo &= todo - 1;
+        const int qs = qb >= 0 ? qb : qa;
+        unsigned long long ya[D], yb[D];
 #pragma unroll
-      for (int d = 0; d < D; ++d) y[d] = __shfl_sync(0xffffffffu, qx[d], qq);
-      unsigned m = 0;
-      if constexpr (PAIRED) {
-        unsigned long long y2[D];
-#pragma unroll
-        for (int d = 0; d < D; ++d) y2[d] = f2_pack((float)y[d], (float)y[d]);
+        for (int d = 0; d < D; ++d) {
+          const float va = (float)__shfl_sync(0xffffffffu, qx[d], qa);
+          const float vb = (float)__shfl_sync(0xffffffffu, qx[d], qs);
+          ya[d] = f2_pack(va, va);
+          yb[d] = f2_pack(vb, vb);
+        }
+        unsigned ma = 0, mb = 0;
 #pragma unroll
         for (int e = 0; e < CPL / 2; ++e) {
-          bool n0, n1;
-          is_nbr_f32x2<D>(y2, cp[e], a.R2f, n0, n1);
-          m += (cv[2 * e] && n0 ? 1u : 0u) + (cv[2 * e + 1] && n1 ? 1u : 0u);
+          bool a0, a1, b0, b1;
+          is_nbr_f32x2<D>(ya, cp[e], a.R2f, a0, a1);
+          is_nbr_f32x2<D>(yb, cp[e], a.R2f, b0, b1);
+          ma += (cv[2 * e] && a0 ? 1u : 0u) + (cv[2 * e + 1] && a1 ? 1u : 0u);
+          mb += (cv[2 * e] && b0 ? 1u : 0u) + (cv[2 * e + 1] && b1 ? 1u : 0u);
         }
-      } else {
+        const unsigned ta = __reduce_add_sync(0xffffffffu, ma);
+        const unsigned tb = __reduce_add_sync(0xffffffffu, mb);
+        if (lane == qa) cnt += (int)ta;
+        if (lane == qb) cnt += (int)tb;
+      }
+    } else {
+      while (todo) {
+        const int qq = __ffs(todo) - 1;
+        todo &= todo - 1;
+        T y[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) y[d] = __shfl_sync(0xffffffffu, qx[d], qq);
+        unsigned m = 0;
 #pragma unroll
         for (int e = 0; e < CPL; ++e) m += (cv[e] && is_nbr<D, PRED, T>(y, cx[e], a.R2f, a.R, a.R2)) ? 1u : 0u;
+        const unsigned tot = __reduce_add_sync(0xffffffffu, m);
+        if (lane == qq) cnt += (int)tot;
       }
-      const unsigned tot = __reduce_add_sync(0xffffffffu, m);
-      if (lane == qq) cnt += (int)tot;
     }
     bool out = false;
     if (has) {

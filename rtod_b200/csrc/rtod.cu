@@ -634,6 +634,13 @@ int32_t group_part(int64_t points, int sm_count) {
   return p;
 }
 
+// Points per listed part of a bin in group mode. Parts are taken from the
+// batch-wide count list (k_count), so short parts keep the launch's tail
+// short; measured on the 8-d streams of the 64-stream workload (B200, median
+// step): parts of up to 512 points 5.00 ms, 256 4.69 ms, 128 4.38 ms.
+constexpr int32_t kGroupPartMax = 128;
+int32_t group_part_size(int64_t points, int sm_count) { return std::min(kGroupPartMax, group_part(points, sm_count)); }
+
 // Whether RTOD_COUNT_AUTO picks group counts for a launch of `points`
 // points: in more than 3 dimensions (no cell is ever all-inlier, so every
 // point is counted and a bin's points are many) when the parts hold at
@@ -693,7 +700,7 @@ int configure(rtod_handle* h, int mode, int jobs, int64_t first_lo, const void* 
   std::vector<Job> tab((size_t)jobs);
   for (int j = 0; j < jobs; ++j) {
     tab[j] = make_job(h, j, mode == MODE_RING, stream_pts);
-    tab[j].gpts = group_part(h->W * jobs, h->sm_count);
+    tab[j].gpts = group_part_size(h->W * jobs, h->sm_count);
   }
   if (tab.size() != h->tab_host.size() ||
       std::memcmp(tab.data(), h->tab_host.data(), sizeof(Job) * tab.size()) != 0) {
@@ -2547,7 +2554,7 @@ int upload_group_jobs(rtod_batch* b, rtod_batch::Group& g) {
   const int ng = (int)g.streams.size();
   std::vector<Job> tab(ng);
   for (int k = 0; k < ng; ++k) tab[k] = make_job(b->hs[g.streams[k]], 0, true, nullptr);
-  for (auto& jb : tab) jb.gpts = group_part(g.out_cap, b->hs[g.streams[0]]->sm_count);
+  for (auto& jb : tab) jb.gpts = group_part_size(g.out_cap, b->hs[g.streams[0]]->sm_count);
   CU(cudaMemcpy(g.jobs, tab.data(), sizeof(Job) * ng, cudaMemcpyHostToDevice));
   return RTOD_OK;
 }
@@ -2728,7 +2735,7 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
       g.out_cap += h->W;
       g.cmp_tiles += (h->W + CMP_TILE - 1) / CMP_TILE;
     }
-    for (auto& jb : tab) jb.gpts = group_part(g.out_cap, b->hs[g.streams[0]]->sm_count);
+    for (auto& jb : tab) jb.gpts = group_part_size(g.out_cap, b->hs[g.streams[0]]->sm_count);
     if (dalloc(&g.jobs, ng, &dummy) || dalloc(&g.bs, 1, &dummy) || dalloc(&g.out, (size_t)g.out_cap, &dummy) ||
         dalloc(&g.active, ng, &dummy) || dalloc(&g.nout, ng, &dummy) || dalloc(&g.bar, 1, &dummy))
       return bail(RTOD_ERR_CUDA);
