@@ -20,7 +20,10 @@
 // at the next chunk boundary, and that point starts its walk at the current
 // chunk and wraps around: the count does not depend on the order of the
 // chunks, so the warp stays full until the group runs out of points instead
-// of rescanning the list for every 32 points.
+// of rescanning the list for every 32 points. Above 3 dimensions under the
+// FP32 predicate the tests run on pairs of candidates with the paired FP32
+// instructions (is_nbr_f32x2: the same sums bit for bit), two queries per
+// step.
 //
 // "Sure" slots (can_sure: the bins hold exactly their cells, D <= 3) hold
 // cells whose points all lie within R of every point of the group's cell:
