@@ -971,8 +971,14 @@ __global__ void __launch_bounds__(256) k_span_count(Batch b, Span sp) {
 // Deferred compaction of a chunk of slides [s0, s0 + n): k_span_compact, one
 // block per slide, turns the slide's bitset row into sorted global indices
 // at the slide's output offset (recorded by finish_batch; 4 words per
-// thread, one block scan per 4096 words) and clears the row.
+// thread, one block scan per 4096 words) and clears the row. The IDs of a
+// step are gathered in shared memory (up to SPAN_CMP_SMEM_IDS) and written
+// by consecutive threads: outliers cluster (a stream's jumps fill whole
+// bitset words), and a thread's run of single 8-byte stores held the
+// window engine's compaction block about 9 us on B200.
 // ---------------------------------------------------------------------------
+constexpr uint32_t SPAN_CMP_SMEM_IDS = 4096;
+
 struct SpanOut {
   uint32_t* bits;
   int64_t words, chunk, W, S;
@@ -984,6 +990,7 @@ struct SpanOut {
 
 static __global__ void __launch_bounds__(1024) k_span_compact(SpanOut o, int64_t s0) {
   __shared__ uint32_t sm[33];
+  __shared__ int64_t s_ids[SPAN_CMP_SMEM_IDS];
   pdl_trigger();
   pdl_wait();
   constexpr int WPT = 4;  // bitset words per thread and step
@@ -1003,17 +1010,34 @@ static __global__ void __launch_bounds__(1024) k_span_compact(SpanOut o, int64_t
     }
     uint32_t total;
     const uint32_t ex = block_exclusive_scan(cnt, &total, sm);
-    int64_t q = out + ex;
+    if (total <= SPAN_CMP_SMEM_IDS && out + total <= o.out_cap) {  // block-uniform
+      uint32_t k = ex;
 #pragma unroll
-    for (int e = 0; e < WPT; ++e) {
-      uint32_t b = bits[e];
-      if (b) row[w0 + e] = 0;
-      while (b) {
-        const int f = __ffs(b) - 1;
-        b &= b - 1;
-        if (q < o.out_cap) o.out_ids[q] = lo + (w0 + e) * 32 + f;
-        else set_err(o.bs, DERR_CAPACITY);
-        ++q;
+      for (int e = 0; e < WPT; ++e) {
+        uint32_t b = bits[e];
+        if (b) row[w0 + e] = 0;
+        while (b) {
+          const int f = __ffs(b) - 1;
+          b &= b - 1;
+          s_ids[k++] = lo + (w0 + e) * 32 + f;
+        }
+      }
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < total; i += blockDim.x) o.out_ids[out + i] = s_ids[i];
+      __syncthreads();  // s_ids is refilled by the next step
+    } else {
+      int64_t q = out + ex;
+#pragma unroll
+      for (int e = 0; e < WPT; ++e) {
+        uint32_t b = bits[e];
+        if (b) row[w0 + e] = 0;
+        while (b) {
+          const int f = __ffs(b) - 1;
+          b &= b - 1;
+          if (q < o.out_cap) o.out_ids[q] = lo + (w0 + e) * 32 + f;
+          else set_err(o.bs, DERR_CAPACITY);
+          ++q;
+        }
       }
     }
     out += total;
