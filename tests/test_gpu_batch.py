@@ -130,3 +130,37 @@ def test_batch_autotuner_keeps_results(rtod, oracle_mod, router):
         after = bd.tuning
         assert all(g["settled"] for g in after)
         assert all(len(v) > 1 for v in seen.values())  # each group tried several settings
+
+
+@pytest.mark.parametrize("dim,count", [(1, "point"), (8, "group")])
+def test_batch_more_streams_of_one_kind_than_one_launch_holds(rtod, oracle_mod, dim, count):
+    """260 streams of one (dimension, predicate, count mode): a launch's
+    count list holds at most 256 jobs, so they run as two groups. Every
+    stream is checked against the oracle slide by slide; every seventh
+    stream sits one step out."""
+    from rtod_b200 import datagen
+    n, W, S, slides, K = 260, 400, 40, 3, 5
+    R = 0.05 if dim == 1 else 0.5
+    streams = [datagen.random_walk(W + slides * S, 0.1, seed=3000 + i, dim=dim) for i in range(n)]
+    expect = [oracle_mod.detect(p, W, S, R, K, "fp32_le", engine="grid", threads=4)[:2] for p in streams]
+    cfg = [dict(window=W, slide=S, R=R, K=K, dim=dim, count=count) for _ in range(n)]
+    with rtod.BatchDetector(cfg) as bd:
+        for i, p in enumerate(streams):
+            bd.push(i, p[:W])
+        done = [0] * n
+        for step in range(slides + 1):
+            pushed = [done[i] < slides and not (i % 7 == 3 and step == 1) for i in range(n)]
+            for i, p in enumerate(streams):
+                if pushed[i]:
+                    bd.push(i, p[W + done[i] * S:W + (done[i] + 1) * S])
+            res = bd.step()
+            for i in range(n):
+                if pushed[i]:
+                    off, ids = expect[i]
+                    j = done[i]
+                    np.testing.assert_array_equal(res[i], ids[off[j]:off[j + 1]])
+                    done[i] += 1
+                else:
+                    assert res[i].size == 0
+        assert done == [slides] * n
+        assert bd.stats["groups"] == 2
