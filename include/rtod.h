@@ -277,10 +277,13 @@ const char* rtod_kernel_name(int32_t i);
    Batched streams: many independent streams, each with its own window,
    slide, R, K and dimension, advanced together one slide per step. A step
    detects the pushed slide of every stream in one replay of a captured CUDA
-   graph (streams grouped by dimension and predicate, one launch sequence per
-   group, all groups in the graph). No counterpart in RTOD (one stream per
-   process). The learned router, when on, is shared by all streams
-   (cfgs[0].router decides for all).
+   graph (streams grouped by dimension, predicate and count mode, at most 256
+   streams per group, one launch sequence per group, all groups in the
+   graph; the count work of a group's streams is shared by all warps of its
+   count launch). n_streams is at most 4096. No counterpart in RTOD (one
+   stream per process). The learned router, when on, is shared by all
+   streams (cfgs[0].router decides for all) and routes the streams counted
+   point by point; streams above 3 dimensions on group counts run unrouted.
    ------------------------------------------------------------------------ */
 typedef struct rtod_batch rtod_batch;
 
