@@ -2479,6 +2479,8 @@ struct rtod_batch {
     int idx = 0, round = 0;
     bool tuned = true;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStream_t st = nullptr;      // the group's branch of a captured step (groups overlap)
+    cudaEvent_t join = nullptr;     // end of that branch
   };
   std::vector<Group> groups;
   RouterState* router = nullptr;
@@ -2489,6 +2491,7 @@ struct rtod_batch {
   cudaGraphExec_t graphs[2] = {nullptr, nullptr};  // without / with the router's training step
   int64_t graph_kernels[2] = {0, 0};
   int64_t steps = 0, launches = 0, detections = 0;
+  cudaEvent_t fork = nullptr;  // start of a captured step whose groups run as parallel branches
 };
 
 namespace {
@@ -2499,11 +2502,14 @@ void batch_free(rtod_batch* b) {
   for (auto& g : b->groups) {
     if (g.e0) cudaEventDestroy(g.e0);
     if (g.e1) cudaEventDestroy(g.e1);
+    if (g.join) cudaEventDestroy(g.join);
+    if (g.st) cudaStreamDestroy(g.st);
     dfree(g.jobs); dfree(g.bs); dfree(g.out); dfree(g.active); dfree(g.nout); dfree(g.bar);
     if (g.active_h) cudaFreeHost(g.active_h);
     if (g.nout_h) cudaFreeHost(g.nout_h);
     if (g.bs_h) cudaFreeHost(g.bs_h);
   }
+  if (b->fork) cudaEventDestroy(b->fork);
   dfree(b->router);
   for (auto* h : b->hs)
     if (h) rtod_destroy(h);
@@ -2525,26 +2531,41 @@ Batch group_batch(const rtod_batch::Group& g, RouterState* router) {
 }
 
 // One step for all groups: active flags in, counters reset, pipeline, counts out.
-int batch_enqueue(rtod_batch* b, bool train, int64_t* nk_total, bool timed = false) {
+int batch_enqueue(rtod_batch* b, bool train, int64_t* nk_total, bool timed = false, bool branches = false) {
   int64_t total = 0;
+  // branches (a captured step with several groups): each group on its own
+  // stream, forked from and joined back into the step's stream, so that the
+  // graph runs the groups side by side. The groups share no device state
+  // (jobs, counters, outputs and flags are per group); the router, shared by
+  // all routed groups, and the cooperative fused launches keep one branch.
+  branches = branches && b->groups.size() > 1 && !b->route && !b->fused;
+  if (branches) CU(cudaEventRecord(b->fork, b->stream));
   for (auto& g : b->groups) {
+    cudaStream_t st = b->stream;
+    if (branches) {
+      st = g.st;
+      CU(cudaStreamWaitEvent(st, b->fork, 0));
+    }
     const int ng = (int)g.streams.size();
-    CU(cudaMemcpyAsync(g.active, g.active_h, sizeof(int32_t) * ng, cudaMemcpyHostToDevice, b->stream));
-    if (timed) CU(cudaEventRecord(g.e0, b->stream));
+    CU(cudaMemcpyAsync(g.active, g.active_h, sizeof(int32_t) * ng, cudaMemcpyHostToDevice, st));
+    if (timed) CU(cudaEventRecord(g.e0, st));
     int64_t nk = 0;
     int r;
     if (b->fused) {
-      r = launch_fused(g.geom, group_batch(g, b->router), g.bar, true, nullptr, 0, nullptr, train, b->stream,
+      r = launch_fused(g.geom, group_batch(g, b->router), g.bar, true, nullptr, 0, nullptr, train, st,
                        &g.fused_grid, &nk);
     } else {
-      r = launch_group(g.geom, group_batch(g, b->router), true, train, b->stream, nullptr, &nk);
+      r = launch_group(g.geom, group_batch(g, b->router), true, train, st, nullptr, &nk);
     }
     if (r) return r;
     total += nk;
-    if (timed) CU(cudaEventRecord(g.e1, b->stream));
-    CU(cudaMemcpyAsync(g.nout_h, g.nout, sizeof(int32_t) * ng, cudaMemcpyDeviceToHost, b->stream));
-    CU(cudaMemcpyAsync(g.bs_h, g.bs, sizeof(BatchState), cudaMemcpyDeviceToHost, b->stream));
+    if (timed) CU(cudaEventRecord(g.e1, st));
+    CU(cudaMemcpyAsync(g.nout_h, g.nout, sizeof(int32_t) * ng, cudaMemcpyDeviceToHost, st));
+    CU(cudaMemcpyAsync(g.bs_h, g.bs, sizeof(BatchState), cudaMemcpyDeviceToHost, st));
+    if (branches) CU(cudaEventRecord(g.join, st));
   }
+  if (branches)
+    for (auto& g : b->groups) CU(cudaStreamWaitEvent(b->stream, g.join, 0));
   *nk_total = total;
   return RTOD_OK;
 }
@@ -2681,7 +2702,8 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
     if (r) return bail(r);
     b->hs.push_back(h);
   }
-  if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking))
+  if (cudaSetDevice(b->device) != cudaSuccess || cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) ||
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming))
     return bail(fail(RTOD_ERR_CUDA, "stream creation failed"));
   int64_t dummy = 0;
   if (dalloc(&b->router, 1, &dummy)) return bail(RTOD_ERR_CUDA);
@@ -2759,7 +2781,10 @@ RTOD_API int rtod_batch_create(const rtod_config* cfgs, int32_t n_streams, rtod_
   for (auto& g : b->groups) {
     const rtod_handle* h0 = b->hs[g.streams[0]];
     g.cur = {h0->n, h0->block_warps, h0->group};
-    if (cudaEventCreate(&g.e0) || cudaEventCreate(&g.e1)) return bail(fail(RTOD_ERR_CUDA, "event creation failed"));
+    if (cudaEventCreate(&g.e0) || cudaEventCreate(&g.e1) ||
+        cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming) ||
+        cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking))
+      return bail(fail(RTOD_ERR_CUDA, "event creation failed"));
     if (!b->tuning) continue;
     init_group_tuning(b, g, cfgs[g.streams[0]]);
     if (!g.tuned) {
@@ -2829,7 +2854,7 @@ RTOD_API int rtod_batch_step(rtod_batch* b, int64_t* out_offsets, int64_t* out_i
     cudaGraph_t gr;
     CU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     int64_t nk0 = 0;
-    int r = batch_enqueue(b, train, &nk0);
+    int r = batch_enqueue(b, train, &nk0, false, true);
     cudaError_t e = cudaStreamEndCapture(b->stream, &gr);
     if (r) return r;
     if (e != cudaSuccess) return fail(RTOD_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
