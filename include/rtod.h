@@ -279,8 +279,9 @@ const char* rtod_kernel_name(int32_t i);
    detects the pushed slide of every stream in one replay of a captured CUDA
    graph (streams grouped by dimension, predicate and count mode, at most 256
    streams per group, one launch sequence per group, all groups in the
-   graph; the count work of a group's streams is shared by all warps of its
-   count launch). n_streams is at most 4096. No counterpart in RTOD (one
+   graph, side by side when the router is off and the launches are staged;
+   the count work of a group's streams is shared by all warps of its count
+   launch). n_streams is at most 4096. No counterpart in RTOD (one
    stream per process). The learned router, when on, is shared by all
    streams (cfgs[0].router decides for all) and routes the streams counted
    point by point; streams above 3 dimensions on group counts run unrouted.
