@@ -279,7 +279,8 @@ const char* rtod_kernel_name(int32_t i);
    detects the pushed slide of every stream in one replay of a captured CUDA
    graph (streams grouped by dimension, predicate and count mode, at most 256
    streams per group, one launch sequence per group, all groups in the
-   graph, side by side when the router is off and the launches are staged;
+   graph, side by side with staged launches (the routed groups, which share
+   the router, one after another);
    the count work of a group's streams is shared by all warps of its count
    launch). n_streams is at most 4096. No counterpart in RTOD (one
    stream per process). The learned router, when on, is shared by all

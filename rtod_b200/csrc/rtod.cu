@@ -2536,15 +2536,21 @@ int batch_enqueue(rtod_batch* b, bool train, int64_t* nk_total, bool timed = fal
   // branches (a captured step with several groups): each group on its own
   // stream, forked from and joined back into the step's stream, so that the
   // graph runs the groups side by side. The groups share no device state
-  // (jobs, counters, outputs and flags are per group); the router, shared by
-  // all routed groups, and the cooperative fused launches keep one branch.
-  branches = branches && b->groups.size() > 1 && !b->route && !b->fused;
+  // (jobs, counters, outputs and flags are per group) except the router,
+  // which every routed group reads and trains: the routed groups form one
+  // branch, one after another. Cooperative fused launches keep one branch.
+  branches = branches && b->groups.size() > 1 && !b->fused;
   if (branches) CU(cudaEventRecord(b->fork, b->stream));
+  cudaStream_t routed_st = nullptr;  // the routed groups' branch
   for (auto& g : b->groups) {
     cudaStream_t st = b->stream;
     if (branches) {
       st = g.st;
-      CU(cudaStreamWaitEvent(st, b->fork, 0));
+      if (g.geom.route) {
+        if (routed_st) st = routed_st;  // follows the previous routed group
+        else routed_st = st;
+      }
+      if (st == g.st) CU(cudaStreamWaitEvent(st, b->fork, 0));
     }
     const int ng = (int)g.streams.size();
     CU(cudaMemcpyAsync(g.active, g.active_h, sizeof(int32_t) * ng, cudaMemcpyHostToDevice, st));

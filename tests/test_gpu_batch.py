@@ -37,15 +37,19 @@ def make_streams(n=9, seed=5, slides=12):
 
 @pytest.mark.parametrize("router,count,pipeline", [(False, "auto", "fused"), (True, "auto", "fused"),
                                                    (False, "group", "fused"), (True, "point", "fused"),
-                                                   (False, "auto", "staged"), (True, "auto", "staged")])
+                                                   (False, "auto", "staged"), (True, "auto", "staged"),
+                                                   (True, "group8", "staged")])
 def test_batch_matches_oracle(rtod, oracle_mod, router, count, pipeline):
+    """count "group8": the 8-d streams on group counts (unrouted, a branch of
+    the step's graph of their own) beside the routed groups (one branch)."""
     streams = make_streams()
     expect = []
     for st in streams:
         off, ids, _ = oracle_mod.detect(st["points"], st["window"], st["slide"], st["R"], st["K"],
                                         st["pred"], engine="grid", threads=4)
         expect.append((off, ids))
-    cfg = [dict({k: st[k] for k in ("window", "slide", "R", "K", "dim", "pred")}, count=count, pipeline=pipeline)
+    cfg = [dict({k: st[k] for k in ("window", "slide", "R", "K", "dim", "pred")},
+                count=("group" if st["dim"] == 8 else "auto") if count == "group8" else count, pipeline=pipeline)
            for st in streams]
     with rtod.BatchDetector(cfg, router=router) as bd:
         for i, st in enumerate(streams):
